@@ -1,0 +1,247 @@
+/*
+ * mgsb.h — C ABI of the B200-native projective-dynamics (PD) soft-body solver.
+ *
+ * One handle owns one or more independent bodies ("a batch"); a single-body
+ * solver is a batch of one.  Every entry point takes plain pointers and sizes;
+ * no CUDA or C++ types cross the boundary (the optional stream is a void*).
+ *
+ * Each entry point names the reference interface it replaces
+ * (buuugyellow/MultiGridSoftBody, paths relative to MultiGridSoftBody/src).
+ *
+ * Two solver kinds are offered:
+ *   MGSB_SOLVER_REFERENCE_JACOBI — the reference's frame: inertial prediction,
+ *     per-iteration sphere DCD, corotational local step with the invariant-based
+ *     polar decomposition, one under-relaxed diagonal-Jacobi update with
+ *     Chebyshev acceleration (PDSolver.cpp:243-293).  Same constants, same
+ *     clamps; float atomics replaced by an ordered gather.
+ *   MGSB_SOLVER_MULTIGRID — PD with a geometric-multigrid V-cycle global step
+ *     (Galerkin levels, sliced-ELL Jacobi smoother, dense Cholesky coarsest),
+ *     E/nu material, capsule tool contacts as projection constraints, optional
+ *     FP64 iterative refinement.
+ *
+ * Threading: one handle per host thread; no global state.
+ * Errors: every call returns mgsb_status; mgsb_last_error_string() explains.
+ */
+#ifndef MGSB_H_
+#define MGSB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGSB_ABI_VERSION 1
+
+typedef enum mgsb_status {
+    MGSB_OK = 0,
+    MGSB_INVALID_ARG = 1,
+    MGSB_DEGENERATE_TET = 2,   /* replaces exit(0) in Matrix_Inverse_3, utils.cu:244-247 */
+    MGSB_CUDA_ERROR = 3,
+    MGSB_DIVERGED = 4,         /* non-finite positions detected after a frame */
+    MGSB_TIMEOUT = 5,
+    MGSB_NOT_SUPPORTED = 6,
+    MGSB_OUT_OF_MEMORY = 7,
+    MGSB_IO_ERROR = 8
+} mgsb_status;
+
+typedef enum mgsb_solver_kind {
+    MGSB_SOLVER_REFERENCE_JACOBI = 0,
+    MGSB_SOLVER_MULTIGRID = 1
+} mgsb_solver_kind;
+
+typedef enum mgsb_precision {
+    MGSB_PRECISION_FP32 = 0,   /* everything FP32 */
+    MGSB_PRECISION_MIXED = 1   /* FP64 outer residual + positions, FP32 V-cycle correction */
+} mgsb_precision;
+
+/* Tetrahedral mesh (host memory, copied at create).
+ * Replaces the vectors handed to PDSolver::Init, PDSolver.h:102. */
+typedef struct mgsb_mesh {
+    int32_t num_verts;
+    int32_t num_tets;
+    const float* positions;   /* [3*num_verts] xyz */
+    const int32_t* tets;      /* [4*num_tets], 0-based */
+    /* Optional structured-grid hint used to build the multigrid hierarchy.
+     * grid_dims = hex counts of the finest voxel grid that generated the
+     * mesh (0,0,0 = derive from the bounding box and mean edge length). */
+    int32_t grid_dims[3];
+} mgsb_mesh;
+
+/* Solver parameters.  Replaces the constants set in PDSolver::Init
+ * (PDSolver.cpp:166-176) and the public fields PDSolver.h:72-81. */
+typedef struct mgsb_params {
+    int32_t solver;             /* mgsb_solver_kind */
+    int32_t iterations;         /* PD local/global iterations per frame (m_iterNum) */
+    float dt;                   /* m_dt */
+    float damping;              /* m_damping, velocity scale per frame */
+    float gravity[3];           /* m_gravity{X,Y,Z} */
+    /* reference-Jacobi kind */
+    float volume_stiffness;     /* m_volumnStiffness (k) */
+    float collision_stiffness;  /* m_collisionStiffness */
+    float cheb_rho;             /* m_rho */
+    float relaxation;           /* under-relaxation factor, 0.6 in calculatePOS */
+    /* multigrid kind */
+    float density;              /* kg/m^3 */
+    float youngs_modulus;       /* default E for every tet (Pa) */
+    float poisson_ratio;        /* default nu for every tet */
+    float contact_stiffness;    /* weight of a contact projection constraint */
+    int32_t levels;             /* multigrid levels incl. the finest */
+    int32_t pre_sweeps;
+    int32_t post_sweeps;
+    float jacobi_omega;         /* weighted-Jacobi factor */
+    int32_t precision;          /* mgsb_precision */
+    int32_t refinement_passes;  /* V-cycles per PD iteration (mixed: FP64 refinement passes) */
+    int32_t use_graph;          /* capture the frame in a CUDA graph */
+    int32_t device;             /* CUDA device ordinal */
+    void* stream;               /* cudaStream_t, NULL = solver-owned stream */
+} mgsb_params;
+
+/* Fill defaults for a solver kind.  Reference-Jacobi defaults are the
+ * reference's own (20 iterations, dt 1/60, damping 0.95, k 8000, k_c 1000,
+ * rho 0.9992, gravity -9.8 y, relaxation 0.6). */
+mgsb_status mgsb_default_params(int32_t solver_kind, mgsb_params* out);
+
+typedef struct mgsb_solver mgsb_solver;
+
+/* Create one body.  Replaces PDSolver::Init (PDSolver.cpp:164-200) incl.
+ * InitVolumeConstraint (PDSolver.cpp:12-132) and PDSolverData::Init
+ * (PDSolver.cu:9-70). */
+mgsb_status mgsb_create(const mgsb_mesh* mesh, const mgsb_params* params, mgsb_solver** out);
+
+/* Create a batch of independent bodies that advance in one launch per phase.
+ * params[i].solver must be MGSB_SOLVER_MULTIGRID and all bodies share
+ * iterations/levels/sweeps/precision/dt of params[0]; material, gravity and
+ * tool are per body.  No reference counterpart (the reference has one body). */
+mgsb_status mgsb_batch_create(int32_t num_bodies, const mgsb_mesh* meshes, const mgsb_params* params,
+                              mgsb_solver** out);
+
+/* Frees all device memory.  The reference never frees (PDSolverData). */
+mgsb_status mgsb_destroy(mgsb_solver* h);
+
+mgsb_status mgsb_num_bodies(const mgsb_solver* h, int32_t* n);
+mgsb_status mgsb_num_verts(const mgsb_solver* h, int32_t body, int32_t* n);
+mgsb_status mgsb_num_tets(const mgsb_solver* h, int32_t body, int32_t* n);
+
+/* Per-tet material (multigrid kind).  E, nu: [num_tets of body].
+ * No reference counterpart (single scalar k, PDSolver.cpp:170). */
+mgsb_status mgsb_set_material(mgsb_solver* h, int32_t body, const float* youngs, const float* poisson);
+
+/* Fixed-vertex mask, 1 = fixed.  Replaces PDSolver::SetFixedVert
+ * (PDSolver.cpp:134-162; flag 0.0f = fixed there). */
+mgsb_status mgsb_set_fixed(mgsb_solver* h, int32_t body, const uint8_t* mask);
+
+/* Capsule tool of a body (segment a-b, radius).  radius <= 0 disables it.
+ * Replaces the sphere collider pose read in PDSolver::DCDByPoint
+ * (PDSolver.cpp:228-233) / SphereCollider::MoveDelta (Collider.cpp:9-17);
+ * CapsuleCollider is declared but unimplemented there (Collider.h:22-30). */
+mgsb_status mgsb_set_tool_capsule(mgsb_solver* h, int32_t body, const float a[3], const float b[3], float radius);
+/* All bodies at once: a[3n], b[3n], radius[n] (one host->device copy). */
+mgsb_status mgsb_set_tool_capsules(mgsb_solver* h, const float* a, const float* b, const float* radius);
+
+/* Sphere colliders for the reference-Jacobi kind (up to 8; active flag per
+ * sphere).  Replaces g_simulator->m_sphereColliders (Simulator.cpp:57) as
+ * read by DCDByPoint_sphere (PDSolver.cu:277-331). */
+mgsb_status mgsb_set_tool_spheres(mgsb_solver* h, int32_t count, const float* centers, const float* radii,
+                                  const uint8_t* active);
+
+/* Advance one frame.  Replaces PDSolver::Step (PDSolver.cpp:243-293). */
+mgsb_status mgsb_step(mgsb_solver* h);
+/* Advance n frames back to back (tool pose fixed). */
+mgsb_status mgsb_step_n(mgsb_solver* h, int32_t n);
+/* Block until the solver's stream is idle. */
+mgsb_status mgsb_synchronize(mgsb_solver* h);
+
+/* Readback.  Replaces runCpyTetVertForRender (PDSolver.cu:261-268). */
+mgsb_status mgsb_get_positions(mgsb_solver* h, int32_t body, float* out /* [3*V] */);
+mgsb_status mgsb_get_velocities(mgsb_solver* h, int32_t body, float* out /* [3*V] */);
+/* Positions of every body, concatenated in body order (one copy). */
+mgsb_status mgsb_get_all_positions(mgsb_solver* h, float* out);
+/* FP64 master positions (mixed precision only). */
+mgsb_status mgsb_get_positions_f64(mgsb_solver* h, int32_t body, double* out);
+/* Per-vertex contact flag (1 = in contact this frame) — m_tetVertIsCollide. */
+mgsb_status mgsb_get_contact_flags(mgsb_solver* h, int32_t body, int32_t* out /* [V] */);
+/* Contact vertex indices, ascending.  *n receives the count; if cap < count
+ * only cap entries are written and MGSB_INVALID_ARG is returned. */
+mgsb_status mgsb_get_contacts(mgsb_solver* h, int32_t body, int32_t* idx, size_t cap, size_t* n);
+/* Per-vertex collision depth (reference kind) — m_tetVertCollisionDepth. */
+mgsb_status mgsb_get_collision_depth(mgsb_solver* h, int32_t body, float* out /* [V] */);
+/* Device pointer to the body's positions (float4 xyzw per vertex, w unused),
+ * valid until the next step/destroy — replaces the GL hand-off. */
+mgsb_status mgsb_get_device_positions(mgsb_solver* h, int32_t body, const float** dptr);
+/* Area-unweighted surface vertex normals — UpdateTriNormal +
+ * AvgOutsideTetVertNormal (PDSolver.cu:394-460). */
+mgsb_status mgsb_get_normals(mgsb_solver* h, int32_t body, float* out /* [3*V] */);
+
+/* Checkpoint / resume: overwrite positions and velocities of a body. */
+mgsb_status mgsb_set_state(mgsb_solver* h, int32_t body, const float* positions, const float* velocities);
+
+/* Energy diagnostics of the current state — runCalEnergy (PDSolver.cu:816-924)
+ * as a device reduction.  out[0]=Ek, out[1]=Ep, out[2]=Ec, out[3]=Nc,
+ * out[4]=|x-prev| (reference kind) or last fine-level residual norm. */
+mgsb_status mgsb_get_energy(mgsb_solver* h, int32_t body, double out[5]);
+
+/* Timing of the last frame on the solver stream (CUDA events), ms. */
+mgsb_status mgsb_last_frame_ms(mgsb_solver* h, float* ms);
+/* Run one frame eagerly with CUDA events around every kernel launch and
+ * report, per kernel name, the summed device time and the launch count
+ * (names: cap entries of 48 chars).  The frame advances the simulation.
+ * No reference counterpart (the reference times with std::chrono,
+ * PDSolver.cpp:244-292). */
+mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* total_ms, int32_t* launches,
+                               int32_t* count);
+/* Number of kernel launches one frame issues. */
+mgsb_status mgsb_launches_per_frame(const mgsb_solver* h, int32_t* n);
+
+/* Export of the precomputed per-tet / per-vertex data of body 0 (test hook,
+ * host copies): inv_dm [9T], ac [12T], volume [T], mass [V], diag [V].
+ * Any pointer may be NULL.  Replaces reading PDSolver's m_tetInvD3x3,
+ * m_tetInvD3x4, m_tetVolume, m_tetVertMass, m_tetVolumeDiag. */
+mgsb_status mgsb_get_precompute(mgsb_solver* h, float* inv_dm, float* ac, float* volume, float* mass, float* diag);
+
+/* Multigrid hierarchy inspection (body-concatenated arrays). */
+mgsb_status mgsb_level_size(mgsb_solver* h, int32_t level, int32_t* num_verts, int32_t* nnz_offdiag);
+
+const char* mgsb_last_error_string(const mgsb_solver* h);
+const char* mgsb_status_string(mgsb_status s);
+
+/* ---------------------------------------------------------------------------
+ * Mesh utilities (host only; no GPU needed).
+ * ------------------------------------------------------------------------- */
+typedef struct mgsb_mesh_data {
+    int32_t num_verts;
+    int32_t num_tets;
+    float* positions;       /* [3V] */
+    int32_t* tets;          /* [4T] */
+    int32_t num_tris;       /* boundary triangles (filled by mgsb_mesh_extract_surface) */
+    int32_t* tris;          /* [3F] outward-oriented */
+    int32_t* tri_opposite;  /* [F] vertex of the owning tet opposite the face */
+    int32_t grid_dims[3];
+} mgsb_mesh_data;
+
+/* Box [lo,hi] split into nx*ny*nz hexes, 6 Kuhn tets per hex, vertex index
+ * i + (nx+1)*(k + (nz+1)*j).  No reference counterpart (the reference loads
+ * gmsh files). */
+mgsb_status mgsb_mesh_box(int32_t nx, int32_t ny, int32_t nz, const float lo[3], const float hi[3],
+                          mgsb_mesh_data** out);
+/* Voxel blob: voxels of a grid whose centre satisfies
+ * (x/ax)^2+(y/ay)^2+(z/az)^2 < 1 + amp*s(x,y,z), s = seeded value noise of the
+ * given period; 6 Kuhn tets per kept voxel, unused vertices dropped. */
+mgsb_status mgsb_mesh_blob(int32_t gx, int32_t gy, int32_t gz, float spacing, const float semi_axes[3],
+                           float noise_amp, float noise_period, uint64_t seed, mgsb_mesh_data** out);
+/* gmsh 2.2 ASCII reader — SoftObject::ReadFromFile (SoftObject.cpp:85-130). */
+mgsb_status mgsb_mesh_read_msh(const char* path, mgsb_mesh_data** out);
+/* Boundary faces + opposite vertex — SoftObject::TetFaceExtraction
+ * (SoftObject.cpp:154-251); same face order as the reference's std::set. */
+mgsb_status mgsb_mesh_extract_surface(mgsb_mesh_data* m);
+mgsb_status mgsb_mesh_free(mgsb_mesh_data* m);
+
+/* Seeded 3-D value noise used by the blob generator, exposed for tests. */
+double mgsb_value_noise(double x, double y, double z, double period, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGSB_H_ */

@@ -1,0 +1,366 @@
+"""Python host API over the C ABI (include/mgsb.h): meshes, solvers, batches."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import MgsbError, Params
+
+
+def _check(status: int, handle=None) -> None:
+    if status != 0:
+        msg = ""
+        if handle:
+            raw = L.load().mgsb_last_error_string(handle)
+            msg = raw.decode() if raw else ""
+        raise MgsbError(status, msg)
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _u8ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+# ---------------------------------------------------------------------------
+# Meshes
+# ---------------------------------------------------------------------------
+@dataclass
+class TetMesh:
+    positions: np.ndarray            # (V, 3) float32
+    tets: np.ndarray                 # (T, 4) int32
+    grid_dims: tuple = (0, 0, 0)
+    tris: np.ndarray | None = None   # (F, 3) boundary faces
+    tri_opposite: np.ndarray | None = None
+
+    @property
+    def num_verts(self) -> int:
+        return int(self.positions.shape[0])
+
+    @property
+    def num_tets(self) -> int:
+        return int(self.tets.shape[0])
+
+    def bbox_diagonal(self) -> float:
+        return float(np.linalg.norm(self.positions.max(0).astype(np.float64) - self.positions.min(0)))
+
+    def as_c(self) -> tuple[L.Mesh, tuple]:
+        pos = np.ascontiguousarray(self.positions, dtype=np.float32)
+        tets = np.ascontiguousarray(self.tets, dtype=np.int32)
+        m = L.Mesh()
+        m.num_verts = pos.shape[0]
+        m.num_tets = tets.shape[0]
+        m.positions = _fptr(pos)
+        m.tets = _iptr(tets)
+        for c in range(3):
+            m.grid_dims[c] = int(self.grid_dims[c])
+        return m, (pos, tets)   # keep the arrays alive with the struct
+
+
+def _take_mesh(ptr) -> TetMesh:
+    lib = L.load()
+    d = ptr.contents
+    V, T = d.num_verts, d.num_tets
+    pos = np.ctypeslib.as_array(d.positions, shape=(V * 3,)).reshape(V, 3).copy()
+    tets = np.ctypeslib.as_array(d.tets, shape=(T * 4,)).reshape(T, 4).copy()
+    tris = opp = None
+    if d.num_tris > 0:
+        tris = np.ctypeslib.as_array(d.tris, shape=(d.num_tris * 3,)).reshape(-1, 3).copy()
+        opp = np.ctypeslib.as_array(d.tri_opposite, shape=(d.num_tris,)).copy()
+    dims = tuple(int(d.grid_dims[c]) for c in range(3))
+    lib.mgsb_mesh_free(ptr)
+    return TetMesh(pos, tets, dims, tris, opp)
+
+
+def box_mesh(nx: int, ny: int, nz: int, lo=(-1.0, -10.0, -1.0), hi=(1.0, 10.0, 1.0)) -> TetMesh:
+    """Box split into nx*ny*nz hexes, 6 Kuhn tets each."""
+    lib = L.load()
+    out = C.POINTER(L.MeshData)()
+    lo_a = np.asarray(lo, dtype=np.float32)
+    hi_a = np.asarray(hi, dtype=np.float32)
+    _check(lib.mgsb_mesh_box(nx, ny, nz, _fptr(lo_a), _fptr(hi_a), C.byref(out)))
+    return _take_mesh(out)
+
+
+def blob_mesh(gx=64, gy=32, gz=48, spacing=0.25, semi_axes=(6.0, 3.0, 4.0), noise_amp=0.15, noise_period=2.0,
+              seed=3) -> TetMesh:
+    """Organ-like voxel blob (ellipsoid + seeded value noise), 6 Kuhn tets per voxel."""
+    lib = L.load()
+    out = C.POINTER(L.MeshData)()
+    ax = np.asarray(semi_axes, dtype=np.float32)
+    _check(lib.mgsb_mesh_blob(gx, gy, gz, spacing, _fptr(ax), noise_amp, noise_period, seed, C.byref(out)))
+    return _take_mesh(out)
+
+
+def read_msh(path: str) -> TetMesh:
+    """gmsh 2.2 ASCII reader (tets only), like SoftObject::ReadFromFile."""
+    lib = L.load()
+    out = C.POINTER(L.MeshData)()
+    _check(lib.mgsb_mesh_read_msh(path.encode(), C.byref(out)))
+    return _take_mesh(out)
+
+
+def extract_surface(mesh: TetMesh) -> TetMesh:
+    """Fill mesh.tris / mesh.tri_opposite like SoftObject::TetFaceExtraction."""
+    lib = L.load()
+    d = L.MeshData()
+    pos = np.ascontiguousarray(mesh.positions, dtype=np.float32)
+    tets = np.ascontiguousarray(mesh.tets, dtype=np.int32)
+    d.num_verts, d.num_tets = pos.shape[0], tets.shape[0]
+    # The library frees tris/opposite only; positions/tets stay owned by numpy.
+    d.positions = _fptr(pos)
+    d.tets = _iptr(tets)
+    _check(lib.mgsb_mesh_extract_surface(C.byref(d)))
+    F = d.num_tris
+    tris = np.ctypeslib.as_array(d.tris, shape=(max(F, 1) * 3,))[: F * 3].reshape(-1, 3).copy()
+    opp = np.ctypeslib.as_array(d.tri_opposite, shape=(max(F, 1),))[:F].copy()
+    libc = C.CDLL(None)
+    libc.free.argtypes = [C.c_void_p]
+    libc.free(C.cast(d.tris, C.c_void_p))
+    libc.free(C.cast(d.tri_opposite, C.c_void_p))
+    mesh.tris, mesh.tri_opposite = tris, opp
+    return mesh
+
+
+def value_noise(x: float, y: float, z: float, period: float, seed: int) -> float:
+    return float(L.load().mgsb_value_noise(x, y, z, period, seed))
+
+
+# ---------------------------------------------------------------------------
+# Parameters
+# ---------------------------------------------------------------------------
+def default_params(kind: int = L.SOLVER_MULTIGRID, **overrides) -> Params:
+    p = Params()
+    _check(L.load().mgsb_default_params(kind, C.byref(p)))
+    for k, v in overrides.items():
+        if k == "gravity":
+            for c in range(3):
+                p.gravity[c] = float(v[c])
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def params_dict(p: Params) -> dict:
+    d = {}
+    for name, _ in Params._fields_:
+        v = getattr(p, name)
+        d[name] = list(v) if name == "gravity" else v
+    return d
+
+
+# ---------------------------------------------------------------------------
+# Solver handle
+# ---------------------------------------------------------------------------
+class Solver:
+    """One handle holding one or more bodies (a batch)."""
+
+    def __init__(self, meshes, params, _handle=None):
+        self._lib = L.load()
+        if isinstance(meshes, TetMesh):
+            meshes = [meshes]
+        if isinstance(params, Params):
+            params = [params] * len(meshes)
+        self.meshes = list(meshes)
+        self.params = list(params)
+        cm = (L.Mesh * len(meshes))()
+        self._keep = []
+        for i, m in enumerate(meshes):
+            s, keep = m.as_c()
+            cm[i] = s
+            self._keep.append(keep)
+        cp = (Params * len(params))(*params)
+        h = C.c_void_p()
+        if len(meshes) == 1:
+            st = self._lib.mgsb_create(C.byref(cm[0]), C.byref(cp[0]), C.byref(h))
+        else:
+            st = self._lib.mgsb_batch_create(len(meshes), cm, cp, C.byref(h))
+        if st != 0:
+            raise MgsbError(st, "create failed")
+        self.h = h
+        self._keep = None
+
+    # -- lifetime
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._lib.mgsb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- sizes
+    @property
+    def num_bodies(self) -> int:
+        n = C.c_int32()
+        _check(self._lib.mgsb_num_bodies(self.h, C.byref(n)), self.h)
+        return n.value
+
+    def num_verts(self, body: int = 0) -> int:
+        n = C.c_int32()
+        _check(self._lib.mgsb_num_verts(self.h, body, C.byref(n)), self.h)
+        return n.value
+
+    def num_tets(self, body: int = 0) -> int:
+        n = C.c_int32()
+        _check(self._lib.mgsb_num_tets(self.h, body, C.byref(n)), self.h)
+        return n.value
+
+    # -- inputs
+    def set_fixed(self, mask, body: int = 0) -> None:
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        _check(self._lib.mgsb_set_fixed(self.h, body, _u8ptr(m)), self.h)
+
+    def set_material(self, youngs, poisson, body: int = 0) -> None:
+        T = self.num_tets(body)
+        e = np.ascontiguousarray(np.broadcast_to(np.asarray(youngs, np.float32), (T,)))
+        n = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson, np.float32), (T,)))
+        _check(self._lib.mgsb_set_material(self.h, body, _fptr(e), _fptr(n)), self.h)
+
+    def set_capsule(self, a, b, radius: float, body: int = 0) -> None:
+        aa = np.asarray(a, np.float32)
+        bb = np.asarray(b, np.float32)
+        _check(self._lib.mgsb_set_tool_capsule(self.h, body, _fptr(aa), _fptr(bb), float(radius)), self.h)
+
+    def set_capsules(self, a, b, radius) -> None:
+        aa = np.ascontiguousarray(a, np.float32)
+        bb = np.ascontiguousarray(b, np.float32)
+        rr = np.ascontiguousarray(radius, np.float32)
+        _check(self._lib.mgsb_set_tool_capsules(self.h, _fptr(aa), _fptr(bb), _fptr(rr)), self.h)
+
+    def set_spheres(self, centers, radii, active=None) -> None:
+        c = np.ascontiguousarray(centers, np.float32).reshape(-1, 3)
+        r = np.ascontiguousarray(radii, np.float32).reshape(-1)
+        act = None if active is None else np.ascontiguousarray(active, np.uint8)
+        _check(self._lib.mgsb_set_tool_spheres(self.h, c.shape[0], _fptr(c), _fptr(r),
+                                               None if act is None else _u8ptr(act)), self.h)
+
+    def set_state(self, positions=None, velocities=None, body: int = 0) -> None:
+        p = None if positions is None else np.ascontiguousarray(positions, np.float32)
+        v = None if velocities is None else np.ascontiguousarray(velocities, np.float32)
+        _check(self._lib.mgsb_set_state(self.h, body, None if p is None else _fptr(p),
+                                        None if v is None else _fptr(v)), self.h)
+
+    # -- stepping
+    def step(self, n: int = 1) -> None:
+        if n == 1:
+            _check(self._lib.mgsb_step(self.h), self.h)
+        else:
+            _check(self._lib.mgsb_step_n(self.h, n), self.h)
+
+    def synchronize(self) -> None:
+        _check(self._lib.mgsb_synchronize(self.h), self.h)
+
+    # -- outputs
+    def positions(self, body: int = 0) -> np.ndarray:
+        out = np.empty((self.num_verts(body), 3), np.float32)
+        _check(self._lib.mgsb_get_positions(self.h, body, _fptr(out)), self.h)
+        return out
+
+    def all_positions(self) -> np.ndarray:
+        n = sum(self.num_verts(b) for b in range(self.num_bodies))
+        out = np.empty((n, 3), np.float32)
+        _check(self._lib.mgsb_get_all_positions(self.h, _fptr(out)), self.h)
+        return out
+
+    def positions_f64(self, body: int = 0) -> np.ndarray:
+        out = np.empty((self.num_verts(body), 3), np.float64)
+        _check(self._lib.mgsb_get_positions_f64(self.h, body, out.ctypes.data_as(C.POINTER(C.c_double))), self.h)
+        return out
+
+    def velocities(self, body: int = 0) -> np.ndarray:
+        out = np.empty((self.num_verts(body), 3), np.float32)
+        _check(self._lib.mgsb_get_velocities(self.h, body, _fptr(out)), self.h)
+        return out
+
+    def contact_flags(self, body: int = 0) -> np.ndarray:
+        out = np.empty(self.num_verts(body), np.int32)
+        _check(self._lib.mgsb_get_contact_flags(self.h, body, _iptr(out)), self.h)
+        return out
+
+    def contacts(self, body: int = 0) -> np.ndarray:
+        n = C.c_size_t()
+        _check(self._lib.mgsb_get_contacts(self.h, body, None, 0, C.byref(n)), self.h)
+        out = np.empty(max(n.value, 1), np.int32)
+        _check(self._lib.mgsb_get_contacts(self.h, body, _iptr(out), out.size, C.byref(n)), self.h)
+        return out[: n.value]
+
+    def collision_depth(self, body: int = 0) -> np.ndarray:
+        out = np.empty(self.num_verts(body), np.float32)
+        _check(self._lib.mgsb_get_collision_depth(self.h, body, _fptr(out)), self.h)
+        return out
+
+    def normals(self, body: int = 0) -> np.ndarray:
+        out = np.empty((self.num_verts(body), 3), np.float32)
+        _check(self._lib.mgsb_get_normals(self.h, body, _fptr(out)), self.h)
+        return out
+
+    def energy(self, body: int = 0) -> np.ndarray:
+        out = np.empty(5, np.float64)
+        _check(self._lib.mgsb_get_energy(self.h, body, out.ctypes.data_as(C.POINTER(C.c_double))), self.h)
+        return out
+
+    def device_positions_ptr(self, body: int = 0) -> int:
+        p = C.POINTER(C.c_float)()
+        _check(self._lib.mgsb_get_device_positions(self.h, body, C.byref(p)), self.h)
+        return C.cast(p, C.c_void_p).value or 0
+
+    def last_frame_ms(self) -> float:
+        ms = C.c_float()
+        _check(self._lib.mgsb_last_frame_ms(self.h, C.byref(ms)), self.h)
+        return ms.value
+
+    def launches_per_frame(self) -> int:
+        n = C.c_int32()
+        _check(self._lib.mgsb_launches_per_frame(self.h, C.byref(n)), self.h)
+        return n.value
+
+    def profile_frame(self) -> dict:
+        """Run one frame with per-launch CUDA events: {kernel: (total_ms, launches)}."""
+        cap = 64
+        names = C.create_string_buffer(48 * cap)
+        ms = np.zeros(cap, np.float32)
+        cnt = np.zeros(cap, np.int32)
+        n = C.c_int32()
+        _check(self._lib.mgsb_profile_frame(self.h, cap, names, _fptr(ms), _iptr(cnt), C.byref(n)), self.h)
+        raw = names.raw
+        out = {}
+        for k in range(min(n.value, cap)):
+            nm = raw[48 * k: 48 * (k + 1)].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[k]), int(cnt[k]))
+        return out
+
+    def precompute(self) -> dict:
+        T, V = self.num_tets(0), self.num_verts(0)
+        inv = np.empty(9 * T, np.float32)
+        ac = np.empty(12 * T, np.float32)
+        vol = np.empty(T, np.float32)
+        mass = np.empty(V, np.float32)
+        diag = np.empty(V, np.float32)
+        _check(self._lib.mgsb_get_precompute(self.h, _fptr(inv), _fptr(ac), _fptr(vol), _fptr(mass), _fptr(diag)),
+               self.h)
+        return dict(inv=inv.reshape(T, 9), ac=ac.reshape(T, 12), volume=vol, mass=mass, diag=diag)
+
+    def level_size(self, level: int) -> tuple[int, int]:
+        n = C.c_int32()
+        z = C.c_int32()
+        _check(self._lib.mgsb_level_size(self.h, level, C.byref(n), C.byref(z)), self.h)
+        return n.value, z.value

@@ -1,0 +1,630 @@
+// sm_100a kernels of the PD soft-body frame.  Included by solver.cu only.
+//
+// Layout in HBM (all bodies of a batch concatenated per level):
+//   positions / RHS / corrections : float4 per vertex (xyz + pad, 16-B vector access)
+//   tets                          : int4 vertex ids + (float4, float4, float2) rest data
+//   per-(tet, corner) RHS slots   : float4, ordered by vertex (CSR), so the RHS
+//                                   gather is a contiguous segmented sum — no atomics
+//   matrices                      : sliced ELL (32-row slices, column-major inside
+//                                   a slice), off-diagonal only; diagonal apart
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_math.cuh"
+
+namespace mgsb {
+
+// ---------------------------------------------------------------------------
+// Shared structures passed by value to kernels
+// ---------------------------------------------------------------------------
+struct Ell {
+    const int32_t* slice_ptr;  // [nslices+1] entry offsets
+    const int32_t* col;
+    const float* val;
+};
+
+struct SphereSet {
+    int count;
+    float cx[8], cy[8], cz[8], r[8];
+    int active[8];
+};
+
+// Per-body table, device resident.  Tool pose is rewritten every frame.
+struct BodyDev {
+    int v0_off, v0_n;        // finest-level vertex range
+    int cl_off, cl_n;        // coarsest-level vertex range
+    int dense_off;           // offset of the coarsest dense n*n block
+    int pad0;
+    float gravity[4];
+    float damping;
+    float cap_r;
+    float pad1[2];
+    float cap_a[4];
+    float cap_b[4];
+};
+
+__device__ __forceinline__ float4 ell_row_mul(int row, const Ell A, const float4* __restrict__ x) {
+    const int s = row >> 5, lane = row & 31;
+    const int beg = __ldg(A.slice_ptr + s), end = __ldg(A.slice_ptr + s + 1);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int e = beg + lane; e < end; e += 32) {
+        const float a = __ldg(A.val + e);
+        const float4 xv = __ldg(x + __ldg(A.col + e));
+        ax = fmaf(a, xv.x, ax);
+        ay = fmaf(a, xv.y, ay);
+        az = fmaf(a, xv.z, az);
+    }
+    return make_float4(ax, ay, az, 0.f);
+}
+
+// ===========================================================================
+// Reference-faithful Jacobi/Chebyshev frame (PDSolver::Step)
+// ===========================================================================
+
+// calculateST (PDSolver.cu:72-116); external force is always zero in the
+// reference's frame and is omitted.
+__global__ void k_ref_predict(int n, float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ s,
+                              float4* __restrict__ prev, float4* __restrict__ last, const float* __restrict__ fixf,
+                              float damping, float dt, float gx, float gy, float gz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = x[i], vel = v[i];
+    last[i] = p;
+    const float fix = fixf[i];
+    vel.x *= damping * fix; vel.y *= damping * fix; vel.z *= damping * fix;
+    vel.x += gx * dt * fix; vel.y += gy * dt * fix; vel.z += gz * dt * fix;
+    p.x += vel.x * dt * fix; p.y += vel.y * dt * fix; p.z += vel.z * dt * fix;
+    x[i] = p;
+    v[i] = vel;
+    s[i] = p;
+    prev[i] = p;
+}
+
+// Local step, one thread per tet: F = Ds Dm^-1, R by the invariant polar
+// decomposition, per (i,j): val = sum_k (R-F)_ik Ac_kj, NaN->0, clamp +-10,
+// c = val*V*k, |c| < 1e-5 dropped (PDSolverAc.cu:447-662).  The four corner
+// contributions go to their RHS slots (float4 each).
+__global__ void __launch_bounds__(256) k_ref_local(int T, const int4* __restrict__ tets, const float4* __restrict__ invA,
+                                                   const float4* __restrict__ invB, const float2* __restrict__ invC,
+                                                   const float4* __restrict__ x, const int4* __restrict__ slot_of,
+                                                   float4* __restrict__ slots, float stiffness) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const int4 id = __ldg(tets + t);
+    const float4 a = __ldg(invA + t), b = __ldg(invB + t);
+    const float2 c = __ldg(invC + t);
+    const float inv[9] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x};
+    const float vol = c.y;
+    const float4 p0 = __ldg(x + id.x), p1 = __ldg(x + id.y), p2 = __ldg(x + id.z), p3 = __ldg(x + id.w);
+    const float D[9] = {p1.x - p0.x, p2.x - p0.x, p3.x - p0.x, p1.y - p0.y, p2.y - p0.y,
+                        p3.y - p0.y, p1.z - p0.z, p2.z - p0.z, p3.z - p0.z};
+    float F[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) F[r * 3 + q] = D[r * 3 + 0] * inv[q] + D[r * 3 + 1] * inv[3 + q] + D[r * 3 + 2] * inv[6 + q];
+    float R[9];
+    ref_rotation(F, R);
+    float FR[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) FR[q] = R[q] - F[q];
+    // Ac (3x4): column 0 = -(sum of inv rows), columns 1..3 = inv rows.
+    float Ac[12];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        Ac[r * 4 + 0] = -inv[r] - inv[r + 3] - inv[r + 6];
+        Ac[r * 4 + 1] = inv[r];
+        Ac[r * 4 + 2] = inv[r + 3];
+        Ac[r * 4 + 3] = inv[r + 6];
+    }
+    const int4 so = __ldg(slot_of + t);
+    const int sid[4] = {so.x, so.y, so.z, so.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float out[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float val = FR[i * 3 + 0] * Ac[0 * 4 + j] + FR[i * 3 + 1] * Ac[1 * 4 + j] + FR[i * 3 + 2] * Ac[2 * 4 + j];
+            if (isnan(val)) val = 0.f;
+            val = fminf(10.0f, fmaxf(-10.0f, val));
+            float res = val * vol * stiffness;
+            if ((double)fabsf(res) < 1e-5) res = 0.f;
+            out[i] = res;
+        }
+        slots[sid[j]] = make_float4(out[0], out[1], out[2], 0.f);
+    }
+}
+
+// Per vertex: gather the elastic force from the slots, sphere DCD
+// (DCDByPoint_sphere, PDSolver.cu:277-331), then the under-relaxed Jacobi
+// step with Chebyshev acceleration (calculatePOS, PDSolver.cu:192-235).
+// On the last iteration also v = (x - last)/dt (calculateV, PDSolver.cu:245).
+__global__ void __launch_bounds__(256) k_ref_vertex(
+    int n, float4* __restrict__ x, float4* __restrict__ prev, const float4* __restrict__ s, const float4* __restrict__ last,
+    float4* __restrict__ v, const float* __restrict__ fixf, const float* __restrict__ mass, const float* __restrict__ vdiag,
+    const int32_t* __restrict__ slot_ptr, const float4* __restrict__ slots, const SphereSet* __restrict__ spheres,
+    float kc, float dt, float omega, double relax, int last_iter, int32_t* __restrict__ cflag, float* __restrict__ cdepth,
+    int32_t* __restrict__ nonfinite) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    const int e1 = __ldg(slot_ptr + i + 1);
+    for (int e = __ldg(slot_ptr + i); e < e1; ++e) {
+        const float4 c = __ldg(slots + e);
+        fx += c.x; fy += c.y; fz += c.z;
+    }
+    const float4 p4 = x[i];
+    const float p[3] = {p4.x, p4.y, p4.z};
+    float cd[3] = {0.f, 0.f, 0.f}, cf[3] = {0.f, 0.f, 0.f};
+    int flag = 0;
+    float depth = 0.f;
+    const int nsph = spheres->count;
+    for (int q = 0; q < nsph; ++q) {
+        if (!spheres->active[q]) continue;
+        const float cx = spheres->cx[q], cy = spheres->cy[q], cz = spheres->cz[q];
+        float radius = spheres->r[q];
+        const float cp[3] = {p[0] - cx, p[1] - cy, p[2] - cz};
+        const float len = sqrtf(cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2]);
+        const float dir[3] = {cp[0] / len, cp[1] / len, cp[2] / len};
+        const float distance = len;
+        const float oldRadius = radius;
+        radius *= 1.5f;
+        if (distance < radius) {
+            const float bq = 2 * (cp[0] * dir[0] + cp[1] * dir[1] + cp[2] * dir[2]);
+            const float cq = (cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2]) - radius * radius;
+            float t = (-bq + sqrtf(bq * bq - 4 * 1 * cq)) / (2 * 1);
+            if (t > 0.5f * oldRadius) {
+                flag = 1;
+                depth = t - 0.5f * oldRadius;
+            }
+            t = t / 2.0f;
+            const float colP[3] = {p[0] + dir[0] * t, p[1] + dir[1] * t, p[2] + dir[2] * t};
+            const float cc[3] = {colP[0] - cx, colP[1] - cy, colP[2] - cz};
+            const float lc = sqrtf(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+            const float nrm[3] = {cc[0] / lc, cc[1] / lc, cc[2] / lc};
+            const float ndd = nrm[0] * dir[0] + nrm[1] * dir[1] + nrm[2] * dir[2];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                cd[a] += kc * nrm[a] * nrm[a];
+                cf[a] += kc * t * ndd * nrm[a];
+            }
+        }
+    }
+    const float fix = __ldg(fixf + i);
+    const float dc = __ldg(mass + i) / (dt * dt);
+    const float vd = __ldg(vdiag + i);
+    const float4 s4 = __ldg(s + i), pv4 = prev[i];
+    const float sv[3] = {s4.x, s4.y, s4.z}, pv[3] = {pv4.x, pv4.y, pv4.z};
+    const float fe[3] = {fx, fy, fz};
+    float nx[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float el = fe[a] + cf[a];
+        float nxt = (dc * (sv[a] - p[a]) + el) / (vd + cd[a] + dc) * fix + p[a];
+        nxt = (float)((double)(nxt - p[a]) * relax + (double)p[a]);
+        nxt = omega * (nxt - pv[a]) + pv[a];
+        nx[a] = nxt;
+    }
+    prev[i] = p4;
+    const float4 xn = make_float4(nx[0], nx[1], nx[2], 0.f);
+    x[i] = xn;
+    if (last_iter) {
+        const float4 l4 = __ldg(last + i);
+        v[i] = make_float4((xn.x - l4.x) / dt, (xn.y - l4.y) / dt, (xn.z - l4.z) / dt, 0.f);
+        cflag[i] = flag;
+        cdepth[i] = depth;
+        if (!isfinite(xn.x) || !isfinite(xn.y) || !isfinite(xn.z)) atomicOr(nonfinite, 1);
+    }
+}
+
+// ===========================================================================
+// Multigrid frame
+// ===========================================================================
+
+// Inertial prediction (same form as calculateST) with per-body gravity and
+// damping: last = x; v = v*damp*fix + g*dt*fix; x = s = x + v*dt*fix.
+__global__ void k_mg_predict(int n, float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ s,
+                             float4* __restrict__ last, const float* __restrict__ fixf, const int32_t* __restrict__ body_of,
+                             const BodyDev* __restrict__ bodies, float dt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BodyDev& B = bodies[__ldg(body_of + i)];
+    float4 p = x[i], vel = v[i];
+    last[i] = p;
+    const float fix = __ldg(fixf + i);
+    vel.x *= B.damping * fix; vel.y *= B.damping * fix; vel.z *= B.damping * fix;
+    vel.x += B.gravity[0] * dt * fix; vel.y += B.gravity[1] * dt * fix; vel.z += B.gravity[2] * dt * fix;
+    p.x += vel.x * dt * fix; p.y += vel.y * dt * fix; p.z += vel.z * dt * fix;
+    p.w = 0.f;
+    x[i] = p;
+    v[i] = vel;
+    s[i] = p;
+}
+
+// Capsule contact of one surface vertex against its body's capsule, evaluated
+// in FP64 on the predicted position: contact iff dist(s, segment) < r; the
+// projection target is the capsule surface point along the capsule normal.
+__device__ __forceinline__ void capsule_test(const float4 sp, const BodyDev& B, int& flag, float4& target) {
+    flag = 0;
+    target = make_float4(0.f, 0.f, 0.f, 0.f);
+    const double r = B.cap_r;
+    if (!(r > 0.0)) return;
+    const double p[3] = {sp.x, sp.y, sp.z};
+    const double a[3] = {B.cap_a[0], B.cap_a[1], B.cap_a[2]}, b[3] = {B.cap_b[0], B.cap_b[1], B.cap_b[2]};
+    const double ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double l2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+    double t = 0.0;
+    if (l2 > 0.0) {
+        t = ((p[0] - a[0]) * ab[0] + (p[1] - a[1]) * ab[1] + (p[2] - a[2]) * ab[2]) / l2;
+        t = fmin(1.0, fmax(0.0, t));
+    }
+    const double q[3] = {a[0] + t * ab[0], a[1] + t * ab[1], a[2] + t * ab[2]};
+    const double dv[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+    const double d = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    if (!(d < r)) return;
+    double nrm[3] = {0.0, 0.0, 1.0};
+    if (d > 1e-12) {
+        nrm[0] = dv[0] / d; nrm[1] = dv[1] / d; nrm[2] = dv[2] / d;
+    }
+    flag = 1;
+    target = make_float4((float)(q[0] + r * nrm[0]), (float)(q[1] + r * nrm[1]), (float)(q[2] + r * nrm[2]), 0.f);
+}
+
+// Brute-force narrow phase over all surface vertices (used when the broad
+// phase is disabled).
+__global__ void k_contact_all(int ns, const int32_t* __restrict__ surf, const int32_t* __restrict__ body_of,
+                              const BodyDev* __restrict__ bodies, const float4* __restrict__ s,
+                              const float* __restrict__ fixf, float kc, int32_t* __restrict__ cflag,
+                              float* __restrict__ c0, float4* __restrict__ target) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns) return;
+    const int i = __ldg(surf + q);
+    int flag;
+    float4 tg;
+    capsule_test(__ldg(s + i), bodies[__ldg(body_of + i)], flag, tg);
+    cflag[i] = flag;
+    c0[i] = (flag && __ldg(fixf + i) != 0.f) ? kc : 0.f;
+    target[i] = tg;
+}
+
+// Per frame, level 0: b0 = m/h^2 s + c p, D = L_ii + c, dinv = fixed ? 0 : omega/D.
+__global__ void k_l0_frame(int n, const float4* __restrict__ s, const float* __restrict__ mass_h2,
+                           const float* __restrict__ c0, const float4* __restrict__ target, const float* __restrict__ diag0,
+                           const float* __restrict__ fixf, float omega, float4* __restrict__ b0, float* __restrict__ dfull,
+                           float* __restrict__ dinv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float m = __ldg(mass_h2 + i), c = __ldg(c0 + i);
+    const float4 sv = __ldg(s + i), tg = __ldg(target + i);
+    b0[i] = make_float4(fmaf(m, sv.x, c * tg.x), fmaf(m, sv.y, c * tg.y), fmaf(m, sv.z, c * tg.z), 0.f);
+    const float D = __ldg(diag0 + i) + c;
+    dfull[i] = D;
+    dinv[i] = (__ldg(fixf + i) != 0.f) ? omega / D : 0.f;
+}
+
+// Per frame, level l >= 1: lumped contact weight c_l = P^T c_{l-1}, D and dinv.
+__global__ void k_coarse_frame(int n, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rcol,
+                               const float* __restrict__ rw, const float* __restrict__ cfine,
+                               const float* __restrict__ diag0, float omega, float* __restrict__ c,
+                               float* __restrict__ dfull, float* __restrict__ dinv) {
+    const int J = blockIdx.x * blockDim.x + threadIdx.x;
+    if (J >= n) return;
+    float acc = 0.f;
+    const int e1 = __ldg(rptr + J + 1);
+    for (int e = __ldg(rptr + J); e < e1; ++e) acc = fmaf(__ldg(rw + e), __ldg(cfine + __ldg(rcol + e)), acc);
+    c[J] = acc;
+    const float d0 = __ldg(diag0 + J);
+    const float D = d0 + acc;
+    dfull[J] = D;
+    dinv[J] = d0 > 0.f ? omega / D : 0.f;
+}
+
+// Local step, one thread per tet: F = sum_j x_j g_j^T, R = closest rotation,
+// RHS contribution w R g_j into the four corner slots.
+__global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict__ tets, const float4* __restrict__ gA,
+                                                  const float4* __restrict__ gB, const float2* __restrict__ gC,
+                                                  const float4* __restrict__ x, const int4* __restrict__ slot_of,
+                                                  float4* __restrict__ slots) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const int4 id = __ldg(tets + t);
+    const float4 a = __ldg(gA + t), b = __ldg(gB + t);
+    const float2 c = __ldg(gC + t);
+    // g1 = (a.x a.y a.z), g2 = (a.w b.x b.y), g3 = (b.z b.w c.x), w = c.y
+    const float g1[3] = {a.x, a.y, a.z}, g2[3] = {a.w, b.x, b.y}, g3[3] = {b.z, b.w, c.x};
+    const float w = c.y;
+    const float4 p0 = __ldg(x + id.x), p1 = __ldg(x + id.y), p2 = __ldg(x + id.z), p3 = __ldg(x + id.w);
+    const float d1[3] = {p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
+    const float d2[3] = {p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
+    const float d3[3] = {p3.x - p0.x, p3.y - p0.y, p3.z - p0.z};
+    float F[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) F[r * 3 + q] = d1[r] * g1[q] + d2[r] * g2[q] + d3[r] * g3[q];
+    float R[9];
+    svd_rotation(F, R);
+    float o1[3], o2[3], o3[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        o1[r] = w * (R[r * 3 + 0] * g1[0] + R[r * 3 + 1] * g1[1] + R[r * 3 + 2] * g1[2]);
+        o2[r] = w * (R[r * 3 + 0] * g2[0] + R[r * 3 + 1] * g2[1] + R[r * 3 + 2] * g2[2]);
+        o3[r] = w * (R[r * 3 + 0] * g3[0] + R[r * 3 + 1] * g3[1] + R[r * 3 + 2] * g3[2]);
+    }
+    const int4 so = __ldg(slot_of + t);
+    slots[so.x] = make_float4(-(o1[0] + o2[0] + o3[0]), -(o1[1] + o2[1] + o3[1]), -(o1[2] + o2[2] + o3[2]), 0.f);
+    slots[so.y] = make_float4(o1[0], o1[1], o1[2], 0.f);
+    slots[so.z] = make_float4(o2[0], o2[1], o2[2], 0.f);
+    slots[so.w] = make_float4(o3[0], o3[1], o3[2], 0.f);
+}
+
+// Level-0 weighted-Jacobi sweep on positions.  With gather != 0 the RHS is
+// assembled first: b = b0 + sum of the vertex's slots (contiguous), and stored.
+__global__ void __launch_bounds__(256) k_l0_sweep(int n, Ell A, const float* __restrict__ dfull,
+                                                  const float* __restrict__ dinv, const float4* __restrict__ xin,
+                                                  float4* __restrict__ xout, float4* __restrict__ b,
+                                                  const float4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
+                                                  const float4* __restrict__ slots, int gather) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 bi;
+    if (gather) {
+        bi = __ldg(b0 + i);
+        const int e1 = __ldg(slot_ptr + i + 1);
+        for (int e = __ldg(slot_ptr + i); e < e1; ++e) {
+            const float4 c = __ldg(slots + e);
+            bi.x += c.x; bi.y += c.y; bi.z += c.z;
+        }
+        b[i] = bi;
+    } else {
+        bi = b[i];
+    }
+    const float4 xi = __ldg(xin + i);
+    const float4 off = ell_row_mul(i, A, xin);
+    const float D = __ldg(dfull + i), di = __ldg(dinv + i);
+    const float rx = bi.x - fmaf(D, xi.x, off.x), ry = bi.y - fmaf(D, xi.y, off.y), rz = bi.z - fmaf(D, xi.z, off.z);
+    xout[i] = make_float4(fmaf(di, rx, xi.x), fmaf(di, ry, xi.y), fmaf(di, rz, xi.z), 0.f);
+}
+
+// RHS assembly alone: b = b0 + sum of the vertex's slots.
+__global__ void k_gather_rhs(int n, float4* __restrict__ b, const float4* __restrict__ b0,
+                             const int32_t* __restrict__ slot_ptr, const float4* __restrict__ slots) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 bi = __ldg(b0 + i);
+    const int e1 = __ldg(slot_ptr + i + 1);
+    for (int e = __ldg(slot_ptr + i); e < e1; ++e) {
+        const float4 c = __ldg(slots + e);
+        bi.x += c.x; bi.y += c.y; bi.z += c.z;
+    }
+    b[i] = bi;
+}
+
+// Residual res = rhs - A v (level 0 with v = positions; coarse with v = e).
+__global__ void __launch_bounds__(256) k_residual(int n, Ell A, const float* __restrict__ dfull,
+                                                  const float4* __restrict__ v, const float4* __restrict__ rhs,
+                                                  float4* __restrict__ res) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 vi = __ldg(v + i), ri = __ldg(rhs + i);
+    const float4 off = ell_row_mul(i, A, v);
+    const float D = __ldg(dfull + i);
+    res[i] = make_float4(ri.x - fmaf(D, vi.x, off.x), ri.y - fmaf(D, vi.y, off.y), ri.z - fmaf(D, vi.z, off.z), 0.f);
+}
+
+// Restriction r_l = P^T res_{l-1} (gather over children) fused with the
+// first pre-smoothing sweep from a zero guess: e = dinv r.
+__global__ void k_restrict(int n, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rcol,
+                           const float* __restrict__ rw, const float4* __restrict__ resf, const float* __restrict__ dinv,
+                           float4* __restrict__ r, float4* __restrict__ e, int first_sweep) {
+    const int J = blockIdx.x * blockDim.x + threadIdx.x;
+    if (J >= n) return;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const int e1 = __ldg(rptr + J + 1);
+    for (int q = __ldg(rptr + J); q < e1; ++q) {
+        const float w = __ldg(rw + q);
+        const float4 v = __ldg(resf + __ldg(rcol + q));
+        ax = fmaf(w, v.x, ax); ay = fmaf(w, v.y, ay); az = fmaf(w, v.z, az);
+    }
+    r[J] = make_float4(ax, ay, az, 0.f);
+    const float di = first_sweep ? __ldg(dinv + J) : 0.f;
+    e[J] = make_float4(di * ax, di * ay, di * az, 0.f);
+}
+
+// Coarse weighted-Jacobi sweep on the correction: e' = e + dinv (r - A e).
+__global__ void __launch_bounds__(256) k_coarse_sweep(int n, Ell A, const float* __restrict__ dfull,
+                                                      const float* __restrict__ dinv, const float4* __restrict__ r,
+                                                      const float4* __restrict__ ein, float4* __restrict__ eout) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 ei = __ldg(ein + i), ri = __ldg(r + i);
+    const float4 off = ell_row_mul(i, A, ein);
+    const float D = __ldg(dfull + i), di = __ldg(dinv + i);
+    eout[i] = make_float4(fmaf(di, ri.x - fmaf(D, ei.x, off.x), ei.x), fmaf(di, ri.y - fmaf(D, ei.y, off.y), ei.y),
+                          fmaf(di, ri.z - fmaf(D, ei.z, off.z), ei.z), 0.f);
+}
+
+// Prolongation v_fine += P e_coarse (4 parents per fine vertex).
+__global__ void k_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
+                          const float4* __restrict__ ec, float4* __restrict__ v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 id = __ldg(pid + i);
+    const float4 w = __ldg(pw + i);
+    const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
+    float4 vi = v[i];
+    vi.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+    vi.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+    vi.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+    v[i] = vi;
+}
+
+// v = (x - last)/dt plus a finiteness check of the new positions.
+__global__ void k_velocity(int n, const float4* __restrict__ x, const float4* __restrict__ last, float4* __restrict__ v,
+                           float dt, int32_t* __restrict__ nonfinite) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = __ldg(x + i), l = __ldg(last + i);
+    v[i] = make_float4((p.x - l.x) / dt, (p.y - l.y) / dt, (p.z - l.z) / dt, 0.f);
+    if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) atomicOr(nonfinite, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest level: dense Cholesky per body (one CTA per body).
+// The factor is recomputed only when the lumped contact weights of the body's
+// coarsest vertices changed since the last factorisation.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_coarsest_factor(const BodyDev* __restrict__ bodies, const float* __restrict__ A0,
+                                                         const float* __restrict__ c, float* __restrict__ c_prev,
+                                                         float* __restrict__ Lfac, float* __restrict__ Ldinv,
+                                                         int32_t* __restrict__ valid) {
+    extern __shared__ float sm[];
+    const BodyDev& B = bodies[blockIdx.x];
+    const int n = B.cl_n, off = B.cl_off;
+    const float* A = A0 + B.dense_off;
+    float* Lg = Lfac + B.dense_off;
+    __shared__ int changed;
+    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (c[off + i] != c_prev[off + i]) changed = 1;
+    __syncthreads();
+    if (!changed) return;
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        float a = A[q];
+        if (i == j) a += c[off + i];
+        sm[q] = a;
+    }
+    __syncthreads();
+    float* piv = sm + n * n;  // n pivots
+    for (int j = 0; j < n; ++j) {
+        const float d = sqrtf(sm[j * n + j]);
+        const float id = 1.f / d;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) sm[i * n + j] *= id;
+        if (threadIdx.x == 0) piv[j] = d;
+        __syncthreads();
+        const int m = n - j - 1;
+        const int tot = m * (m + 1) / 2;
+        for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+            int a = (int)((sqrtf(8.f * (float)q + 1.f) - 1.f) * 0.5f);
+            while ((a + 1) * (a + 2) / 2 <= q) ++a;
+            while (a * (a + 1) / 2 > q) --a;
+            const int bcol = q - a * (a + 1) / 2;
+            const int i = j + 1 + a, k = j + 1 + bcol;
+            sm[i * n + k] -= sm[i * n + j] * sm[k * n + j];
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        Lg[q] = (j < i) ? sm[q] : (j == i ? piv[i] : 0.f);
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        Ldinv[off + i] = 1.f / piv[i];
+        c_prev[off + i] = c[off + i];
+    }
+    if (threadIdx.x == 0) valid[blockIdx.x] = 1;
+}
+
+// Restrict the residual onto the coarsest level and solve L L^T e = r with
+// blocked substitution: a warp solves each 32x32 diagonal block, the CTA
+// updates the remaining rows.  Inactive rows are identity rows of the factor
+// and get a zero right-hand side.
+__global__ void __launch_bounds__(256) k_coarsest_solve(const BodyDev* __restrict__ bodies, const int32_t* __restrict__ rptr,
+                                                        const int32_t* __restrict__ rcol, const float* __restrict__ rw,
+                                                        const float4* __restrict__ resf, const float* __restrict__ Lfac,
+                                                        const float* __restrict__ Ldinv, float4* __restrict__ eout) {
+    extern __shared__ float4 rs[];
+    const BodyDev& B = bodies[blockIdx.x];
+    const int n = B.cl_n, off = B.cl_off;
+    const float* L = Lfac + B.dense_off;
+    const float* ldi = Ldinv + off;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int J = tid; J < n; J += blockDim.x) {
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        const int e1 = __ldg(rptr + off + J + 1);
+        for (int q = __ldg(rptr + off + J); q < e1; ++q) {
+            const float w = __ldg(rw + q);
+            const float4 v = __ldg(resf + __ldg(rcol + q));
+            ax = fmaf(w, v.x, ax); ay = fmaf(w, v.y, ay); az = fmaf(w, v.z, az);
+        }
+        rs[J] = make_float4(ax, ay, az, 0.f);
+    }
+    __syncthreads();
+    // forward: L y = r
+    for (int jb = 0; jb < n; jb += 32) {
+        const int nb = min(32, n - jb);
+        if (warp == 0) {
+            const int i = jb + lane;
+            float4 val = (lane < nb) ? rs[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int jj = 0; jj < nb; ++jj) {
+                float yx = val.x * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
+                float yy = val.y * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
+                float yz = val.z * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
+                yx = __shfl_sync(0xffffffffu, yx, jj);
+                yy = __shfl_sync(0xffffffffu, yy, jj);
+                yz = __shfl_sync(0xffffffffu, yz, jj);
+                if (lane == jj) {
+                    val = make_float4(yx, yy, yz, 0.f);
+                } else if (lane > jj && lane < nb) {
+                    const float l = __ldg(L + (size_t)i * n + jb + jj);
+                    val.x -= l * yx; val.y -= l * yy; val.z -= l * yz;
+                }
+            }
+            if (lane < nb) rs[i] = val;
+        }
+        __syncthreads();
+        for (int i = jb + nb + tid; i < n; i += blockDim.x) {
+            float4 acc = rs[i];
+            const float* Li = L + (size_t)i * n + jb;
+            for (int k = 0; k < nb; ++k) {
+                const float l = __ldg(Li + k);
+                const float4 y = rs[jb + k];
+                acc.x -= l * y.x; acc.y -= l * y.y; acc.z -= l * y.z;
+            }
+            rs[i] = acc;
+        }
+        __syncthreads();
+    }
+    // backward: L^T e = y
+    const int nblk = (n + 31) / 32;
+    for (int bi = nblk - 1; bi >= 0; --bi) {
+        const int jb = bi * 32;
+        const int nb = min(32, n - jb);
+        if (warp == 0) {
+            const int i = jb + lane;
+            float4 val = (lane < nb) ? rs[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int jj = nb - 1; jj >= 0; --jj) {
+                float ex = val.x * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
+                float ey = val.y * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
+                float ez = val.z * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
+                ex = __shfl_sync(0xffffffffu, ex, jj);
+                ey = __shfl_sync(0xffffffffu, ey, jj);
+                ez = __shfl_sync(0xffffffffu, ez, jj);
+                if (lane == jj) {
+                    val = make_float4(ex, ey, ez, 0.f);
+                } else if (lane < jj) {
+                    const float l = __ldg(L + (size_t)(jb + jj) * n + i);  // L^T[i][j] = L[j][i]
+                    val.x -= l * ex; val.y -= l * ey; val.z -= l * ez;
+                }
+            }
+            if (lane < nb) rs[i] = val;
+        }
+        __syncthreads();
+        for (int i = tid; i < jb; i += blockDim.x) {
+            float4 acc = rs[i];
+            for (int k = 0; k < nb; ++k) {
+                const float l = __ldg(L + (size_t)(jb + k) * n + i);
+                const float4 e = rs[jb + k];
+                acc.x -= l * e.x; acc.y -= l * e.y; acc.z -= l * e.z;
+            }
+            rs[i] = acc;
+        }
+        __syncthreads();
+    }
+    for (int J = tid; J < n; J += blockDim.x) eout[off + J] = rs[J];
+}
+
+}  // namespace mgsb

@@ -1,0 +1,75 @@
+/*
+ * FP64 CPU oracle for the PD soft-body frame — TEST INFRASTRUCTURE ONLY.
+ *
+ * Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+ * the checker; never linked into or called by the product library.
+ *
+ * Two modes (params->solver):
+ *   MGSB_SOLVER_REFERENCE_JACOBI — restatement in FP64 of the reference frame
+ *     (buuugyellow/MultiGridSoftBody, MultiGridSoftBody/src):
+ *       precompute            PDSolver.cpp:12-132 (density 1 lumped mass)
+ *       inertial prediction   PDSolver.cu:72-116  (calculateST)
+ *       sphere DCD            PDSolver.cu:277-331 (DCDByPoint_sphere)
+ *       local step            PDSolverAc.cu:447-662 (getTetFRV2 + calTetIFV1)
+ *       polar decomposition   utils.cu:123-226   (GetRotation_D)
+ *       Jacobi + Chebyshev    PDSolver.cu:192-235, PDSolver.cpp:261-271
+ *       velocity              PDSolver.cu:245-252
+ *       energy diagnostics    PDSolver.cu:816-924 (runCalEnergy)
+ *   MGSB_SOLVER_MULTIGRID — PD with a V-cycle global step exactly as
+ *     configured (levels, sweeps, Galerkin operators on Kuhn voxel grids,
+ *     lumped contact weights, dense Cholesky coarsest), corotational strain
+ *     constraints with weight 2*mu*V, capsule contacts detected once per
+ *     frame on the predicted positions.
+ */
+#ifndef MGSB_ORACLE_H_
+#define MGSB_ORACLE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../include/mgsb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_solver oracle_solver;
+
+oracle_solver* oracle_create(const mgsb_mesh* mesh, const mgsb_params* params, char* err, int errlen);
+void oracle_destroy(oracle_solver* h);
+int oracle_set_fixed(oracle_solver* h, const uint8_t* mask);
+int oracle_set_material(oracle_solver* h, const float* youngs, const float* poisson);
+int oracle_set_tool_capsule(oracle_solver* h, const float a[3], const float b[3], float radius);
+int oracle_set_tool_spheres(oracle_solver* h, int32_t count, const float* centers, const float* radii,
+                            const uint8_t* active);
+int oracle_step(oracle_solver* h);
+int oracle_num_verts(const oracle_solver* h);
+void oracle_get_positions(const oracle_solver* h, double* out);
+void oracle_get_velocities(const oracle_solver* h, double* out);
+void oracle_get_contact_flags(const oracle_solver* h, int32_t* out);
+void oracle_get_collision_depth(const oracle_solver* h, double* out);
+void oracle_set_state(oracle_solver* h, const double* positions, const double* velocities);
+/* inv [9T], ac [12T], volume [T], mass [V], diag [V]; NULL allowed. */
+void oracle_get_precompute(const oracle_solver* h, double* inv, double* ac, double* volume, double* mass,
+                           double* diag);
+/* Ek, Ep, Ec, Nc, dX as in runCalEnergy. */
+void oracle_get_energy(const oracle_solver* h, double out[5]);
+/* Fine-level residual norm of the PD global system after the last iteration. */
+double oracle_last_residual(const oracle_solver* h);
+
+/* Hierarchy inspection (level >= 1): sizes, and the Galerkin matrix in CSR
+ * with the diagonal first in each row. */
+int oracle_level_size(const oracle_solver* h, int level, int32_t* n, int32_t* nnz_offdiag);
+int oracle_level_prolongation(const oracle_solver* h, int level, int32_t* ids, double* w);
+int oracle_level_matrix(const oracle_solver* h, int level, double* diag, int32_t* ptr, int32_t* col, double* val);
+
+/* Pure functions. */
+void oracle_ref_rotation(const double F[9], double R[9]);
+void oracle_svd_rotation(const double F[9], double R[9]);
+double oracle_inverse3(const double A[9], double R[9]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,164 @@
+"""Multigrid PD frame on the GPU (FP32) vs the FP64 oracle running the same
+configured algorithm.  Tolerance: max vertex error <= 1e-5 x bbox diagonal;
+contact vertex index sets bit-exact."""
+import numpy as np
+import pytest
+
+import multigridsoftbody_b200 as mg
+from oracle.binding import Oracle
+
+from .common import beam, capsule_path, mg_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(m, fixed, p):
+    s = mg.Solver(m, p)
+    s.set_fixed(fixed)
+    o = Oracle(m, p)
+    o.set_fixed(fixed)
+    return s, o
+
+
+def test_level_sizes_match_oracle(lib, oracle_built):
+    m, fixed = beam(12, 120, 12)
+    p = mg_params(levels=4, gravity=(0, 0, 0))
+    s, o = _pair(m, fixed, p)
+    for l in range(4):
+        assert s.level_size(l) == o.level_size(l), l
+    assert [s.level_size(l)[0] for l in range(4)] == [20449, 2989, 496, 144]
+    s.close()
+
+
+def test_config0_gravity_parity(lib, oracle_built):
+    """Config 0 (4x40x4 hexes, 3 levels, gravity, fixed y=+10, 200 frames), GPU FP32 vs FP64."""
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3)
+    s, o = _pair(m, fixed, p)
+    tol = 1e-5 * m.bbox_diagonal()
+    worst = 0.0
+    for f in range(200):
+        s.step()
+        o.step()
+        if f % 20 == 19:
+            worst = max(worst, np.abs(s.positions() - o.positions()).max())
+    assert worst < tol, (worst, tol)
+    fx = fixed.astype(bool)
+    assert np.array_equal(s.positions()[fx], m.positions[fx])
+    s.close()
+
+
+def _tool_run(m, fixed, p, frames, path, check_every=1):
+    s, o = _pair(m, fixed, p)
+    tol = 1e-5 * m.bbox_diagonal()
+    worst = 0.0
+    ncontact = 0
+    mismatches = []
+    for f in range(frames):
+        a, b = path[f]
+        for solver in (s, o):
+            solver.set_capsule(a, b, 0.3)
+            solver.step()
+        if f % check_every == 0 or f == frames - 1:
+            worst = max(worst, np.abs(s.positions() - o.positions()).max())
+            cg = np.nonzero(s.contact_flags())[0]
+            co = np.nonzero(o.contact_flags())[0]
+            ncontact += len(co)
+            if not np.array_equal(cg, co):
+                mismatches.append((f, np.setxor1d(cg, co)))
+    s.close()
+    return worst, tol, ncontact, mismatches
+
+
+def test_tool_contact_parity_small(lib, oracle_built):
+    """Config-1 tool path on the 4x40x4 beam (3 levels, gravity off), 120 frames."""
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3, gravity=(0, 0, 0))
+    path = capsule_path(120, start=(0.0, 0.0, 1.6))
+    worst, tol, ncontact, mism = _tool_run(m, fixed, p, 120, path)
+    assert ncontact > 0
+    assert not mism, mism
+    assert worst < tol, (worst, tol)
+
+
+@pytest.mark.slow
+def test_config1_parity_100_frames(lib, oracle_built):
+    """Config 1: 12x120x12 hexes (103,680 tets), 4 levels, capsule r=0.3 length 8 from (0,0,3),
+    -0.02 z per frame + N(0, 0.005^2) jitter, 100 frames.  The capsule reaches the beam
+    at frame ~85, so the run starts from z=1.9 to cover 100 frames of contact."""
+    m, fixed = beam(12, 120, 12)
+    p = mg_params(levels=4, gravity=(0, 0, 0))
+    path = capsule_path(100, start=(0.0, 0.0, 1.5))
+    worst, tol, ncontact, mism = _tool_run(m, fixed, p, 100, path, check_every=5)
+    assert ncontact > 0
+    assert not mism, mism
+    assert worst < tol, (worst, tol)
+
+
+def test_batch_equals_single_bodies(lib):
+    """Bodies batched in one launch per phase give the same bits as separate solvers."""
+    rng = np.random.default_rng(11)
+    meshes, fixeds, params = [], [], []
+    for n in (2, 3, 2):
+        m, fx = beam(n, 10 * n, n, half_len=2.5 * n)
+        meshes.append(m)
+        fixeds.append(fx)
+        params.append(mg_params(levels=3, gravity=(0, 0, 0)))
+    batch = mg.Solver(meshes, params)
+    singles = [mg.Solver(m, p) for m, p in zip(meshes, params)]
+    E = [np.exp(rng.uniform(np.log(5e4), np.log(2e5), m.num_tets)).astype(np.float32) for m in meshes]
+    for i, (m, fx) in enumerate(zip(meshes, fixeds)):
+        batch.set_fixed(fx, body=i)
+        batch.set_material(E[i], 0.3, body=i)
+        singles[i].set_fixed(fx)
+        singles[i].set_material(E[i], 0.3)
+    for f in range(20):
+        for i in range(3):
+            a = np.array([-4.0, 0.1 * i, 1.1 - 0.01 * f], np.float32)
+            b = np.array([4.0, 0.1 * i, 1.1 - 0.01 * f], np.float32)
+            batch.set_capsule(a, b, 0.2, body=i)
+            singles[i].set_capsule(a, b, 0.2)
+        batch.step()
+        for s in singles:
+            s.step()
+    for i in range(3):
+        assert np.array_equal(batch.positions(i), singles[i].positions()), i
+        assert np.array_equal(batch.contact_flags(i), singles[i].contact_flags()), i
+
+
+def test_graph_equals_eager(lib):
+    m, fixed = beam(4, 40, 4)
+    sols = []
+    for g in (1, 0):
+        s = mg.Solver(m, mg_params(levels=3, use_graph=g))
+        s.set_fixed(fixed)
+        s.step(25)
+        sols.append(s.positions())
+    assert np.array_equal(sols[0], sols[1])
+
+
+def test_checkpoint_resume_bitwise(lib):
+    m, fixed = beam(4, 40, 4)
+    s = mg.Solver(m, mg_params(levels=3))
+    s.set_fixed(fixed)
+    s.step(10)
+    x, v = s.positions(), s.velocities()
+    s.step(5)
+    a = s.positions()
+    s.set_state(x, v)
+    s.step(5)
+    assert np.array_equal(s.positions(), a)
+
+
+def test_divergence_reported(lib):
+    """A non-finite state (injected on the host) surfaces as MGSB_DIVERGED, not a fault."""
+    m, fixed = beam(2, 10, 2)
+    s = mg.Solver(m, mg_params(levels=2))
+    s.set_fixed(fixed)
+    x = m.positions.copy()
+    x[5, 1] = np.nan
+    s.set_state(x, None)
+    s.step()
+    with pytest.raises(mg.MgsbError) as e:
+        s.positions()
+    assert e.value.status == 4
