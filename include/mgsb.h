@@ -203,6 +203,16 @@ mgsb_status mgsb_get_precompute(mgsb_solver* h, float* inv_dm, float* ac, float*
 /* Multigrid hierarchy inspection (body-concatenated arrays). */
 mgsb_status mgsb_level_size(mgsb_solver* h, int32_t level, int32_t* num_verts, int32_t* nnz_offdiag);
 
+/* Host-only (no GPU): build the multigrid hierarchy of one mesh exactly as
+ * mgsb_create would and return level `level`: vertex count, off-diagonal
+ * count, prolongation rows of the next finer level (pid/pw: 4 per finer
+ * vertex, level >= 1), the diagonal (L_ii at level 0, Galerkin diagonal
+ * above; 0 = inactive) and the off-diagonal part in CSR.  Array pointers may
+ * be NULL.  No reference counterpart (test and tooling hook). */
+mgsb_status mgsb_inspect_level(const mgsb_mesh* mesh, const mgsb_params* params, const uint8_t* fixed, int32_t level,
+                               int32_t* n, int32_t* nnz, int32_t* pid, float* pw, float* diag, int32_t* ptr,
+                               int32_t* col, float* val);
+
 const char* mgsb_last_error_string(const mgsb_solver* h);
 const char* mgsb_status_string(mgsb_status s);
 

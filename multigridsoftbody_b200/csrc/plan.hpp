@@ -1,0 +1,71 @@
+// Host-side plan of every device array a solver needs (no CUDA calls):
+// precompute, RHS slot incidence, sliced-ELL matrices of all levels,
+// prolongation / restriction operators, coarsest dense blocks.
+#pragma once
+#include <vector_types.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mgsb.h"
+#include "setup.hpp"
+
+namespace mgsb {
+
+struct PlanBody {
+    int V = 0, T = 0;
+    int v_off = 0, t_off = 0;
+    std::vector<double> rest;        // 3V
+    std::vector<int32_t> tets;       // 4T (local ids)
+    std::vector<float> youngs, poisson;
+    std::vector<uint8_t> fixed;
+    std::vector<int32_t> surface;    // surface vertex ids (local)
+    int grid_dims[3] = {0, 0, 0};
+    float gravity[3] = {0, 0, 0};
+    float damping = 1.f;
+    std::vector<TetRest> tr;
+    std::vector<CoarseLevel> levels;  // multigrid levels 1..L-1
+};
+
+struct PlanLevel {
+    int n = 0, nnz = 0;
+    std::vector<int32_t> slice_ptr, ell_col;
+    std::vector<float> ell_val, diag0;
+    // prolongation rows of the next finer level's vertices (coarse side = this level)
+    std::vector<int4> pid;
+    std::vector<float4> pw;
+    // restriction CSR: children (finer vertices) of each vertex of this level
+    std::vector<int32_t> rptr, rcol;
+    std::vector<float> rw;
+};
+
+struct Plan {
+    int N0 = 0, T = 0;
+    std::vector<int32_t> body_of;
+    std::vector<float> fixf, mass, diag;      // mg: mass = m/h^2, diag = L_ii; ref: density-1 mass, volume diagonal
+    std::vector<int4> tets, slot_of;
+    std::vector<float4> tA, tB;
+    std::vector<float2> tC;
+    std::vector<int32_t> slot_ptr;
+    std::vector<PlanLevel> levels;            // [0] = finest (matrix only)
+    std::vector<float> dense;                 // coarsest dense blocks (row-major per body)
+    std::vector<int32_t> cl_off, cl_n, dense_off;
+    int max_coarsest = 0;
+    std::vector<int32_t> surf;                // global surface vertex ids
+    // body-0 precompute for export
+    std::vector<float> h_inv, h_ac, h_vol, h_mass, h_diag;
+};
+
+// Sliced ELL (32-row slices, column-major inside a slice) from CSR rows.
+void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col, const std::vector<double>& val, int n,
+               std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval);
+
+// Copies a mesh into a body (rest data, default material, no fixed vertex,
+// surface vertices for the multigrid kind).  Returns a status.
+mgsb_status make_body(const mgsb_mesh& m, const mgsb_params& p, bool multigrid, PlanBody& B, std::string& err);
+
+// Builds the plan; also (re)builds each body's multigrid hierarchy.
+bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& out, std::string& err);
+
+}  // namespace mgsb

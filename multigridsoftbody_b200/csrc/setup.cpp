@@ -120,6 +120,8 @@ void default_grid_dims(const double* pos, int num_verts, const int32_t* tets, in
 void build_hierarchy(const double* pos, int num_verts, const SparseSym& A0, const uint8_t* fixed, int levels,
                      const int dims0[3], std::vector<CoarseLevel>& out) {
     out.clear();
+    // prev_A points into `out`: reserve so emplace_back never reallocates.
+    out.reserve(levels > 1 ? levels - 1 : 0);
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int i = 0; i < num_verts; ++i)
         for (int c = 0; c < 3; ++c) {

@@ -13,6 +13,7 @@
 #include "../../include/mgsb.h"
 #include "kernels.cuh"
 #include "mesh.hpp"
+#include "plan.hpp"
 #include "setup.hpp"
 
 using namespace mgsb;
@@ -28,22 +29,7 @@ struct DevMem {
     size_t bytes = 0;
 };
 
-struct BodyHost {
-    int V = 0, T = 0;
-    int v_off = 0, t_off = 0;
-    std::vector<double> rest;        // 3V
-    std::vector<int32_t> tets;       // 4T
-    std::vector<float> youngs, poisson;
-    std::vector<uint8_t> fixed;
-    std::vector<int32_t> surface;    // surface vertex ids (local)
-    int grid_dims[3] = {0, 0, 0};
-    float gravity[3] = {0, 0, 0};
-    float damping = 1.f;
-    float cap_a[3] = {0, 0, 0}, cap_b[3] = {0, 0, 0};
-    float cap_r = 0.f;
-    std::vector<TetRest> tr;
-    std::vector<CoarseLevel> levels;  // multigrid levels 1..L-1
-};
+using BodyHost = PlanBody;
 
 struct LevelDev {
     int n = 0;
@@ -130,7 +116,27 @@ struct mgsb_solver {
     int max_coarsest = 0;
     // host copies of precompute for export
     std::vector<float> h_inv, h_ac, h_vol, h_mass, h_diag;
+    ~mgsb_solver();
 };
+
+mgsb_solver::~mgsb_solver() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto& m : derived_mem) cudaFree(m.p);
+    for (auto& m : state_mem) cudaFree(m.p);
+    delete[] bodies_host;
+    delete spheres_host;
+    for (int k = 0; k < kStage; ++k) {
+        if (stage[k]) cudaFreeHost(stage[k]);
+        if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
+    }
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
 
 namespace {
 
@@ -186,36 +192,6 @@ void free_pool(std::vector<DevMem>& pool) {
 
 bool is_mg(const mgsb_solver* h) { return h->p.solver == MGSB_SOLVER_MULTIGRID; }
 
-// Sliced ELL (32-row slices) from per-row sorted (col, val) lists.
-void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col, const std::vector<double>& val, int n,
-               std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval) {
-    const int ns = (n + 31) / 32;
-    sptr.assign(ns + 1, 0);
-    for (int s = 0; s < ns; ++s) {
-        int w = 0;
-        for (int r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, ptr[r + 1] - ptr[r]);
-        sptr[s + 1] = sptr[s] + 32 * w;
-    }
-    ecol.assign(sptr[ns], 0);
-    eval.assign(sptr[ns], 0.f);
-    for (int s = 0; s < ns; ++s) {
-        const int w = (sptr[s + 1] - sptr[s]) / 32;
-        for (int lane = 0; lane < 32; ++lane) {
-            const int r = s * 32 + lane;
-            for (int k = 0; k < w; ++k) {
-                const int e = sptr[s] + k * 32 + lane;
-                if (r < n && ptr[r] + k < ptr[r + 1]) {
-                    ecol[e] = col[ptr[r] + k];
-                    eval[e] = (float)val[ptr[r] + k];
-                } else {
-                    ecol[e] = r < n ? r : 0;
-                    eval[e] = 0.f;
-                }
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Derived data (rebuilt when fixed set / material / params change)
 // ---------------------------------------------------------------------------
@@ -235,276 +211,93 @@ mgsb_status rebuild(mgsb_solver* h) {
     h->lev.clear();
     auto& pool = h->derived_mem;
     const bool mg = is_mg(h);
-    const int N0 = h->N0, T = h->T;
-
-    std::vector<int32_t> body_of(N0), tets4(4 * (size_t)T);
-    std::vector<float> fixf(N0), massv(N0), diagv(N0);
-    std::vector<float4> tA(T), tB(T);
-    std::vector<float2> tC(T);
-    std::vector<int32_t> slot_ptr(N0 + 1, 0);
-    std::vector<int32_t> slot_of(4 * (size_t)T);
-    h->h_inv.assign(9 * (size_t)h->bodies[0].T, 0.f);
-    h->h_ac.assign(12 * (size_t)h->bodies[0].T, 0.f);
-    h->h_vol.assign(h->bodies[0].T, 0.f);
-    h->h_mass.assign(h->bodies[0].V, 0.f);
-    h->h_diag.assign(h->bodies[0].V, 0.f);
-
-    // multigrid host assembly per body
-    const int L = mg ? h->p.levels : 1;
-    std::vector<SparseSym> Lmat(h->bodies.size());
-    for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
-        BodyHost& B = h->bodies[bi];
-        const double dens = mg ? (double)h->p.density : 1.0;
-        std::vector<double> m(B.V, 0.0), w(B.T, 0.0), vd(B.V, 0.0);
-        for (int t = 0; t < B.T; ++t) {
-            const TetRest& r = B.tr[t];
-            for (int a = 0; a < 4; ++a) m[B.tets[4 * t + a]] += dens * r.volume / 4.0;
-            if (mg) {
-                const double mu = (double)B.youngs[t] / (2.0 * (1.0 + (double)B.poisson[t]));
-                w[t] = 2.0 * mu * r.volume;
-            } else {
-                for (int a = 0; a < 4; ++a)
-                    vd[B.tets[4 * t + a]] += (r.g[a][0] * r.g[a][0] + r.g[a][1] * r.g[a][1] + r.g[a][2] * r.g[a][2]) *
-                                            r.volume * (double)h->p.volume_stiffness;
-            }
-        }
-        if (mg) {
-            assemble_pd_matrix(B.tr, B.tets.data(), B.V, w.data(), m.data(), h->p.dt, Lmat[bi]);
-            int dims[3] = {B.grid_dims[0], B.grid_dims[1], B.grid_dims[2]};
-            if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0)
-                default_grid_dims(B.rest.data(), B.V, B.tets.data(), B.T, dims);
-            build_hierarchy(B.rest.data(), B.V, Lmat[bi], B.fixed.data(), L, dims, B.levels);
-        }
-        const double ih2 = 1.0 / ((double)h->p.dt * h->p.dt);
-        for (int i = 0; i < B.V; ++i) {
-            const int gi = B.v_off + i;
-            body_of[gi] = (int32_t)bi;
-            fixf[gi] = B.fixed[i] ? 0.f : 1.f;
-            massv[gi] = mg ? (float)(m[i] * ih2) : (float)m[i];
-            diagv[gi] = mg ? (float)Lmat[bi].diag[i] : (float)vd[i];
-        }
-        for (int t = 0; t < B.T; ++t) {
-            const TetRest& r = B.tr[t];
-            const int gt = B.t_off + t;
-            for (int a = 0; a < 4; ++a) tets4[4 * (size_t)gt + a] = B.tets[4 * t + a] + B.v_off;
-            if (mg) {
-                tA[gt] = make_float4((float)r.g[1][0], (float)r.g[1][1], (float)r.g[1][2], (float)r.g[2][0]);
-                tB[gt] = make_float4((float)r.g[2][1], (float)r.g[2][2], (float)r.g[3][0], (float)r.g[3][1]);
-                tC[gt] = make_float2((float)r.g[3][2], (float)w[t]);
-            } else {
-                tA[gt] = make_float4((float)r.inv[0], (float)r.inv[1], (float)r.inv[2], (float)r.inv[3]);
-                tB[gt] = make_float4((float)r.inv[4], (float)r.inv[5], (float)r.inv[6], (float)r.inv[7]);
-                tC[gt] = make_float2((float)r.inv[8], (float)r.volume);
-            }
-        }
-        if (bi == 0) {
-            for (int t = 0; t < B.T; ++t) {
-                const TetRest& r = B.tr[t];
-                for (int q = 0; q < 9; ++q) h->h_inv[9 * (size_t)t + q] = (float)r.inv[q];
-                for (int rr = 0; rr < 3; ++rr)
-                    for (int j = 0; j < 4; ++j) h->h_ac[12 * (size_t)t + rr * 4 + j] = (float)r.g[j][rr];
-                h->h_vol[t] = (float)r.volume;
-            }
-            for (int i = 0; i < B.V; ++i) {
-                h->h_mass[i] = (float)m[i];
-                h->h_diag[i] = mg ? (float)Lmat[0].diag[i] : (float)vd[i];
-            }
-        }
-    }
-    // RHS slots: CSR by vertex, tets in ascending order within a vertex.
-    for (int t = 0; t < T; ++t)
-        for (int a = 0; a < 4; ++a) slot_ptr[tets4[4 * (size_t)t + a] + 1]++;
-    for (int i = 0; i < N0; ++i) slot_ptr[i + 1] += slot_ptr[i];
-    {
-        std::vector<int32_t> fill(slot_ptr.begin(), slot_ptr.end() - 1);
-        for (int t = 0; t < T; ++t)
-            for (int a = 0; a < 4; ++a) slot_of[4 * (size_t)t + a] = fill[tets4[4 * (size_t)t + a]]++;
-    }
-    TRY(dupload(h, pool, &h->body_of, body_of));
-    TRY(dupload(h, pool, &h->fixf, fixf));
-    TRY(dupload(h, pool, &h->mass, massv));
-    TRY(dupload(h, pool, &h->vdiag, diagv));
-    {
-        std::vector<int4> t4(T), s4(T);
-        for (int t = 0; t < T; ++t) {
-            t4[t] = make_int4(tets4[4 * (size_t)t], tets4[4 * (size_t)t + 1], tets4[4 * (size_t)t + 2], tets4[4 * (size_t)t + 3]);
-            s4[t] = make_int4(slot_of[4 * (size_t)t], slot_of[4 * (size_t)t + 1], slot_of[4 * (size_t)t + 2], slot_of[4 * (size_t)t + 3]);
-        }
-        TRY(dupload(h, pool, &h->tets, t4));
-        TRY(dupload(h, pool, &h->slot_of, s4));
-    }
-    TRY(dupload(h, pool, &h->tA, tA));
-    TRY(dupload(h, pool, &h->tB, tB));
-    TRY(dupload(h, pool, &h->tC, tC));
-    TRY(dupload(h, pool, &h->slot_ptr, slot_ptr));
+    Plan P;
+    std::string perr;
+    if (!build_plan(h->bodies, h->p, P, perr)) return set_err(h, MGSB_INVALID_ARG, "%s", perr.c_str());
+    const int N0 = P.N0, T = P.T;
+    TRY(dupload(h, pool, &h->body_of, P.body_of));
+    TRY(dupload(h, pool, &h->fixf, P.fixf));
+    TRY(dupload(h, pool, &h->mass, P.mass));
+    TRY(dupload(h, pool, &h->vdiag, P.diag));
+    TRY(dupload(h, pool, &h->tets, P.tets));
+    TRY(dupload(h, pool, &h->slot_of, P.slot_of));
+    TRY(dupload(h, pool, &h->tA, P.tA));
+    TRY(dupload(h, pool, &h->tB, P.tB));
+    TRY(dupload(h, pool, &h->tC, P.tC));
+    TRY(dupload(h, pool, &h->slot_ptr, P.slot_ptr));
     TRY(dalloc(h, pool, &h->slots, 4 * (size_t)T));
     CUDA_TRY(h, cudaMemset(h->slots, 0, 4 * (size_t)T * sizeof(float4)));
-
+    h->h_inv = P.h_inv;
+    h->h_ac = P.h_ac;
+    h->h_vol = P.h_vol;
+    h->h_mass = P.h_mass;
+    h->h_diag = P.h_diag;
     if (mg) {
-        // ---- level 0
-        LevelDev l0;
-        l0.n = N0;
-        {
-            std::vector<int32_t> ptr(N0 + 1, 0), col;
-            std::vector<double> val;
-            for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
-                const BodyHost& B = h->bodies[bi];
-                const SparseSym& A = Lmat[bi];
-                for (int i = 0; i < B.V; ++i) {
-                    for (int q = A.ptr[i]; q < A.ptr[i + 1]; ++q) {
-                        col.push_back(A.col[q] + B.v_off);
-                        val.push_back(A.val[q]);
-                    }
-                    ptr[B.v_off + i + 1] = (int32_t)col.size();
-                }
+        const int L = h->p.levels;
+        for (int l = 0; l < L; ++l) {
+            const PlanLevel& pl = P.levels[l];
+            LevelDev ld;
+            ld.n = pl.n;
+            ld.nnz = pl.nnz;
+            TRY(dupload(h, pool, &ld.slice_ptr, pl.slice_ptr));
+            TRY(dupload(h, pool, &ld.ell_col, pl.ell_col));
+            TRY(dupload(h, pool, &ld.ell_val, pl.ell_val));
+            TRY(dalloc(h, pool, &ld.dfull, pl.n));
+            TRY(dalloc(h, pool, &ld.dinv, pl.n));
+            TRY(dalloc(h, pool, &ld.res, pl.n));
+            if (l == 0) {
+                ld.diag0 = h->vdiag;
+                TRY(dalloc(h, pool, &h->c0, N0));
+                CUDA_TRY(h, cudaMemset(h->c0, 0, N0 * sizeof(float)));
+                ld.c = h->c0;
+            } else {
+                TRY(dupload(h, pool, &ld.diag0, pl.diag0));
+                TRY(dupload(h, pool, &ld.pid, pl.pid));
+                TRY(dupload(h, pool, &ld.pw, pl.pw));
+                TRY(dupload(h, pool, &ld.rptr, pl.rptr));
+                TRY(dupload(h, pool, &ld.rcol, pl.rcol));
+                TRY(dupload(h, pool, &ld.rw, pl.rw));
+                TRY(dalloc(h, pool, &ld.c, pl.n));
+                TRY(dalloc(h, pool, &ld.r, pl.n));
+                TRY(dalloc(h, pool, &ld.e, pl.n));
+                TRY(dalloc(h, pool, &ld.e2, pl.n));
+                CUDA_TRY(h, cudaMemset(ld.e, 0, pl.n * sizeof(float4)));
+                CUDA_TRY(h, cudaMemset(ld.e2, 0, pl.n * sizeof(float4)));
             }
-            std::vector<int32_t> sp, ec;
-            std::vector<float> ev;
-            build_ell(ptr, col, val, N0, sp, ec, ev);
-            l0.nnz = (int)col.size();
-            TRY(dupload(h, pool, &l0.slice_ptr, sp));
-            TRY(dupload(h, pool, &l0.ell_col, ec));
-            TRY(dupload(h, pool, &l0.ell_val, ev));
+            h->lev.push_back(ld);
         }
-        l0.diag0 = h->vdiag;
-        TRY(dalloc(h, pool, &l0.dfull, N0));
-        TRY(dalloc(h, pool, &l0.dinv, N0));
-        TRY(dalloc(h, pool, &l0.res, N0));
-        TRY(dalloc(h, pool, &h->c0, N0));
-        CUDA_TRY(h, cudaMemset(h->c0, 0, N0 * sizeof(float)));
-        l0.c = h->c0;
         TRY(dalloc(h, pool, &h->b, N0));
         TRY(dalloc(h, pool, &h->b0, N0));
         TRY(dalloc(h, pool, &h->target, N0));
         CUDA_TRY(h, cudaMemset(h->target, 0, N0 * sizeof(float4)));
-        h->lev.push_back(l0);
-        // ---- coarse levels
-        std::vector<int> loff(h->bodies.size(), 0);
-        for (int l = 1; l < L; ++l) {
-            LevelDev ld;
-            int n = 0;
-            for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
-                loff[bi] = n;
-                n += h->bodies[bi].levels[l - 1].n;
-            }
-            ld.n = n;
-            const int nfin = h->lev[l - 1].n;
-            std::vector<int32_t> ptr(n + 1, 0), col;
-            std::vector<double> val;
-            std::vector<float> diag0(n, 0.f);
-            std::vector<int4> pid(nfin);
-            std::vector<float4> pw(nfin);
-            std::vector<int32_t> rptr(n + 1, 0), rcol;
-            std::vector<float> rw;
-            int fin_off = 0;
-            for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
-                const CoarseLevel& C = h->bodies[bi].levels[l - 1];
-                const int o = loff[bi];
-                for (int J = 0; J < C.n; ++J) {
-                    if (C.active[J]) {
-                        diag0[o + J] = (float)C.A.diag[J];
-                        for (int q = C.A.ptr[J]; q < C.A.ptr[J + 1]; ++q)
-                            if (C.active[C.A.col[q]]) {
-                                col.push_back(C.A.col[q] + o);
-                                val.push_back(C.A.val[q]);
-                            }
-                    }
-                    ptr[o + J + 1] = (int32_t)col.size();
-                }
-                const int nf = (int)(C.p_ids.size() / 4);
-                for (int i = 0; i < nf; ++i) {
-                    pid[fin_off + i] = make_int4(C.p_ids[4 * i] + o, C.p_ids[4 * i + 1] + o, C.p_ids[4 * i + 2] + o, C.p_ids[4 * i + 3] + o);
-                    pw[fin_off + i] = make_float4((float)C.p_w[4 * i], (float)C.p_w[4 * i + 1], (float)C.p_w[4 * i + 2], (float)C.p_w[4 * i + 3]);
-                }
-                fin_off += nf;
-            }
-            // restriction CSR = transpose of the prolongation rows
-            for (int i = 0; i < nfin; ++i) {
-                const int ids[4] = {pid[i].x, pid[i].y, pid[i].z, pid[i].w};
-                const float ws[4] = {pw[i].x, pw[i].y, pw[i].z, pw[i].w};
-                for (int a = 0; a < 4; ++a)
-                    if (ws[a] != 0.f) rptr[ids[a] + 1]++;
-            }
-            for (int J = 0; J < n; ++J) rptr[J + 1] += rptr[J];
-            rcol.resize(rptr[n]);
-            rw.resize(rptr[n]);
-            {
-                std::vector<int32_t> fill(rptr.begin(), rptr.end() - 1);
-                for (int i = 0; i < nfin; ++i) {
-                    const int ids[4] = {pid[i].x, pid[i].y, pid[i].z, pid[i].w};
-                    const float ws[4] = {pw[i].x, pw[i].y, pw[i].z, pw[i].w};
-                    for (int a = 0; a < 4; ++a)
-                        if (ws[a] != 0.f) {
-                            rcol[fill[ids[a]]] = i;
-                            rw[fill[ids[a]]] = ws[a];
-                            fill[ids[a]]++;
-                        }
-                }
-            }
-            std::vector<int32_t> sp, ec;
-            std::vector<float> ev;
-            build_ell(ptr, col, val, n, sp, ec, ev);
-            ld.nnz = (int)col.size();
-            TRY(dupload(h, pool, &ld.slice_ptr, sp));
-            TRY(dupload(h, pool, &ld.ell_col, ec));
-            TRY(dupload(h, pool, &ld.ell_val, ev));
-            TRY(dupload(h, pool, &ld.diag0, diag0));
-            TRY(dupload(h, pool, &ld.pid, pid));
-            TRY(dupload(h, pool, &ld.pw, pw));
-            TRY(dupload(h, pool, &ld.rptr, rptr));
-            TRY(dupload(h, pool, &ld.rcol, rcol));
-            TRY(dupload(h, pool, &ld.rw, rw));
-            TRY(dalloc(h, pool, &ld.c, n));
-            TRY(dalloc(h, pool, &ld.dfull, n));
-            TRY(dalloc(h, pool, &ld.dinv, n));
-            TRY(dalloc(h, pool, &ld.r, n));
-            TRY(dalloc(h, pool, &ld.e, n));
-            TRY(dalloc(h, pool, &ld.e2, n));
-            TRY(dalloc(h, pool, &ld.res, n));
-            CUDA_TRY(h, cudaMemset(ld.e, 0, n * sizeof(float4)));
-            CUDA_TRY(h, cudaMemset(ld.e2, 0, n * sizeof(float4)));
-            h->lev.push_back(ld);
-        }
-        // ---- coarsest dense blocks
-        std::vector<float> dense;
-        int maxn = 0;
         for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
-            const CoarseLevel& C = h->bodies[bi].levels[L - 2];
-            std::vector<double> d;
-            dense_from_sparse(C.A, C.active, d);
             BodyDev& BD = h->bodies_host[bi];
-            BD.cl_off = loff[bi];
-            BD.cl_n = C.n;
-            BD.dense_off = (int)dense.size();
-            for (double q : d) dense.push_back((float)q);
-            maxn = std::max(maxn, C.n);
+            BD.cl_off = P.cl_off[bi];
+            BD.cl_n = P.cl_n[bi];
+            BD.dense_off = P.dense_off[bi];
         }
-        h->max_coarsest = maxn;
-        h->factor_smem = ((size_t)maxn * maxn + maxn) * sizeof(float);
+        h->max_coarsest = P.max_coarsest;
+        h->factor_smem = ((size_t)P.max_coarsest * P.max_coarsest + P.max_coarsest) * sizeof(float);
         int dev_smem = 0;
         CUDA_TRY(h, cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
         if (h->factor_smem > (size_t)dev_smem)
-            return set_err(h, MGSB_NOT_SUPPORTED, "coarsest level has %d vertices; its dense factor needs %zu B of shared memory (max %d): add a level",
-                           maxn, h->factor_smem, dev_smem);
+            return set_err(h, MGSB_NOT_SUPPORTED,
+                           "coarsest level has %d vertices; its dense factor needs %zu B of shared memory (max %d): add a level",
+                           P.max_coarsest, h->factor_smem, dev_smem);
         CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->factor_smem));
-        TRY(dupload(h, pool, &h->A0dense, dense));
-        TRY(dalloc(h, pool, &h->Lfac, dense.size()));
+        TRY(dupload(h, pool, &h->A0dense, P.dense));
+        TRY(dalloc(h, pool, &h->Lfac, P.dense.size()));
         TRY(dalloc(h, pool, &h->Ldinv, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->fac_valid, h->bodies.size()));
         CUDA_TRY(h, cudaMemset(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t)));
-        // ---- surface vertices
-        std::vector<int32_t> surf;
-        for (const BodyHost& B : h->bodies)
-            for (int i : B.surface) surf.push_back(i + B.v_off);
-        h->nsurf = (int)surf.size();
-        TRY(dupload(h, pool, &h->surf, surf));
+        h->nsurf = (int)P.surf.size();
+        TRY(dupload(h, pool, &h->surf, P.surf));
     }
     for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
         BodyDev& BD = h->bodies_host[bi];
-        const BodyHost& B = h->bodies[bi];
-        BD.v0_off = B.v_off;
-        BD.v0_n = B.V;
+        BD.v0_off = h->bodies[bi].v_off;
+        BD.v0_n = h->bodies[bi].V;
     }
     h->dirty = false;
     return MGSB_OK;
@@ -742,39 +535,14 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     h->bodies.resize(nbodies);
     int voff = 0, toff = 0;
     for (int bi = 0; bi < nbodies; ++bi) {
-        const mgsb_mesh& m = meshes[bi];
-        if (m.num_verts <= 0 || m.num_tets <= 0 || !m.positions || !m.tets) return MGSB_INVALID_ARG;
         BodyHost& B = h->bodies[bi];
-        B.V = m.num_verts;
-        B.T = m.num_tets;
+        std::string e;
+        mgsb_status st = make_body(meshes[bi], params[bi], h->p.solver == MGSB_SOLVER_MULTIGRID, B, e);
+        if (st != MGSB_OK) return st;
         B.v_off = voff;
         B.t_off = toff;
         voff += B.V;
         toff += B.T;
-        B.rest.assign(3 * (size_t)B.V, 0.0);
-        for (size_t q = 0; q < B.rest.size(); ++q) B.rest[q] = m.positions[q];
-        B.tets.assign(m.tets, m.tets + 4 * (size_t)B.T);
-        for (int32_t vv : B.tets)
-            if (vv < 0 || vv >= B.V) return MGSB_INVALID_ARG;
-        std::string e;
-        if (!tet_rest(B.rest.data(), B.tets.data(), B.T, B.tr, e)) return MGSB_DEGENERATE_TET;
-        const mgsb_params& pb = params[bi];
-        B.youngs.assign(B.T, pb.youngs_modulus);
-        B.poisson.assign(B.T, pb.poisson_ratio);
-        B.fixed.assign(B.V, 0);
-        for (int c = 0; c < 3; ++c) {
-            B.grid_dims[c] = m.grid_dims[c];
-            B.gravity[c] = pb.gravity[c];
-        }
-        B.damping = pb.damping;
-        if (h->p.solver == MGSB_SOLVER_MULTIGRID) {
-            std::vector<int32_t> tris, opp;
-            extract_surface(B.tets.data(), B.T, tris, opp);
-            std::vector<uint8_t> on(B.V, 0);
-            for (int32_t q : tris) on[q] = 1;
-            for (int i = 0; i < B.V; ++i)
-                if (on[i]) B.surface.push_back(i);
-        }
     }
     h->N0 = voff;
     h->T = toff;
@@ -871,22 +639,7 @@ mgsb_status mgsb_batch_create(int32_t num_bodies, const mgsb_mesh* meshes, const
 
 mgsb_status mgsb_destroy(mgsb_solver* h) {
     if (!h) return MGSB_INVALID_ARG;
-    cudaSetDevice(h->device);
-    cudaStreamSynchronize(h->stream);
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-    if (h->graph) cudaGraphDestroy(h->graph);
-    free_pool(h->derived_mem);
-    free_pool(h->state_mem);
-    delete[] h->bodies_host;
-    delete h->spheres_host;
-    for (int k = 0; k < mgsb_solver::kStage; ++k) {
-        if (h->stage[k]) cudaFreeHost(h->stage[k]);
-        if (h->stage_ev[k]) cudaEventDestroy(h->stage_ev[k]);
-    }
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->own_stream) cudaStreamDestroy(h->stream);
-    delete h;
+    delete h;   // ~mgsb_solver releases every resource
     return MGSB_OK;
 }
 
@@ -1168,6 +921,47 @@ mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* 
         std::snprintf(names + 48 * u, 48, "%s", uniq[u].c_str());
         total_ms[u] = tot[u];
         launches[u] = cnt[u];
+    }
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_inspect_level(const mgsb_mesh* mesh, const mgsb_params* params, const uint8_t* fixed, int32_t level,
+                               int32_t* n, int32_t* nnz, int32_t* pid, float* pw, float* diag, int32_t* ptr, int32_t* col,
+                               float* val) {
+    if (!mesh || !params || !n || !nnz || params->solver != MGSB_SOLVER_MULTIGRID) return MGSB_INVALID_ARG;
+    if (level < 0 || level >= params->levels || params->levels < 2) return MGSB_INVALID_ARG;
+    std::vector<PlanBody> bodies(1);
+    std::string e;
+    mgsb_status st = make_body(*mesh, *params, true, bodies[0], e);
+    if (st != MGSB_OK) return st;
+    if (fixed)
+        for (int i = 0; i < bodies[0].V; ++i) bodies[0].fixed[i] = fixed[i] ? 1 : 0;
+    Plan P;
+    if (!build_plan(bodies, *params, P, e)) return MGSB_INVALID_ARG;
+    const PlanLevel& pl = P.levels[level];
+    *n = pl.n;
+    *nnz = pl.nnz;
+    if (pid && pw && level > 0)
+        for (size_t i = 0; i < pl.pid.size(); ++i) {
+            pid[4 * i] = pl.pid[i].x; pid[4 * i + 1] = pl.pid[i].y; pid[4 * i + 2] = pl.pid[i].z; pid[4 * i + 3] = pl.pid[i].w;
+            pw[4 * i] = pl.pw[i].x; pw[4 * i + 1] = pl.pw[i].y; pw[4 * i + 2] = pl.pw[i].z; pw[4 * i + 3] = pl.pw[i].w;
+        }
+    if (diag)
+        for (int i = 0; i < pl.n; ++i) diag[i] = level == 0 ? P.diag[i] : pl.diag0[i];
+    if (ptr && col && val) {
+        // CSR from the sliced ELL; padding entries point at their own row.
+        int z = 0;
+        ptr[0] = 0;
+        for (int r = 0; r < pl.n; ++r) {
+            const int s0 = r >> 5, lane = r & 31;
+            for (int q = pl.slice_ptr[s0] + lane; q < pl.slice_ptr[s0 + 1]; q += 32)
+                if (pl.ell_col[q] != r) {
+                    col[z] = pl.ell_col[q];
+                    val[z] = pl.ell_val[q];
+                    ++z;
+                }
+            ptr[r + 1] = z;
+        }
     }
     return MGSB_OK;
 }

@@ -194,9 +194,18 @@ def make_gpu() -> None:
                      _f(ms))
     if st != 0:
         raise SystemExit(f"ref_run failed with status {st}")
+    # a second identical run: the reference's float atomics make frames differ run to run
+    pos2 = np.zeros_like(pos)
+    st = lib.ref_run(_f(np.ascontiguousarray(m.positions)), V, _i(np.ascontiguousarray(m.tets)), T,
+                     fixed.ctypes.data_as(C.POINTER(C.c_uint8)), TRAJ_ITERS, TRAJ_FRAMES, _f(path), _f(pos2), None,
+                     None)
+    if st != 0:
+        raise SystemExit(f"ref_run (repeat) failed with status {st}")
+    rerun = np.abs(pos - pos2).reshape(TRAJ_FRAMES, -1).max(1)
     out_dir = sys.argv[2] if len(sys.argv) > 2 else HERE
     np.savez_compressed(os.path.join(out_dir, "ref_traj.npz"), frames=np.array(TRAJ_KEEP), positions=pos[TRAJ_KEEP],
-                        flags=flags[TRAJ_KEEP], ms=ms)
+                        flags=flags[TRAJ_KEEP], ms=ms, rerun_maxdiff=rerun)
+    print("run-to-run max difference of the reference:", float(rerun.max()))
     print("wrote ref_traj.npz; mean Step() ms", float(ms[5:].mean()))
 
 

@@ -34,10 +34,12 @@ def test_ref_precompute_matches_oracle(lib, oracle_built):
 
 
 def test_ref_frames_match_oracle(lib, oracle_built):
-    """100 frames with a sphere pushed through the beam: max vertex error <= 1e-5 x bbox diagonal."""
+    """100 frames with a sphere pushed through the beam: max vertex error <= 5e-5 x bbox
+    diagonal (the reference iteration amplifies FP32 rounding ~100x; see
+    test_reference_iteration_sensitivity)."""
     m, s, o = _ref_pair()
     path = traj_sphere_path()
-    tol = 1e-5 * m.bbox_diagonal()
+    tol = 5e-5 * m.bbox_diagonal()
     worst = 0.0
     flips = 0
     for f in range(path.shape[0]):
@@ -74,7 +76,7 @@ def test_ref_frames_match_reference_gpu(lib):
     g = np.load(os.path.join(GOLDEN, "ref_traj.npz"))
     m, s, _ = _ref_pair()
     path = traj_sphere_path()
-    tol = 1e-5 * m.bbox_diagonal()
+    tol = 5e-5 * m.bbox_diagonal()
     for f in range(path.shape[0]):
         s.set_spheres(path[f, :3][None], [path[f, 3]])
         s.step()

@@ -117,7 +117,11 @@ def test_planted_mistake_is_detected(oracle_built):
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(GOLDEN, "ref_traj.npz")), reason="GPU golden not generated")
 def test_oracle_ref_mode_matches_reference_trajectory(oracle_built):
-    """FP64 restatement of PDSolver::Step vs the reference's own GPU frames."""
+    """FP64 restatement of PDSolver::Step vs the reference's own GPU frames.
+
+    Tolerance 5e-5 x bbox diagonal: the reference's 20-iteration Jacobi/Chebyshev
+    frame amplifies a 1e-6 perturbation of the state to ~1e-4 within a few frames
+    (measured), so FP32 rounding alone separates FP32 and FP64 runs by ~1e-4."""
     from .golden.make_golden import TRAJ_ITERS, traj_scene, traj_sphere_path
     g = np.load(os.path.join(GOLDEN, "ref_traj.npz"))
     m, fixed = traj_scene()
@@ -125,7 +129,7 @@ def test_oracle_ref_mode_matches_reference_trajectory(oracle_built):
     o.set_fixed(fixed)
     path = traj_sphere_path()
     keep = list(g["frames"])
-    tol = 1e-5 * m.bbox_diagonal()
+    tol = 5e-5 * m.bbox_diagonal()
     for f in range(path.shape[0]):
         o.set_spheres(path[f, :3][None], [path[f, 3]])
         o.step()
@@ -133,3 +137,25 @@ def test_oracle_ref_mode_matches_reference_trajectory(oracle_built):
             k = keep.index(f)
             err = np.abs(o.positions() - g["positions"][k]).max()
             assert err < tol, (f, err, tol)
+            assert np.array_equal(o.contact_flags(), g["flags"][k]), f
+
+
+def test_reference_iteration_sensitivity(oracle_built):
+    """Documents why the reference kind is pinned at 5e-5 x diag: a 1e-6 state
+    perturbation grows to > 1e-5 within ten frames of the reference iteration."""
+    from .golden.make_golden import TRAJ_ITERS, traj_scene, traj_sphere_path
+    m, fixed = traj_scene()
+    path = traj_sphere_path()
+    runs = []
+    for pert in (0.0, 1e-6):
+        o = Oracle(m, mg.default_params(mg.SOLVER_REFERENCE_JACOBI, iterations=TRAJ_ITERS))
+        o.set_fixed(fixed)
+        x = m.positions.astype(np.float64) + np.random.default_rng(0).normal(0, pert, m.positions.shape)
+        x[fixed.astype(bool)] = m.positions[fixed.astype(bool)]
+        o.set_state(x, None)
+        for f in range(10):
+            o.set_spheres(path[f, :3][None], [path[f, 3]])
+            o.step()
+        runs.append(o.positions())
+    amp = np.abs(runs[0] - runs[1]).max() / 1e-6
+    assert amp > 10.0
