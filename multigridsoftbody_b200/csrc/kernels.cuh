@@ -18,12 +18,6 @@ namespace mgsb {
 // ---------------------------------------------------------------------------
 // Shared structures passed by value to kernels
 // ---------------------------------------------------------------------------
-struct Ell {
-    const int32_t* slice_ptr;  // [nslices+1] entry offsets
-    const int32_t* col;
-    const float* val;
-};
-
 struct SphereSet {
     int count;
     float cx[8], cy[8], cz[8], r[8];
@@ -43,20 +37,6 @@ struct BodyDev {
     float cap_a[4];
     float cap_b[4];
 };
-
-__device__ __forceinline__ float4 ell_row_mul(int row, const Ell A, const float4* __restrict__ x) {
-    const int s = row >> 5, lane = row & 31;
-    const int beg = __ldg(A.slice_ptr + s), end = __ldg(A.slice_ptr + s + 1);
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    for (int e = beg + lane; e < end; e += 32) {
-        const float a = __ldg(A.val + e);
-        const float4 xv = __ldg(x + __ldg(A.col + e));
-        ax = fmaf(a, xv.x, ax);
-        ay = fmaf(a, xv.y, ay);
-        az = fmaf(a, xv.z, az);
-    }
-    return make_float4(ax, ay, az, 0.f);
-}
 
 // ===========================================================================
 // Reference-faithful Jacobi/Chebyshev frame (PDSolver::Step)
@@ -288,19 +268,40 @@ __global__ void k_contact_all(int ns, const int32_t* __restrict__ surf, const in
     target[i] = tg;
 }
 
-// Per frame, level 0: b0 = m/h^2 s + c p, D = L_ii + c, dinv = fixed ? 0 : omega/D.
-__global__ void k_l0_frame(int n, const float4* __restrict__ s, const float* __restrict__ mass_h2,
-                           const float* __restrict__ c0, const float4* __restrict__ target, const float* __restrict__ diag0,
+// Per frame, level 0.  The global step is solved for the displacement from
+// the prediction, d = x - s, so every right-hand-side term is a small
+// difference: b0 = c (p - s), D = L_ii + c, dinv = fixed ? 0 : omega/D, d = 0.
+__global__ void k_l0_frame(int n, const float4* __restrict__ s, const float* __restrict__ c0,
+                           const float4* __restrict__ target, const float* __restrict__ diag0,
                            const float* __restrict__ fixf, float omega, float4* __restrict__ b0, float* __restrict__ dfull,
-                           float* __restrict__ dinv) {
+                           float* __restrict__ dinv, float4* __restrict__ d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float m = __ldg(mass_h2 + i), c = __ldg(c0 + i);
+    const float c = __ldg(c0 + i);
     const float4 sv = __ldg(s + i), tg = __ldg(target + i);
-    b0[i] = make_float4(fmaf(m, sv.x, c * tg.x), fmaf(m, sv.y, c * tg.y), fmaf(m, sv.z, c * tg.z), 0.f);
+    b0[i] = c != 0.f ? make_float4(c * (tg.x - sv.x), c * (tg.y - sv.y), c * (tg.z - sv.z), 0.f)
+                     : make_float4(0.f, 0.f, 0.f, 0.f);
     const float D = __ldg(diag0 + i) + c;
     dfull[i] = D;
     dinv[i] = (__ldg(fixf + i) != 0.f) ? omega / D : 0.f;
+    d[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// End of frame: x = s + d, v = v_predicted + d/dt (= (x - x_prev)/dt), and a
+// finiteness check of the new positions.
+__global__ void k_mg_finish(int n, const float4* __restrict__ s, const float4* __restrict__ d, float4* __restrict__ x,
+                            float4* __restrict__ v, float inv_dt, int32_t* __restrict__ nonfinite) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 sv = __ldg(s + i), dv = __ldg(d + i);
+    float4 vel = v[i];
+    const float4 p = make_float4(sv.x + dv.x, sv.y + dv.y, sv.z + dv.z, 0.f);
+    vel.x = fmaf(dv.x, inv_dt, vel.x);
+    vel.y = fmaf(dv.y, inv_dt, vel.y);
+    vel.z = fmaf(dv.z, inv_dt, vel.z);
+    x[i] = p;
+    v[i] = vel;
+    if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) atomicOr(nonfinite, 1);
 }
 
 // Per frame, level l >= 1: lumped contact weight c_l = P^T c_{l-1}, D and dinv.
@@ -320,12 +321,13 @@ __global__ void k_coarse_frame(int n, const int32_t* __restrict__ rptr, const in
     dinv[J] = d0 > 0.f ? omega / D : 0.f;
 }
 
-// Local step, one thread per tet: F = sum_j x_j g_j^T, R = closest rotation,
-// RHS contribution w R g_j into the four corner slots.
+// Local step, one thread per tet, on x = s + d: F = sum_j x_j g_j^T from the
+// edge vectors (s_k - s_0) + (d_k - d_0), R = closest rotation; the RHS of
+// the displacement system gets w (R - F(s)) g_j in the four corner slots.
 __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict__ tets, const float4* __restrict__ gA,
                                                   const float4* __restrict__ gB, const float2* __restrict__ gC,
-                                                  const float4* __restrict__ x, const int4* __restrict__ slot_of,
-                                                  float4* __restrict__ slots) {
+                                                  const float4* __restrict__ s, const float4* __restrict__ d,
+                                                  const int4* __restrict__ slot_of, float4* __restrict__ slots) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const int4 id = __ldg(tets + t);
@@ -334,17 +336,26 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
     // g1 = (a.x a.y a.z), g2 = (a.w b.x b.y), g3 = (b.z b.w c.x), w = c.y
     const float g1[3] = {a.x, a.y, a.z}, g2[3] = {a.w, b.x, b.y}, g3[3] = {b.z, b.w, c.x};
     const float w = c.y;
-    const float4 p0 = __ldg(x + id.x), p1 = __ldg(x + id.y), p2 = __ldg(x + id.z), p3 = __ldg(x + id.w);
-    const float d1[3] = {p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
-    const float d2[3] = {p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
-    const float d3[3] = {p3.x - p0.x, p3.y - p0.y, p3.z - p0.z};
-    float F[9];
+    const float4 s0 = __ldg(s + id.x), s1 = __ldg(s + id.y), s2 = __ldg(s + id.z), s3 = __ldg(s + id.w);
+    const float4 q0 = __ldg(d + id.x), q1 = __ldg(d + id.y), q2 = __ldg(d + id.z), q3 = __ldg(d + id.w);
+    const float e1[3] = {s1.x - s0.x, s1.y - s0.y, s1.z - s0.z};
+    const float e2[3] = {s2.x - s0.x, s2.y - s0.y, s2.z - s0.z};
+    const float e3[3] = {s3.x - s0.x, s3.y - s0.y, s3.z - s0.z};
+    const float f1[3] = {q1.x - q0.x, q1.y - q0.y, q1.z - q0.z};
+    const float f2[3] = {q2.x - q0.x, q2.y - q0.y, q2.z - q0.z};
+    const float f3[3] = {q3.x - q0.x, q3.y - q0.y, q3.z - q0.z};
+    float Fs[9], F[9];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int q = 0; q < 3; ++q) F[r * 3 + q] = d1[r] * g1[q] + d2[r] * g2[q] + d3[r] * g3[q];
+        for (int q = 0; q < 3; ++q) {
+            Fs[r * 3 + q] = e1[r] * g1[q] + e2[r] * g2[q] + e3[r] * g3[q];
+            F[r * 3 + q] = (e1[r] + f1[r]) * g1[q] + (e2[r] + f2[r]) * g2[q] + (e3[r] + f3[r]) * g3[q];
+        }
     float R[9];
     svd_rotation(F, R);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) R[q] -= Fs[q];
     float o1[3], o2[3], o3[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
@@ -357,34 +368,6 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
     slots[so.y] = make_float4(o1[0], o1[1], o1[2], 0.f);
     slots[so.z] = make_float4(o2[0], o2[1], o2[2], 0.f);
     slots[so.w] = make_float4(o3[0], o3[1], o3[2], 0.f);
-}
-
-// Level-0 weighted-Jacobi sweep on positions.  With gather != 0 the RHS is
-// assembled first: b = b0 + sum of the vertex's slots (contiguous), and stored.
-__global__ void __launch_bounds__(256) k_l0_sweep(int n, Ell A, const float* __restrict__ dfull,
-                                                  const float* __restrict__ dinv, const float4* __restrict__ xin,
-                                                  float4* __restrict__ xout, float4* __restrict__ b,
-                                                  const float4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
-                                                  const float4* __restrict__ slots, int gather) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float4 bi;
-    if (gather) {
-        bi = __ldg(b0 + i);
-        const int e1 = __ldg(slot_ptr + i + 1);
-        for (int e = __ldg(slot_ptr + i); e < e1; ++e) {
-            const float4 c = __ldg(slots + e);
-            bi.x += c.x; bi.y += c.y; bi.z += c.z;
-        }
-        b[i] = bi;
-    } else {
-        bi = b[i];
-    }
-    const float4 xi = __ldg(xin + i);
-    const float4 off = ell_row_mul(i, A, xin);
-    const float D = __ldg(dfull + i), di = __ldg(dinv + i);
-    const float rx = bi.x - fmaf(D, xi.x, off.x), ry = bi.y - fmaf(D, xi.y, off.y), rz = bi.z - fmaf(D, xi.z, off.z);
-    xout[i] = make_float4(fmaf(di, rx, xi.x), fmaf(di, ry, xi.y), fmaf(di, rz, xi.z), 0.f);
 }
 
 // RHS assembly alone: b = b0 + sum of the vertex's slots.
@@ -401,65 +384,6 @@ __global__ void k_gather_rhs(int n, float4* __restrict__ b, const float4* __rest
     b[i] = bi;
 }
 
-// Residual res = rhs - A v (level 0 with v = positions; coarse with v = e).
-__global__ void __launch_bounds__(256) k_residual(int n, Ell A, const float* __restrict__ dfull,
-                                                  const float4* __restrict__ v, const float4* __restrict__ rhs,
-                                                  float4* __restrict__ res) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 vi = __ldg(v + i), ri = __ldg(rhs + i);
-    const float4 off = ell_row_mul(i, A, v);
-    const float D = __ldg(dfull + i);
-    res[i] = make_float4(ri.x - fmaf(D, vi.x, off.x), ri.y - fmaf(D, vi.y, off.y), ri.z - fmaf(D, vi.z, off.z), 0.f);
-}
-
-// Restriction r_l = P^T res_{l-1} (gather over children) fused with the
-// first pre-smoothing sweep from a zero guess: e = dinv r.
-__global__ void k_restrict(int n, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rcol,
-                           const float* __restrict__ rw, const float4* __restrict__ resf, const float* __restrict__ dinv,
-                           float4* __restrict__ r, float4* __restrict__ e, int first_sweep) {
-    const int J = blockIdx.x * blockDim.x + threadIdx.x;
-    if (J >= n) return;
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    const int e1 = __ldg(rptr + J + 1);
-    for (int q = __ldg(rptr + J); q < e1; ++q) {
-        const float w = __ldg(rw + q);
-        const float4 v = __ldg(resf + __ldg(rcol + q));
-        ax = fmaf(w, v.x, ax); ay = fmaf(w, v.y, ay); az = fmaf(w, v.z, az);
-    }
-    r[J] = make_float4(ax, ay, az, 0.f);
-    const float di = first_sweep ? __ldg(dinv + J) : 0.f;
-    e[J] = make_float4(di * ax, di * ay, di * az, 0.f);
-}
-
-// Coarse weighted-Jacobi sweep on the correction: e' = e + dinv (r - A e).
-__global__ void __launch_bounds__(256) k_coarse_sweep(int n, Ell A, const float* __restrict__ dfull,
-                                                      const float* __restrict__ dinv, const float4* __restrict__ r,
-                                                      const float4* __restrict__ ein, float4* __restrict__ eout) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 ei = __ldg(ein + i), ri = __ldg(r + i);
-    const float4 off = ell_row_mul(i, A, ein);
-    const float D = __ldg(dfull + i), di = __ldg(dinv + i);
-    eout[i] = make_float4(fmaf(di, ri.x - fmaf(D, ei.x, off.x), ei.x), fmaf(di, ri.y - fmaf(D, ei.y, off.y), ei.y),
-                          fmaf(di, ri.z - fmaf(D, ei.z, off.z), ei.z), 0.f);
-}
-
-// Prolongation v_fine += P e_coarse (4 parents per fine vertex).
-__global__ void k_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
-                          const float4* __restrict__ ec, float4* __restrict__ v) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int4 id = __ldg(pid + i);
-    const float4 w = __ldg(pw + i);
-    const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
-    float4 vi = v[i];
-    vi.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
-    vi.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
-    vi.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
-    v[i] = vi;
-}
-
 // v = (x - last)/dt plus a finiteness check of the new positions.
 __global__ void k_velocity(int n, const float4* __restrict__ x, const float4* __restrict__ last, float4* __restrict__ v,
                            float dt, int32_t* __restrict__ nonfinite) {
@@ -468,163 +392,6 @@ __global__ void k_velocity(int n, const float4* __restrict__ x, const float4* __
     const float4 p = __ldg(x + i), l = __ldg(last + i);
     v[i] = make_float4((p.x - l.x) / dt, (p.y - l.y) / dt, (p.z - l.z) / dt, 0.f);
     if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) atomicOr(nonfinite, 1);
-}
-
-// ---------------------------------------------------------------------------
-// Coarsest level: dense Cholesky per body (one CTA per body).
-// The factor is recomputed only when the lumped contact weights of the body's
-// coarsest vertices changed since the last factorisation.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_coarsest_factor(const BodyDev* __restrict__ bodies, const float* __restrict__ A0,
-                                                         const float* __restrict__ c, float* __restrict__ c_prev,
-                                                         float* __restrict__ Lfac, float* __restrict__ Ldinv,
-                                                         int32_t* __restrict__ valid) {
-    extern __shared__ float sm[];
-    const BodyDev& B = bodies[blockIdx.x];
-    const int n = B.cl_n, off = B.cl_off;
-    const float* A = A0 + B.dense_off;
-    float* Lg = Lfac + B.dense_off;
-    __shared__ int changed;
-    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        if (c[off + i] != c_prev[off + i]) changed = 1;
-    __syncthreads();
-    if (!changed) return;
-    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-        const int i = q / n, j = q - i * n;
-        float a = A[q];
-        if (i == j) a += c[off + i];
-        sm[q] = a;
-    }
-    __syncthreads();
-    float* piv = sm + n * n;  // n pivots
-    for (int j = 0; j < n; ++j) {
-        const float d = sqrtf(sm[j * n + j]);
-        const float id = 1.f / d;
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) sm[i * n + j] *= id;
-        if (threadIdx.x == 0) piv[j] = d;
-        __syncthreads();
-        const int m = n - j - 1;
-        const int tot = m * (m + 1) / 2;
-        for (int q = threadIdx.x; q < tot; q += blockDim.x) {
-            int a = (int)((sqrtf(8.f * (float)q + 1.f) - 1.f) * 0.5f);
-            while ((a + 1) * (a + 2) / 2 <= q) ++a;
-            while (a * (a + 1) / 2 > q) --a;
-            const int bcol = q - a * (a + 1) / 2;
-            const int i = j + 1 + a, k = j + 1 + bcol;
-            sm[i * n + k] -= sm[i * n + j] * sm[k * n + j];
-        }
-        __syncthreads();
-    }
-    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-        const int i = q / n, j = q - i * n;
-        Lg[q] = (j < i) ? sm[q] : (j == i ? piv[i] : 0.f);
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        Ldinv[off + i] = 1.f / piv[i];
-        c_prev[off + i] = c[off + i];
-    }
-    if (threadIdx.x == 0) valid[blockIdx.x] = 1;
-}
-
-// Restrict the residual onto the coarsest level and solve L L^T e = r with
-// blocked substitution: a warp solves each 32x32 diagonal block, the CTA
-// updates the remaining rows.  Inactive rows are identity rows of the factor
-// and get a zero right-hand side.
-__global__ void __launch_bounds__(256) k_coarsest_solve(const BodyDev* __restrict__ bodies, const int32_t* __restrict__ rptr,
-                                                        const int32_t* __restrict__ rcol, const float* __restrict__ rw,
-                                                        const float4* __restrict__ resf, const float* __restrict__ Lfac,
-                                                        const float* __restrict__ Ldinv, float4* __restrict__ eout) {
-    extern __shared__ float4 rs[];
-    const BodyDev& B = bodies[blockIdx.x];
-    const int n = B.cl_n, off = B.cl_off;
-    const float* L = Lfac + B.dense_off;
-    const float* ldi = Ldinv + off;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int J = tid; J < n; J += blockDim.x) {
-        float ax = 0.f, ay = 0.f, az = 0.f;
-        const int e1 = __ldg(rptr + off + J + 1);
-        for (int q = __ldg(rptr + off + J); q < e1; ++q) {
-            const float w = __ldg(rw + q);
-            const float4 v = __ldg(resf + __ldg(rcol + q));
-            ax = fmaf(w, v.x, ax); ay = fmaf(w, v.y, ay); az = fmaf(w, v.z, az);
-        }
-        rs[J] = make_float4(ax, ay, az, 0.f);
-    }
-    __syncthreads();
-    // forward: L y = r
-    for (int jb = 0; jb < n; jb += 32) {
-        const int nb = min(32, n - jb);
-        if (warp == 0) {
-            const int i = jb + lane;
-            float4 val = (lane < nb) ? rs[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int jj = 0; jj < nb; ++jj) {
-                float yx = val.x * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
-                float yy = val.y * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
-                float yz = val.z * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
-                yx = __shfl_sync(0xffffffffu, yx, jj);
-                yy = __shfl_sync(0xffffffffu, yy, jj);
-                yz = __shfl_sync(0xffffffffu, yz, jj);
-                if (lane == jj) {
-                    val = make_float4(yx, yy, yz, 0.f);
-                } else if (lane > jj && lane < nb) {
-                    const float l = __ldg(L + (size_t)i * n + jb + jj);
-                    val.x -= l * yx; val.y -= l * yy; val.z -= l * yz;
-                }
-            }
-            if (lane < nb) rs[i] = val;
-        }
-        __syncthreads();
-        for (int i = jb + nb + tid; i < n; i += blockDim.x) {
-            float4 acc = rs[i];
-            const float* Li = L + (size_t)i * n + jb;
-            for (int k = 0; k < nb; ++k) {
-                const float l = __ldg(Li + k);
-                const float4 y = rs[jb + k];
-                acc.x -= l * y.x; acc.y -= l * y.y; acc.z -= l * y.z;
-            }
-            rs[i] = acc;
-        }
-        __syncthreads();
-    }
-    // backward: L^T e = y
-    const int nblk = (n + 31) / 32;
-    for (int bi = nblk - 1; bi >= 0; --bi) {
-        const int jb = bi * 32;
-        const int nb = min(32, n - jb);
-        if (warp == 0) {
-            const int i = jb + lane;
-            float4 val = (lane < nb) ? rs[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int jj = nb - 1; jj >= 0; --jj) {
-                float ex = val.x * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
-                float ey = val.y * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
-                float ez = val.z * ((lane == jj) ? __ldg(ldi + jb + jj) : 0.f);
-                ex = __shfl_sync(0xffffffffu, ex, jj);
-                ey = __shfl_sync(0xffffffffu, ey, jj);
-                ez = __shfl_sync(0xffffffffu, ez, jj);
-                if (lane == jj) {
-                    val = make_float4(ex, ey, ez, 0.f);
-                } else if (lane < jj) {
-                    const float l = __ldg(L + (size_t)(jb + jj) * n + i);  // L^T[i][j] = L[j][i]
-                    val.x -= l * ex; val.y -= l * ey; val.z -= l * ez;
-                }
-            }
-            if (lane < nb) rs[i] = val;
-        }
-        __syncthreads();
-        for (int i = tid; i < jb; i += blockDim.x) {
-            float4 acc = rs[i];
-            for (int k = 0; k < nb; ++k) {
-                const float l = __ldg(L + (size_t)(jb + k) * n + i);
-                const float4 e = rs[jb + k];
-                acc.x -= l * e.x; acc.y -= l * e.y; acc.z -= l * e.z;
-            }
-            rs[i] = acc;
-        }
-        __syncthreads();
-    }
-    for (int J = tid; J < n; J += blockDim.x) eout[off + J] = rs[J];
 }
 
 }  // namespace mgsb

@@ -1,0 +1,458 @@
+// Multigrid global-step kernels (sm_100a).  Included by solver.cu only.
+//
+// SpMV layout: sliced ELL with slice height S = 32/G; entry k of row r of
+// slice s sits at slice_ptr[s] + k*S + (r mod S).  A warp covers S rows with
+// G lanes per row; lane l handles entries k = l/S, l/S + G, ... so a warp
+// reads 32 consecutive entries per step, and the G partial sums of a row are
+// combined with xor-shuffles over lane offsets S, 2S, ..., 16.
+#pragma once
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.cuh"
+
+namespace mgsb {
+
+namespace cg = cooperative_groups;
+
+constexpr int kMaxLevels = 12;
+constexpr int kLanesL0 = 4;   // lanes per row at level 0 (slice height 8)
+constexpr int kLanesC = 8;    // lanes per row on coarse levels (slice height 4)
+
+struct LevelView {
+    int n;
+    const int32_t* slice_ptr;
+    const int32_t* col;
+    const float* val;
+    const float* dfull;
+    const float* dinv;
+    float4* r;
+    float4* e;
+    float4* e2;
+    float4* res;
+    const int4* pid;      // prolongation rows of the next finer level
+    const float4* pw;
+    const int32_t* rptr;  // restriction: children in the next finer level
+    const int32_t* rcol;
+    const float* rw;
+};
+
+struct CoarseArgs {
+    int L;
+    int pre, post;
+    int fuse_l0;             // level-0 residual and prolongation inside the kernel
+    const int2* range;       // [nbody * L]: (first row, rows) of each body on each level
+    const int32_t* dense_off;
+    const float* Ainv;       // coarsest inverse blocks (row-major per body)
+    const float4* b;         // level-0 right-hand side
+    float4* d;               // level-0 unknown (displacement)
+    LevelView lv[kMaxLevels];
+};
+
+__device__ __forceinline__ float4 f4z() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+
+// Load of a vector that may have been written earlier in the same kernel by
+// another CTA of the cluster: a plain (coherent) load, never the read-only path.
+template <bool kReadOnly>
+__device__ __forceinline__ float4 vload(const float4* p) {
+    if constexpr (kReadOnly)
+        return __ldg(p);
+    else
+        return *p;
+}
+
+// Partial off-diagonal product of `row` for this lane (sub = lane / S), then
+// reduced over the G lanes of the row.  Every lane of the warp must call it.
+// kReadOnly: x is not written during the calling kernel.
+template <int G, bool kReadOnly = true>
+__device__ __forceinline__ float4 rg_offdiag(int row, bool valid, int lane, const int32_t* __restrict__ sp,
+                                             const int32_t* __restrict__ col, const float* __restrict__ val,
+                                             const float4* x) {
+    constexpr int S = 32 / G;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (valid) {
+        const int slice = row / S;
+        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
+#pragma unroll 2
+        for (int e = beg + (lane / S) * S + (row - slice * S); e < end; e += 32) {
+            const float a = __ldg(val + e);
+            const float4 xv = vload<kReadOnly>(x + __ldg(col + e));
+            ax = fmaf(a, xv.x, ax);
+            ay = fmaf(a, xv.y, ay);
+            az = fmaf(a, xv.z, az);
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return make_float4(ax, ay, az, 0.f);
+}
+
+// Sum of w * v[idx] over a CSR row split across the G lanes of the row.
+template <int G, bool kReadOnly = true>
+__device__ __forceinline__ float4 rg_csr_sum(bool valid, int lane, int beg, int end, const int32_t* __restrict__ idx,
+                                             const float* __restrict__ w, const float4* v) {
+    constexpr int S = 32 / G;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (valid) {
+#pragma unroll 2
+        for (int q = beg + lane / S; q < end; q += G) {
+            const float c = __ldg(w + q);
+            const float4 t = vload<kReadOnly>(v + __ldg(idx + q));
+            ax = fmaf(c, t.x, ax);
+            ay = fmaf(c, t.y, ay);
+            az = fmaf(c, t.z, az);
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return make_float4(ax, ay, az, 0.f);
+}
+
+// Sum of the contiguous float4 slots [beg, end) split across the G lanes.
+template <int G>
+__device__ __forceinline__ float4 rg_slot_sum(bool valid, int lane, int beg, int end, const float4* __restrict__ slots) {
+    constexpr int S = 32 / G;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (valid) {
+#pragma unroll 2
+        for (int q = beg + lane / S; q < end; q += G) {
+            const float4 t = __ldg(slots + q);
+            ax += t.x;
+            ay += t.y;
+            az += t.z;
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return make_float4(ax, ay, az, 0.f);
+}
+
+// ---------------------------------------------------------------------------
+// Level-0 weighted-Jacobi sweep on the displacement: d' = d + dinv (b - A d).
+// With gather != 0 the RHS is assembled first (b = b0 + slots) and stored.
+// One warp per 8 rows, 4 lanes per row.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_l0_sweep_rg(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                                     const float* __restrict__ val, const float* __restrict__ dfull,
+                                                     const float* __restrict__ dinv, const float4* __restrict__ din,
+                                                     float4* __restrict__ dout, float4* __restrict__ b,
+                                                     const float4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
+                                                     const float4* __restrict__ slots, int gather) {
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    float4 bi;
+    if (gather) {
+        const int beg = valid ? __ldg(slot_ptr + row) : 0, end = valid ? __ldg(slot_ptr + row + 1) : 0;
+        const float4 sl = rg_slot_sum<G>(valid, lane, beg, end, slots);
+        const float4 bb = valid ? __ldg(b0 + row) : f4z();
+        bi = make_float4(bb.x + sl.x, bb.y + sl.y, bb.z + sl.z, 0.f);
+        if (valid && lane < S) b[row] = bi;
+    } else {
+        bi = valid ? b[row] : f4z();
+    }
+    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, din);
+    if (!valid || lane >= S) return;
+    const float4 di4 = __ldg(din + row);
+    const float D = __ldg(dfull + row), w = __ldg(dinv + row);
+    dout[row] = make_float4(fmaf(w, bi.x - fmaf(D, di4.x, off.x), di4.x), fmaf(w, bi.y - fmaf(D, di4.y, off.y), di4.y),
+                            fmaf(w, bi.z - fmaf(D, di4.z, off.z), di4.z), 0.f);
+}
+
+// Level-0 residual res = b - A d (used when the coarse kernel does not fuse it).
+__global__ void __launch_bounds__(256) k_l0_residual_rg(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                                        const float* __restrict__ val, const float* __restrict__ dfull,
+                                                        const float4* __restrict__ dvec, const float4* __restrict__ b,
+                                                        float4* __restrict__ res) {
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, dvec);
+    if (!valid || lane >= S) return;
+    const float4 x = __ldg(dvec + row), bi = __ldg(b + row);
+    const float D = __ldg(dfull + row);
+    res[row] = make_float4(bi.x - fmaf(D, x.x, off.x), bi.y - fmaf(D, x.y, off.y), bi.z - fmaf(D, x.z, off.z), 0.f);
+}
+
+// Level-0 prolongation d += P e1 (used when the coarse kernel does not fuse it).
+__global__ void k_l0_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
+                             const float4* __restrict__ ec, float4* __restrict__ v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 id = __ldg(pid + i);
+    const float4 w = __ldg(pw + i);
+    const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
+    float4 vi = v[i];
+    vi.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+    vi.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+    vi.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+    v[i] = vi;
+}
+
+// ---------------------------------------------------------------------------
+// Coarse part of the V-cycle, one thread-block cluster per body; phases are
+// separated by cluster barriers (release/acquire on global memory).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_coarse_vcycle(const CoarseArgs A) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int cs = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int body = blockIdx.x / cs;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int warp_c = rank * wpb + (threadIdx.x >> 5);
+    const int nwarp = cs * wpb;
+    const int tid_c = rank * blockDim.x + threadIdx.x;
+    const int nthr = cs * blockDim.x;
+    const int L = A.L;
+    constexpr int Sc = 32 / kLanesC;
+    constexpr int S0 = 32 / kLanesL0;
+
+    // level-0 residual res0 = b - A0 d over this body's rows
+    if (A.fuse_l0) {
+        const int2 rg = A.range[body * L + 0];
+        const LevelView& V0 = A.lv[0];
+        for (int base = rg.x + warp_c * S0; base < rg.x + rg.y; base += nwarp * S0) {
+            const int row = base + (lane % S0);
+            const bool valid = row < rg.x + rg.y;
+            const float4 off = rg_offdiag<kLanesL0, false>(row, valid, lane, V0.slice_ptr, V0.col, V0.val, A.d);
+            if (valid && lane < S0) {
+                const float4 x = A.d[row], bi = __ldg(A.b + row);
+                const float D = __ldg(V0.dfull + row);
+                V0.res[row] = make_float4(bi.x - fmaf(D, x.x, off.x), bi.y - fmaf(D, x.y, off.y), bi.z - fmaf(D, x.z, off.z), 0.f);
+            }
+        }
+        cluster.sync();
+    }
+    float4* ecur[kMaxLevels];
+    float4* eoth[kMaxLevels];
+    // descend
+    for (int l = 1; l < L - 1; ++l) {
+        const LevelView& C = A.lv[l];
+        const int2 rg = A.range[body * L + l];
+        ecur[l] = C.e;
+        eoth[l] = C.e2;
+        for (int base = rg.x + warp_c * Sc; base < rg.x + rg.y; base += nwarp * Sc) {
+            const int row = base + (lane % Sc);
+            const bool valid = row < rg.x + rg.y;
+            const int beg = valid ? __ldg(C.rptr + row) : 0, end = valid ? __ldg(C.rptr + row + 1) : 0;
+            const float4 r = rg_csr_sum<kLanesC, false>(valid, lane, beg, end, C.rcol, C.rw, A.lv[l - 1].res);
+            if (valid && lane < Sc) {
+                C.r[row] = r;
+                const float di = A.pre > 0 ? __ldg(C.dinv + row) : 0.f;
+                C.e[row] = make_float4(di * r.x, di * r.y, di * r.z, 0.f);
+            }
+        }
+        cluster.sync();
+        for (int k = 1; k < A.pre; ++k) {
+            for (int base = rg.x + warp_c * Sc; base < rg.x + rg.y; base += nwarp * Sc) {
+                const int row = base + (lane % Sc);
+                const bool valid = row < rg.x + rg.y;
+                const float4 off = rg_offdiag<kLanesC, false>(row, valid, lane, C.slice_ptr, C.col, C.val, ecur[l]);
+                if (valid && lane < Sc) {
+                    const float4 x = ecur[l][row], ri = C.r[row];
+                    const float D = __ldg(C.dfull + row), w = __ldg(C.dinv + row);
+                    eoth[l][row] = make_float4(fmaf(w, ri.x - fmaf(D, x.x, off.x), x.x), fmaf(w, ri.y - fmaf(D, x.y, off.y), x.y),
+                                               fmaf(w, ri.z - fmaf(D, x.z, off.z), x.z), 0.f);
+                }
+            }
+            float4* t = ecur[l];
+            ecur[l] = eoth[l];
+            eoth[l] = t;
+            cluster.sync();
+        }
+        for (int base = rg.x + warp_c * Sc; base < rg.x + rg.y; base += nwarp * Sc) {
+            const int row = base + (lane % Sc);
+            const bool valid = row < rg.x + rg.y;
+            const float4 off = rg_offdiag<kLanesC, false>(row, valid, lane, C.slice_ptr, C.col, C.val, ecur[l]);
+            if (valid && lane < Sc) {
+                const float4 x = ecur[l][row], ri = C.r[row];
+                const float D = __ldg(C.dfull + row);
+                C.res[row] = make_float4(ri.x - fmaf(D, x.x, off.x), ri.y - fmaf(D, x.y, off.y), ri.z - fmaf(D, x.z, off.z), 0.f);
+            }
+        }
+        cluster.sync();
+    }
+    // coarsest: restrict, then e = A^-1 r (dense, warp per row)
+    {
+        const int l = L - 1;
+        const LevelView& C = A.lv[l];
+        const int2 rg = A.range[body * L + l];
+        for (int base = rg.x + warp_c * Sc; base < rg.x + rg.y; base += nwarp * Sc) {
+            const int row = base + (lane % Sc);
+            const bool valid = row < rg.x + rg.y;
+            const int beg = valid ? __ldg(C.rptr + row) : 0, end = valid ? __ldg(C.rptr + row + 1) : 0;
+            const float4 r = rg_csr_sum<kLanesC, false>(valid, lane, beg, end, C.rcol, C.rw, A.lv[l - 1].res);
+            if (valid && lane < Sc) C.r[row] = r;
+        }
+        cluster.sync();
+        const int n = rg.y;
+        const float* Ai = A.Ainv + __ldg(A.dense_off + body);
+        for (int i = warp_c; i < n; i += nwarp) {
+            float ax = 0.f, ay = 0.f, az = 0.f;
+            for (int k = lane; k < n; k += 32) {
+                const float a = __ldg(Ai + (size_t)i * n + k);
+                const float4 r = C.r[rg.x + k];
+                ax = fmaf(a, r.x, ax);
+                ay = fmaf(a, r.y, ay);
+                az = fmaf(a, r.z, az);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                az += __shfl_xor_sync(0xffffffffu, az, o);
+            }
+            if (lane == 0) C.e[rg.x + i] = make_float4(ax, ay, az, 0.f);
+        }
+        ecur[l] = C.e;
+        cluster.sync();
+    }
+    // ascend
+    for (int l = L - 2; l >= 1; --l) {
+        const LevelView& C = A.lv[l];
+        const LevelView& Cc = A.lv[l + 1];
+        const int2 rg = A.range[body * L + l];
+        for (int row = rg.x + tid_c; row < rg.x + rg.y; row += nthr) {
+            const int4 id = __ldg(Cc.pid + row);
+            const float4 w = __ldg(Cc.pw + row);
+            const float4 e0 = ecur[l + 1][id.x], e1 = ecur[l + 1][id.y], e2 = ecur[l + 1][id.z], e3 = ecur[l + 1][id.w];
+            float4 v = ecur[l][row];
+            v.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+            v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+            v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+            ecur[l][row] = v;
+        }
+        cluster.sync();
+        for (int k = 0; k < A.post; ++k) {
+            for (int base = rg.x + warp_c * Sc; base < rg.x + rg.y; base += nwarp * Sc) {
+                const int row = base + (lane % Sc);
+                const bool valid = row < rg.x + rg.y;
+                const float4 off = rg_offdiag<kLanesC, false>(row, valid, lane, C.slice_ptr, C.col, C.val, ecur[l]);
+                if (valid && lane < Sc) {
+                    const float4 x = ecur[l][row], ri = C.r[row];
+                    const float D = __ldg(C.dfull + row), w = __ldg(C.dinv + row);
+                    eoth[l][row] = make_float4(fmaf(w, ri.x - fmaf(D, x.x, off.x), x.x), fmaf(w, ri.y - fmaf(D, x.y, off.y), x.y),
+                                               fmaf(w, ri.z - fmaf(D, x.z, off.z), x.z), 0.f);
+                }
+            }
+            float4* t = ecur[l];
+            ecur[l] = eoth[l];
+            eoth[l] = t;
+            cluster.sync();
+        }
+    }
+    // level-0 prolongation d += P1 e1
+    if (A.fuse_l0) {
+        const LevelView& C1 = A.lv[1];
+        const int2 rg = A.range[body * L + 0];
+        for (int row = rg.x + tid_c; row < rg.x + rg.y; row += nthr) {
+            const int4 id = __ldg(C1.pid + row);
+            const float4 w = __ldg(C1.pw + row);
+            const float4 e0 = ecur[1][id.x], e1 = ecur[1][id.y], e2 = ecur[1][id.z], e3 = ecur[1][id.w];
+            float4 v = A.d[row];
+            v.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+            v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+            v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+            A.d[row] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest level per body (one CTA): A = A0 + diag(c); Cholesky A = L L^T in
+// shared memory, X = L^-1 in place (row by row), then A^-1 = X^T X written to
+// global memory.  Skipped when c is unchanged since the last factorisation.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_coarsest_factor_inv(const int2* __restrict__ range, int L,
+                                                              const int32_t* __restrict__ dense_off,
+                                                              const float* __restrict__ A0, const float* __restrict__ c,
+                                                              float* __restrict__ c_prev, float* __restrict__ Ainv,
+                                                              int32_t* __restrict__ valid) {
+    extern __shared__ float sm[];
+    const int2 rg = range[blockIdx.x * L + (L - 1)];
+    const int n = rg.y, off = rg.x;
+    const float* A = A0 + dense_off[blockIdx.x];
+    float* Ai = Ainv + dense_off[blockIdx.x];
+    __shared__ int changed;
+    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (c[off + i] != c_prev[off + i]) changed = 1;
+    __syncthreads();
+    if (!changed) return;
+    float* M = sm;            // n*n
+    float* tmp = sm + n * n;  // n
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        float a = A[q];
+        if (i == j) a += c[off + i];
+        M[q] = a;
+    }
+    __syncthreads();
+    // Cholesky, right-looking; the diagonal holds L_jj afterwards
+    for (int j = 0; j < n; ++j) {
+        const float d = sqrtf(M[j * n + j]);
+        const float id = 1.f / d;
+        __syncthreads();
+        if (threadIdx.x == 0) M[j * n + j] = d;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i * n + j] *= id;
+        __syncthreads();
+        const int m = n - j - 1;
+        const int tot = m * (m + 1) / 2;
+        for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+            int a = (int)((sqrtf(8.f * (float)q + 1.f) - 1.f) * 0.5f);
+            while ((a + 1) * (a + 2) / 2 <= q) ++a;
+            while (a * (a + 1) / 2 > q) --a;
+            const int bcol = q - a * (a + 1) / 2;
+            const int i = j + 1 + a, k = j + 1 + bcol;
+            M[i * n + k] -= M[i * n + j] * M[k * n + j];
+        }
+        __syncthreads();
+    }
+    // X = L^-1 in place, row by row: X_ii = 1/L_ii, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = 0; i < n; ++i) {
+        const float xii = 1.f / M[i * n + i];
+        for (int j = wid; j < i; j += nw) {
+            float s = 0.f;
+            for (int k = j + lane; k < i; k += 32) s = fmaf(M[i * n + k], M[k * n + j], s);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) tmp[j] = -xii * s;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < i; j += blockDim.x) M[i * n + j] = tmp[j];
+        if (threadIdx.x == 0) M[i * n + i] = xii;
+        __syncthreads();
+    }
+    // A^-1 = X^T X: (i, j) = sum_{k >= max(i,j)} X_ki X_kj
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        const int k0 = i > j ? i : j;
+        float s = 0.f;
+        for (int k = k0; k < n; ++k) s = fmaf(M[k * n + i], M[k * n + j], s);
+        Ai[q] = s;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) c_prev[off + i] = c[off + i];
+    if (threadIdx.x == 0) valid[blockIdx.x] = 1;
+}
+
+}  // namespace mgsb

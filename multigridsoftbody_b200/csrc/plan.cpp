@@ -45,22 +45,22 @@ mgsb_status make_body(const mgsb_mesh& m, const mgsb_params& p, bool multigrid, 
 }
 
 void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col, const std::vector<double>& val, int n,
-               std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval) {
-    const int ns = (n + 31) / 32;
+               int S, std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval) {
+    const int ns = (n + S - 1) / S;
     sptr.assign(ns + 1, 0);
     for (int s = 0; s < ns; ++s) {
         int w = 0;
-        for (int r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, ptr[r + 1] - ptr[r]);
-        sptr[s + 1] = sptr[s] + 32 * w;
+        for (int r = s * S; r < std::min(n, s * S + S); ++r) w = std::max(w, ptr[r + 1] - ptr[r]);
+        sptr[s + 1] = sptr[s] + S * w;
     }
     ecol.assign(sptr[ns], 0);
     eval.assign(sptr[ns], 0.f);
     for (int s = 0; s < ns; ++s) {
-        const int w = (sptr[s + 1] - sptr[s]) / 32;
-        for (int lane = 0; lane < 32; ++lane) {
-            const int r = s * 32 + lane;
+        const int w = (sptr[s + 1] - sptr[s]) / S;
+        for (int lane = 0; lane < S; ++lane) {
+            const int r = s * S + lane;
             for (int k = 0; k < w; ++k) {
-                const int e = sptr[s] + k * 32 + lane;
+                const int e = sptr[s] + k * S + lane;
                 if (r < n && ptr[r] + k < ptr[r + 1]) {
                     ecol[e] = col[ptr[r] + k];
                     eval[e] = (float)val[ptr[r] + k];
@@ -201,7 +201,8 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
                 ptr[B.v_off + i + 1] = (int32_t)col.size();
             }
         }
-        build_ell(ptr, col, val, N0, l0.slice_ptr, l0.ell_col, l0.ell_val);
+        l0.S = kSliceL0;
+        build_ell(ptr, col, val, N0, l0.S, l0.slice_ptr, l0.ell_col, l0.ell_val);
         l0.nnz = (int)col.size();
         l0.diag0 = P.diag;
         P.levels.push_back(std::move(l0));
@@ -273,9 +274,20 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
                     }
             }
         }
-        build_ell(ptr, col, val, n, ld.slice_ptr, ld.ell_col, ld.ell_val);
+        ld.S = kSliceCoarse;
+        build_ell(ptr, col, val, n, ld.S, ld.slice_ptr, ld.ell_col, ld.ell_val);
         ld.nnz = (int)col.size();
         P.levels.push_back(std::move(ld));
+    }
+    // ---- per-body row ranges on every level
+    P.range.assign(bodies.size() * L, int2{0, 0});
+    for (size_t bi = 0; bi < bodies.size(); ++bi) P.range[bi * L] = int2{bodies[bi].v_off, bodies[bi].V};
+    for (int l = 1; l < L; ++l) {
+        int o = 0;
+        for (size_t bi = 0; bi < bodies.size(); ++bi) {
+            P.range[bi * L + l] = int2{o, bodies[bi].levels[l - 1].n};
+            o += bodies[bi].levels[l - 1].n;
+        }
     }
     // ---- coarsest dense blocks
     P.cl_off = loff;

@@ -30,6 +30,7 @@ struct PlanBody {
 
 struct PlanLevel {
     int n = 0, nnz = 0;
+    int S = 32;                      // slice height of the sliced ELL
     std::vector<int32_t> slice_ptr, ell_col;
     std::vector<float> ell_val, diag0;
     // prolongation rows of the next finer level's vertices (coarse side = this level)
@@ -51,15 +52,20 @@ struct Plan {
     std::vector<PlanLevel> levels;            // [0] = finest (matrix only)
     std::vector<float> dense;                 // coarsest dense blocks (row-major per body)
     std::vector<int32_t> cl_off, cl_n, dense_off;
+    std::vector<int2> range;                  // [body * L + level]: (first row, rows)
     int max_coarsest = 0;
     std::vector<int32_t> surf;                // global surface vertex ids
     // body-0 precompute for export
     std::vector<float> h_inv, h_ac, h_vol, h_mass, h_diag;
 };
 
-// Sliced ELL (32-row slices, column-major inside a slice) from CSR rows.
+// Sliced ELL (slices of S rows, column-major inside a slice: entry k of row r
+// at sptr[r / S] + k * S + r % S) from CSR rows.
 void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col, const std::vector<double>& val, int n,
-               std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval);
+               int S, std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval);
+
+constexpr int kSliceL0 = 8;       // 4 lanes per row at level 0
+constexpr int kSliceCoarse = 4;   // 8 lanes per row on coarse levels
 
 // Copies a mesh into a body (rest data, default material, no fixed vertex,
 // surface vertices for the multigrid kind).  Returns a status.

@@ -12,6 +12,7 @@
 
 #include "../../include/mgsb.h"
 #include "kernels.cuh"
+#include "kernels_mg.cuh"
 #include "mesh.hpp"
 #include "plan.hpp"
 #include "setup.hpp"
@@ -33,6 +34,7 @@ using BodyHost = PlanBody;
 
 struct LevelDev {
     int n = 0;
+    int S = 32;
     int nnz = 0;
     // sliced ELL (off-diagonal)
     int32_t* slice_ptr = nullptr;
@@ -53,7 +55,6 @@ struct LevelDev {
     int32_t* rptr = nullptr;
     int32_t* rcol = nullptr;
     float* rw = nullptr;
-    Ell ell() const { return Ell{slice_ptr, ell_col, ell_val}; }
 };
 
 }  // namespace
@@ -105,12 +106,16 @@ struct mgsb_solver {
     int32_t* slot_ptr = nullptr;
     float4* slots = nullptr;
     // multigrid
-    float4 *b = nullptr, *b0 = nullptr, *target = nullptr;
+    float4 *b = nullptr, *b0 = nullptr, *target = nullptr, *d = nullptr, *d2 = nullptr;
     float* c0 = nullptr;
     int32_t* surf = nullptr;
     int nsurf = 0;
     std::vector<LevelDev> lev;   // lev[0] = finest
     float *A0dense = nullptr, *Lfac = nullptr, *Ldinv = nullptr, *c_prev = nullptr;
+    int2* range = nullptr;
+    int32_t* dense_off_d = nullptr;
+    int cluster = 1;
+    int fuse_l0 = 1;
     int32_t* fac_valid = nullptr;
     size_t factor_smem = 0;
     int max_coarsest = 0;
@@ -238,6 +243,7 @@ mgsb_status rebuild(mgsb_solver* h) {
             const PlanLevel& pl = P.levels[l];
             LevelDev ld;
             ld.n = pl.n;
+            ld.S = pl.S;
             ld.nnz = pl.nnz;
             TRY(dupload(h, pool, &ld.slice_ptr, pl.slice_ptr));
             TRY(dupload(h, pool, &ld.ell_col, pl.ell_col));
@@ -268,6 +274,10 @@ mgsb_status rebuild(mgsb_solver* h) {
         }
         TRY(dalloc(h, pool, &h->b, N0));
         TRY(dalloc(h, pool, &h->b0, N0));
+        TRY(dalloc(h, pool, &h->d, N0));
+        TRY(dalloc(h, pool, &h->d2, N0));
+        CUDA_TRY(h, cudaMemset(h->d, 0, N0 * sizeof(float4)));
+        CUDA_TRY(h, cudaMemset(h->d2, 0, N0 * sizeof(float4)));
         TRY(dalloc(h, pool, &h->target, N0));
         CUDA_TRY(h, cudaMemset(h->target, 0, N0 * sizeof(float4)));
         for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
@@ -284,10 +294,24 @@ mgsb_status rebuild(mgsb_solver* h) {
             return set_err(h, MGSB_NOT_SUPPORTED,
                            "coarsest level has %d vertices; its dense factor needs %zu B of shared memory (max %d): add a level",
                            P.max_coarsest, h->factor_smem, dev_smem);
-        CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->factor_smem));
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_factor_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)h->factor_smem));
         TRY(dupload(h, pool, &h->A0dense, P.dense));
-        TRY(dalloc(h, pool, &h->Lfac, P.dense.size()));
-        TRY(dalloc(h, pool, &h->Ldinv, (size_t)h->lev[L - 1].n));
+        TRY(dalloc(h, pool, &h->Lfac, P.dense.size()));   // explicit inverse of the coarsest matrix
+        TRY(dupload(h, pool, &h->range, P.range));
+        TRY(dupload(h, pool, &h->dense_off_d, P.dense_off));
+        // cluster size of the coarse V-cycle kernel: sized by the rows one body
+        // brings to it (level 0 when fused, else level 1)
+        int maxv0 = 0, maxv1 = 0;
+        for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
+            maxv0 = std::max(maxv0, P.range[bi * L].y);
+            maxv1 = std::max(maxv1, P.range[bi * L + 1].y);
+        }
+        h->fuse_l0 = maxv0 <= 40000 ? 1 : 0;
+        const int work = h->fuse_l0 ? maxv0 : maxv1;
+        h->cluster = std::min(16, std::max(1, (work + 2559) / 2560));
+        if (h->cluster > 8)
+            CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->fac_valid, h->bodies.size()));
         CUDA_TRY(h, cudaMemset(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t)));
@@ -343,6 +367,29 @@ void enqueue_ref_frame(mgsb_solver* h) {
     }
 }
 
+mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(h->bodies.size() * h->cluster));
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)h->cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (h->profiling) prof_mark(h, "k_coarse_vcycle");
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_coarse_vcycle, args);
+    if (h->profiling) prof_mark(h, nullptr);
+    ++h->launches;
+    if (e != cudaSuccess) return set_err(h, MGSB_CUDA_ERROR, "coarse V-cycle launch failed: %s", cudaGetErrorString(e));
+    return MGSB_OK;
+}
+
+inline int grid_rows(int n, int S) { return ((n + S - 1) / S * 32 + kBlock - 1) / kBlock; }
+
 void enqueue_mg_frame(mgsb_solver* h) {
     const mgsb_params& p = h->p;
     const int n0 = h->N0, T = h->T, L = p.levels;
@@ -353,66 +400,74 @@ void enqueue_mg_frame(mgsb_solver* h) {
     if (h->nsurf > 0)
         LAUNCH(h, k_contact_all, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bodies_dev, h->s,
                h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target);
-    LAUNCH(h, k_l0_frame, grid_for(n0), kBlock, 0, n0, h->s, h->mass, h->c0, h->target, h->vdiag, h->fixf, om, h->b0,
-           lv[0].dfull, lv[0].dinv);
+    float4* xa = h->d;    // displacement d = x - s (ping)
+    float4* xb = h->d2;   // pong
+    LAUNCH(h, k_l0_frame, grid_for(n0), kBlock, 0, n0, h->s, h->c0, h->target, h->vdiag, h->fixf, om, h->b0,
+           lv[0].dfull, lv[0].dinv, xa);
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
                lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
-    LAUNCH(h, k_coarsest_factor, nb, 512, h->factor_smem, h->bodies_dev, h->A0dense, lv[L - 1].c, h->c_prev, h->Lfac,
-           h->Ldinv, h->fac_valid);
-    float4* xa = h->x;
-    float4* xb = h->xb;
+    LAUNCH(h, k_coarsest_factor_inv, nb, 1024, h->factor_smem, h->range, L, h->dense_off_d, h->A0dense, lv[L - 1].c,
+           h->c_prev, h->Lfac, h->fac_valid);
+    CoarseArgs ca = {};
+    ca.L = L;
+    ca.pre = p.pre_sweeps;
+    ca.post = p.post_sweeps;
+    ca.fuse_l0 = h->fuse_l0;
+    ca.range = h->range;
+    ca.dense_off = h->dense_off_d;
+    ca.Ainv = h->Lfac;
+    ca.b = h->b;
+    for (int l = 0; l < L; ++l) {
+        LevelView& v = ca.lv[l];
+        v.n = lv[l].n;
+        v.slice_ptr = lv[l].slice_ptr;
+        v.col = lv[l].ell_col;
+        v.val = lv[l].ell_val;
+        v.dfull = lv[l].dfull;
+        v.dinv = lv[l].dinv;
+        v.r = lv[l].r;
+        v.e = lv[l].e;
+        v.e2 = lv[l].e2;
+        v.res = lv[l].res;
+        v.pid = lv[l].pid;
+        v.pw = lv[l].pw;
+        v.rptr = lv[l].rptr;
+        v.rcol = lv[l].rcol;
+        v.rw = lv[l].rw;
+    }
+    const int g0 = grid_rows(n0, lv[0].S);
     for (int it = 0; it < p.iterations; ++it) {
-        LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, xa, h->slot_of, h->slots);
+        LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
         for (int pass = 0; pass < p.refinement_passes; ++pass) {
-            // ---- level 0 pre-smoothing (the first sweep of the first pass assembles the RHS)
             bool gathered = pass > 0;
             for (int k = 0; k < p.pre_sweeps; ++k) {
-                LAUNCH(h, k_l0_sweep, grid_for(n0), kBlock, 0, n0, lv[0].ell(), lv[0].dfull, lv[0].dinv, xa, xb, h->b,
-                       h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1);
+                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
+                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1);
                 gathered = true;
                 std::swap(xa, xb);
             }
             if (!gathered) LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
-            LAUNCH(h, k_residual, grid_for(n0), kBlock, 0, n0, lv[0].ell(), lv[0].dfull, xa, h->b, lv[0].res);
-            // ---- descend
-            std::vector<float4*> ecur(L, nullptr), eoth(L, nullptr);
-            for (int l = 1; l < L - 1; ++l) {
-                LevelDev& C = lv[l];
-                LAUNCH(h, k_restrict, grid_for(C.n), kBlock, 0, C.n, C.rptr, C.rcol, C.rw, lv[l - 1].res, C.dinv, C.r, C.e,
-                       p.pre_sweeps > 0 ? 1 : 0);
-                ecur[l] = C.e;
-                eoth[l] = C.e2;
-                for (int k = 1; k < p.pre_sweeps; ++k) {
-                    LAUNCH(h, k_coarse_sweep, grid_for(C.n), kBlock, 0, C.n, C.ell(), C.dfull, C.dinv, C.r, ecur[l], eoth[l]);
-                    std::swap(ecur[l], eoth[l]);
-                }
-                LAUNCH(h, k_residual, grid_for(C.n), kBlock, 0, C.n, C.ell(), C.dfull, ecur[l], C.r, C.res);
+            if (!h->fuse_l0)
+                LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
+                       lv[0].dfull, xa, h->b, lv[0].res);
+            ca.d = xa;
+            launch_coarse(h, ca);
+            if (!h->fuse_l0) {
+                // the coarse kernel leaves the level-1 correction in the buffer its last sweep
+                // wrote: it starts in e and swaps once per sweep after the restriction
+                const int swaps = (p.pre_sweeps > 0 ? p.pre_sweeps - 1 : 0) + p.post_sweeps;
+                const float4* e1 = (swaps % 2 == 0) ? lv[1].e : lv[1].e2;
+                LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, e1, xa);
             }
-            LAUNCH(h, k_coarsest_solve, nb, 256, (size_t)h->max_coarsest * sizeof(float4), h->bodies_dev, lv[L - 1].rptr,
-                   lv[L - 1].rcol, lv[L - 1].rw, lv[L - 2].res, h->Lfac, h->Ldinv, lv[L - 1].e);
-            ecur[L - 1] = lv[L - 1].e;
-            // ---- ascend
-            for (int l = L - 2; l >= 1; --l) {
-                LevelDev& C = lv[l];
-                LAUNCH(h, k_prolong, grid_for(C.n), kBlock, 0, C.n, lv[l + 1].pid, lv[l + 1].pw, ecur[l + 1], ecur[l]);
-                for (int k = 0; k < p.post_sweeps; ++k) {
-                    LAUNCH(h, k_coarse_sweep, grid_for(C.n), kBlock, 0, C.n, C.ell(), C.dfull, C.dinv, C.r, ecur[l], eoth[l]);
-                    std::swap(ecur[l], eoth[l]);
-                }
-            }
-            LAUNCH(h, k_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, ecur[1], xa);
             for (int k = 0; k < p.post_sweeps; ++k) {
-                LAUNCH(h, k_l0_sweep, grid_for(n0), kBlock, 0, n0, lv[0].ell(), lv[0].dfull, lv[0].dinv, xa, xb, h->b,
-                       h->b0, h->slot_ptr, h->slots, 0);
+                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
+                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0);
                 std::swap(xa, xb);
             }
         }
     }
-    if (xa != h->x) {
-        cudaMemcpyAsync(h->x, xa, n0 * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
-    }
-    LAUNCH(h, k_velocity, grid_for(n0), kBlock, 0, n0, h->x, h->last, h->v, p.dt, h->nonfinite);
+    LAUNCH(h, k_mg_finish, grid_for(n0), kBlock, 0, n0, h->s, xa, h->x, h->v, 1.0f / p.dt, h->nonfinite);
 }
 
 void enqueue_frame(mgsb_solver* h) {
@@ -953,8 +1008,8 @@ mgsb_status mgsb_inspect_level(const mgsb_mesh* mesh, const mgsb_params* params,
         int z = 0;
         ptr[0] = 0;
         for (int r = 0; r < pl.n; ++r) {
-            const int s0 = r >> 5, lane = r & 31;
-            for (int q = pl.slice_ptr[s0] + lane; q < pl.slice_ptr[s0 + 1]; q += 32)
+            const int s0 = r / pl.S, lane = r % pl.S;
+            for (int q = pl.slice_ptr[s0] + lane; q < pl.slice_ptr[s0 + 1]; q += pl.S)
                 if (pl.ell_col[q] != r) {
                     col[z] = pl.ell_col[q];
                     val[z] = pl.ell_val[q];

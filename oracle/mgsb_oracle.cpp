@@ -742,53 +742,73 @@ void mg_frame(Oracle& o) {
         }
         coarsest_factor(o);
     }
-    Vec b0(V);
+    // The global system A x = M/h^2 s + C p + sum_t w G^T R_t is solved for the
+    // displacement from the prediction, d = x - s (same solution): A d = b_d with
+    // b_d = C (p - s) + sum_t w G_t^T (R_t - F_t(s)), every term built from small
+    // position differences.
+    Vec d(V, V3{0, 0, 0});
+    Vec bbase(V);
     for (int i = 0; i < V; ++i)
-        for (int c = 0; c < 3; ++c) b0[i][c] = o.mass[i] * ih2 * o.s[i][c] + o.c0[i] * o.target[i][c];
-    std::vector<double> rot(9 * (size_t)o.T);
-    Vec b(V), Ax, r(V), e;
+        for (int c = 0; c < 3; ++c) bbase[i][c] = o.c0[i] * (o.target[i][c] - o.s[i][c]);
+    (void)ih2;
+    std::vector<double> rot(9 * (size_t)o.T), Fs(9 * (size_t)o.T);
+    auto defgrad = [&](int t, const Vec& p0, const Vec* p1, double* F) {
+        const int* id = &o.tets[4 * t];
+        const double* iv = &o.inv[9 * (size_t)t];
+        double D[9];
+        for (int rr = 0; rr < 3; ++rr)
+            for (int c = 0; c < 3; ++c) {
+                D[rr * 3 + c] = p0[id[c + 1]][rr] - p0[id[0]][rr];
+                if (p1) D[rr * 3 + c] += (*p1)[id[c + 1]][rr] - (*p1)[id[0]][rr];
+            }
+        for (int rr = 0; rr < 3; ++rr)
+            for (int c = 0; c < 3; ++c) F[rr * 3 + c] = D[rr * 3] * iv[c] + D[rr * 3 + 1] * iv[3 + c] + D[rr * 3 + 2] * iv[6 + c];
+    };
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < o.T; ++t) defgrad(t, o.s, nullptr, &Fs[9 * (size_t)t]);
+    Vec b(V), Ad, r(V), e;
     for (int it = 0; it < o.p.iterations; ++it) {
-        // local step: R_t = closest rotation of F_t
+        // local step: R_t = closest rotation of F_t(s + d)
 #pragma omp parallel for schedule(static)
         for (int t = 0; t < o.T; ++t) {
-            const int* id = &o.tets[4 * t];
-            const double* iv = &o.inv[9 * (size_t)t];
-            double D[9], F[9];
-            for (int rr = 0; rr < 3; ++rr)
-                for (int c = 0; c < 3; ++c) D[rr * 3 + c] = o.x[id[c + 1]][rr] - o.x[id[0]][rr];
-            for (int rr = 0; rr < 3; ++rr)
-                for (int c = 0; c < 3; ++c)
-                    F[rr * 3 + c] = D[rr * 3] * iv[c] + D[rr * 3 + 1] * iv[3 + c] + D[rr * 3 + 2] * iv[6 + c];
+            double F[9];
+            defgrad(t, o.s, &d, F);
             svd_rotation(F, &rot[9 * (size_t)t]);
         }
-        b = b0;
+        b = bbase;
         for (int t = 0; t < o.T; ++t) {
             const int* id = &o.tets[4 * t];
             const double* A = &o.ac[12 * (size_t)t];
             const double* R = &rot[9 * (size_t)t];
+            const double* F0 = &Fs[9 * (size_t)t];
             for (int j = 0; j < 4; ++j)
                 for (int i = 0; i < 3; ++i)
-                    b[id[j]][i] += o.w[t] * (R[i * 3] * A[j] + R[i * 3 + 1] * A[4 + j] + R[i * 3 + 2] * A[8 + j]);
+                    b[id[j]][i] += o.w[t] * ((R[i * 3] - F0[i * 3]) * A[j] + (R[i * 3 + 1] - F0[i * 3 + 1]) * A[4 + j] +
+                                             (R[i * 3 + 2] - F0[i * 3 + 2]) * A[8 + j]);
         }
         for (int pass = 0; pass < o.p.refinement_passes; ++pass) {
-            spmv_level(o, 0, o.x, Ax);
+            spmv_level(o, 0, d, Ad);
             for (int i = 0; i < V; ++i)
-                for (int c = 0; c < 3; ++c) r[i][c] = b[i][c] - Ax[i][c];
+                for (int c = 0; c < 3; ++c) r[i][c] = b[i][c] - Ad[i][c];
             vcycle(o, 0, r, e);
             for (int i = 0; i < V; ++i)
-                for (int c = 0; c < 3; ++c) o.x[i][c] += e[i][c];
+                for (int c = 0; c < 3; ++c) d[i][c] += e[i][c];
         }
         if (it == o.p.iterations - 1) {
-            spmv_level(o, 0, o.x, Ax);
+            spmv_level(o, 0, d, Ad);
             double rr2 = 0;
             for (int i = 0; i < V; ++i)
                 if (!o.fixed[i])
-                    for (int c = 0; c < 3; ++c) rr2 += (b[i][c] - Ax[i][c]) * (b[i][c] - Ax[i][c]);
+                    for (int c = 0; c < 3; ++c) rr2 += (b[i][c] - Ad[i][c]) * (b[i][c] - Ad[i][c]);
             o.last_residual = std::sqrt(rr2);
         }
     }
+    // x = s + d and v = (x - last)/dt = v_predicted + d/dt
     for (int i = 0; i < V; ++i)
-        for (int c = 0; c < 3; ++c) o.v[i][c] = (o.x[i][c] - o.last[i][c]) / dt;
+        for (int c = 0; c < 3; ++c) {
+            o.x[i][c] = o.s[i][c] + d[i][c];
+            o.v[i][c] += d[i][c] / dt;
+        }
 }
 
 }  // namespace
