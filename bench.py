@@ -117,21 +117,46 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # Algorithmic bytes per launch of the main kernels (FP32, each array once)
 # ---------------------------------------------------------------------------
-def algorithmic_bytes(kernel, solver, meshes):
+def coarse_vcycle_bytes(solver, params):
+    """Algorithmic bytes of one k_coarse_vcycle launch (every array of every
+    phase counted once; FP32 values, int32 indices, float4 vectors)."""
+    L, pre, post = params.levels, params.pre_sweeps, params.post_sweeps
+    lv = [solver.level_info(l) for l in range(L)]
+    n = [x["n"] for x in lv]
+    nnz = [x["nnz"] for x in lv]
+    nch = [x["nchild"] for x in lv]
+    fuse = lv[0]["fuse_l0"]
+    sweep = lambda l: 8 * nnz[l] + n[l] * (16 + 16 + 8 + 16)        # ELL + e_in, r, dfull/dinv, e_out
+    resid = lambda l: 8 * nnz[l] + n[l] * (16 + 16 + 4 + 16)
+    restrict = lambda l: 8 * nch[l] + 16 * n[l - 1] + n[l] * (4 + 16 + 4 + 16)
+    prolong = lambda l: n[l] * (16 + 16 + 16 + 16) + 16 * n[l + 1]
+    b = 0
+    if fuse:
+        b += 8 * nnz[0] + n[0] * (16 + 16 + 4 + 16)                     # level-0 residual
+        b += n[0] * (16 + 16 + 16 + 16) + 16 * n[1]                     # d += P e1
+    for l in range(1, L - 1):
+        b += restrict(l) + max(pre - 1, 0) * sweep(l) + resid(l) + prolong(l) + post * sweep(l)
+    c = L - 1
+    b += 8 * nch[c] + 16 * n[c - 1] + n[c] * 20                         # coarsest restriction
+    b += 4 * n[c] * n[c] + 32 * n[c]                                     # dense inverse x r
+    return float(b)
+
+
+def algorithmic_bytes(kernel, solver, meshes, params):
     V = sum(m.num_verts for m in meshes)
     T = sum(m.num_tets for m in meshes)
     n0, nnz0 = solver.level_size(0)
     if kernel == "k_mg_local":
-        # tet ids 16 + g vectors 40 + slot ids 16 + 4 slot writes 64; positions 16 per vertex
-        return 136 * T + 16 * V
-    if kernel == "k_l0_sweep":
-        # average of the gathering sweep and the plain sweeps of one V-cycle:
-        # plain: x 16 + b 16 + dfull 4 + dinv 4 + x_out 16 + ELL 8 per nnz
+        # tet ids 16 + g vectors 40 + slot ids 16 + 4 slot writes 64; s and d 16 each per vertex
+        return 136 * T + 32 * V
+    if kernel == "k_l0_sweep_rg":
+        # average over one V-cycle's level-0 sweeps (the first also assembles the RHS)
         plain = 56 * n0 + 8 * nnz0
         gather = plain + 16 * n0 + 4 * n0 + 16 * 4 * T   # b0, slot_ptr, slots
-        return (gather + 3 * plain) / 4.0
-    if kernel == "k_residual":
-        return 52 * n0 + 8 * nnz0
+        k = params.pre_sweeps + params.post_sweeps
+        return (gather + (k - 1) * plain) / k
+    if kernel == "k_coarse_vcycle":
+        return coarse_vcycle_bytes(solver, params)
     return None
 
 
@@ -232,6 +257,7 @@ def run_ours(args):
             torch.cuda.synchronize()
 
     frame = 0
+    tuned = solver.autotune(frames=5) if not args.no_tune else None
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             tool(solver, frame)
@@ -284,7 +310,7 @@ def run_ours(args):
         dom = max(prof.items(), key=lambda kv: kv[1][0])
         kname, (ktot, kcnt) = dom
         kavg_ms = ktot / max(kcnt, 1)
-        alg = algorithmic_bytes(kname, solver, meshes)
+        alg = algorithmic_bytes(kname, solver, meshes, params[0])
         peak, peak_kind = measured_peaks()
         roof = None
         if alg is not None:
@@ -304,7 +330,8 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": desc, "variant": "plain FP32 multigrid", "parallelism": f"replicas x{world}",
-                           "l2": "flushed (256 MB write) before every timed frame, outside the timed span"},
+                           "l2": "flushed (256 MB write) before every timed frame, outside the timed span",
+                           "autotuned_coarse_kernel": tuned},
                 "clocks": clk.summary(),
                 "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches * args.steps,
@@ -328,6 +355,7 @@ def main():
     ap.add_argument("--workload", default="beam")
     ap.add_argument("--cpu-frames", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

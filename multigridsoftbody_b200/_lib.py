@@ -116,6 +116,9 @@ SIGNATURES = [
     ("mgsb_profile_frame", C.c_int, [_P, C.c_int32, C.c_char_p, _FP, _IP, _IP]),
     ("mgsb_get_precompute", C.c_int, [_P, _FP, _FP, _FP, _FP, _FP]),
     ("mgsb_level_size", C.c_int, [_P, C.c_int32, _IP, _IP]),
+    ("mgsb_level_info", C.c_int, [_P, C.c_int32, _IP]),
+    ("mgsb_autotune", C.c_int, [_P, C.c_int32, _IP]),
+    ("mgsb_set_kernel_shape", C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     ("mgsb_inspect_level", C.c_int, [C.POINTER(Mesh), C.POINTER(Params), _U8P, C.c_int32, _IP, _IP, _IP, _FP, _FP, _IP,
                                      _IP, _FP]),
     ("mgsb_last_error_string", C.c_char_p, [_P]),

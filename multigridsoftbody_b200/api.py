@@ -359,6 +359,21 @@ class Solver:
                self.h)
         return dict(inv=inv.reshape(T, 9), ac=ac.reshape(T, 12), volume=vol, mass=mass, diag=diag)
 
+    def level_info(self, level: int) -> dict:
+        info = np.zeros(8, np.int32)
+        _check(self._lib.mgsb_level_info(self.h, level, _iptr(info)), self.h)
+        keys = ("n", "nnz", "nchild", "slice", "ell_entries", "cluster", "block", "fuse_l0")
+        return {k: int(v) for k, v in zip(keys, info)}
+
+    def autotune(self, frames: int = 5) -> dict:
+        """Pick the coarse-kernel shape by timing candidates; the state is restored."""
+        ch = np.zeros(3, np.int32)
+        _check(self._lib.mgsb_autotune(self.h, frames, _iptr(ch)), self.h)
+        return {"cluster": int(ch[0]), "block": int(ch[1]), "fuse_l0": int(ch[2])}
+
+    def set_kernel_shape(self, cluster: int = 0, block: int = 0, fuse_level0: int = -1) -> None:
+        _check(self._lib.mgsb_set_kernel_shape(self.h, cluster, block, fuse_level0), self.h)
+
     def level_size(self, level: int) -> tuple[int, int]:
         n = C.c_int32()
         z = C.c_int32()

@@ -210,7 +210,7 @@ __global__ void k_l0_prolong(int n, const int4* __restrict__ pid, const float4* 
 // Coarse part of the V-cycle, one thread-block cluster per body; phases are
 // separated by cluster barriers (release/acquire on global memory).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_coarse_vcycle(const CoarseArgs A) {
+__global__ void __launch_bounds__(1024) k_coarse_vcycle(const CoarseArgs A) {
     cg::cluster_group cluster = cg::this_cluster();
     const int cs = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
@@ -373,6 +373,228 @@ __global__ void __launch_bounds__(512) k_coarse_vcycle(const CoarseArgs A) {
             v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
             A.d[row] = v;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse part of the V-cycle with every coarse-level vector resident in the
+// cluster's distributed shared memory.  CTA `rank` of the body's cluster owns
+// rows [rank*B_l, min((rank+1)*B_l, n_l)) of level l (body-local numbering)
+// and keeps r, e, e2, res of those rows in its shared memory; a row of
+// another CTA is read through the cluster shared-memory window.  Matrix and
+// transfer operators stay in global memory (read-only, L2-resident).
+// Inputs: level-0 residual (global).  Output: level-1 correction (global,
+// lv[1].e) for the level-0 prolongation kernel.
+// ---------------------------------------------------------------------------
+struct SmemLevel {
+    int off, n, B, base;   // first global row, rows, rows per CTA, float4 offset of [r|e|e2|res]
+};
+
+__device__ __forceinline__ float4* dsm_ptr(cg::cluster_group& cl, float4* sm, const SmemLevel& q, int vec, int li) {
+    const int rank = li / q.B;
+    const int loc = li - rank * q.B;
+    return cl.map_shared_rank(sm + q.base + vec * q.B + loc, rank);
+}
+
+template <int G>
+__device__ __forceinline__ float4 rg_offdiag_dsm(cg::cluster_group& cl, float4* sm, const SmemLevel& q, int vec, int row,
+                                                 bool valid, int lane, const int32_t* __restrict__ sp,
+                                                 const int32_t* __restrict__ col, const float* __restrict__ val) {
+    constexpr int S = 32 / G;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    if (valid) {
+        const int slice = row / S;
+        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
+#pragma unroll 4
+        for (int e = beg + (lane / S) * S + (row - slice * S); e < end; e += 32) {
+            const float a = __ldg(val + e);
+            const float4 xv = *dsm_ptr(cl, sm, q, vec, __ldg(col + e) - q.off);
+            ax = fmaf(a, xv.x, ax);
+            ay = fmaf(a, xv.y, ay);
+            az = fmaf(a, xv.z, az);
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return make_float4(ax, ay, az, 0.f);
+}
+
+// Dynamic shared memory (float4 units) the kernel needs for a cluster size.
+__host__ __device__ inline int coarse_smem_float4(const int* nl, int L, int cs, int ncoarsest) {
+    int tot = 0;
+    for (int l = 1; l < L; ++l) tot += 4 * ((nl[l] + cs - 1) / cs);
+    return tot + ncoarsest;
+}
+
+__global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) {
+    extern __shared__ float4 smv[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int cs = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int body = blockIdx.x / cs;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarp = blockDim.x >> 5;
+    const int L = A.L;
+    constexpr int Sc = 32 / kLanesC;
+    constexpr int R = 0, E = 1, E2 = 2, RES = 3;
+    SmemLevel q[kMaxLevels];
+    int base = 0;
+    for (int l = 1; l < L; ++l) {
+        const int2 rg = A.range[body * L + l];
+        q[l].off = rg.x;
+        q[l].n = rg.y;
+        q[l].B = (rg.y + cs - 1) / cs;
+        q[l].base = base;
+        base += 4 * q[l].B;
+    }
+    float4* rfull = smv + base;   // full coarsest right-hand side (every CTA)
+    int ec[kMaxLevels];           // which of E / E2 holds the current correction
+    auto first_row = [&](int l) { return rank * q[l].B; };
+    auto own_rows = [&](int l) { return max(0, min(q[l].B, q[l].n - rank * q[l].B)); };
+    auto loc = [&](int l, int vec, int i) -> float4& { return smv[q[l].base + vec * q[l].B + i]; };
+
+    // ---- descend
+    for (int l = 1; l < L; ++l) {
+        const LevelView& C = A.lv[l];
+        const int r0 = first_row(l), cnt = own_rows(l);
+        // restriction r = P^T res_{l-1} (level 0 residual from global memory)
+        for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
+            const int li = b0 + (lane % Sc);
+            const bool valid = li < cnt;
+            const int row = q[l].off + r0 + li;
+            const int beg = valid ? __ldg(C.rptr + row) : 0, end = valid ? __ldg(C.rptr + row + 1) : 0;
+            float ax = 0.f, ay = 0.f, az = 0.f;
+            if (valid) {
+#pragma unroll 4
+                for (int k = beg + lane / Sc; k < end; k += kLanesC) {
+                    const float w = __ldg(C.rw + k);
+                    const int ch = __ldg(C.rcol + k);
+                    const float4 t = (l == 1) ? __ldg(A.lv[0].res + ch) : *dsm_ptr(cluster, smv, q[l - 1], RES, ch - q[l - 1].off);
+                    ax = fmaf(w, t.x, ax);
+                    ay = fmaf(w, t.y, ay);
+                    az = fmaf(w, t.z, az);
+                }
+            }
+#pragma unroll
+            for (int o = Sc; o < 32; o <<= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                az += __shfl_xor_sync(0xffffffffu, az, o);
+            }
+            if (valid && lane < Sc) {
+                loc(l, R, li) = make_float4(ax, ay, az, 0.f);
+                const float di = (l < L - 1 && A.pre > 0) ? __ldg(C.dinv + row) : 0.f;
+                loc(l, E, li) = make_float4(di * ax, di * ay, di * az, 0.f);
+            }
+        }
+        ec[l] = E;
+        cluster.sync();
+        if (l == L - 1) break;
+        for (int k = 1; k < A.pre; ++k) {
+            const int src = ec[l], dst = (src == E) ? E2 : E;
+            for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
+                const int li = b0 + (lane % Sc);
+                const bool valid = li < cnt;
+                const int row = q[l].off + r0 + li;
+                const float4 off = rg_offdiag_dsm<kLanesC>(cluster, smv, q[l], src, row, valid, lane, C.slice_ptr, C.col, C.val);
+                if (valid && lane < Sc) {
+                    const float4 x = loc(l, src, li), ri = loc(l, R, li);
+                    const float D = __ldg(C.dfull + row), w = __ldg(C.dinv + row);
+                    loc(l, dst, li) = make_float4(fmaf(w, ri.x - fmaf(D, x.x, off.x), x.x), fmaf(w, ri.y - fmaf(D, x.y, off.y), x.y),
+                                                  fmaf(w, ri.z - fmaf(D, x.z, off.z), x.z), 0.f);
+                }
+            }
+            ec[l] = dst;
+            cluster.sync();
+        }
+        for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
+            const int li = b0 + (lane % Sc);
+            const bool valid = li < cnt;
+            const int row = q[l].off + r0 + li;
+            const float4 off = rg_offdiag_dsm<kLanesC>(cluster, smv, q[l], ec[l], row, valid, lane, C.slice_ptr, C.col, C.val);
+            if (valid && lane < Sc) {
+                const float4 x = loc(l, ec[l], li), ri = loc(l, R, li);
+                const float D = __ldg(C.dfull + row);
+                loc(l, RES, li) = make_float4(ri.x - fmaf(D, x.x, off.x), ri.y - fmaf(D, x.y, off.y), ri.z - fmaf(D, x.z, off.z), 0.f);
+            }
+        }
+        cluster.sync();
+    }
+    // ---- coarsest: every CTA gathers the whole right-hand side, then e = A^-1 r for its rows
+    {
+        const int l = L - 1;
+        const int n = q[l].n;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) rfull[i] = *dsm_ptr(cluster, smv, q[l], R, i);
+        __syncthreads();
+        const float* Ai = A.Ainv + __ldg(A.dense_off + body);
+        const int r0 = first_row(l), cnt = own_rows(l);
+        for (int li = warp; li < cnt; li += nwarp) {
+            const int i = r0 + li;
+            float ax = 0.f, ay = 0.f, az = 0.f;
+            for (int k = lane; k < n; k += 32) {
+                const float a = __ldg(Ai + (size_t)i * n + k);
+                const float4 r = rfull[k];
+                ax = fmaf(a, r.x, ax);
+                ay = fmaf(a, r.y, ay);
+                az = fmaf(a, r.z, az);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                az += __shfl_xor_sync(0xffffffffu, az, o);
+            }
+            if (lane == 0) loc(l, E, li) = make_float4(ax, ay, az, 0.f);
+        }
+        ec[l] = E;
+        cluster.sync();
+    }
+    // ---- ascend
+    for (int l = L - 2; l >= 1; --l) {
+        const LevelView& C = A.lv[l];
+        const LevelView& Cc = A.lv[l + 1];
+        const int r0 = first_row(l), cnt = own_rows(l);
+        for (int li = threadIdx.x; li < cnt; li += blockDim.x) {
+            const int row = q[l].off + r0 + li;
+            const int4 id = __ldg(Cc.pid + row);
+            const float4 w = __ldg(Cc.pw + row);
+            const float4 e0 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.x - q[l + 1].off);
+            const float4 e1 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.y - q[l + 1].off);
+            const float4 e2 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.z - q[l + 1].off);
+            const float4 e3 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.w - q[l + 1].off);
+            float4& v = loc(l, ec[l], li);
+            v.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+            v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+            v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+        }
+        cluster.sync();
+        for (int k = 0; k < A.post; ++k) {
+            const int src = ec[l], dst = (src == E) ? E2 : E;
+            for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
+                const int li = b0 + (lane % Sc);
+                const bool valid = li < cnt;
+                const int row = q[l].off + r0 + li;
+                const float4 off = rg_offdiag_dsm<kLanesC>(cluster, smv, q[l], src, row, valid, lane, C.slice_ptr, C.col, C.val);
+                if (valid && lane < Sc) {
+                    const float4 x = loc(l, src, li), ri = loc(l, R, li);
+                    const float D = __ldg(C.dfull + row), w = __ldg(C.dinv + row);
+                    loc(l, dst, li) = make_float4(fmaf(w, ri.x - fmaf(D, x.x, off.x), x.x), fmaf(w, ri.y - fmaf(D, x.y, off.y), x.y),
+                                                  fmaf(w, ri.z - fmaf(D, x.z, off.z), x.z), 0.f);
+                }
+            }
+            ec[l] = dst;
+            cluster.sync();
+        }
+    }
+    // ---- level-1 correction to global memory (own rows only: no remote access after the last barrier)
+    {
+        const int r0 = first_row(1), cnt = own_rows(1);
+        for (int li = threadIdx.x; li < cnt; li += blockDim.x) A.lv[1].e[q[1].off + r0 + li] = loc(1, ec[1], li);
     }
 }
 

@@ -36,6 +36,8 @@ struct LevelDev {
     int n = 0;
     int S = 32;
     int nnz = 0;
+    int nchild = 0;        // restriction entries (children of this level's vertices)
+    int ell_entries = 0;   // stored sliced-ELL entries incl. padding
     // sliced ELL (off-diagonal)
     int32_t* slice_ptr = nullptr;
     int32_t* ell_col = nullptr;
@@ -116,6 +118,12 @@ struct mgsb_solver {
     int32_t* dense_off_d = nullptr;
     int cluster = 1;
     int fuse_l0 = 1;
+    int coarse_block = 512;
+    // autotuner overrides (0 / -1 = pick by size)
+    int tune_cluster = 0, tune_fuse = -1;
+    int maxv0 = 0, maxv1 = 0;   // largest body on levels 0 and 1
+    std::vector<int2> range_host;
+    int max_smem_optin = 0;
     int32_t* fac_valid = nullptr;
     size_t factor_smem = 0;
     int max_coarsest = 0;
@@ -197,6 +205,35 @@ void free_pool(std::vector<DevMem>& pool) {
 
 bool is_mg(const mgsb_solver* h) { return h->p.solver == MGSB_SOLVER_MULTIGRID; }
 
+// Shape of the coarse V-cycle kernel: explicit tuning if set, else by size
+// (level-0 work fused for bodies up to 40k vertices; ~2.5k rows per CTA).
+size_t coarse_smem_bytes(const mgsb_solver* h, int cs);
+
+void apply_tuning(mgsb_solver* h) {
+    // Default: the distributed-shared-memory kernel with <= 256 level-1 rows per CTA.
+    h->fuse_l0 = h->tune_fuse >= 0 ? h->tune_fuse : 0;
+    if (h->tune_cluster > 0) {
+        h->cluster = h->tune_cluster;
+    } else if (h->fuse_l0) {
+        h->cluster = std::min(16, std::max(1, (h->maxv0 + 2559) / 2560));
+    } else {
+        h->cluster = std::min(16, std::max(1, (h->maxv1 + 255) / 256));
+        while (h->cluster < 16 && coarse_smem_bytes(h, h->cluster) > (size_t)h->max_smem_optin) ++h->cluster;
+    }
+}
+
+void invalidate_graph(mgsb_solver* h) {
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    if (h->graph) {
+        cudaGraphDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    h->graph_valid = false;
+}
+
 // ---------------------------------------------------------------------------
 // Derived data (rebuilt when fixed set / material / params change)
 // ---------------------------------------------------------------------------
@@ -245,6 +282,8 @@ mgsb_status rebuild(mgsb_solver* h) {
             ld.n = pl.n;
             ld.S = pl.S;
             ld.nnz = pl.nnz;
+            ld.nchild = pl.rptr.empty() ? 0 : pl.rptr.back();
+            ld.ell_entries = (int)pl.ell_col.size();
             TRY(dupload(h, pool, &ld.slice_ptr, pl.slice_ptr));
             TRY(dupload(h, pool, &ld.ell_col, pl.ell_col));
             TRY(dupload(h, pool, &ld.ell_val, pl.ell_val));
@@ -299,6 +338,12 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dupload(h, pool, &h->A0dense, P.dense));
         TRY(dalloc(h, pool, &h->Lfac, P.dense.size()));   // explicit inverse of the coarsest matrix
         TRY(dupload(h, pool, &h->range, P.range));
+        h->range_host = P.range;
+        if (L > kMaxLevels) return set_err(h, MGSB_NOT_SUPPORTED, "at most %d levels", kMaxLevels);
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle_dsm, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        CUDA_TRY(h, cudaDeviceGetAttribute(&h->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle_dsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         h->max_smem_optin));
         TRY(dupload(h, pool, &h->dense_off_d, P.dense_off));
         // cluster size of the coarse V-cycle kernel: sized by the rows one body
         // brings to it (level 0 when fused, else level 1)
@@ -307,11 +352,10 @@ mgsb_status rebuild(mgsb_solver* h) {
             maxv0 = std::max(maxv0, P.range[bi * L].y);
             maxv1 = std::max(maxv1, P.range[bi * L + 1].y);
         }
-        h->fuse_l0 = maxv0 <= 40000 ? 1 : 0;
-        const int work = h->fuse_l0 ? maxv0 : maxv1;
-        h->cluster = std::min(16, std::max(1, (work + 2559) / 2560));
-        if (h->cluster > 8)
-            CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        h->maxv0 = maxv0;
+        h->maxv1 = maxv1;
+        apply_tuning(h);
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->fac_valid, h->bodies.size()));
         CUDA_TRY(h, cudaMemset(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t)));
@@ -333,7 +377,8 @@ mgsb_status rebuild(mgsb_solver* h) {
 void prof_mark(mgsb_solver* h, const char* name) {
     cudaEvent_t e;
     cudaEventCreate(&e);
-    cudaEventRecord(e, h->stream);
+    // External: inside stream capture this becomes a real event-record node.
+    cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal);
     h->prof_ev.push_back(e);
     if (name) h->prof_names.push_back(name);
 }
@@ -367,11 +412,25 @@ void enqueue_ref_frame(mgsb_solver* h) {
     }
 }
 
+// Dynamic shared memory of the distributed-shared-memory coarse kernel: the
+// largest body's rows per CTA on every coarse level (4 vectors) + the whole
+// coarsest right-hand side.
+size_t coarse_smem_bytes(const mgsb_solver* h, int cs) {
+    const int L = h->p.levels;
+    int best = 0;
+    for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
+        int nl[kMaxLevels] = {0};
+        for (int l = 0; l < L; ++l) nl[l] = h->range_host[bi * L + l].y;
+        best = std::max(best, coarse_smem_float4(nl, L, cs, nl[L - 1]));
+    }
+    return (size_t)best * sizeof(float4);
+}
+
 mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(h->bodies.size() * h->cluster));
-    cfg.blockDim = dim3(512);
-    cfg.dynamicSmemBytes = 0;
+    cfg.blockDim = dim3((unsigned)h->coarse_block);
+    cfg.dynamicSmemBytes = h->fuse_l0 ? 0 : coarse_smem_bytes(h, h->cluster);
     cfg.stream = h->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -381,7 +440,10 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (h->profiling) prof_mark(h, "k_coarse_vcycle");
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_coarse_vcycle, args);
+    // fused: global-memory kernel that also owns the level-0 residual and prolongation;
+    // else the distributed-shared-memory kernel over levels >= 1
+    cudaError_t e = h->fuse_l0 ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle, args)
+                               : cudaLaunchKernelEx(&cfg, k_coarse_vcycle_dsm, args);
     if (h->profiling) prof_mark(h, nullptr);
     ++h->launches;
     if (e != cudaSuccess) return set_err(h, MGSB_CUDA_ERROR, "coarse V-cycle launch failed: %s", cudaGetErrorString(e));
@@ -453,13 +515,8 @@ void enqueue_mg_frame(mgsb_solver* h) {
                        lv[0].dfull, xa, h->b, lv[0].res);
             ca.d = xa;
             launch_coarse(h, ca);
-            if (!h->fuse_l0) {
-                // the coarse kernel leaves the level-1 correction in the buffer its last sweep
-                // wrote: it starts in e and swaps once per sweep after the restriction
-                const int swaps = (p.pre_sweeps > 0 ? p.pre_sweeps - 1 : 0) + p.post_sweeps;
-                const float4* e1 = (swaps % 2 == 0) ? lv[1].e : lv[1].e2;
-                LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, e1, xa);
-            }
+            if (!h->fuse_l0)   // the shared-memory kernel leaves the level-1 correction in lv[1].e
+                LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, xa);
             for (int k = 0; k < p.post_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                        lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0);
@@ -946,12 +1003,24 @@ mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* 
     TRY(ensure_ready(h));
     CUDA_TRY(h, cudaSetDevice(h->device));
     TRY(push_tool(h));
+    // The frame is captured into its own graph with an event-record node on
+    // both sides of every kernel, so the timings contain no host launch gaps.
     h->profiling = true;
     h->prof_names.clear();
     h->prof_ev.clear();
-    enqueue_frame(h);
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_frame(h);
+        e = cudaStreamEndCapture(h->stream, &g);
+    }
     h->profiling = false;
-    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ge, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
     std::vector<std::string> uniq;
     std::vector<float> tot;
     std::vector<int32_t> cnt;
@@ -976,6 +1045,100 @@ mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* 
         std::snprintf(names + 48 * u, 48, "%s", uniq[u].c_str());
         total_ms[u] = tot[u];
         launches[u] = cnt[u];
+    }
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_set_kernel_shape(mgsb_solver* h, int32_t cluster, int32_t block, int32_t fuse_level0) {
+    if (!h) return MGSB_INVALID_ARG;
+    if (cluster < 0 || cluster > 16 || (block != 0 && block != 256 && block != 512 && block != 1024) || fuse_level0 < -1 ||
+        fuse_level0 > 1)
+        return set_err(h, MGSB_INVALID_ARG, "bad kernel shape (cluster %d, block %d, fuse %d)", cluster, block, fuse_level0);
+    h->tune_cluster = cluster;
+    h->tune_fuse = fuse_level0;
+    if (block) h->coarse_block = block;
+    apply_tuning(h);
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
+    if (!h || frames < 1) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "autotuning applies to the multigrid kind");
+    TRY(ensure_ready(h));
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    // Snapshot the state: every candidate starts from it and it is restored at the end.
+    const size_t nbytes = (size_t)h->N0 * sizeof(float4);
+    float4 *sx = nullptr, *sv = nullptr;
+    CUDA_TRY(h, cudaMalloc(&sx, nbytes));
+    CUDA_TRY(h, cudaMalloc(&sv, nbytes));
+    cudaMemcpyAsync(sx, h->x, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(sv, h->v, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+    struct Cand {
+        int cluster, block, fuse;
+    };
+    std::vector<Cand> cands;
+    const int nb = (int)h->bodies.size();
+    const int cls[] = {1, 2, 4, 8, 12, 16};
+    for (int c : cls) {
+        if (nb > 1 && c > 2) continue;   // many bodies: small clusters, one per body
+        for (int blk : {256, 512, 1024}) {
+            if (coarse_smem_bytes(h, c) <= (size_t)h->max_smem_optin) cands.push_back({c, blk, 0});
+            if (blk >= 512 && c >= 2) cands.push_back({c, blk, 1});
+        }
+    }
+    float best = 1e30f;
+    Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0};
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    mgsb_status st = MGSB_OK;
+    for (const Cand& c : cands) {
+        h->tune_cluster = c.cluster;
+        h->tune_fuse = c.fuse;
+        h->coarse_block = c.block;
+        apply_tuning(h);
+        invalidate_graph(h);
+        cudaMemsetAsync(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t), h->stream);
+        cudaMemcpyAsync(h->x, sx, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->v, sv, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+        if ((st = step_once(h)) != MGSB_OK) break;   // warm-up: capture + coarsest factorisation
+        cudaEventRecord(a, h->stream);
+        for (int f = 0; f < frames && st == MGSB_OK; ++f) st = step_once(h);
+        cudaEventRecord(b, h->stream);
+        if (st != MGSB_OK) break;
+        if (cudaEventSynchronize(b) != cudaSuccess) {
+            st = set_err(h, MGSB_CUDA_ERROR, "autotune candidate failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) {
+            best = ms;
+            bestc = c;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->tune_cluster = bestc.cluster;
+    h->tune_fuse = bestc.fuse;
+    h->coarse_block = bestc.block;
+    apply_tuning(h);
+    invalidate_graph(h);
+    const mgsb_status st2 = MGSB_OK;
+    cudaMemsetAsync(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t), h->stream);
+    cudaMemcpyAsync(h->x, sx, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->v, sv, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(sx);
+    cudaFree(sv);
+    if (st != MGSB_OK) return st;
+    if (st2 != MGSB_OK) return st2;
+    if (chosen) {
+        chosen[0] = bestc.cluster;
+        chosen[1] = bestc.block;
+        chosen[2] = bestc.fuse;
     }
     return MGSB_OK;
 }
@@ -1044,6 +1207,22 @@ mgsb_status mgsb_level_size(mgsb_solver* h, int32_t level, int32_t* num_verts, i
     if (level < 0 || level >= (int32_t)h->lev.size()) return set_err(h, MGSB_INVALID_ARG, "level %d out of range", level);
     *num_verts = h->lev[level].n;
     *nnz_offdiag = h->lev[level].nnz;
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_level_info(mgsb_solver* h, int32_t level, int32_t info[8]) {
+    if (!h || !info) return MGSB_INVALID_ARG;
+    TRY(ensure_ready(h));
+    if (level < 0 || level >= (int32_t)h->lev.size()) return set_err(h, MGSB_INVALID_ARG, "level %d out of range", level);
+    const LevelDev& l = h->lev[level];
+    info[0] = l.n;
+    info[1] = l.nnz;
+    info[2] = l.nchild;
+    info[3] = l.S;
+    info[4] = l.ell_entries;
+    info[5] = h->cluster;
+    info[6] = h->coarse_block;
+    info[7] = h->fuse_l0;
     return MGSB_OK;
 }
 

@@ -162,3 +162,35 @@ def test_divergence_reported(lib):
     with pytest.raises(mg.MgsbError) as e:
         s.positions()
     assert e.value.status == 4
+
+
+@pytest.mark.parametrize("shape", [(1, 256, 0), (4, 1024, 1), (16, 512, 0), (2, 512, 1)])
+def test_kernel_shapes_match_oracle(lib, oracle_built, shape):
+    """Every coarse-kernel shape (cluster size, block size, level-0 fusion) gives
+    the oracle's result on the tool scene."""
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3, gravity=(0, 0, 0))
+    s, o = _pair(m, fixed, p)
+    s.set_kernel_shape(*shape)
+    path = capsule_path(40, start=(0.0, 0.0, 1.4))
+    for f in range(40):
+        for solver in (s, o):
+            solver.set_capsule(*path[f], 0.3)
+            solver.step()
+    assert np.abs(s.positions() - o.positions()).max() < 1e-5 * m.bbox_diagonal()
+    assert np.array_equal(np.nonzero(s.contact_flags())[0], np.nonzero(o.contact_flags())[0])
+    info = s.level_info(0)
+    assert (info["cluster"], info["block"], info["fuse_l0"]) == shape
+
+
+def test_autotune_restores_state(lib, oracle_built):
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3)
+    s, o = _pair(m, fixed, p)
+    s.step(5)
+    o.step(5)
+    chosen = s.autotune(frames=2)
+    assert chosen["cluster"] >= 1 and chosen["block"] in (512, 1024)
+    s.step(5)
+    o.step(5)
+    assert np.abs(s.positions() - o.positions()).max() < 1e-5 * m.bbox_diagonal()
