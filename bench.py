@@ -298,13 +298,10 @@ def run_ours(args):
         torch.cuda.synchronize()
         tool(solver, frame)
         prof = solver.profile_frame()
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t[0]), float(t[1])
-    frames_total = args.steps * world
-    value = frames_total / (ms / 1e3)
-    e2e_value = frames_total / (e2e_ms / 1e3)
+    from multigridsoftbody_b200.replicas import job_throughput, max_over_ranks
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist)
+    value = job_throughput(args.steps, world, ms)
+    e2e_value = job_throughput(args.steps, world, e2e_ms)
     if rank == 0:
         launches = solver.launches_per_frame()
         dom = max(prof.items(), key=lambda kv: kv[1][0])
