@@ -43,24 +43,65 @@ def capsule_path(frames, start=(0.0, 0.0, 3.0), dz=-0.02, sigma=0.005, half_leng
 
 
 def make_workload(name, mg):
-    """Returns (meshes, params list, fixed masks, per-frame tool callback, description)."""
-    if name in ("beam", "beam_mixed", "small"):
-        dims = (4, 40, 4) if name == "small" else (12, 120, 12)
-        levels = 3 if name == "small" else 4
+    """Returns (meshes, params list, fixed masks, per-frame tool callback, description,
+    per-body materials or None)."""
+    if name in ("beam", "beam_mixed", "small", "large_mixed"):
+        dims = {"small": (4, 40, 4), "large_mixed": (24, 240, 24)}.get(name, (12, 120, 12))
+        levels = {"small": 3, "large_mixed": 5}.get(name, 4)
+        mixed = name in ("beam_mixed", "large_mixed")
         m = mg.box_mesh(*dims)
         fixed = (np.abs(m.positions[:, 1] - 10.0) < 1e-5).astype(np.uint8)
-        p = mg.default_params(mg.SOLVER_MULTIGRID, levels=levels, iterations=10, gravity=(0.0, 0.0, 0.0))
+        p = mg.default_params(mg.SOLVER_MULTIGRID, levels=levels, iterations=10, gravity=(0.0, 0.0, 0.0),
+                              precision=mg.PRECISION_MIXED if mixed else mg.PRECISION_FP32,
+                              refinement_passes=2 if mixed else 1)
         # Start the tool 0.3 above the top face so every timed frame has contacts.
         path = capsule_path(4096, start=(0.0, 0.0, 1.5))
 
-        def tool(solver, f):
+        def tool(f):
             a, b = path[f % len(path)]
-            solver.set_capsule(a, b, 0.3)
+            return a[None], b[None], np.array([0.3], np.float32)
 
+        mats = None
+        if name == "large_mixed":
+            rng = np.random.default_rng(7)
+            mats = [(np.exp(rng.uniform(np.log(5e4), np.log(2e5), m.num_tets)).astype(np.float32), 0.3)]
         desc = (f"beam {dims[0]}x{dims[1]}x{dims[2]} hexes ({m.num_verts} verts, {m.num_tets} tets), "
                 f"{levels} MG levels, 2+2 Jacobi sweeps, 10 PD iterations/frame, capsule r=0.3 len 8 "
-                f"moving -z 0.02/frame + N(0,0.005^2) jitter (seed 1), in contact")
-        return [m], [p], [fixed], tool, desc
+                f"moving -z 0.02/frame + N(0,0.005^2) jitter (seed 1), in contact"
+                + (", mixed precision (FP64 residual, 2 refinement passes)" if mixed else "")
+                + (", E log-uniform [5e4,2e5] per tet (seed 7)" if name == "large_mixed" else ""))
+        return [m], [p], [fixed], tool, desc, mats
+    if name == "batch":
+        rng = np.random.default_rng(11)
+        ns = rng.integers(2, 9, size=256)
+        meshes, params, fixeds, mats = [], [], [], []
+        for n in ns:
+            L = 2.5 * n
+            m = mg.box_mesh(int(n), int(10 * n), int(n), (-1.0, -L, -1.0), (1.0, L, 1.0))
+            meshes.append(m)
+            fixeds.append((np.abs(m.positions[:, 1] - L) < 1e-5).astype(np.uint8))
+            params.append(mg.default_params(mg.SOLVER_MULTIGRID, levels=3, iterations=10, gravity=(0.0, 0.0, 0.0)))
+            E = float(np.exp(rng.uniform(np.log(5e4), np.log(2e5))))
+            nu = float(rng.uniform(0.25, 0.45))
+            mats.append((np.full(m.num_tets, E, np.float32), nu))
+        start = np.array([0.0, 0.0, 1.15]) + rng.uniform(-0.5, 0.5, (256, 3))
+        vel = np.random.default_rng(12)
+
+        traj = [start]
+        for _ in range(4096):
+            traj.append(traj[-1] + vel.normal(0.0, 0.01, (256, 3)))
+
+        def tool(f):
+            c = traj[f % len(traj)]
+            return ((c - [2.0, 0, 0]).astype(np.float32), (c + [2.0, 0, 0]).astype(np.float32),
+                    np.full(256, 0.2, np.float32))
+
+        V = sum(m.num_verts for m in meshes)
+        T = sum(m.num_tets for m in meshes)
+        desc = (f"batch of 256 beams n x 10n x n hexes, n~U{{2..8}} (seed 11): {V} verts, {T} tets in total; "
+                f"E log-uniform [5e4,2e5], nu U[0.25,0.45] per body; capsule r=0.2 len 4 per body, start "
+                f"(0,0,1.15)+U(-0.5,0.5)^3, velocity N(0,0.01^2)/axis/frame; 3 levels, 10 PD iterations; one launch per phase")
+        return meshes, params, fixeds, tool, desc, mats
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -179,17 +220,39 @@ def ncu_traffic(kernel):
 # ---------------------------------------------------------------------------
 # CPU baseline / reference arm: the FP64 oracle on the host cores
 # ---------------------------------------------------------------------------
-def cpu_frames_per_s(meshes, params, fixeds, tool, frames, warm=1):
+def apply_tool(solver, poses):
+    a, b, r = poses
+    if len(r) == 1:
+        solver.set_capsule(a[0], b[0], float(r[0]))
+    else:
+        solver.set_capsules(a, b, r)
+
+
+def make_oracles(meshes, params, fixeds, mats):
     from oracle.binding import Oracle
-    o = Oracle(meshes[0], params[0])
-    o.set_fixed(fixeds[0])
-    for f in range(warm):
-        tool(o, f)
-        o.step()
+    out = []
+    for i, m in enumerate(meshes):
+        o = Oracle(m, params[i])
+        o.set_fixed(fixeds[i])
+        if mats is not None:
+            o.set_material(*mats[i])
+        out.append(o)
+    return out
+
+
+def oracle_frames(oracles, tool, f0, frames):
+    for f in range(f0, f0 + frames):
+        a, b, r = tool(f)
+        for i, o in enumerate(oracles):
+            o.set_capsule(a[i], b[i], float(r[i]))
+            o.step()
+
+
+def cpu_frames_per_s(meshes, params, fixeds, tool, mats, frames, warm=1):
+    os_ = make_oracles(meshes, params, fixeds, mats)
+    oracle_frames(os_, tool, 0, warm)
     t0 = time.perf_counter()
-    for f in range(frames):
-        tool(o, warm + f)
-        o.step()
+    oracle_frames(os_, tool, warm, frames)
     dt = time.perf_counter() - t0
     return frames / dt, dt
 
@@ -199,18 +262,12 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    meshes, params, fixeds, tool, desc = make_workload(args.workload, mg)
+    meshes, params, fixeds, tool, desc, mats = make_workload(args.workload, mg)
     cores = os.cpu_count()
-    from oracle.binding import Oracle
-    o = Oracle(meshes[0], params[0])
-    o.set_fixed(fixeds[0])
-    for f in range(args.warmup):
-        tool(o, f)
-        o.step()
+    os_ = make_oracles(meshes, params, fixeds, mats)
+    oracle_frames(os_, tool, 0, args.warmup)
     t0 = time.perf_counter()
-    for f in range(args.steps):
-        tool(o, args.warmup + f)
-        o.step()
+    oracle_frames(os_, tool, args.warmup, args.steps)
     dt = time.perf_counter() - t0
     v = args.steps / dt
     line = {"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -241,13 +298,15 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     stream = torch.cuda.Stream(device=local)
-    meshes, params, fixeds, tool, desc = make_workload(args.workload, mg)
+    meshes, params, fixeds, tool, desc, mats = make_workload(args.workload, mg)
     for p in params:
         p.device = local
         p.stream = stream.cuda_stream
     solver = mg.Solver(meshes, params)
     for b, fx in enumerate(fixeds):
         solver.set_fixed(fx, body=b)
+        if mats is not None:
+            solver.set_material(*mats[b], body=b)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
 
     def barrier():
@@ -260,7 +319,7 @@ def run_ours(args):
     tuned = solver.autotune(frames=5) if not args.no_tune else None
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            tool(solver, frame)
+            apply_tool(solver, tool(frame))
             solver.step()
             frame += 1
         solver.synchronize()
@@ -270,7 +329,7 @@ def run_ours(args):
             for k in range(args.steps):
                 flush.zero_()
                 evs[k][0].record(stream)
-                tool(solver, frame)
+                apply_tool(solver, tool(frame))
                 solver.step()
                 evs[k][1].record(stream)
                 frame += 1
@@ -284,7 +343,7 @@ def run_ours(args):
         for k in range(args.steps):
             flush.zero_()
             e2e_evs[k][0].record(stream)
-            tool(solver, frame)
+            apply_tool(solver, tool(frame))
             solver.step()
             for b in range(len(meshes)):
                 solver.positions(b)
@@ -296,7 +355,7 @@ def run_ours(args):
         # live per-kernel profile of one frame (eager, events around every launch), cold L2
         flush.zero_()
         torch.cuda.synchronize()
-        tool(solver, frame)
+        apply_tool(solver, tool(frame))
         prof = solver.profile_frame()
     from multigridsoftbody_b200.replicas import job_throughput, max_over_ranks
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist)
@@ -318,15 +377,15 @@ def run_ours(args):
                     "share_of_frame": ktot / sum(v[0] for v in prof.values())}
         cpu = None
         if world == 1 and not args.no_cpu:
-            fps, dt = cpu_frames_per_s(meshes, params, fixeds, tool, frames=args.cpu_frames)
+            fps, dt = cpu_frames_per_s(meshes, params, fixeds, tool, mats, frames=args.cpu_frames)
             cpu = {"value": fps, "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"{args.cpu_frames} frames of the same workload, FP64 oracle ({dt:.1f} s)"}
-        h2d = len(meshes) * 64 + 164          # body table + sphere set per frame
+        h2d = len(meshes) * 88 + 164          # body table (88 B per body) + sphere set per frame
         d2h = nverts * 16 + nverts * 4        # float4 positions + contact flags
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": desc, "variant": "plain FP32 multigrid", "parallelism": f"replicas x{world}",
+                "config": {"workload": desc, "variant": "mixed precision multigrid" if params[0].precision == 1 else "plain FP32 multigrid", "parallelism": f"replicas x{world}",
                            "l2": "flushed (256 MB write) before every timed frame, outside the timed span",
                            "autotuned_coarse_kernel": tuned},
                 "clocks": clk.summary(),

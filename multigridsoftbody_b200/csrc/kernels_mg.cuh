@@ -45,6 +45,7 @@ struct CoarseArgs {
     const int2* range;       // [nbody * L]: (first row, rows) of each body on each level
     const int32_t* dense_off;
     const float* Ainv;       // coarsest inverse blocks (row-major per body)
+    const double* Ainv64;    // FP64 coarsest inverse (mixed precision), else null
     const float4* b;         // level-0 right-hand side
     float4* d;               // level-0 unknown (displacement)
     LevelView lv[kMaxLevels];
@@ -531,25 +532,48 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
         const int n = q[l].n;
         for (int i = threadIdx.x; i < n; i += blockDim.x) rfull[i] = *dsm_ptr(cluster, smv, q[l], R, i);
         __syncthreads();
-        const float* Ai = A.Ainv + __ldg(A.dense_off + body);
         const int r0 = first_row(l), cnt = own_rows(l);
-        for (int li = warp; li < cnt; li += nwarp) {
-            const int i = r0 + li;
-            float ax = 0.f, ay = 0.f, az = 0.f;
-            for (int k = lane; k < n; k += 32) {
-                const float a = __ldg(Ai + (size_t)i * n + k);
-                const float4 r = rfull[k];
-                ax = fmaf(a, r.x, ax);
-                ay = fmaf(a, r.y, ay);
-                az = fmaf(a, r.z, az);
-            }
+        if (A.Ainv64) {
+            // FP64 coarsest solve (mixed precision)
+            const double* Ai = A.Ainv64 + __ldg(A.dense_off + body);
+            for (int li = warp; li < cnt; li += nwarp) {
+                const int i = r0 + li;
+                double ax = 0.0, ay = 0.0, az = 0.0;
+                for (int k = lane; k < n; k += 32) {
+                    const double a = __ldg(Ai + (size_t)i * n + k);
+                    const float4 r = rfull[k];
+                    ax = fma(a, (double)r.x, ax);
+                    ay = fma(a, (double)r.y, ay);
+                    az = fma(a, (double)r.z, az);
+                }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                ax += __shfl_xor_sync(0xffffffffu, ax, o);
-                ay += __shfl_xor_sync(0xffffffffu, ay, o);
-                az += __shfl_xor_sync(0xffffffffu, az, o);
+                for (int o = 16; o > 0; o >>= 1) {
+                    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                    az += __shfl_xor_sync(0xffffffffu, az, o);
+                }
+                if (lane == 0) loc(l, E, li) = make_float4((float)ax, (float)ay, (float)az, 0.f);
             }
-            if (lane == 0) loc(l, E, li) = make_float4(ax, ay, az, 0.f);
+        } else {
+            const float* Ai = A.Ainv + __ldg(A.dense_off + body);
+            for (int li = warp; li < cnt; li += nwarp) {
+                const int i = r0 + li;
+                float ax = 0.f, ay = 0.f, az = 0.f;
+                for (int k = lane; k < n; k += 32) {
+                    const float a = __ldg(Ai + (size_t)i * n + k);
+                    const float4 r = rfull[k];
+                    ax = fmaf(a, r.x, ax);
+                    ay = fmaf(a, r.y, ay);
+                    az = fmaf(a, r.z, az);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                    az += __shfl_xor_sync(0xffffffffu, az, o);
+                }
+                if (lane == 0) loc(l, E, li) = make_float4(ax, ay, az, 0.f);
+            }
         }
         ec[l] = E;
         cluster.sync();

@@ -1,0 +1,256 @@
+// Mixed-precision multigrid frame (sm_100a).  Included by solver.cu only.
+//
+// FP64: positions, velocities, prediction s, displacement d = x - s, the
+// right-hand side and the outer residual r = b - A d (level-0 matrix in FP64),
+// the coarsest factor and solve.  FP32: the local step (on FP32 mirrors of s
+// and d) and the V-cycle that computes each correction e ~= A^-1 r.
+// Every PD iteration runs `refinement_passes` FP64-residual / FP32-correction
+// passes (iterative refinement).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels_mg.cuh"
+
+namespace mgsb {
+
+__device__ __forceinline__ double4 d4z() { return make_double4(0.0, 0.0, 0.0, 0.0); }
+
+// Prediction in FP64 (same form as calculateST): last = x; v = v*damp*fix + g*dt*fix;
+// x = s = x + v*dt*fix.  FP32 mirrors s32 (local step) and x32 (readback).
+__global__ void k_mx_predict(int n, double4* __restrict__ x, double4* __restrict__ v, double4* __restrict__ s,
+                             double4* __restrict__ last, float4* __restrict__ s32, float4* __restrict__ x32,
+                             const float* __restrict__ fixf, const int32_t* __restrict__ body_of,
+                             const BodyDev* __restrict__ bodies, double dt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BodyDev& B = bodies[__ldg(body_of + i)];
+    double4 p = x[i], vel = v[i];
+    last[i] = p;
+    const double fix = __ldg(fixf + i);
+    const double damp = B.damping;
+    vel.x *= damp * fix; vel.y *= damp * fix; vel.z *= damp * fix;
+    vel.x += (double)B.gravity[0] * dt * fix; vel.y += (double)B.gravity[1] * dt * fix; vel.z += (double)B.gravity[2] * dt * fix;
+    p.x += vel.x * dt * fix; p.y += vel.y * dt * fix; p.z += vel.z * dt * fix;
+    p.w = 0.0;
+    x[i] = p;
+    v[i] = vel;
+    s[i] = p;
+    const float4 f = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+    s32[i] = f;
+    x32[i] = f;
+}
+
+__device__ __forceinline__ void capsule_test64(const double4 sp, const BodyDev& B, int& flag, double4& target) {
+    flag = 0;
+    target = d4z();
+    const double r = B.cap_r;
+    if (!(r > 0.0)) return;
+    const double p[3] = {sp.x, sp.y, sp.z};
+    const double a[3] = {B.cap_a[0], B.cap_a[1], B.cap_a[2]}, b[3] = {B.cap_b[0], B.cap_b[1], B.cap_b[2]};
+    const double ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double l2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+    double t = 0.0;
+    if (l2 > 0.0) {
+        t = ((p[0] - a[0]) * ab[0] + (p[1] - a[1]) * ab[1] + (p[2] - a[2]) * ab[2]) / l2;
+        t = fmin(1.0, fmax(0.0, t));
+    }
+    const double q[3] = {a[0] + t * ab[0], a[1] + t * ab[1], a[2] + t * ab[2]};
+    const double dv[3] = {p[0] - q[0], p[1] - q[1], p[2] - q[2]};
+    const double d = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    if (!(d < r)) return;
+    double nrm[3] = {0.0, 0.0, 1.0};
+    if (d > 1e-12) {
+        nrm[0] = dv[0] / d; nrm[1] = dv[1] / d; nrm[2] = dv[2] / d;
+    }
+    flag = 1;
+    target = make_double4(q[0] + r * nrm[0], q[1] + r * nrm[1], q[2] + r * nrm[2], 0.0);
+}
+
+// Contact on the FP64 prediction; b0 = c (p - s) in FP64; D, dinv (FP32, for
+// the correction V-cycle); d = 0 in both precisions.
+__global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const float* __restrict__ fixf,
+                                   const int32_t* __restrict__ body_of, const BodyDev* __restrict__ bodies,
+                                   const uint8_t* __restrict__ is_surf, float kc, const float* __restrict__ diag0,
+                                   float omega, int32_t* __restrict__ cflag, float* __restrict__ c0,
+                                   double4* __restrict__ b0, float* __restrict__ dfull, float* __restrict__ dinv,
+                                   double4* __restrict__ d64, float4* __restrict__ d32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int flag = 0;
+    double4 tg = d4z();
+    const double4 sv = s[i];
+    if (__ldg(is_surf + i)) capsule_test64(sv, bodies[__ldg(body_of + i)], flag, tg);
+    const bool free_v = __ldg(fixf + i) != 0.f;
+    const float c = (flag && free_v) ? kc : 0.f;
+    cflag[i] = flag;
+    c0[i] = c;
+    b0[i] = c != 0.f ? make_double4((double)c * (tg.x - sv.x), (double)c * (tg.y - sv.y), (double)c * (tg.z - sv.z), 0.0) : d4z();
+    const float D = __ldg(diag0 + i) + c;
+    dfull[i] = D;
+    dinv[i] = free_v ? omega / D : 0.f;
+    d64[i] = d4z();
+    d32[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// b = b0 + sum of the vertex's slots, accumulated in FP64.
+__global__ void __launch_bounds__(256) k_mx_rhs(int n, const double4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
+                                                const float4* __restrict__ slots, double4* __restrict__ b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 acc = b0[i];
+    const int e1 = __ldg(slot_ptr + i + 1);
+    for (int e = __ldg(slot_ptr + i); e < e1; ++e) {
+        const float4 c = __ldg(slots + e);
+        acc.x += c.x;
+        acc.y += c.y;
+        acc.z += c.z;
+    }
+    b[i] = acc;
+}
+
+// Outer FP64 residual r = b - A d with A = diag + off-diagonal (FP64 values),
+// stored as FP32 for the correction V-cycle, fused with its first Jacobi
+// sweep from a zero guess: e = dinv r.  4 lanes per row.
+__global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                                     const double* __restrict__ val, const double* __restrict__ dfull64,
+                                                     const double4* __restrict__ d, const double4* __restrict__ b,
+                                                     const float* __restrict__ dinv, float4* __restrict__ r32,
+                                                     float4* __restrict__ e, int first_sweep) {
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    if (valid) {
+        const int slice = row / S;
+        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
+#pragma unroll 2
+        for (int q = beg + (lane / S) * S + (row - slice * S); q < end; q += 32) {
+            const double a = __ldg(val + q);
+            const double4 xv = d[__ldg(col + q)];
+            ax = fma(a, xv.x, ax);
+            ay = fma(a, xv.y, ay);
+            az = fma(a, xv.z, az);
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (!valid || lane >= S) return;
+    const double4 x = d[row], bi = b[row];
+    const double D = __ldg(dfull64 + row);
+    const float rx = (float)(bi.x - fma(D, x.x, ax)), ry = (float)(bi.y - fma(D, x.y, ay)), rz = (float)(bi.z - fma(D, x.z, az));
+    r32[row] = make_float4(rx, ry, rz, 0.f);
+    const float w = first_sweep ? __ldg(dinv + row) : 0.f;
+    e[row] = make_float4(w * rx, w * ry, w * rz, 0.f);
+}
+
+// d += e (FP64), FP32 mirror for the local step.
+__global__ void k_mx_update(int n, const float4* __restrict__ e, double4* __restrict__ d, float4* __restrict__ d32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 c = __ldg(e + i);
+    double4 v = d[i];
+    v.x += c.x;
+    v.y += c.y;
+    v.z += c.z;
+    d[i] = v;
+    d32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+}
+
+// x = s + d, v = v_predicted + d/dt (FP64); FP32 mirror; finiteness check.
+__global__ void k_mx_finish(int n, const double4* __restrict__ s, const double4* __restrict__ d, double4* __restrict__ x,
+                            double4* __restrict__ v, float4* __restrict__ x32, double inv_dt, int32_t* __restrict__ nonfinite) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 sv = s[i], dv = d[i];
+    double4 vel = v[i];
+    const double4 p = make_double4(sv.x + dv.x, sv.y + dv.y, sv.z + dv.z, 0.0);
+    vel.x += dv.x * inv_dt;
+    vel.y += dv.y * inv_dt;
+    vel.z += dv.z * inv_dt;
+    x[i] = p;
+    v[i] = vel;
+    x32[i] = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+    if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) atomicOr(nonfinite, 1);
+}
+
+// Coarsest level in FP64: Cholesky + explicit inverse (same algorithm as
+// k_coarsest_factor_inv).
+__global__ void __launch_bounds__(1024) k_coarsest_factor_inv64(const int2* __restrict__ range, int L,
+                                                                const int32_t* __restrict__ dense_off,
+                                                                const double* __restrict__ A0, const float* __restrict__ c,
+                                                                float* __restrict__ c_prev, double* __restrict__ Ainv,
+                                                                int32_t* __restrict__ valid) {
+    extern __shared__ double smd[];
+    const int2 rg = range[blockIdx.x * L + (L - 1)];
+    const int n = rg.y, off = rg.x;
+    const double* A = A0 + dense_off[blockIdx.x];
+    double* Ai = Ainv + dense_off[blockIdx.x];
+    __shared__ int changed;
+    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (c[off + i] != c_prev[off + i]) changed = 1;
+    __syncthreads();
+    if (!changed) return;
+    double* M = smd;
+    double* tmp = smd + n * n;
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        double a = A[q];
+        if (i == j) a += c[off + i];
+        M[q] = a;
+    }
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        const double dd = sqrt(M[j * n + j]);
+        const double id = 1.0 / dd;
+        __syncthreads();
+        if (threadIdx.x == 0) M[j * n + j] = dd;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i * n + j] *= id;
+        __syncthreads();
+        const int m = n - j - 1;
+        const int tot = m * (m + 1) / 2;
+        for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+            int a = (int)((sqrtf(8.f * (float)q + 1.f) - 1.f) * 0.5f);
+            while ((a + 1) * (a + 2) / 2 <= q) ++a;
+            while (a * (a + 1) / 2 > q) --a;
+            const int bcol = q - a * (a + 1) / 2;
+            const int i = j + 1 + a, k = j + 1 + bcol;
+            M[i * n + k] -= M[i * n + j] * M[k * n + j];
+        }
+        __syncthreads();
+    }
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = 0; i < n; ++i) {
+        const double xii = 1.0 / M[i * n + i];
+        for (int j = wid; j < i; j += nw) {
+            double s = 0.0;
+            for (int k = j + lane; k < i; k += 32) s = fma(M[i * n + k], M[k * n + j], s);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) tmp[j] = -xii * s;
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < i; j += blockDim.x) M[i * n + j] = tmp[j];
+        if (threadIdx.x == 0) M[i * n + i] = xii;
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const int i = q / n, j = q - i * n;
+        const int k0 = i > j ? i : j;
+        double s = 0.0;
+        for (int k = k0; k < n; ++k) s = fma(M[k * n + i], M[k * n + j], s);
+        Ai[q] = s;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) c_prev[off + i] = c[off + i];
+    if (threadIdx.x == 0) valid[blockIdx.x] = 1;
+}
+
+}  // namespace mgsb

@@ -203,6 +203,18 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
         }
         l0.S = kSliceL0;
         build_ell(ptr, col, val, N0, l0.S, l0.slice_ptr, l0.ell_col, l0.ell_val);
+        {
+            // FP64 values in the same sliced-ELL positions
+            l0.ell_val64.assign(l0.ell_val.size(), 0.0);
+            const int S = l0.S;
+            for (int r = 0; r < N0; ++r) {
+                const int sl = r / S, ln = r % S;
+                for (int k = 0; k < ptr[r + 1] - ptr[r]; ++k) l0.ell_val64[l0.slice_ptr[sl] + k * S + ln] = val[ptr[r] + k];
+            }
+            P.diag64.assign(N0, 0.0);
+            for (size_t bi = 0; bi < bodies.size(); ++bi)
+                for (int i = 0; i < bodies[bi].V; ++i) P.diag64[bodies[bi].v_off + i] = Lmat[bi].diag[i];
+        }
         l0.nnz = (int)col.size();
         l0.diag0 = P.diag;
         P.levels.push_back(std::move(l0));
@@ -299,12 +311,19 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
         dense_from_sparse(C.A, C.active, d);
         P.cl_n[bi] = C.n;
         P.dense_off[bi] = (int32_t)P.dense.size();
-        for (double q : d) P.dense.push_back((float)q);
+        for (double q : d) {
+            P.dense.push_back((float)q);
+            P.dense64.push_back(q);
+        }
         P.max_coarsest = std::max(P.max_coarsest, C.n);
     }
     // ---- surface vertices
+    P.is_surf.assign(N0, 0);
     for (const PlanBody& B : bodies)
-        for (int i : B.surface) P.surf.push_back(i + B.v_off);
+        for (int i : B.surface) {
+            P.surf.push_back(i + B.v_off);
+            P.is_surf[i + B.v_off] = 1;
+        }
     return true;
 }
 

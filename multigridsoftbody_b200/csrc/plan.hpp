@@ -33,6 +33,7 @@ struct PlanLevel {
     int S = 32;                      // slice height of the sliced ELL
     std::vector<int32_t> slice_ptr, ell_col;
     std::vector<float> ell_val, diag0;
+    std::vector<double> ell_val64;   // level 0 only: FP64 copy for the mixed-precision residual
     // prolongation rows of the next finer level's vertices (coarse side = this level)
     std::vector<int4> pid;
     std::vector<float4> pw;
@@ -51,6 +52,9 @@ struct Plan {
     std::vector<int32_t> slot_ptr;
     std::vector<PlanLevel> levels;            // [0] = finest (matrix only)
     std::vector<float> dense;                 // coarsest dense blocks (row-major per body)
+    std::vector<double> dense64;              // the same in FP64
+    std::vector<double> diag64;               // level-0 diagonal in FP64
+    std::vector<uint8_t> is_surf;             // per vertex: on the boundary surface
     std::vector<int32_t> cl_off, cl_n, dense_off;
     std::vector<int2> range;                  // [body * L + level]: (first row, rows)
     int max_coarsest = 0;

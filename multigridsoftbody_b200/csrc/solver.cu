@@ -13,6 +13,7 @@
 #include "../../include/mgsb.h"
 #include "kernels.cuh"
 #include "kernels_mg.cuh"
+#include "kernels_mixed.cuh"
 #include "mesh.hpp"
 #include "plan.hpp"
 #include "setup.hpp"
@@ -109,6 +110,13 @@ struct mgsb_solver {
     float4* slots = nullptr;
     // multigrid
     float4 *b = nullptr, *b0 = nullptr, *target = nullptr, *d = nullptr, *d2 = nullptr;
+    // mixed precision (FP64 master state and outer residual)
+    double4 *x64 = nullptr, *v64 = nullptr, *s64 = nullptr, *last64 = nullptr, *dd64 = nullptr, *b64 = nullptr,
+            *b0_64 = nullptr;
+    float4 *d32 = nullptr, *r32 = nullptr;
+    double *ell_val64 = nullptr, *diag64 = nullptr, *A0dense64 = nullptr, *Ainv64 = nullptr;
+    uint8_t* is_surf = nullptr;
+    size_t factor_smem64 = 0;
     float* c0 = nullptr;
     int32_t* surf = nullptr;
     int nsurf = 0;
@@ -212,6 +220,7 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs);
 void apply_tuning(mgsb_solver* h) {
     // Default: the distributed-shared-memory kernel with <= 256 level-1 rows per CTA.
     h->fuse_l0 = h->tune_fuse >= 0 ? h->tune_fuse : 0;
+    if (h->p.precision == MGSB_PRECISION_MIXED) h->fuse_l0 = 0;   // mixed precision runs the DSM kernel
     if (h->tune_cluster > 0) {
         h->cluster = h->tune_cluster;
     } else if (h->fuse_l0) {
@@ -359,6 +368,26 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->fac_valid, h->bodies.size()));
         CUDA_TRY(h, cudaMemset(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t)));
+        if (h->p.precision == MGSB_PRECISION_MIXED) {
+            TRY(dalloc(h, pool, &h->s64, N0));
+            TRY(dalloc(h, pool, &h->last64, N0));
+            TRY(dalloc(h, pool, &h->dd64, N0));
+            TRY(dalloc(h, pool, &h->b64, N0));
+            TRY(dalloc(h, pool, &h->b0_64, N0));
+            TRY(dalloc(h, pool, &h->d32, N0));
+            TRY(dalloc(h, pool, &h->r32, N0));
+            TRY(dupload(h, pool, &h->ell_val64, P.levels[0].ell_val64));
+            TRY(dupload(h, pool, &h->diag64, P.diag64));
+            TRY(dupload(h, pool, &h->A0dense64, P.dense64));
+            TRY(dalloc(h, pool, &h->Ainv64, P.dense64.size()));
+            TRY(dupload(h, pool, &h->is_surf, P.is_surf));
+            h->factor_smem64 = ((size_t)P.max_coarsest * P.max_coarsest + P.max_coarsest) * sizeof(double);
+            if (h->factor_smem64 > (size_t)h->max_smem_optin)
+                return set_err(h, MGSB_NOT_SUPPORTED, "coarsest level has %d vertices; its FP64 factor needs %zu B of shared memory",
+                               P.max_coarsest, h->factor_smem64);
+            CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_factor_inv64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)h->factor_smem64));
+        }
         h->nsurf = (int)P.surf.size();
         TRY(dupload(h, pool, &h->surf, P.surf));
     }
@@ -527,9 +556,95 @@ void enqueue_mg_frame(mgsb_solver* h) {
     LAUNCH(h, k_mg_finish, grid_for(n0), kBlock, 0, n0, h->s, xa, h->x, h->v, 1.0f / p.dt, h->nonfinite);
 }
 
+void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
+    const mgsb_params& p = h->p;
+    const int L = p.levels;
+    std::vector<LevelDev>& lv = h->lev;
+    ca = CoarseArgs{};
+    ca.L = L;
+    ca.pre = p.pre_sweeps;
+    ca.post = p.post_sweeps;
+    ca.fuse_l0 = h->fuse_l0;
+    ca.range = h->range;
+    ca.dense_off = h->dense_off_d;
+    ca.Ainv = h->Lfac;
+    ca.Ainv64 = nullptr;
+    ca.b = h->b;
+    for (int l = 0; l < L; ++l) {
+        LevelView& v = ca.lv[l];
+        v.n = lv[l].n;
+        v.slice_ptr = lv[l].slice_ptr;
+        v.col = lv[l].ell_col;
+        v.val = lv[l].ell_val;
+        v.dfull = lv[l].dfull;
+        v.dinv = lv[l].dinv;
+        v.r = lv[l].r;
+        v.e = lv[l].e;
+        v.e2 = lv[l].e2;
+        v.res = lv[l].res;
+        v.pid = lv[l].pid;
+        v.pw = lv[l].pw;
+        v.rptr = lv[l].rptr;
+        v.rcol = lv[l].rcol;
+        v.rw = lv[l].rw;
+    }
+}
+
+// Mixed precision: FP64 state and outer residual, FP32 local step and
+// correction V-cycles (refinement_passes per PD iteration).
+void enqueue_mixed_frame(mgsb_solver* h) {
+    const mgsb_params& p = h->p;
+    const int n0 = h->N0, T = h->T, L = p.levels;
+    const int nb = (int)h->bodies.size();
+    const float om = p.jacobi_omega;
+    std::vector<LevelDev>& lv = h->lev;
+    LAUNCH(h, k_mx_predict, grid_for(n0), kBlock, 0, n0, h->x64, h->v64, h->s64, h->last64, h->s, h->x, h->fixf,
+           h->body_of, h->bodies_dev, (double)p.dt);
+    LAUNCH(h, k_mx_contact_frame, grid_for(n0), kBlock, 0, n0, h->s64, h->fixf, h->body_of, h->bodies_dev, h->is_surf,
+           p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32);
+    for (int l = 1; l < L; ++l)
+        LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
+               lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
+    LAUNCH(h, k_coarsest_factor_inv64, nb, 1024, h->factor_smem64, h->range, L, h->dense_off_d, h->A0dense64, lv[L - 1].c,
+           h->c_prev, h->Ainv64, h->fac_valid);
+    CoarseArgs ca;
+    fill_coarse_args(h, ca);
+    ca.Ainv64 = h->Ainv64;
+    const int g0 = grid_rows(n0, lv[0].S);
+    for (int it = 0; it < p.iterations; ++it) {
+        LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, h->d32, h->slot_of, h->slots);
+        LAUNCH(h, k_mx_rhs, grid_for(n0), kBlock, 0, n0, h->b0_64, h->slot_ptr, h->slots, h->b64);
+        for (int pass = 0; pass < p.refinement_passes; ++pass) {
+            float4* ea = h->d;
+            float4* eb = h->d2;
+            LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->dd64,
+                   h->b64, lv[0].dinv, h->r32, ea, p.pre_sweeps > 0 ? 1 : 0);
+            for (int k = 1; k < p.pre_sweeps; ++k) {
+                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
+                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0);
+                std::swap(ea, eb);
+            }
+            LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
+                   ea, h->r32, lv[0].res);
+            launch_coarse(h, ca);
+            LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, ea);
+            for (int k = 0; k < p.post_sweeps; ++k) {
+                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
+                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0);
+                std::swap(ea, eb);
+            }
+            LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
+        }
+    }
+    LAUNCH(h, k_mx_finish, grid_for(n0), kBlock, 0, n0, h->s64, h->dd64, h->x64, h->v64, h->x, 1.0 / (double)p.dt,
+           h->nonfinite);
+}
+
 void enqueue_frame(mgsb_solver* h) {
     h->launches = 0;
-    if (is_mg(h))
+    if (is_mg(h) && h->p.precision == MGSB_PRECISION_MIXED)
+        enqueue_mixed_frame(h);
+    else if (is_mg(h))
         enqueue_mg_frame(h);
     else
         enqueue_ref_frame(h);
@@ -628,8 +743,8 @@ mgsb_status validate_params(mgsb_solver* h, const mgsb_params& p) {
         if (p.levels < 2 || p.levels > 12) return set_err(h, MGSB_INVALID_ARG, "levels must be in [2,12]");
         if (p.pre_sweeps < 0 || p.post_sweeps < 0 || p.refinement_passes < 1)
             return set_err(h, MGSB_INVALID_ARG, "bad sweep/refinement counts");
-        if (p.precision != MGSB_PRECISION_FP32)
-            return set_err(h, MGSB_NOT_SUPPORTED, "precision %d not available in this build", p.precision);
+        if (p.precision != MGSB_PRECISION_FP32 && p.precision != MGSB_PRECISION_MIXED)
+            return set_err(h, MGSB_INVALID_ARG, "unknown precision %d", p.precision);
     }
     return MGSB_OK;
 }
@@ -694,6 +809,15 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     TRY(dalloc(hp, pool, &h->cflag, N0));
     TRY(dalloc(hp, pool, &h->cdepth, N0));
     TRY(dalloc(hp, pool, &h->nonfinite, 1));
+    if (h->p.precision == MGSB_PRECISION_MIXED) {
+        TRY(dalloc(hp, pool, &h->x64, N0));
+        TRY(dalloc(hp, pool, &h->v64, N0));
+        std::vector<double4> x(N0);
+        for (const BodyHost& B : h->bodies)
+            for (int i = 0; i < B.V; ++i) x[B.v_off + i] = make_double4(B.rest[3 * i], B.rest[3 * i + 1], B.rest[3 * i + 2], 0.0);
+        CUDA_TRY(hp, cudaMemcpy(h->x64, x.data(), N0 * sizeof(double4), cudaMemcpyHostToDevice));
+        CUDA_TRY(hp, cudaMemset(h->v64, 0, N0 * sizeof(double4)));
+    }
     TRY(dalloc(hp, pool, &h->bodies_dev, nbodies));
     TRY(dalloc(hp, pool, &h->spheres_dev, 1));
     {
@@ -870,6 +994,17 @@ mgsb_status mgsb_get_velocities(mgsb_solver* h, int32_t body, float* out) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
     TRY(sync_check(h));
+    if (h->v64) {
+        const BodyHost& B = h->bodies[body];
+        std::vector<double4> tmp(B.V);
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->v64 + B.v_off, B.V * sizeof(double4), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < B.V; ++i) {
+            out[3 * i] = (float)tmp[i].x;
+            out[3 * i + 1] = (float)tmp[i].y;
+            out[3 * i + 2] = (float)tmp[i].z;
+        }
+        return MGSB_OK;
+    }
     return copy_body_f4(h, body, h->v, [&](int i, float4 v) {
         out[3 * i] = v.x;
         out[3 * i + 1] = v.y;
@@ -893,7 +1028,17 @@ mgsb_status mgsb_get_all_positions(mgsb_solver* h, float* out) {
 mgsb_status mgsb_get_positions_f64(mgsb_solver* h, int32_t body, double* out) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
-    return set_err(h, MGSB_NOT_SUPPORTED, "FP64 positions exist only in mixed precision");
+    if (!h->x64) return set_err(h, MGSB_NOT_SUPPORTED, "FP64 positions exist only in mixed precision");
+    TRY(sync_check(h));
+    const BodyHost& B = h->bodies[body];
+    std::vector<double4> tmp(B.V);
+    CUDA_TRY(h, cudaMemcpy(tmp.data(), h->x64 + B.v_off, B.V * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < B.V; ++i) {
+        out[3 * i] = tmp[i].x;
+        out[3 * i + 1] = tmp[i].y;
+        out[3 * i + 2] = tmp[i].z;
+    }
+    return MGSB_OK;
 }
 
 mgsb_status mgsb_get_contact_flags(mgsb_solver* h, int32_t body, int32_t* out) {
@@ -978,6 +1123,17 @@ mgsb_status mgsb_set_state(mgsb_solver* h, int32_t body, const float* positions,
     if (velocities) {
         for (int i = 0; i < B.V; ++i) tmp[i] = make_float4(velocities[3 * i], velocities[3 * i + 1], velocities[3 * i + 2], 0.f);
         CUDA_TRY(h, cudaMemcpy(h->v + B.v_off, tmp.data(), B.V * sizeof(float4), cudaMemcpyHostToDevice));
+    }
+    if (h->x64) {
+        std::vector<double4> t64(B.V);
+        if (positions) {
+            for (int i = 0; i < B.V; ++i) t64[i] = make_double4(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], 0.0);
+            CUDA_TRY(h, cudaMemcpy(h->x64 + B.v_off, t64.data(), B.V * sizeof(double4), cudaMemcpyHostToDevice));
+        }
+        if (velocities) {
+            for (int i = 0; i < B.V; ++i) t64[i] = make_double4(velocities[3 * i], velocities[3 * i + 1], velocities[3 * i + 2], 0.0);
+            CUDA_TRY(h, cudaMemcpy(h->v64 + B.v_off, t64.data(), B.V * sizeof(double4), cudaMemcpyHostToDevice));
+        }
     }
     CUDA_TRY(h, cudaMemset(h->nonfinite, 0, sizeof(int32_t)));
     return MGSB_OK;
@@ -1075,6 +1231,22 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     CUDA_TRY(h, cudaMalloc(&sv, nbytes));
     cudaMemcpyAsync(sx, h->x, nbytes, cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(sv, h->v, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+    double4 *sx64 = nullptr, *sv64 = nullptr;
+    const size_t nbytes64 = (size_t)h->N0 * sizeof(double4);
+    if (h->x64) {
+        CUDA_TRY(h, cudaMalloc(&sx64, nbytes64));
+        CUDA_TRY(h, cudaMalloc(&sv64, nbytes64));
+        cudaMemcpyAsync(sx64, h->x64, nbytes64, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(sv64, h->v64, nbytes64, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    auto restore = [&]() {
+        cudaMemcpyAsync(h->x, sx, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->v, sv, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+        if (h->x64) {
+            cudaMemcpyAsync(h->x64, sx64, nbytes64, cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync(h->v64, sv64, nbytes64, cudaMemcpyDeviceToDevice, h->stream);
+        }
+    };
     struct Cand {
         int cluster, block, fuse;
     };
@@ -1101,8 +1273,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
         apply_tuning(h);
         invalidate_graph(h);
         cudaMemsetAsync(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t), h->stream);
-        cudaMemcpyAsync(h->x, sx, nbytes, cudaMemcpyDeviceToDevice, h->stream);
-        cudaMemcpyAsync(h->v, sv, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+        restore();
         if ((st = step_once(h)) != MGSB_OK) break;   // warm-up: capture + coarsest factorisation
         cudaEventRecord(a, h->stream);
         for (int f = 0; f < frames && st == MGSB_OK; ++f) st = step_once(h);
@@ -1128,11 +1299,12 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     invalidate_graph(h);
     const mgsb_status st2 = MGSB_OK;
     cudaMemsetAsync(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t), h->stream);
-    cudaMemcpyAsync(h->x, sx, nbytes, cudaMemcpyDeviceToDevice, h->stream);
-    cudaMemcpyAsync(h->v, sv, nbytes, cudaMemcpyDeviceToDevice, h->stream);
+    restore();
     cudaStreamSynchronize(h->stream);
     cudaFree(sx);
     cudaFree(sv);
+    if (sx64) cudaFree(sx64);
+    if (sv64) cudaFree(sv64);
     if (st != MGSB_OK) return st;
     if (st2 != MGSB_OK) return st2;
     if (chosen) {

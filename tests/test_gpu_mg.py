@@ -194,3 +194,51 @@ def test_autotune_restores_state(lib, oracle_built):
     s.step(5)
     o.step(5)
     assert np.abs(s.positions() - o.positions()).max() < 1e-5 * m.bbox_diagonal()
+
+
+def test_mixed_precision_matches_oracle(lib, oracle_built):
+    """Mixed precision (FP64 state and outer residual, FP32 V-cycle correction,
+    FP64 coarsest, 2 refinement passes) vs the FP64 oracle running 2 V-cycles
+    per PD iteration; closer to the oracle than the all-FP32 form."""
+    m, fixed = beam(4, 40, 4)
+    path = capsule_path(60, start=(0.0, 0.0, 1.4))
+    errs = {}
+    for prec in (mg.PRECISION_FP32, mg.PRECISION_MIXED):
+        p = mg_params(levels=3, precision=prec, refinement_passes=2)
+        s, o = _pair(m, fixed, p)
+        for f in range(60):
+            for solver in (s, o):
+                solver.set_capsule(*path[f], 0.3)
+                solver.step()
+        xo = o.positions()
+        errs[prec] = np.abs(s.positions().astype(np.float64) - xo).max()
+        if prec == mg.PRECISION_MIXED:
+            x64 = s.positions_f64()
+            errs["f64"] = np.abs(x64 - xo).max()
+            assert np.array_equal(np.nonzero(s.contact_flags())[0], np.nonzero(o.contact_flags())[0])
+        s.close()
+    tol = 1e-5 * m.bbox_diagonal()
+    assert errs[mg.PRECISION_MIXED] < tol and errs["f64"] < tol, errs
+    assert errs["f64"] <= errs[mg.PRECISION_FP32], errs
+
+
+@pytest.mark.slow
+def test_config2_mixed_precision(lib, oracle_built):
+    """Config 2: 24x240x24 hexes (829,440 tets), 5 levels, per-tet E log-uniform in
+    [5e4, 2e5] (seed 7), mixed precision with 2 refinement passes, config-1 tool path."""
+    m, fixed = beam(24, 240, 24)
+    rng = np.random.default_rng(7)
+    E = np.exp(rng.uniform(np.log(5e4), np.log(2e5), m.num_tets)).astype(np.float32)
+    p = mg_params(levels=5, gravity=(0, 0, 0), precision=mg.PRECISION_MIXED, refinement_passes=2)
+    s, o = _pair(m, fixed, p)
+    s.set_material(E, 0.3)
+    o.set_material(E, 0.3)
+    path = capsule_path(12, start=(0.0, 0.0, 1.25))
+    for f in range(12):
+        for solver in (s, o):
+            solver.set_capsule(*path[f], 0.3)
+            solver.step()
+    xo = o.positions()
+    assert np.abs(s.positions_f64() - xo).max() < 1e-5 * m.bbox_diagonal()
+    assert np.array_equal(np.nonzero(s.contact_flags())[0], np.nonzero(o.contact_flags())[0])
+    assert o.contact_flags().sum() > 0
