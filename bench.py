@@ -345,9 +345,8 @@ def run_ours(args):
             e2e_evs[k][0].record(stream)
             apply_tool(solver, tool(frame))
             solver.step()
-            for b in range(len(meshes)):
-                solver.positions(b)
-                solver.contacts(b)
+            solver.all_positions()
+            solver.all_contact_flags()
             e2e_evs[k][1].record(stream)
             frame += 1
         torch.cuda.synchronize()

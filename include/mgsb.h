@@ -162,6 +162,9 @@ mgsb_status mgsb_get_all_positions(mgsb_solver* h, float* out);
 mgsb_status mgsb_get_positions_f64(mgsb_solver* h, int32_t body, double* out);
 /* Per-vertex contact flag (1 = in contact this frame) — m_tetVertIsCollide. */
 mgsb_status mgsb_get_contact_flags(mgsb_solver* h, int32_t body, int32_t* out /* [V] */);
+/* Contact flags of every body, concatenated in body order (one copy).  No
+ * reference counterpart (the reference simulates one body). */
+mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out /* [sum V] */);
 /* Contact vertex indices, ascending.  *n receives the count; if cap < count
  * only cap entries are written and MGSB_INVALID_ARG is returned. */
 mgsb_status mgsb_get_contacts(mgsb_solver* h, int32_t body, int32_t* idx, size_t cap, size_t* n);

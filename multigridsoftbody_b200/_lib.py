@@ -105,6 +105,7 @@ SIGNATURES = [
     ("mgsb_get_all_positions", C.c_int, [_P, _FP]),
     ("mgsb_get_positions_f64", C.c_int, [_P, C.c_int32, _DP]),
     ("mgsb_get_contact_flags", C.c_int, [_P, C.c_int32, _IP]),
+    ("mgsb_get_all_contact_flags", C.c_int, [_P, _IP]),
     ("mgsb_get_contacts", C.c_int, [_P, C.c_int32, _IP, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("mgsb_get_collision_depth", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_get_device_positions", C.c_int, [_P, C.c_int32, C.POINTER(_FP)]),

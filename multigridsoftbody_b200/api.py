@@ -281,6 +281,12 @@ class Solver:
         _check(self._lib.mgsb_get_all_positions(self.h, _fptr(out)), self.h)
         return out
 
+    def all_contact_flags(self) -> np.ndarray:
+        n = sum(self.num_verts(b) for b in range(self.num_bodies))
+        out = np.empty(n, np.int32)
+        _check(self._lib.mgsb_get_all_contact_flags(self.h, _iptr(out)), self.h)
+        return out
+
     def positions_f64(self, body: int = 0) -> np.ndarray:
         out = np.empty((self.num_verts(body), 3), np.float64)
         _check(self._lib.mgsb_get_positions_f64(self.h, body, out.ctypes.data_as(C.POINTER(C.c_double))), self.h)

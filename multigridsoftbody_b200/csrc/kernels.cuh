@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
     float4* __restrict__ v, const float* __restrict__ fixf, const float* __restrict__ mass, const float* __restrict__ vdiag,
     const int32_t* __restrict__ slot_ptr, const float4* __restrict__ slots, const SphereSet* __restrict__ spheres,
     float kc, float dt, float omega, double relax, int last_iter, int32_t* __restrict__ cflag, float* __restrict__ cdepth,
-    int32_t* __restrict__ nonfinite) {
+    float* __restrict__ cenergy, int32_t* __restrict__ nonfinite) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float fx = 0.f, fy = 0.f, fz = 0.f;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
     const float p[3] = {p4.x, p4.y, p4.z};
     float cd[3] = {0.f, 0.f, 0.f}, cf[3] = {0.f, 0.f, 0.f};
     int flag = 0;
-    float depth = 0.f;
+    float depth = 0.f, ce = 0.f;
     const int nsph = spheres->count;
     for (int q = 0; q < nsph; ++q) {
         if (!spheres->active[q]) continue;
@@ -169,6 +169,8 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
                 cd[a] += kc * nrm[a] * nrm[a];
                 cf[a] += kc * t * ndd * nrm[a];
             }
+            const float pe = (p[0] - colP[0]) * nrm[0] + (p[1] - colP[1]) * nrm[1] + (p[2] - colP[2]) * nrm[2];
+            ce += kc * pe * pe;
         }
     }
     const float fix = __ldg(fixf + i);
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
         v[i] = make_float4((xn.x - l4.x) / dt, (xn.y - l4.y) / dt, (xn.z - l4.z) / dt, 0.f);
         cflag[i] = flag;
         cdepth[i] = depth;
+        cenergy[i] = ce;
         if (!isfinite(xn.x) || !isfinite(xn.y) || !isfinite(xn.z)) atomicOr(nonfinite, 1);
     }
 }

@@ -623,40 +623,42 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
 }
 
 // ---------------------------------------------------------------------------
-// Coarsest level per body (one CTA): A = A0 + diag(c); Cholesky A = L L^T in
-// shared memory, X = L^-1 in place (row by row), then A^-1 = X^T X written to
-// global memory.  Skipped when c is unchanged since the last factorisation.
+// Coarsest level: explicit inverse of A = A0 + diag(c) per body, refreshed
+// only when the lumped contact stiffness c changed.  A0^-1 = B0 is computed
+// once at set-up; with k coarsest vertices in contact (K = {i : c_i != 0}) the
+// inverse follows from the Woodbury identity
+//     A^-1 = B0 - U S^-1 U^T,   U = B0[:, K],   S = diag(1/c_K) + B0[K, K],
+// an n*n*k update instead of a fresh O(n^3) factorisation.  Above
+// kWoodburyMaxRank contacts it falls back to Cholesky + explicit inverse of A.
+// One CTA of 1024 threads per body; T = float or double.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_coarsest_factor_inv(const int2* __restrict__ range, int L,
-                                                              const int32_t* __restrict__ dense_off,
-                                                              const float* __restrict__ A0, const float* __restrict__ c,
-                                                              float* __restrict__ c_prev, float* __restrict__ Ainv,
-                                                              int32_t* __restrict__ valid) {
-    extern __shared__ float sm[];
-    const int2 rg = range[blockIdx.x * L + (L - 1)];
-    const int n = rg.y, off = rg.x;
-    const float* A = A0 + dense_off[blockIdx.x];
-    float* Ai = Ainv + dense_off[blockIdx.x];
-    __shared__ int changed;
-    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        if (c[off + i] != c_prev[off + i]) changed = 1;
-    __syncthreads();
-    if (!changed) return;
-    float* M = sm;            // n*n
-    float* tmp = sm + n * n;  // n
+constexpr int kWoodburyMaxRank = 64;
+
+// Shared memory (elements of T) either path needs for an n x n block.
+__host__ __device__ inline size_t coarsest_smem_elems(int n) {
+    const size_t k = (size_t)(n < kWoodburyMaxRank ? n : kWoodburyMaxRank);
+    const size_t refactor = (size_t)n * n + n;
+    const size_t woodbury = 2 * k * n + k * k;
+    return refactor > woodbury ? refactor : woodbury;
+}
+
+// Cholesky (right-looking, L_jj on the diagonal), X = L^-1 in place row by
+// row, then A^-1 = X^T X.
+template <typename T>
+__device__ void coarsest_refactor(int n, const T* __restrict__ A, const float* __restrict__ c, T* __restrict__ Ai,
+                                  T* sm) {
+    T* M = sm;            // n*n
+    T* tmp = sm + n * n;  // n
     for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
         const int i = q / n, j = q - i * n;
-        float a = A[q];
-        if (i == j) a += c[off + i];
+        T a = A[q];
+        if (i == j) a += (T)c[i];
         M[q] = a;
     }
     __syncthreads();
-    // Cholesky, right-looking; the diagonal holds L_jj afterwards
     for (int j = 0; j < n; ++j) {
-        const float d = sqrtf(M[j * n + j]);
-        const float id = 1.f / d;
+        const T d = sqrt(M[j * n + j]);
+        const T id = T(1) / d;
         __syncthreads();
         if (threadIdx.x == 0) M[j * n + j] = d;
         for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i * n + j] *= id;
@@ -673,13 +675,13 @@ __global__ void __launch_bounds__(1024) k_coarsest_factor_inv(const int2* __rest
         }
         __syncthreads();
     }
-    // X = L^-1 in place, row by row: X_ii = 1/L_ii, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
+    // X_ii = 1/L_ii, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int i = 0; i < n; ++i) {
-        const float xii = 1.f / M[i * n + i];
+        const T xii = T(1) / M[i * n + i];
         for (int j = wid; j < i; j += nw) {
-            float s = 0.f;
-            for (int k = j + lane; k < i; k += 32) s = fmaf(M[i * n + k], M[k * n + j], s);
+            T s = 0;
+            for (int k = j + lane; k < i; k += 32) s = fma(M[i * n + k], M[k * n + j], s);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) tmp[j] = -xii * s;
@@ -693,11 +695,109 @@ __global__ void __launch_bounds__(1024) k_coarsest_factor_inv(const int2* __rest
     for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
         const int i = q / n, j = q - i * n;
         const int k0 = i > j ? i : j;
-        float s = 0.f;
-        for (int k = k0; k < n; ++k) s = fmaf(M[k * n + i], M[k * n + j], s);
+        T s = 0;
+        for (int k = k0; k < n; ++k) s = fma(M[k * n + i], M[k * n + j], s);
         Ai[q] = s;
     }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) c_prev[off + i] = c[off + i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarsest_update(const int2* __restrict__ range, int L,
+                                                          const int32_t* __restrict__ dense_off,
+                                                          const T* __restrict__ A0, const T* __restrict__ B0,
+                                                          const float* __restrict__ c, float* __restrict__ c_prev,
+                                                          T* __restrict__ Ainv, int32_t* __restrict__ valid) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* sm = reinterpret_cast<T*>(sm_raw);
+    __shared__ int changed, k;
+    __shared__ int K[kWoodburyMaxRank];
+    const int2 rg = range[blockIdx.x * L + (L - 1)];
+    const int n = rg.y, off = rg.x;
+    const T* A = A0 + dense_off[blockIdx.x];
+    const T* B = B0 + dense_off[blockIdx.x];
+    T* Ai = Ainv + dense_off[blockIdx.x];
+    const float* cb = c + off;
+    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (cb[i] != c_prev[off + i]) changed = 1;
+    __syncthreads();
+    if (!changed) return;
+    // K in ascending order: warp 0 compacts 32 rows at a time with a ballot
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int cnt = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            const bool hit = i < n && cb[i] != 0.f;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+            if (hit && pos < kWoodburyMaxRank) K[pos] = i;
+            cnt += __popc(m);
+        }
+        if (lane == 0) k = cnt;
+    }
+    __syncthreads();
+    const int kk = k;
+    if (kk > kWoodburyMaxRank) {
+        coarsest_refactor<T>(n, A, cb, Ai, sm);
+    } else if (kk == 0) {
+        for (int q = threadIdx.x; q < n * n; q += blockDim.x) Ai[q] = B[q];
+    } else {
+        T* Ut = sm;                 // kk x n: rows K of B0 (= columns, B0 symmetric)
+        T* W = sm + kk * n;         // kk x n: S^-1 Ut
+        T* S = sm + 2 * kk * n;     // kk x kk
+        for (int q = threadIdx.x; q < kk * n; q += blockDim.x) {
+            const int a = q / n, i = q - a * n;
+            Ut[q] = B[K[a] * n + i];
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < kk * kk; q += blockDim.x) {
+            const int a = q / kk, b = q - a * kk;
+            T v = Ut[a * n + K[b]];
+            if (a == b) v += T(1) / (T)cb[K[a]];
+            S[q] = v;
+        }
+        __syncthreads();
+        // Cholesky of S in one warp (lower triangle, L_jj on the diagonal)
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            for (int j = 0; j < kk; ++j) {
+                const T d = sqrt(S[j * kk + j]);
+                __syncwarp();
+                for (int i = j + 1 + lane; i < kk; i += 32) S[i * kk + j] /= d;
+                __syncwarp();
+                if (lane == 0) S[j * kk + j] = d;
+                for (int i = j + 1 + lane; i < kk; i += 32) {
+                    const T lij = S[i * kk + j];
+                    for (int l = j + 1; l <= i; ++l) S[i * kk + l] -= lij * S[l * kk + j];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // W[:, i] = S^-1 Ut[:, i]: forward then backward substitution, one column per thread
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            for (int a = 0; a < kk; ++a) {
+                T s = Ut[a * n + i];
+                for (int b = 0; b < a; ++b) s -= S[a * kk + b] * W[b * n + i];
+                W[a * n + i] = s / S[a * kk + a];
+            }
+            for (int a = kk - 1; a >= 0; --a) {
+                T s = W[a * n + i];
+                for (int b = a + 1; b < kk; ++b) s -= S[b * kk + a] * W[b * n + i];
+                W[a * n + i] = s / S[a * kk + a];
+            }
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+            const int i = q / n, j = q - i * n;
+            T s = B[q];
+            for (int a = 0; a < kk; ++a) s -= Ut[a * n + i] * W[a * n + j];
+            Ai[q] = s;
+        }
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) c_prev[off + i] = cb[i];
     if (threadIdx.x == 0) valid[blockIdx.x] = 1;
 }
 

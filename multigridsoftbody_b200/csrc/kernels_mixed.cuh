@@ -74,7 +74,7 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
                                    const uint8_t* __restrict__ is_surf, float kc, const float* __restrict__ diag0,
                                    float omega, int32_t* __restrict__ cflag, float* __restrict__ c0,
                                    double4* __restrict__ b0, float* __restrict__ dfull, float* __restrict__ dinv,
-                                   double4* __restrict__ d64, float4* __restrict__ d32) {
+                                   double4* __restrict__ d64, float4* __restrict__ d32, float4* __restrict__ target) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int flag = 0;
@@ -85,6 +85,7 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
     const float c = (flag && free_v) ? kc : 0.f;
     cflag[i] = flag;
     c0[i] = c;
+    target[i] = make_float4((float)tg.x, (float)tg.y, (float)tg.z, 0.f);
     b0[i] = c != 0.f ? make_double4((double)c * (tg.x - sv.x), (double)c * (tg.y - sv.y), (double)c * (tg.z - sv.z), 0.0) : d4z();
     const float D = __ldg(diag0 + i) + c;
     dfull[i] = D;
@@ -109,12 +110,12 @@ __global__ void __launch_bounds__(256) k_mx_rhs(int n, const double4* __restrict
     b[i] = acc;
 }
 
-// Outer FP64 residual r = b - A d with A = diag + off-diagonal (FP64 values),
-// stored as FP32 for the correction V-cycle, fused with its first Jacobi
+// Outer FP64 residual r = b - A d with A = diag + c + off-diagonal (FP64
+// values; c = this frame's contact stiffness), stored as FP32 for the correction V-cycle, fused with its first Jacobi
 // sweep from a zero guess: e = dinv r.  4 lanes per row.
 __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
-                                                     const double* __restrict__ val, const double* __restrict__ dfull64,
-                                                     const double4* __restrict__ d, const double4* __restrict__ b,
+                                                     const double* __restrict__ val, const double* __restrict__ diag64,
+                                                     const float* __restrict__ c, const double4* __restrict__ d, const double4* __restrict__ b,
                                                      const float* __restrict__ dinv, float4* __restrict__ r32,
                                                      float4* __restrict__ e, int first_sweep) {
     constexpr int G = kLanesL0, S = 32 / G;
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
     }
     if (!valid || lane >= S) return;
     const double4 x = d[row], bi = b[row];
-    const double D = __ldg(dfull64 + row);
+    const double D = __ldg(diag64 + row) + (double)__ldg(c + row);
     const float rx = (float)(bi.x - fma(D, x.x, ax)), ry = (float)(bi.y - fma(D, x.y, ay)), rz = (float)(bi.z - fma(D, x.z, az));
     r32[row] = make_float4(rx, ry, rz, 0.f);
     const float w = first_sweep ? __ldg(dinv + row) : 0.f;
@@ -180,77 +181,5 @@ __global__ void k_mx_finish(int n, const double4* __restrict__ s, const double4*
     if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) atomicOr(nonfinite, 1);
 }
 
-// Coarsest level in FP64: Cholesky + explicit inverse (same algorithm as
-// k_coarsest_factor_inv).
-__global__ void __launch_bounds__(1024) k_coarsest_factor_inv64(const int2* __restrict__ range, int L,
-                                                                const int32_t* __restrict__ dense_off,
-                                                                const double* __restrict__ A0, const float* __restrict__ c,
-                                                                float* __restrict__ c_prev, double* __restrict__ Ainv,
-                                                                int32_t* __restrict__ valid) {
-    extern __shared__ double smd[];
-    const int2 rg = range[blockIdx.x * L + (L - 1)];
-    const int n = rg.y, off = rg.x;
-    const double* A = A0 + dense_off[blockIdx.x];
-    double* Ai = Ainv + dense_off[blockIdx.x];
-    __shared__ int changed;
-    if (threadIdx.x == 0) changed = valid[blockIdx.x] ? 0 : 1;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-        if (c[off + i] != c_prev[off + i]) changed = 1;
-    __syncthreads();
-    if (!changed) return;
-    double* M = smd;
-    double* tmp = smd + n * n;
-    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-        const int i = q / n, j = q - i * n;
-        double a = A[q];
-        if (i == j) a += c[off + i];
-        M[q] = a;
-    }
-    __syncthreads();
-    for (int j = 0; j < n; ++j) {
-        const double dd = sqrt(M[j * n + j]);
-        const double id = 1.0 / dd;
-        __syncthreads();
-        if (threadIdx.x == 0) M[j * n + j] = dd;
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i * n + j] *= id;
-        __syncthreads();
-        const int m = n - j - 1;
-        const int tot = m * (m + 1) / 2;
-        for (int q = threadIdx.x; q < tot; q += blockDim.x) {
-            int a = (int)((sqrtf(8.f * (float)q + 1.f) - 1.f) * 0.5f);
-            while ((a + 1) * (a + 2) / 2 <= q) ++a;
-            while (a * (a + 1) / 2 > q) --a;
-            const int bcol = q - a * (a + 1) / 2;
-            const int i = j + 1 + a, k = j + 1 + bcol;
-            M[i * n + k] -= M[i * n + j] * M[k * n + j];
-        }
-        __syncthreads();
-    }
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int i = 0; i < n; ++i) {
-        const double xii = 1.0 / M[i * n + i];
-        for (int j = wid; j < i; j += nw) {
-            double s = 0.0;
-            for (int k = j + lane; k < i; k += 32) s = fma(M[i * n + k], M[k * n + j], s);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) tmp[j] = -xii * s;
-        }
-        __syncthreads();
-        for (int j = threadIdx.x; j < i; j += blockDim.x) M[i * n + j] = tmp[j];
-        if (threadIdx.x == 0) M[i * n + i] = xii;
-        __syncthreads();
-    }
-    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-        const int i = q / n, j = q - i * n;
-        const int k0 = i > j ? i : j;
-        double s = 0.0;
-        for (int k = k0; k < n; ++k) s = fma(M[k * n + i], M[k * n + j], s);
-        Ai[q] = s;
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) c_prev[off + i] = c[off + i];
-    if (threadIdx.x == 0) valid[blockIdx.x] = 1;
-}
 
 }  // namespace mgsb

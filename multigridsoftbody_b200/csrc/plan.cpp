@@ -315,6 +315,15 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
             P.dense.push_back((float)q);
             P.dense64.push_back(q);
         }
+        std::vector<double> inv;
+        if (!spd_inverse(d, C.n, inv)) {
+            err = "coarsest-level matrix of body " + std::to_string(bi) + " is not positive definite";
+            return false;
+        }
+        for (double q : inv) {
+            P.dense_inv.push_back((float)q);
+            P.dense_inv64.push_back(q);
+        }
         P.max_coarsest = std::max(P.max_coarsest, C.n);
     }
     // ---- surface vertices

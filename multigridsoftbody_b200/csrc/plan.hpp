@@ -53,6 +53,8 @@ struct Plan {
     std::vector<PlanLevel> levels;            // [0] = finest (matrix only)
     std::vector<float> dense;                 // coarsest dense blocks (row-major per body)
     std::vector<double> dense64;              // the same in FP64
+    std::vector<float> dense_inv;             // inverse of each block without contact (Woodbury base)
+    std::vector<double> dense_inv64;
     std::vector<double> diag64;               // level-0 diagonal in FP64
     std::vector<uint8_t> is_surf;             // per vertex: on the boundary surface
     std::vector<int32_t> cl_off, cl_n, dense_off;

@@ -292,4 +292,38 @@ void dense_from_sparse(const SparseSym& A, const std::vector<uint8_t>& active, s
     }
 }
 
+bool spd_inverse(const std::vector<double>& A, int n, std::vector<double>& inv) {
+    std::vector<double> Lm(A);   // lower triangle: L
+    for (int j = 0; j < n; ++j) {
+        double d = Lm[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) d -= Lm[(size_t)j * n + k] * Lm[(size_t)j * n + k];
+        if (!(d > 0.0)) return false;
+        d = std::sqrt(d);
+        Lm[(size_t)j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double s = Lm[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) s -= Lm[(size_t)i * n + k] * Lm[(size_t)j * n + k];
+            Lm[(size_t)i * n + j] = s / d;
+        }
+    }
+    // X = L^-1 (lower), then A^-1 = X^T X
+    std::vector<double> X((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        X[(size_t)j * n + j] = 1.0 / Lm[(size_t)j * n + j];
+        for (int i = j + 1; i < n; ++i) {
+            double s = 0.0;
+            for (int k = j; k < i; ++k) s += Lm[(size_t)i * n + k] * X[(size_t)k * n + j];
+            X[(size_t)i * n + j] = -s / Lm[(size_t)i * n + i];
+        }
+    }
+    inv.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double s = 0.0;
+            for (int k = i; k < n; ++k) s += X[(size_t)k * n + i] * X[(size_t)k * n + j];
+            inv[(size_t)i * n + j] = inv[(size_t)j * n + i] = s;
+        }
+    return true;
+}
+
 }  // namespace mgsb

@@ -61,5 +61,7 @@ void default_grid_dims(const double* pos, int num_verts, const int32_t* tets, in
 
 // Row-major dense copy of a level matrix; inactive rows/cols become identity.
 void dense_from_sparse(const SparseSym& A, const std::vector<uint8_t>& active, std::vector<double>& dense);
+// Inverse of a row-major SPD matrix (Cholesky in FP64); false if not SPD.
+bool spd_inverse(const std::vector<double>& A, int n, std::vector<double>& inv);
 
 }  // namespace mgsb

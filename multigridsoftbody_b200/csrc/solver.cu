@@ -12,6 +12,7 @@
 
 #include "../../include/mgsb.h"
 #include "kernels.cuh"
+#include "kernels_diag.cuh"
 #include "kernels_mg.cuh"
 #include "kernels_mixed.cuh"
 #include "mesh.hpp"
@@ -90,10 +91,13 @@ struct mgsb_solver {
     char* stage[kStage] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t stage_ev[kStage] = {nullptr, nullptr, nullptr, nullptr};
     int stage_idx = 0;
+    // pinned host buffer for readbacks (N0 x 16 bytes: positions, velocities, flags)
+    char* readback = nullptr;
     // ---- state (kept across rebuilds)
     float4 *x = nullptr, *xb = nullptr, *v = nullptr, *s = nullptr, *last = nullptr, *prev = nullptr;
     int32_t* cflag = nullptr;
     float* cdepth = nullptr;
+    float* cenergy = nullptr;    // reference kind: contact energy of the last iteration
     int32_t* nonfinite = nullptr;
     BodyDev* bodies_dev = nullptr;
     SphereSet* spheres_dev = nullptr;
@@ -114,14 +118,26 @@ struct mgsb_solver {
     double4 *x64 = nullptr, *v64 = nullptr, *s64 = nullptr, *last64 = nullptr, *dd64 = nullptr, *b64 = nullptr,
             *b0_64 = nullptr;
     float4 *d32 = nullptr, *r32 = nullptr;
-    double *ell_val64 = nullptr, *diag64 = nullptr, *A0dense64 = nullptr, *Ainv64 = nullptr;
+    double *ell_val64 = nullptr, *diag64 = nullptr, *A0dense64 = nullptr, *B0dense64 = nullptr, *Ainv64 = nullptr;
     uint8_t* is_surf = nullptr;
     size_t factor_smem64 = 0;
     float* c0 = nullptr;
     int32_t* surf = nullptr;
     int nsurf = 0;
+    float4* d_final = nullptr;   // displacement buffer that holds the last frame's d (FP32 multigrid)
+    // surface normals: triangles (global vertex ids), surface vertices, and the
+    // vertex->triangle CSR (triangle ids local to the body); per body the
+    // triangle range [f_off, f_off+nf) and surface-vertex range [sv_off, sv_off+nsv)
+    int4* nrm_tris = nullptr;
+    int32_t *nrm_sv = nullptr, *nrm_ptr = nullptr, *nrm_fidx = nullptr;
+    std::vector<int> nrm_f_off, nrm_nf, nrm_sv_off, nrm_nsv;
+    std::vector<int32_t> nrm_sv_host;
+    int nrm_max_f = 0, nrm_max_sv = 0;
+    float4 *nrm_face = nullptr, *nrm_out = nullptr;   // scratch: triangle normals, vertex normals
+    // energy reduction scratch: per-block partials and the five results
+    double *energy_part = nullptr, *energy_out = nullptr;
     std::vector<LevelDev> lev;   // lev[0] = finest
-    float *A0dense = nullptr, *Lfac = nullptr, *Ldinv = nullptr, *c_prev = nullptr;
+    float *A0dense = nullptr, *B0dense = nullptr, *Lfac = nullptr, *Ldinv = nullptr, *c_prev = nullptr;
     int2* range = nullptr;
     int32_t* dense_off_d = nullptr;
     int cluster = 1;
@@ -153,6 +169,7 @@ mgsb_solver::~mgsb_solver() {
         if (stage[k]) cudaFreeHost(stage[k]);
         if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
     }
+    if (readback) cudaFreeHost(readback);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
@@ -241,6 +258,57 @@ void invalidate_graph(mgsb_solver* h) {
         h->graph = nullptr;
     }
     h->graph_valid = false;
+}
+
+// Surface triangles of every body (extract_surface order), the surface
+// vertices in ascending order and, per surface vertex, its triangles in
+// ascending order; plus the two scratch arrays the normals pass writes.
+mgsb_status upload_normals_data(mgsb_solver* h, std::vector<DevMem>& pool) {
+    std::vector<int4> tris_all;
+    std::vector<int32_t> sv_all, ptr_all{0}, fidx_all;
+    h->nrm_f_off.clear();
+    h->nrm_nf.clear();
+    h->nrm_sv_off.clear();
+    h->nrm_nsv.clear();
+    h->nrm_max_f = h->nrm_max_sv = 0;
+    for (const BodyHost& B : h->bodies) {
+        std::vector<int32_t> tris, opp;
+        extract_surface(B.tets.data(), B.T, tris, opp);
+        const int nf = (int)(tris.size() / 3);
+        h->nrm_f_off.push_back((int)tris_all.size());
+        h->nrm_nf.push_back(nf);
+        std::vector<int32_t> cnt(B.V + 1, 0);
+        for (int f = 0; f < nf; ++f) {
+            tris_all.push_back(int4{tris[3 * f] + B.v_off, tris[3 * f + 1] + B.v_off, tris[3 * f + 2] + B.v_off, 0});
+            for (int q = 0; q < 3; ++q) ++cnt[tris[3 * f + q] + 1];
+        }
+        std::vector<int32_t> start(B.V + 1, 0);
+        for (int i = 0; i < B.V; ++i) start[i + 1] = start[i] + cnt[i + 1];
+        std::vector<int32_t> list(start[B.V]);
+        std::vector<int32_t> fill(start.begin(), start.end() - 1);
+        for (int f = 0; f < nf; ++f)
+            for (int q = 0; q < 3; ++q) list[fill[tris[3 * f + q]]++] = f;   // ascending f per vertex
+        h->nrm_sv_off.push_back((int)sv_all.size());
+        int nsv = 0;
+        for (int i = 0; i < B.V; ++i) {
+            if (start[i + 1] == start[i]) continue;
+            sv_all.push_back(i + B.v_off);
+            for (int e = start[i]; e < start[i + 1]; ++e) fidx_all.push_back(list[e]);
+            ptr_all.push_back((int32_t)fidx_all.size());
+            ++nsv;
+        }
+        h->nrm_nsv.push_back(nsv);
+        h->nrm_max_f = std::max(h->nrm_max_f, nf);
+        h->nrm_max_sv = std::max(h->nrm_max_sv, nsv);
+    }
+    h->nrm_sv_host = sv_all;
+    TRY(dupload(h, pool, &h->nrm_tris, tris_all));
+    TRY(dupload(h, pool, &h->nrm_sv, sv_all));
+    TRY(dupload(h, pool, &h->nrm_ptr, ptr_all));
+    TRY(dupload(h, pool, &h->nrm_fidx, fidx_all));
+    TRY(dalloc(h, pool, &h->nrm_face, (size_t)std::max(1, h->nrm_max_f)));
+    TRY(dalloc(h, pool, &h->nrm_out, (size_t)std::max(1, h->nrm_max_sv)));
+    return MGSB_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -335,16 +403,17 @@ mgsb_status rebuild(mgsb_solver* h) {
             BD.dense_off = P.dense_off[bi];
         }
         h->max_coarsest = P.max_coarsest;
-        h->factor_smem = ((size_t)P.max_coarsest * P.max_coarsest + P.max_coarsest) * sizeof(float);
+        h->factor_smem = coarsest_smem_elems(P.max_coarsest) * sizeof(float);
         int dev_smem = 0;
         CUDA_TRY(h, cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
         if (h->factor_smem > (size_t)dev_smem)
             return set_err(h, MGSB_NOT_SUPPORTED,
                            "coarsest level has %d vertices; its dense factor needs %zu B of shared memory (max %d): add a level",
                            P.max_coarsest, h->factor_smem, dev_smem);
-        CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_factor_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)h->factor_smem));
         TRY(dupload(h, pool, &h->A0dense, P.dense));
+        TRY(dupload(h, pool, &h->B0dense, P.dense_inv));
         TRY(dalloc(h, pool, &h->Lfac, P.dense.size()));   // explicit inverse of the coarsest matrix
         TRY(dupload(h, pool, &h->range, P.range));
         h->range_host = P.range;
@@ -379,13 +448,14 @@ mgsb_status rebuild(mgsb_solver* h) {
             TRY(dupload(h, pool, &h->ell_val64, P.levels[0].ell_val64));
             TRY(dupload(h, pool, &h->diag64, P.diag64));
             TRY(dupload(h, pool, &h->A0dense64, P.dense64));
+            TRY(dupload(h, pool, &h->B0dense64, P.dense_inv64));
             TRY(dalloc(h, pool, &h->Ainv64, P.dense64.size()));
             TRY(dupload(h, pool, &h->is_surf, P.is_surf));
-            h->factor_smem64 = ((size_t)P.max_coarsest * P.max_coarsest + P.max_coarsest) * sizeof(double);
+            h->factor_smem64 = coarsest_smem_elems(P.max_coarsest) * sizeof(double);
             if (h->factor_smem64 > (size_t)h->max_smem_optin)
                 return set_err(h, MGSB_NOT_SUPPORTED, "coarsest level has %d vertices; its FP64 factor needs %zu B of shared memory",
                                P.max_coarsest, h->factor_smem64);
-            CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_factor_inv64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            CUDA_TRY(h, cudaFuncSetAttribute(k_coarsest_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)h->factor_smem64));
         }
         h->nsurf = (int)P.surf.size();
@@ -396,6 +466,9 @@ mgsb_status rebuild(mgsb_solver* h) {
         BD.v0_off = h->bodies[bi].v_off;
         BD.v0_n = h->bodies[bi].V;
     }
+    TRY(upload_normals_data(h, pool));
+    TRY(dalloc(h, pool, &h->energy_part, (size_t)kEnergyBlocks * kEnergyTerms));
+    TRY(dalloc(h, pool, &h->energy_out, kEnergyTerms));
     h->dirty = false;
     return MGSB_OK;
 }
@@ -433,7 +506,8 @@ void enqueue_ref_frame(mgsb_solver* h) {
         omega = 4 / (4 - p.cheb_rho * p.cheb_rho * omega);
         LAUNCH(h, k_ref_vertex, grid_for(n), kBlock, 0, n, h->x, h->prev, h->s, h->last, h->v, h->fixf, h->mass,
                h->vdiag, h->slot_ptr, h->slots, h->spheres_dev, p.collision_stiffness, p.dt, omega,
-               (double)p.relaxation, it == p.iterations - 1 ? 1 : 0, h->cflag, h->cdepth, h->nonfinite);
+               (double)p.relaxation, it == p.iterations - 1 ? 1 : 0, h->cflag, h->cdepth, h->cenergy,
+               h->nonfinite);
     }
     if (p.iterations == 0) {
         // velocity only
@@ -453,6 +527,31 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs) {
         best = std::max(best, coarse_smem_float4(nl, L, cs, nl[L - 1]));
     }
     return (size_t)best * sizeof(float4);
+}
+
+// Can the device co-schedule one cluster of this shape?
+bool coarse_shape_feasible(mgsb_solver* h, int cs, int block, int fused) {
+    const size_t smem = fused ? 0 : coarse_smem_bytes(h, cs);
+    if (smem > (size_t)h->max_smem_optin) return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cs);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    const cudaError_t e = fused ? cudaOccupancyMaxActiveClusters(&nclusters, k_coarse_vcycle, &cfg)
+                                : cudaOccupancyMaxActiveClusters(&nclusters, k_coarse_vcycle_dsm, &cfg);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return nclusters > 0;
 }
 
 mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
@@ -498,8 +597,8 @@ void enqueue_mg_frame(mgsb_solver* h) {
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
                lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
-    LAUNCH(h, k_coarsest_factor_inv, nb, 1024, h->factor_smem, h->range, L, h->dense_off_d, h->A0dense, lv[L - 1].c,
-           h->c_prev, h->Lfac, h->fac_valid);
+    LAUNCH(h, k_coarsest_update<float>, nb, 1024, h->factor_smem, h->range, L, h->dense_off_d, h->A0dense, h->B0dense,
+           lv[L - 1].c, h->c_prev, h->Lfac, h->fac_valid);
     CoarseArgs ca = {};
     ca.L = L;
     ca.pre = p.pre_sweeps;
@@ -554,6 +653,7 @@ void enqueue_mg_frame(mgsb_solver* h) {
         }
     }
     LAUNCH(h, k_mg_finish, grid_for(n0), kBlock, 0, n0, h->s, xa, h->x, h->v, 1.0f / p.dt, h->nonfinite);
+    h->d_final = xa;
 }
 
 void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
@@ -601,12 +701,13 @@ void enqueue_mixed_frame(mgsb_solver* h) {
     LAUNCH(h, k_mx_predict, grid_for(n0), kBlock, 0, n0, h->x64, h->v64, h->s64, h->last64, h->s, h->x, h->fixf,
            h->body_of, h->bodies_dev, (double)p.dt);
     LAUNCH(h, k_mx_contact_frame, grid_for(n0), kBlock, 0, n0, h->s64, h->fixf, h->body_of, h->bodies_dev, h->is_surf,
-           p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32);
+           p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32,
+           h->target);
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
                lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
-    LAUNCH(h, k_coarsest_factor_inv64, nb, 1024, h->factor_smem64, h->range, L, h->dense_off_d, h->A0dense64, lv[L - 1].c,
-           h->c_prev, h->Ainv64, h->fac_valid);
+    LAUNCH(h, k_coarsest_update<double>, nb, 1024, h->factor_smem64, h->range, L, h->dense_off_d, h->A0dense64,
+           h->B0dense64, lv[L - 1].c, h->c_prev, h->Ainv64, h->fac_valid);
     CoarseArgs ca;
     fill_coarse_args(h, ca);
     ca.Ainv64 = h->Ainv64;
@@ -617,8 +718,8 @@ void enqueue_mixed_frame(mgsb_solver* h) {
         for (int pass = 0; pass < p.refinement_passes; ++pass) {
             float4* ea = h->d;
             float4* eb = h->d2;
-            LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->dd64,
-                   h->b64, lv[0].dinv, h->r32, ea, p.pre_sweeps > 0 ? 1 : 0);
+            LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
+                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, p.pre_sweeps > 0 ? 1 : 0);
             for (int k = 1; k < p.pre_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                        lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0);
@@ -800,6 +901,7 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     }
     auto& pool = h->state_mem;
     const int N0 = h->N0;
+    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback, (size_t)std::max(N0, 1) * sizeof(float4)));
     TRY(dalloc(hp, pool, &h->x, N0));
     TRY(dalloc(hp, pool, &h->xb, N0));
     TRY(dalloc(hp, pool, &h->v, N0));
@@ -808,6 +910,7 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     TRY(dalloc(hp, pool, &h->prev, N0));
     TRY(dalloc(hp, pool, &h->cflag, N0));
     TRY(dalloc(hp, pool, &h->cdepth, N0));
+    TRY(dalloc(hp, pool, &h->cenergy, N0));
     TRY(dalloc(hp, pool, &h->nonfinite, 1));
     if (h->p.precision == MGSB_PRECISION_MIXED) {
         TRY(dalloc(hp, pool, &h->x64, N0));
@@ -834,6 +937,7 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     CUDA_TRY(hp, cudaMemset(h->v, 0, N0 * sizeof(float4)));
     CUDA_TRY(hp, cudaMemset(h->cflag, 0, N0 * sizeof(int32_t)));
     CUDA_TRY(hp, cudaMemset(h->cdepth, 0, N0 * sizeof(float)));
+    CUDA_TRY(hp, cudaMemset(h->cenergy, 0, N0 * sizeof(float)));
     CUDA_TRY(hp, cudaMemset(h->nonfinite, 0, sizeof(int32_t)));
     TRY(rebuild(hp));
     *out = h.release();
@@ -844,10 +948,41 @@ template <typename F>
 mgsb_status copy_body_f4(mgsb_solver* h, int32_t body, const float4* src, F&& sink) {
     TRY(check_body(h, body));
     const BodyHost& B = h->bodies[body];
-    std::vector<float4> tmp(B.V);
-    CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), src + B.v_off, B.V * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+    float4* tmp = reinterpret_cast<float4*>(h->readback);
+    CUDA_TRY(h, cudaMemcpyAsync(tmp, src + B.v_off, B.V * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     for (int i = 0; i < B.V; ++i) sink(i, tmp[i]);
+    return MGSB_OK;
+}
+
+// Surface normals of one body from the current positions: triangle normals
+// into fscratch (>= the body's triangle count), vertex normals of the
+// surface vertices into vscratch (>= its surface-vertex count), then a copy
+// to the host and a scatter into out[3V] (zero for interior vertices).
+mgsb_status run_normals(mgsb_solver* h, int32_t body, float4* fscratch, float4* vscratch, float* out) {
+    const BodyHost& B = h->bodies[body];
+    const int nf = h->nrm_nf[body], nsv = h->nrm_nsv[body];
+    const int f_off = h->nrm_f_off[body], sv_off = h->nrm_sv_off[body];
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    if (nf > 0) {
+        k_tri_normals<<<(nf + 255) / 256, 256, 0, h->stream>>>(nf, h->nrm_tris + f_off, h->x, fscratch);
+        k_vert_normals<<<(nsv + 255) / 256, 256, 0, h->stream>>>(nsv, h->nrm_ptr + sv_off, h->nrm_fidx, fscratch, vscratch);
+        CUDA_TRY(h, cudaGetLastError());
+    }
+    std::vector<float4> vn(nsv);
+    if (nsv > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(vn.data(), vscratch, nsv * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    int32_t nf_flag = 0;
+    CUDA_TRY(h, cudaMemcpy(&nf_flag, h->nonfinite, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (nf_flag) return set_err(h, MGSB_DIVERGED, "non-finite positions detected");
+    std::fill(out, out + 3 * (size_t)B.V, 0.f);
+    for (int j = 0; j < nsv; ++j) {
+        const int i = h->nrm_sv_host[sv_off + j] - B.v_off;
+        out[3 * i] = vn[j].x;
+        out[3 * i + 1] = vn[j].y;
+        out[3 * i + 2] = vn[j].z;
+    }
     return MGSB_OK;
 }
 
@@ -1015,8 +1150,9 @@ mgsb_status mgsb_get_velocities(mgsb_solver* h, int32_t body, float* out) {
 mgsb_status mgsb_get_all_positions(mgsb_solver* h, float* out) {
     if (!h || !out) return MGSB_INVALID_ARG;
     TRY(sync_check(h));
-    std::vector<float4> tmp(h->N0);
-    CUDA_TRY(h, cudaMemcpy(tmp.data(), h->x, h->N0 * sizeof(float4), cudaMemcpyDeviceToHost));
+    const float4* tmp = reinterpret_cast<const float4*>(h->readback);
+    CUDA_TRY(h, cudaMemcpyAsync(h->readback, h->x, h->N0 * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     for (int i = 0; i < h->N0; ++i) {
         out[3 * i] = tmp[i].x;
         out[3 * i + 1] = tmp[i].y;
@@ -1046,7 +1182,18 @@ mgsb_status mgsb_get_contact_flags(mgsb_solver* h, int32_t body, int32_t* out) {
     TRY(check_body(h, body));
     TRY(sync_check(h));
     const BodyHost& B = h->bodies[body];
-    CUDA_TRY(h, cudaMemcpy(out, h->cflag + B.v_off, B.V * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpyAsync(h->readback, h->cflag + B.v_off, B.V * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(out, h->readback, B.V * sizeof(int32_t));
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out) {
+    if (!h || !out) return MGSB_INVALID_ARG;
+    TRY(sync_check(h));
+    CUDA_TRY(h, cudaMemcpyAsync(h->readback, h->cflag, h->N0 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(out, h->readback, h->N0 * sizeof(int32_t));
     return MGSB_OK;
 }
 
@@ -1086,28 +1233,8 @@ mgsb_status mgsb_get_device_positions(mgsb_solver* h, int32_t body, const float*
 mgsb_status mgsb_get_normals(mgsb_solver* h, int32_t body, float* out) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
-    // Surface normals from the current positions (host side for now).
-    const BodyHost& B = h->bodies[body];
-    std::vector<float> pos(3 * (size_t)B.V);
-    TRY(mgsb_get_positions(h, body, pos.data()));
-    std::vector<int32_t> tris, opp;
-    extract_surface(B.tets.data(), B.T, tris, opp);
-    std::vector<float> nrm(3 * (size_t)B.V, 0.f);
-    for (size_t f = 0; f < tris.size() / 3; ++f) {
-        const int a = tris[3 * f], b = tris[3 * f + 1], c = tris[3 * f + 2];
-        const float ab[3] = {pos[3 * b] - pos[3 * a], pos[3 * b + 1] - pos[3 * a + 1], pos[3 * b + 2] - pos[3 * a + 2]};
-        const float ac[3] = {pos[3 * c] - pos[3 * a], pos[3 * c + 1] - pos[3 * a + 1], pos[3 * c + 2] - pos[3 * a + 2]};
-        float n[3] = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2], ab[0] * ac[1] - ab[1] * ac[0]};
-        const float l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-        for (int q = 0; q < 3; ++q) n[q] /= l;
-        for (int v : {a, b, c})
-            for (int q = 0; q < 3; ++q) nrm[3 * v + q] += n[q];
-    }
-    for (int i = 0; i < B.V; ++i) {
-        const float l = std::sqrt(nrm[3 * i] * nrm[3 * i] + nrm[3 * i + 1] * nrm[3 * i + 1] + nrm[3 * i + 2] * nrm[3 * i + 2]);
-        for (int q = 0; q < 3; ++q) out[3 * i + q] = l > 1.1920929e-07f ? nrm[3 * i + q] / l : nrm[3 * i + q];
-    }
-    return MGSB_OK;
+    TRY(ensure_ready(h));
+    return run_normals(h, body, h->nrm_face, h->nrm_out, out);
 }
 
 mgsb_status mgsb_set_state(mgsb_solver* h, int32_t body, const float* positions, const float* velocities) {
@@ -1142,7 +1269,59 @@ mgsb_status mgsb_set_state(mgsb_solver* h, int32_t body, const float* positions,
 mgsb_status mgsb_get_energy(mgsb_solver* h, int32_t body, double out[5]) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
-    return set_err(h, MGSB_NOT_SUPPORTED, "energy diagnostics not built yet");
+    TRY(ensure_ready(h));
+    TRY(sync_check(h));
+    const BodyHost& B = h->bodies[body];
+    const mgsb_params& p = h->p;
+    EnergyArgs a{};
+    a.kind = !is_mg(h) ? kEnergyReference : (p.precision == MGSB_PRECISION_MIXED ? kEnergyMixed : kEnergyMultigrid);
+    a.v0 = B.v_off;
+    a.nv = B.V;
+    a.t0 = B.t_off;
+    a.nt = B.T;
+    a.inv_2h2 = 1.0 / (2.0 * (double)p.dt * (double)p.dt);
+    a.kv = p.volume_stiffness;
+    a.x = h->x;
+    a.s = h->s;
+    a.prev = h->prev;
+    a.x64 = a.kind == kEnergyMixed ? h->x64 : nullptr;
+    a.s64 = a.kind == kEnergyMixed ? h->s64 : nullptr;
+    // the reference kind stores density-1 masses; the multigrid kinds m/h^2
+    a.mass = h->mass;
+    if (a.kind != kEnergyReference) a.inv_2h2 = 0.5;
+    a.fixf = h->fixf;
+    a.tets = h->tets;
+    a.tA = h->tA;
+    a.tB = h->tB;
+    a.tC = h->tC;
+    a.cflag = h->cflag;
+    a.c0 = h->c0;
+    a.cenergy = h->cenergy;
+    a.target = h->target;
+    if (a.kind != kEnergyReference) {
+        // the residual exists once a frame has run
+        a.residual = a.kind == kEnergyMixed ? (h->timed ? 1 : 0) : (h->d_final ? 1 : 0);
+        a.S = h->lev[0].S;
+        a.sp = h->lev[0].slice_ptr;
+        a.col = h->lev[0].ell_col;
+        a.val = h->lev[0].ell_val;
+        a.dfull = h->lev[0].dfull;
+        a.b = h->b;
+        a.d = h->d_final;
+        a.val64 = h->ell_val64;
+        a.diag64 = h->diag64;
+        a.b64 = h->b64;
+        a.d64 = h->dd64;
+    }
+    const int work = std::max(B.V, B.T);
+    const int nblk = std::max(1, std::min(kEnergyBlocks, (work + kEnergyThreads - 1) / kEnergyThreads));
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    k_energy_partial<<<nblk, kEnergyThreads, 0, h->stream>>>(a, h->energy_part);
+    k_energy_final<<<1, kEnergyThreads, 0, h->stream>>>(h->energy_part, nblk, h->energy_out);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->energy_out, kEnergyTerms * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return MGSB_OK;
 }
 
 mgsb_status mgsb_last_frame_ms(mgsb_solver* h, float* ms) {
@@ -1256,8 +1435,9 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     for (int c : cls) {
         if (nb > 1 && c > 2) continue;   // many bodies: small clusters, one per body
         for (int blk : {256, 512, 1024}) {
-            if (coarse_smem_bytes(h, c) <= (size_t)h->max_smem_optin) cands.push_back({c, blk, 0});
-            if (blk >= 512 && c >= 2) cands.push_back({c, blk, 1});
+            if (coarse_shape_feasible(h, c, blk, 0)) cands.push_back({c, blk, 0});
+            if (blk >= 512 && c >= 2 && h->p.precision != MGSB_PRECISION_MIXED && coarse_shape_feasible(h, c, blk, 1))
+                cands.push_back({c, blk, 1});
         }
     }
     float best = 1e30f;
@@ -1274,7 +1454,14 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
         invalidate_graph(h);
         cudaMemsetAsync(h->fac_valid, 0, h->bodies.size() * sizeof(int32_t), h->stream);
         restore();
-        if ((st = step_once(h)) != MGSB_OK) break;   // warm-up: capture + coarsest factorisation
+        st = step_once(h);   // warm-up: capture + coarsest factorisation
+        if (st != MGSB_OK) {
+            // a shape the device cannot launch: skip it (the capture already ended)
+            cudaGetLastError();
+            invalidate_graph(h);
+            st = MGSB_OK;
+            continue;
+        }
         cudaEventRecord(a, h->stream);
         for (int f = 0; f < frames && st == MGSB_OK; ++f) st = step_once(h);
         cudaEventRecord(b, h->stream);

@@ -51,6 +51,7 @@ def _load():
         "oracle_level_size": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP]),
         "oracle_level_prolongation": (C.c_int, [C.c_void_p, C.c_int, _IP, _DP]),
         "oracle_level_matrix": (C.c_int, [C.c_void_p, C.c_int, _DP, _IP, _IP, _DP]),
+        "oracle_surface_normals": (None, [_DP, C.c_int32, _IP, C.c_int32, _DP]),
         "oracle_ref_rotation": (None, [_DP, _DP]),
         "oracle_svd_rotation": (None, [_DP, _DP]),
         "oracle_inverse3": (C.c_double, [_DP, _DP]),
@@ -203,3 +204,13 @@ def svd_rotation(F):
     R = np.empty(9)
     lib.oracle_svd_rotation(_dp(F), _dp(R))
     return R.reshape(3, 3)
+
+
+def surface_normals(positions, tris):
+    """Vertex normals of the triangle surface `tris` [F,3] at `positions` [V,3]."""
+    lib = _load()
+    pos = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    out = np.empty_like(pos)
+    lib.oracle_surface_normals(_dp(pos), pos.shape[0], t.ctypes.data_as(_IP), t.shape[0], _dp(out))
+    return out

@@ -1035,6 +1035,32 @@ void oracle_get_energy(const oracle_solver* h, double out[5]) {
 
 double oracle_last_residual(const oracle_solver* h) { return h->o.last_residual; }
 
+void oracle_surface_normals(const double* pos, int32_t V, const int32_t* tris, int32_t F, double* out) {
+    // UpdateTriNormal (PDSolver.cu:394-424): unit normal (B-A) x (C-A) / |.| of
+    // each triangle (normalize, utils.cu:293, has no epsilon test), summed into
+    // its three vertices in triangle order; AvgOutsideTetVertNormal
+    // (PDSolver.cu:438-450): divide by the length when it exceeds FLT_EPSILON.
+    std::fill(out, out + 3 * (size_t)V, 0.0);
+    for (int32_t f = 0; f < F; ++f) {
+        const int32_t a = tris[3 * f], b = tris[3 * f + 1], c = tris[3 * f + 2];
+        double ab[3], ac[3];
+        for (int q = 0; q < 3; ++q) {
+            ab[q] = pos[3 * b + q] - pos[3 * a + q];
+            ac[q] = pos[3 * c + q] - pos[3 * a + q];
+        }
+        double n[3] = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2], ab[0] * ac[1] - ab[1] * ac[0]};
+        const double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        for (int q = 0; q < 3; ++q) n[q] /= len;
+        for (int32_t v : {a, b, c})
+            for (int q = 0; q < 3; ++q) out[3 * v + q] += n[q];
+    }
+    for (int32_t i = 0; i < V; ++i) {
+        const double len = std::sqrt(out[3 * i] * out[3 * i] + out[3 * i + 1] * out[3 * i + 1] + out[3 * i + 2] * out[3 * i + 2]);
+        if (len > 1.1920928955078125e-07)
+            for (int q = 0; q < 3; ++q) out[3 * i + q] /= len;
+    }
+}
+
 int oracle_level_size(const oracle_solver* h, int level, int32_t* n, int32_t* nnz) {
     Oracle& o = const_cast<Oracle&>(h->o);
     if (o.p.solver != MGSB_SOLVER_MULTIGRID || level < 0 || level >= o.p.levels) return MGSB_INVALID_ARG;

@@ -64,6 +64,9 @@ int oracle_level_prolongation(const oracle_solver* h, int level, int32_t* ids, d
 int oracle_level_matrix(const oracle_solver* h, int level, double* diag, int32_t* ptr, int32_t* col, double* val);
 
 /* Pure functions. */
+/* Vertex normals of a triangle surface: UpdateTriNormal + AvgOutsideTetVertNormal
+ * (PDSolver.cu:394-460).  pos [3V], tris [3F]; out [3V], zero where no triangle. */
+void oracle_surface_normals(const double* pos, int32_t V, const int32_t* tris, int32_t F, double* out);
 void oracle_ref_rotation(const double F[9], double R[9]);
 void oracle_svd_rotation(const double F[9], double R[9]);
 double oracle_inverse3(const double A[9], double R[9]);

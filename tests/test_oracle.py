@@ -159,3 +159,21 @@ def test_reference_iteration_sensitivity(oracle_built):
         runs.append(o.positions())
     amp = np.abs(runs[0] - runs[1]).max() / 1e-6
     assert amp > 10.0
+
+
+def test_oracle_surface_normals_box():
+    """UpdateTriNormal + AvgOutsideTetVertNormal restated: on a box every surface
+    normal is a unit vector pointing outward, a face-interior vertex gets the
+    face's axis, and interior vertices get zero."""
+    from oracle.binding import surface_normals
+    m = mg.box_mesh(3, 4, 5, (0.0, 0.0, 0.0), (3.0, 4.0, 5.0))
+    mg.extract_surface(m)
+    n = surface_normals(m.positions, m.tris)
+    surf = np.unique(m.tris)
+    inner = np.setdiff1d(np.arange(m.num_verts), surf)
+    assert np.all(n[inner] == 0.0)
+    assert np.allclose(np.linalg.norm(n[surf], axis=1), 1.0)
+    assert np.all(np.einsum("ij,ij->i", n[surf], m.positions[surf] - m.positions.mean(0)) > 0)
+    x = m.positions
+    face = np.nonzero((x[:, 2] == 5.0) & (x[:, 0] == 1.0) & (x[:, 1] == 2.0))[0]
+    assert np.allclose(n[face], [[0.0, 0.0, 1.0]])
