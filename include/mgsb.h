@@ -176,6 +176,19 @@ mgsb_status mgsb_get_device_positions(mgsb_solver* h, int32_t body, const float*
 /* Area-unweighted surface vertex normals — UpdateTriNormal +
  * AvgOutsideTetVertNormal (PDSolver.cu:394-460). */
 mgsb_status mgsb_get_normals(mgsb_solver* h, int32_t body, float* out /* [3*V] */);
+/* The same normals without allocating anything, for callers that cannot call
+ * cudaMalloc while they run (a host that owns the GPU memory budget and forbids
+ * driver allocations in its frame loop; a real-time thread that cannot take the
+ * implicit synchronisation of cudaMalloc/cudaFree).  No counterpart in the
+ * reference.  Scratch is a fixed 2 MiB device array inside the library, held by
+ * every GPU that loads it until exit; a body may have at most 65,536 surface
+ * triangles and 65,536 surface vertices, else MGSB_NOT_SUPPORTED.  A pending
+ * set-up (after mgsb_set_fixed / mgsb_set_material) is not rebuilt here:
+ * MGSB_INVALID_ARG until a mgsb_step or mgsb_get_normals call has done it.  The
+ * first call on a device looks up the scratch address; make it outside any
+ * stream capture.  All calls on one device share the scratch, so calls that
+ * overlap in time (other threads, other handles) race. */
+mgsb_status mgsb_get_normals_noalloc(mgsb_solver* h, int32_t body, float* out /* [3*V] */);
 
 /* Checkpoint / resume: overwrite positions and velocities of a body. */
 mgsb_status mgsb_set_state(mgsb_solver* h, int32_t body, const float* positions, const float* velocities);

@@ -110,6 +110,7 @@ SIGNATURES = [
     ("mgsb_get_collision_depth", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_get_device_positions", C.c_int, [_P, C.c_int32, C.POINTER(_FP)]),
     ("mgsb_get_normals", C.c_int, [_P, C.c_int32, _FP]),
+    ("mgsb_get_normals_noalloc", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_set_state", C.c_int, [_P, C.c_int32, _FP, _FP]),
     ("mgsb_get_energy", C.c_int, [_P, C.c_int32, _DP]),
     ("mgsb_last_frame_ms", C.c_int, [_P, _FP]),

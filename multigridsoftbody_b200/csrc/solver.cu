@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1603,3 +1604,93 @@ const char* mgsb_status_string(mgsb_status s) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free normals readback
+// ===========================================================================
+// Some callers cannot allocate device memory while they run: a host that hands
+// the library a fixed memory budget and forbids driver allocations inside its
+// frame loop, or a real-time render/haptics thread that cannot take the
+// implicit device synchronisation and latency of cudaMalloc/cudaFree.
+// mgsb_get_normals may (re)allocate its scratch when a set-up is pending; this
+// variant runs the same two kernels (k_tri_normals, k_vert_normals) on a fixed
+// scratch array compiled into the library and allocates nothing.
+namespace {
+
+constexpr int kNoAllocMaxTris = 65536;        // triangle normals of one body
+constexpr int kNoAllocMaxSurfVerts = 65536;   // surface-vertex normals of one body
+constexpr int kNoAllocMaxDevices = 64;
+
+// 131,072 float4 = 2 MiB: triangle normals in [0, kNoAllocMaxTris), vertex
+// normals after them.  Every GPU that loads the library holds this array until
+// the process exits.  Nothing in it needs to start at zero: each call writes
+// every triangle slot it reads and every vertex slot it copies out.
+static __device__ __align__(256) float4 g_noalloc_scratch[kNoAllocMaxTris + kNoAllocMaxSurfVerts];
+
+// Device address of the scratch on h's device, looked up once per device with
+// that device current (cudaGetSymbolAddress; no allocation).  The first call on
+// a device does this set-up, so make that first call outside any stream capture.
+mgsb_status noalloc_scratch(mgsb_solver* h, float4** out) {
+    static std::mutex mu;
+    static float4* ptr[kNoAllocMaxDevices] = {};
+    if (h->device < 0 || h->device >= kNoAllocMaxDevices)
+        return set_err(h, MGSB_NOT_SUPPORTED, "device %d: the allocation-free path supports devices 0..%d", h->device,
+                       kNoAllocMaxDevices - 1);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[h->device]) {
+        CUDA_TRY(h, cudaSetDevice(h->device));
+        float4* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return set_err(h, MGSB_CUDA_ERROR, "cudaGetSymbolAddress of the normals scratch failed on device %d: %s",
+                           h->device, cudaGetErrorString(e));
+        ptr[h->device] = p;
+    }
+    *out = ptr[h->device];
+    return MGSB_OK;
+}
+
+}  // namespace
+
+extern "C" mgsb_status mgsb_get_normals_noalloc(mgsb_solver* h, int32_t body, float* out) {
+    if (!out) return MGSB_INVALID_ARG;
+    TRY(check_body(h, body));
+    if (h->dirty)
+        return set_err(h, MGSB_INVALID_ARG,
+                       "set-up pending (fixed set, material or parameters changed): the allocation-free normals do not "
+                       "rebuild; call mgsb_step or mgsb_get_normals once first");
+    const int nf = h->nrm_nf[body], nsv = h->nrm_nsv[body];
+    if (nf > kNoAllocMaxTris || nsv > kNoAllocMaxSurfVerts)
+        return set_err(h, MGSB_NOT_SUPPORTED,
+                       "body %d has %d surface triangles and %d surface vertices; the allocation-free normals hold at "
+                       "most %d and %d (use mgsb_get_normals)",
+                       body, nf, nsv, kNoAllocMaxTris, kNoAllocMaxSurfVerts);
+    float4* scratch = nullptr;
+    TRY(noalloc_scratch(h, &scratch));
+    float4* fscratch = scratch;
+    float4* vscratch = scratch + kNoAllocMaxTris;
+    const int f_off = h->nrm_f_off[body], sv_off = h->nrm_sv_off[body];
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    if (nf > 0) {
+        k_tri_normals<<<(nf + 255) / 256, 256, 0, h->stream>>>(nf, h->nrm_tris + f_off, h->x, fscratch);
+        k_vert_normals<<<(nsv + 255) / 256, 256, 0, h->stream>>>(nsv, h->nrm_ptr + sv_off, h->nrm_fidx, fscratch, vscratch);
+        CUDA_TRY(h, cudaGetLastError());
+    }
+    // the solver's pinned readback buffer (N0 float4, allocated at create) takes the copy
+    if (nsv > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(h->readback, vscratch, nsv * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    int32_t nonfinite = 0;
+    CUDA_TRY(h, cudaMemcpy(&nonfinite, h->nonfinite, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (nonfinite) return set_err(h, MGSB_DIVERGED, "non-finite positions detected");
+    const BodyHost& B = h->bodies[body];
+    const float4* vn = reinterpret_cast<const float4*>(h->readback);
+    std::fill(out, out + 3 * (size_t)B.V, 0.f);
+    for (int j = 0; j < nsv; ++j) {
+        const int i = h->nrm_sv_host[sv_off + j] - B.v_off;
+        out[3 * i] = vn[j].x;
+        out[3 * i + 1] = vn[j].y;
+        out[3 * i + 2] = vn[j].z;
+    }
+    return MGSB_OK;
+}
