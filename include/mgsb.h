@@ -280,6 +280,33 @@ mgsb_status mgsb_mesh_free(mgsb_mesh_data* m);
 /* Seeded 3-D value noise used by the blob generator, exposed for tests. */
 double mgsb_value_noise(double x, double y, double z, double period, uint64_t seed);
 
+/* ------------------------------------------------------------------------
+ * Learned smoother network (config 4).  No counterpart in the reference: its
+ * multigrid smoother is plain Jacobi (PDSolver.cu:192-235).
+ * A per-vertex MLP 9 -> 64 -> 64 -> 3 with GELU, BF16 weights/activations and
+ * FP32 accumulation; inference runs as tcgen05 tensor-core GEMMs over 128-row
+ * tiles, training as a hand-written forward/backward kernel plus Adam.
+ * Parameters (FP32, mgsb_mlp_num_params() = 4995 floats), row-major:
+ *   W1[64][9] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]
+ * ------------------------------------------------------------------------ */
+typedef struct mgsb_mlp mgsb_mlp;
+int32_t mgsb_mlp_num_params(void);
+/* Seeded uniform Glorot initialisation, zero biases. */
+mgsb_status mgsb_mlp_create(int32_t device, uint64_t seed, mgsb_mlp** out);
+mgsb_status mgsb_mlp_destroy(mgsb_mlp* h);
+const char* mgsb_mlp_last_error(const mgsb_mlp* h);
+mgsb_status mgsb_mlp_set_params(mgsb_mlp* h, const float* params, int32_t n);
+mgsb_status mgsb_mlp_get_params(mgsb_mlp* h, float* params, int32_t n);
+/* y[n][3] = MLP(x[n][9]) on the tensor cores (host buffers). */
+mgsb_status mgsb_mlp_forward(mgsb_mlp* h, const float* x, int32_t n, float* y);
+/* Mean squared error over all n samples and its gradient (host buffers). */
+mgsb_status mgsb_mlp_loss_grad(mgsb_mlp* h, const float* x, const float* t, int32_t n, float* grad, float* loss);
+/* Adam on minibatches of `batch` samples drawn uniformly (seeded) from the n
+ * pairs; step size lr with cosine decay to 10 %.  losses (optional) receives
+ * the minibatch loss of every step. */
+mgsb_status mgsb_mlp_train(mgsb_mlp* h, const float* x, const float* t, int64_t n, int32_t steps, int32_t batch,
+                           float lr, uint64_t seed, float* losses);
+
 #ifdef __cplusplus
 }
 #endif

@@ -111,6 +111,15 @@ SIGNATURES = [
     ("mgsb_get_device_positions", C.c_int, [_P, C.c_int32, C.POINTER(_FP)]),
     ("mgsb_get_normals", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_get_normals_noalloc", C.c_int, [_P, C.c_int32, _FP]),
+    ("mgsb_mlp_num_params", C.c_int32, []),
+    ("mgsb_mlp_create", C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_P)]),
+    ("mgsb_mlp_destroy", C.c_int, [_P]),
+    ("mgsb_mlp_last_error", C.c_char_p, [_P]),
+    ("mgsb_mlp_set_params", C.c_int, [_P, _FP, C.c_int32]),
+    ("mgsb_mlp_get_params", C.c_int, [_P, _FP, C.c_int32]),
+    ("mgsb_mlp_forward", C.c_int, [_P, _FP, C.c_int32, _FP]),
+    ("mgsb_mlp_loss_grad", C.c_int, [_P, _FP, _FP, C.c_int32, _FP, _FP]),
+    ("mgsb_mlp_train", C.c_int, [_P, _FP, _FP, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _FP]),
     ("mgsb_set_state", C.c_int, [_P, C.c_int32, _FP, _FP]),
     ("mgsb_get_energy", C.c_int, [_P, C.c_int32, _DP]),
     ("mgsb_last_frame_ms", C.c_int, [_P, _FP]),

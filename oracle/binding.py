@@ -52,6 +52,8 @@ def _load():
         "oracle_level_prolongation": (C.c_int, [C.c_void_p, C.c_int, _IP, _DP]),
         "oracle_level_matrix": (C.c_int, [C.c_void_p, C.c_int, _DP, _IP, _IP, _DP]),
         "oracle_surface_normals": (None, [_DP, C.c_int32, _IP, C.c_int32, _DP]),
+        "oracle_mlp_forward": (None, [_DP, _DP, C.c_int32, C.c_int32, _DP]),
+        "oracle_mlp_loss_grad": (C.c_double, [_DP, _DP, _DP, C.c_int32, C.c_int32, _DP]),
         "oracle_ref_rotation": (None, [_DP, _DP]),
         "oracle_svd_rotation": (None, [_DP, _DP]),
         "oracle_inverse3": (C.c_double, [_DP, _DP]),
@@ -214,3 +216,23 @@ def surface_normals(positions, tris):
     out = np.empty_like(pos)
     lib.oracle_surface_normals(_dp(pos), pos.shape[0], t.ctypes.data_as(_IP), t.shape[0], _dp(out))
     return out
+
+
+def mlp_forward(params, x, bf16=True):
+    """Learned-smoother MLP on rows of x [n, 9] -> [n, 3] (FP64, optional BF16 rounding)."""
+    lib = _load()
+    p = np.ascontiguousarray(params, np.float64)
+    x = np.ascontiguousarray(x, np.float64).reshape(-1, 9)
+    y = np.empty((x.shape[0], 3))
+    lib.oracle_mlp_forward(_dp(p), _dp(x), x.shape[0], int(bf16), _dp(y))
+    return y
+
+
+def mlp_loss_grad(params, x, t, bf16=True):
+    lib = _load()
+    p = np.ascontiguousarray(params, np.float64)
+    x = np.ascontiguousarray(x, np.float64).reshape(-1, 9)
+    t = np.ascontiguousarray(t, np.float64).reshape(-1, 3)
+    g = np.empty(p.shape[0])
+    loss = lib.oracle_mlp_loss_grad(_dp(p), _dp(x), _dp(t), x.shape[0], int(bf16), _dp(g))
+    return float(loss), g

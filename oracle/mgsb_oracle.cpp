@@ -1117,3 +1117,109 @@ void oracle_svd_rotation(const double F[9], double R[9]) { svd_rotation(F, R); }
 double oracle_inverse3(const double A[9], double R[9]) { return inverse3(A, R); }
 
 }  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// Learned-smoother MLP (libmgsb's network; no reference counterpart)
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kIn = 9, kHid = 64, kOut = 3;
+constexpr int kW1 = 0, kB1 = kW1 + kHid * kIn, kW2 = kB1 + kHid, kB2 = kW2 + kHid * kHid, kW3 = kB2 + kHid,
+              kB3 = kW3 + kOut * kHid, kNP = kB3 + kOut;
+
+double bf16_round(double v) {
+    float f = (float)v;
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    b += 0x7FFFu + ((b >> 16) & 1u);
+    b &= 0xFFFF0000u;
+    std::memcpy(&f, &b, 4);
+    return (double)f;
+}
+double gelu64(double x) { return 0.5 * x * (1.0 + std::erf(x / std::sqrt(2.0))); }
+double gelu64_grad(double x) {
+    return 0.5 * (1.0 + std::erf(x / std::sqrt(2.0))) + x * std::exp(-0.5 * x * x) / std::sqrt(2.0 * M_PI);
+}
+
+struct MlpPass {
+    double x[kIn], z1[kHid], h1[kHid], z2[kHid], h2[kHid], y[kOut];
+};
+
+void mlp_pass(const std::vector<double>& w, const double* xin, bool bf, MlpPass& P) {
+    for (int k = 0; k < kIn; ++k) P.x[k] = bf ? bf16_round(xin[k]) : xin[k];
+    for (int j = 0; j < kHid; ++j) {
+        double a = w[kB1 + j];
+        for (int k = 0; k < kIn; ++k) a += w[kW1 + j * kIn + k] * P.x[k];
+        P.z1[j] = a;
+        P.h1[j] = bf ? bf16_round(gelu64(a)) : gelu64(a);
+    }
+    for (int j = 0; j < kHid; ++j) {
+        double a = w[kB2 + j];
+        for (int k = 0; k < kHid; ++k) a += w[kW2 + j * kHid + k] * P.h1[k];
+        P.z2[j] = a;
+        P.h2[j] = bf ? bf16_round(gelu64(a)) : gelu64(a);
+    }
+    for (int o = 0; o < kOut; ++o) {
+        double a = w[kB3 + o];
+        for (int k = 0; k < kHid; ++k) a += w[kW3 + o * kHid + k] * P.h2[k];
+        P.y[o] = a;
+    }
+}
+
+std::vector<double> mlp_weights(const double* params, bool bf) {
+    std::vector<double> w(params, params + kNP);
+    if (bf) {
+        for (int q = kW1; q < kB1; ++q) w[q] = bf16_round(w[q]);
+        for (int q = kW2; q < kB2; ++q) w[q] = bf16_round(w[q]);
+        for (int q = kW3; q < kB3; ++q) w[q] = bf16_round(w[q]);
+    }
+    return w;
+}
+}  // namespace
+
+void oracle_mlp_forward(const double* params, const double* x, int32_t n, int32_t bf16, double* y) {
+    const std::vector<double> w = mlp_weights(params, bf16 != 0);
+#pragma omp parallel for schedule(static)
+    for (int32_t i = 0; i < n; ++i) {
+        MlpPass P;
+        mlp_pass(w, x + (size_t)i * kIn, bf16 != 0, P);
+        for (int o = 0; o < kOut; ++o) y[(size_t)i * kOut + o] = P.y[o];
+    }
+}
+
+double oracle_mlp_loss_grad(const double* params, const double* x, const double* t, int32_t n, int32_t bf16,
+                            double* grad) {
+    const std::vector<double> w = mlp_weights(params, bf16 != 0);
+    std::vector<double> g(kNP, 0.0);
+    double loss = 0.0;
+    const double inv = 1.0 / ((double)n * kOut);
+    for (int32_t i = 0; i < n; ++i) {
+        MlpPass P;
+        mlp_pass(w, x + (size_t)i * kIn, bf16 != 0, P);
+        double dy[kOut];
+        for (int o = 0; o < kOut; ++o) {
+            const double d = P.y[o] - t[(size_t)i * kOut + o];
+            loss += d * d;
+            dy[o] = 2.0 * d * inv;
+            g[kB3 + o] += dy[o];
+            for (int k = 0; k < kHid; ++k) g[kW3 + o * kHid + k] += dy[o] * P.h2[k];
+        }
+        double dz2[kHid], dz1[kHid];
+        for (int k = 0; k < kHid; ++k) {
+            double a = 0.0;
+            for (int o = 0; o < kOut; ++o) a += dy[o] * w[kW3 + o * kHid + k];
+            dz2[k] = a * gelu64_grad(P.z2[k]);
+            g[kB2 + k] += dz2[k];
+            for (int j = 0; j < kHid; ++j) g[kW2 + k * kHid + j] += dz2[k] * P.h1[j];
+        }
+        for (int k = 0; k < kHid; ++k) {
+            double a = 0.0;
+            for (int j = 0; j < kHid; ++j) a += dz2[j] * w[kW2 + j * kHid + k];
+            dz1[k] = a * gelu64_grad(P.z1[k]);
+            g[kB1 + k] += dz1[k];
+            for (int m = 0; m < kIn; ++m) g[kW1 + k * kIn + m] += dz1[k] * P.x[m];
+        }
+    }
+    if (grad) std::copy(g.begin(), g.end(), grad);
+    return loss * inv;
+}

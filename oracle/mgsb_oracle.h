@@ -67,6 +67,15 @@ int oracle_level_matrix(const oracle_solver* h, int level, double* diag, int32_t
 /* Vertex normals of a triangle surface: UpdateTriNormal + AvgOutsideTetVertNormal
  * (PDSolver.cu:394-460).  pos [3V], tris [3F]; out [3V], zero where no triangle. */
 void oracle_surface_normals(const double* pos, int32_t V, const int32_t* tris, int32_t F, double* out);
+/* Learned-smoother MLP 9 -> 64 -> 64 -> 3 (GELU), parameters in the libmgsb
+ * layout W1[64][9] b1[64] W2[64][64] b2[64] W3[3][64] b3[3].  With bf16 != 0
+ * the weights (not the biases), the inputs and the hidden activations are
+ * rounded to BF16 (round to nearest even) as on the tensor cores, and the
+ * gradient passes straight through the roundings. */
+void oracle_mlp_forward(const double* params, const double* x, int32_t n, int32_t bf16, double* y);
+/* Mean over samples and outputs of (y - t)^2 and its gradient. */
+double oracle_mlp_loss_grad(const double* params, const double* x, const double* t, int32_t n, int32_t bf16,
+                            double* grad);
 void oracle_ref_rotation(const double F[9], double R[9]);
 void oracle_svd_rotation(const double F[9], double R[9]);
 double oracle_inverse3(const double A[9], double R[9]);
