@@ -307,6 +307,32 @@ mgsb_status mgsb_mlp_loss_grad(mgsb_mlp* h, const float* x, const float* t, int3
 mgsb_status mgsb_mlp_train(mgsb_mlp* h, const float* x, const float* t, int64_t n, int32_t steps, int32_t batch,
                            float lr, uint64_t seed, float* losses);
 
+/* Attach (net != NULL) or detach the learned smoother of a multigrid solver.
+ * Each V-cycle then smooths level 0 with one learned sweep before and one after
+ * the coarse correction (in place of the Jacobi sweeps), and checks the
+ * residual: unless |r_end| <= guard_ratio * |r_start| (finite), it restores the
+ * start and runs the plain V-cycle instead.  The network must live on the
+ * solver's device and outlive the attachment; retraining it updates the solver
+ * in place.  No counterpart in the reference. */
+mgsb_status mgsb_set_learned_smoother(mgsb_solver* h, const mgsb_mlp* net, float guard_ratio);
+/* Learned V-cycles run and fallbacks taken since the network was attached. */
+mgsb_status mgsb_learned_stats(mgsb_solver* h, uint64_t out[2]);
+/* Training pairs from the plain FP32 multigrid solver's current state: the
+ * learned sweep is trained to reproduce `sweeps` weighted-Jacobi sweeps from
+ * zero in one step.  Two residuals are used: r = b - A d of the last global
+ * step (what pre-smoothing sees) and the residual left after plain
+ * pre-smoothing and the coarse correction of r (what post-smoothing sees).  One
+ * pair per free vertex whose residual scale s_i is at least 1e-2 of the state's
+ * RMS: features x[9] of the residual against the Jacobi result in the network's
+ * output space, t = e_sweeps / (s_i / D_i).  *n receives the count (up to
+ * 2 x vertices); with x = t = NULL only counts. */
+mgsb_status mgsb_smoother_pairs(mgsb_solver* h, int32_t sweeps, float* x, float* t, int64_t cap, int64_t* n);
+/* Smoother comparison on the last global step: V-cycles on A e = r from e = 0;
+ * mode 0 plain (configured sweeps), 1 plain with 1+1 sweeps, 2 learned (no
+ * fallback).  out[0] = |r|, out[k] = residual norm after k cycles (cycles + 1
+ * values).  Plain FP32 multigrid solver only. */
+mgsb_status mgsb_vcycle_residuals(mgsb_solver* h, int32_t cycles, int32_t mode, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -111,6 +111,10 @@ SIGNATURES = [
     ("mgsb_get_device_positions", C.c_int, [_P, C.c_int32, C.POINTER(_FP)]),
     ("mgsb_get_normals", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_get_normals_noalloc", C.c_int, [_P, C.c_int32, _FP]),
+    ("mgsb_set_learned_smoother", C.c_int, [_P, _P, C.c_float]),
+    ("mgsb_learned_stats", C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    ("mgsb_smoother_pairs", C.c_int, [_P, C.c_int32, _FP, _FP, C.c_int64, C.POINTER(C.c_int64)]),
+    ("mgsb_vcycle_residuals", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     ("mgsb_mlp_num_params", C.c_int32, []),
     ("mgsb_mlp_create", C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_P)]),
     ("mgsb_mlp_destroy", C.c_int, [_P]),

@@ -287,6 +287,31 @@ class Solver:
         _check(self._lib.mgsb_get_all_contact_flags(self.h, _iptr(out)), self.h)
         return out
 
+    def set_learned_smoother(self, net, guard_ratio: float = 0.5) -> None:
+        """Attach a trained learned.MLP (None detaches); see mgsb_set_learned_smoother."""
+        self._net = net   # keep the network alive while attached
+        _check(self._lib.mgsb_set_learned_smoother(self.h, net.h if net is not None else None, guard_ratio), self.h)
+
+    def learned_stats(self) -> tuple[int, int]:
+        out = (C.c_uint64 * 2)()
+        _check(self._lib.mgsb_learned_stats(self.h, out), self.h)
+        return int(out[0]), int(out[1])
+
+    def smoother_pairs(self, sweeps: int = 4) -> tuple[np.ndarray, np.ndarray]:
+        """Training pairs (features [n,9], targets [n,3]) from the current state (mgsb_smoother_pairs)."""
+        n = C.c_int64()
+        cap = 2 * sum(self.num_verts(b) for b in range(self.num_bodies))
+        x = np.empty((cap, 9), np.float32)
+        t = np.empty((cap, 3), np.float32)
+        _check(self._lib.mgsb_smoother_pairs(self.h, sweeps, _fptr(x), _fptr(t), cap, C.byref(n)), self.h)
+        return x[: n.value], t[: n.value]
+
+    def vcycle_residuals(self, cycles: int = 5, mode: int = 0) -> np.ndarray:
+        """Residual norms of V-cycles on the last global step (mode 0 plain, 1 plain 1+1, 2 learned)."""
+        out = np.empty(cycles + 1, np.float64)
+        _check(self._lib.mgsb_vcycle_residuals(self.h, cycles, mode, out.ctypes.data_as(C.POINTER(C.c_double))), self.h)
+        return out
+
     def positions_f64(self, body: int = 0) -> np.ndarray:
         out = np.empty((self.num_verts(body), 3), np.float64)
         _check(self._lib.mgsb_get_positions_f64(self.h, body, out.ctypes.data_as(C.POINTER(C.c_double))), self.h)

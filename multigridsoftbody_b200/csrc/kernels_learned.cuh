@@ -1,0 +1,279 @@
+// Level-0 kernels of the learned smoother (the network itself is in
+// kernels_mlp.cuh).  A learned sweep is
+//     features(r) -> MLP -> d += (s_i / D_i) * MLP(x_i)
+// with, per vertex i (4 lanes per row over the sliced-ELL level-0 matrix):
+//     rbar_i = sum_j |a_ij| r_j / sum_j |a_ij|        (1-ring mean residual, coupling weighted)
+//     dring_i = sum_j |a_ij| D_j / sum_j |a_ij|       (1-ring mean diagonal)
+//     s_i = sqrt(|r_i|^2 + |rbar_i|^2)
+//     x_i = [r_i / s_i (3), D_i / sum_j |a_ij|, (D_i - L_ii) / D_i, D_i / dring_i, rbar_i / s_i (3)]
+// D_i = L_ii + c_i is the diagonal with this frame's contact stiffness.  Fixed
+// vertices take no update and count as zero residual for their neighbours.
+// Normalising by s_i makes the sweep homogeneous of degree 1 in r, like a
+// linear smoother.
+#pragma once
+
+#include <cstdint>
+
+#include "kernels_mg.cuh"
+#include "kernels_mlp.cuh"
+
+namespace mgsb {
+namespace {
+
+constexpr int kLsThreads = 256;
+constexpr int kLsRowsPerBlock = kLsThreads / kLanesL0;   // 64 rows per block
+
+__device__ __forceinline__ float block_sum_f(float v, float* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    float t = 0.f;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    return t;   // valid in thread 0
+}
+
+// r = fix * (b - A d) on level 0; optionally dsave = d and part[block] = sum |r|^2.
+__global__ void __launch_bounds__(kLsThreads) k_ls_residual(int n, const int32_t* __restrict__ sp,
+                                                            const int32_t* __restrict__ col, const float* __restrict__ val,
+                                                            const float* __restrict__ dfull, const float* __restrict__ fixf,
+                                                            const float4* __restrict__ d, const float4* __restrict__ b,
+                                                            float4* __restrict__ r, float4* __restrict__ dsave,
+                                                            float* __restrict__ part) {
+    __shared__ float red[kLsThreads / 32];
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const float4 off = rg_offdiag<G, false>(row, valid, lane, sp, col, val, d);
+    float rr = 0.f;
+    if (valid && lane < S) {
+        const float4 x = d[row], bi = b[row];
+        const float D = __ldg(dfull + row), fx = __ldg(fixf + row);
+        const float4 q = make_float4(fx * (bi.x - fmaf(D, x.x, off.x)), fx * (bi.y - fmaf(D, x.y, off.y)),
+                                     fx * (bi.z - fmaf(D, x.z, off.z)), 0.f);
+        if (r) r[row] = q;
+        if (dsave) dsave[row] = x;
+        rr = q.x * q.x + q.y * q.y + q.z * q.z;
+    }
+    if (part) {
+        const float t = block_sum_f(rr, red);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+}
+
+// Features and update scale of one row from its 1-ring sums
+// (sum |a| f_j r_j, sum |a|, sum |a| D_j).
+__device__ __forceinline__ float ls_row_features(int row, float sx, float sy, float sz, float sa, float sd,
+                                                 const float* __restrict__ dfull, const float* __restrict__ diag0,
+                                                 const float* __restrict__ fixf, const float4* __restrict__ r,
+                                                 float (&f)[kMlpIn]) {
+    const float fx = __ldg(fixf + row);
+    const float4 ri = r[row];
+    const float rx = fx * ri.x, ry = fx * ri.y, rz = fx * ri.z;
+    const float inv_a = sa > 0.f ? 1.f / sa : 0.f;
+    const float bx = sx * inv_a, by = sy * inv_a, bz = sz * inv_a;
+    const float D = __ldg(dfull + row), L = __ldg(diag0 + row);
+    const float s = sqrtf(rx * rx + ry * ry + rz * rz + bx * bx + by * by + bz * bz);
+    const float is = s > 0.f ? 1.f / s : 0.f;
+    f[0] = rx * is;
+    f[1] = ry * is;
+    f[2] = rz * is;
+    f[3] = D * inv_a;
+    f[4] = (D - L) / D;
+    f[5] = sd > 0.f ? D * sa / sd : 1.f;
+    f[6] = bx * is;
+    f[7] = by * is;
+    f[8] = bz * is;
+    return (fx != 0.f && s > 0.f) ? s / D : 0.f;
+}
+
+// 16 BF16 features (9 used) of one row into a K-major interleaved tile.
+__device__ __forceinline__ void ls_store_tile_row(uint8_t* tile, int row_in_tile, const float (&f)[kMlpIn]) {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float lo = 2 * i < kMlpIn ? f[2 * i] : 0.f;
+        const float hi = 2 * i + 1 < kMlpIn ? f[2 * i + 1] : 0.f;
+        const __nv_bfloat162 two = __floats2bfloat162_rn(lo, hi);
+        w[i] = *reinterpret_cast<const uint32_t*>(&two);
+    }
+    uint8_t* base = tile + interleaved_offset(row_in_tile, 0, kMlpInPad);
+    *reinterpret_cast<uint4*>(base) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(base + 128) = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+// Features of every row into the BF16 tensor-core tiles and the update scale
+// s_i / D_i (0 for fixed vertices or a zero residual); optionally the FP32
+// features row-major into xf[n][9].  4 lanes per row.
+__global__ void __launch_bounds__(kLsThreads) k_ls_features(int n, const int32_t* __restrict__ sp,
+                                                            const int32_t* __restrict__ col, const float* __restrict__ val,
+                                                            const float* __restrict__ dfull, const float* __restrict__ diag0,
+                                                            const float* __restrict__ fixf, const float4* __restrict__ r,
+                                                            uint8_t* __restrict__ tiles, float* __restrict__ scale,
+                                                            float* __restrict__ xf) {
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    float sx = 0.f, sy = 0.f, sz = 0.f, sa = 0.f, sd = 0.f;
+    if (valid) {
+        const int slice = row / S;
+        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
+        for (int e = beg + (lane / S) * S + (row - slice * S); e < end; e += 32) {
+            const float a = fabsf(__ldg(val + e));
+            const int j = __ldg(col + e);
+            const float4 rj = r[j];
+            const float fj = __ldg(fixf + j);
+            sx = fmaf(a * fj, rj.x, sx);
+            sy = fmaf(a * fj, rj.y, sy);
+            sz = fmaf(a * fj, rj.z, sz);
+            sa += a;
+            sd = fmaf(a, __ldg(dfull + j), sd);
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        sz += __shfl_xor_sync(0xffffffffu, sz, o);
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sd += __shfl_xor_sync(0xffffffffu, sd, o);
+    }
+    if (!valid || lane >= S) return;
+    float f[kMlpIn];
+    scale[row] = ls_row_features(row, sx, sy, sz, sa, sd, dfull, diag0, fixf, r, f);
+    if (tiles) ls_store_tile_row(tiles + (size_t)(row / kMlpTile) * kTileBytes, row % kMlpTile, f);
+    if (xf)
+        for (int k = 0; k < kMlpIn; ++k) xf[(size_t)row * kMlpIn + k] = f[k];
+}
+
+// One learned sweep in a single kernel: per 128-row tile, each thread forms its
+// row's features straight into the shared-memory operand tile, the tensor-core
+// MLP runs on the tile, and the same thread applies d_i += (s_i/D_i) y_i.
+__global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, const int32_t* __restrict__ sp,
+                                                             const int32_t* __restrict__ col, const float* __restrict__ val,
+                                                             const float* __restrict__ dfull,
+                                                             const float* __restrict__ diag0,
+                                                             const float* __restrict__ fixf, const float4* __restrict__ r,
+                                                             const uint8_t* __restrict__ img, float4* __restrict__ d,
+                                                             int32_t* __restrict__ err) {
+    constexpr int S = 32 / kLanesL0;   // level-0 slice height
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    MlpSmem& Sm = *reinterpret_cast<MlpSmem*>(smem_raw);
+    WaitState ws;
+    uint32_t ph_load = 0, ph_mma = 0;
+    const uint32_t tmem = mlp_cta_setup(Sm, img, ws, ph_load, err);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        __syncthreads();
+        if (Sm.stop) break;
+        const int row = tile * kMlpTile + (int)threadIdx.x;
+        float f[kMlpIn];
+        float sc = 0.f;
+        if (row < n) {
+            float sx = 0.f, sy = 0.f, sz = 0.f, sa = 0.f, sd = 0.f;
+            const int slice = row / S;
+            const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
+            for (int e = beg + (row - slice * S); e < end; e += S) {
+                const float a = fabsf(__ldg(val + e));
+                const int j = __ldg(col + e);
+                const float4 rj = r[j];
+                const float fj = __ldg(fixf + j);
+                sx = fmaf(a * fj, rj.x, sx);
+                sy = fmaf(a * fj, rj.y, sy);
+                sz = fmaf(a * fj, rj.z, sz);
+                sa += a;
+                sd = fmaf(a, __ldg(dfull + j), sd);
+            }
+            sc = ls_row_features(row, sx, sy, sz, sa, sd, dfull, diag0, fixf, r, f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+        }
+        ls_store_tile_row(Sm.x, threadIdx.x, f);
+        fence_async_shared();
+        tc_fence_before();
+        __syncthreads();
+        float out[3];
+        const bool ok = mlp_tile_layers(Sm, tmem, ph_mma, ws, true, out);
+        if (!ok) {
+            Sm.stop = 1;
+            if (err) atomicExch(err, 1);
+        }
+        if (ok && row < n && sc != 0.f) {
+            float4 q = d[row];
+            q.x += sc * out[0];
+            q.y += sc * out[1];
+            q.z += sc * out[2];
+            d[row] = q;
+        }
+    }
+    mlp_cta_teardown(Sm, tmem, ws);
+}
+
+// Guard: the learned V-cycle passes when |r_after|^2 <= gamma^2 |r_before|^2
+// (and both are finite); gate = 1 selects the plain fallback.  Counters:
+// stats[0] = learned V-cycles, stats[1] = fallbacks.
+// In a CUDA graph the decision also sets the conditional handle of the IF node
+// that holds the fallback (use_cond != 0).
+__global__ void k_ls_guard(int n0, const float* __restrict__ p0, int n1, const float* __restrict__ p1, float gamma2,
+                           int32_t* __restrict__ gate, unsigned long long* __restrict__ stats,
+                           cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ float red[kLsThreads / 32];
+    float a = 0.f, b = 0.f;
+    for (int i = threadIdx.x; i < n0; i += blockDim.x) a += p0[i];
+    for (int i = threadIdx.x; i < n1; i += blockDim.x) b += p1[i];
+    const float before = block_sum_f(a, red);
+    __syncthreads();
+    const float after = block_sum_f(b, red);
+    if (threadIdx.x == 0) {
+        const bool pass = isfinite(before) && isfinite(after) && after <= gamma2 * before;
+        *gate = pass ? 0 : 1;
+        if (use_cond) cudaGraphSetConditional(cond, pass ? 0u : 1u);
+        stats[0] += 1ull;
+        if (!pass) stats[1] += 1ull;
+    }
+}
+
+// Fallback entry: d = dsave (or 0 when dsave is null) when the gate is set.
+__global__ void k_ls_restore(int n, const int32_t* __restrict__ gate, const float4* __restrict__ dsave,
+                             float4* __restrict__ d) {
+    if (__ldg(gate) == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    d[i] = dsave ? dsave[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Gated copy (fallback result back into the frame's displacement buffer).
+__global__ void k_ls_copy(int n, const int32_t* __restrict__ gate, const float4* __restrict__ src, float4* __restrict__ dst) {
+    if (__ldg(gate) == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = src[i];
+}
+
+// Training targets in the network's output space: t_i = (e*_i - ec_i) / scale_i
+// for rows with scale_i > 0 (mask_i = 1), else mask_i = 0.
+// Also snorm_i = s_i (the residual scale of the row) for the host-side filter.
+__global__ void k_ls_targets(int n, const float* __restrict__ scale, const float* __restrict__ dfull,
+                             const float4* __restrict__ estar, const float4* __restrict__ ecoarse, float* __restrict__ t,
+                             uint8_t* __restrict__ mask, float* __restrict__ snorm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float s = scale[i];
+    snorm[i] = s * dfull[i];
+    const float4 a = estar[i], c = ecoarse[i];
+    const bool ok = s > 0.f;
+    const float is = ok ? 1.f / s : 0.f;
+    t[3 * (size_t)i] = (a.x - c.x) * is;
+    t[3 * (size_t)i + 1] = (a.y - c.y) * is;
+    t[3 * (size_t)i + 2] = (a.z - c.z) * is;
+    mask[i] = ok ? 1 : 0;
+}
+
+}  // namespace
+}  // namespace mgsb

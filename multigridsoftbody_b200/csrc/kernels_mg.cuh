@@ -48,6 +48,7 @@ struct CoarseArgs {
     const double* Ainv64;    // FP64 coarsest inverse (mixed precision), else null
     const float4* b;         // level-0 right-hand side
     float4* d;               // level-0 unknown (displacement)
+    const int32_t* gate;     // if set, the kernel runs only when *gate != 0 (learned-smoother fallback)
     LevelView lv[kMaxLevels];
 };
 
@@ -151,7 +152,9 @@ __global__ void __launch_bounds__(256) k_l0_sweep_rg(int n, const int32_t* __res
                                                      const float* __restrict__ dinv, const float4* __restrict__ din,
                                                      float4* __restrict__ dout, float4* __restrict__ b,
                                                      const float4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
-                                                     const float4* __restrict__ slots, int gather) {
+                                                     const float4* __restrict__ slots, int gather,
+                                                     const int32_t* __restrict__ gate = nullptr) {
+    if (gate && __ldg(gate) == 0) return;   // gated launches run only when the learned V-cycle was rejected
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -179,7 +182,8 @@ __global__ void __launch_bounds__(256) k_l0_sweep_rg(int n, const int32_t* __res
 __global__ void __launch_bounds__(256) k_l0_residual_rg(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
                                                         const float* __restrict__ val, const float* __restrict__ dfull,
                                                         const float4* __restrict__ dvec, const float4* __restrict__ b,
-                                                        float4* __restrict__ res) {
+                                                        float4* __restrict__ res, const int32_t* __restrict__ gate = nullptr) {
+    if (gate && __ldg(gate) == 0) return;
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -194,7 +198,8 @@ __global__ void __launch_bounds__(256) k_l0_residual_rg(int n, const int32_t* __
 
 // Level-0 prolongation d += P e1 (used when the coarse kernel does not fuse it).
 __global__ void k_l0_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
-                             const float4* __restrict__ ec, float4* __restrict__ v) {
+                             const float4* __restrict__ ec, float4* __restrict__ v, const int32_t* __restrict__ gate = nullptr) {
+    if (gate && __ldg(gate) == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 id = __ldg(pid + i);
@@ -212,6 +217,7 @@ __global__ void k_l0_prolong(int n, const int4* __restrict__ pid, const float4* 
 // separated by cluster barriers (release/acquire on global memory).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_coarse_vcycle(const CoarseArgs A) {
+    if (A.gate && __ldg(A.gate) == 0) return;   // uniform over the cluster, before any barrier
     cg::cluster_group cluster = cg::this_cluster();
     const int cs = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
@@ -432,6 +438,7 @@ __host__ __device__ inline int coarse_smem_float4(const int* nl, int L, int cs, 
 }
 
 __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) {
+    if (A.gate && __ldg(A.gate) == 0) return;   // uniform over the cluster, before any barrier
     extern __shared__ float4 smv[];
     cg::cluster_group cluster = cg::this_cluster();
     const int cs = (int)cluster.num_blocks();

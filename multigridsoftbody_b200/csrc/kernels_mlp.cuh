@@ -181,13 +181,30 @@ struct MlpSmem {
     int stop;
 };
 
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_tc(int n, int ntiles, const uint8_t* __restrict__ tiles,
-                                                        const uint8_t* __restrict__ img, int out_mode,
-                                                        float4* __restrict__ y, float4* __restrict__ e,
-                                                        const float* __restrict__ scale, int32_t* __restrict__ err) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// Dynamic shared memory of k_mlp_tc: at least 80 KiB, so that at most two CTAs
+// (2 x 256 TMEM columns) are resident per SM and tcgen05.alloc never waits.
+inline size_t mlp_tc_smem_bytes() { return sizeof(MlpSmem) > 80 * 1024 ? sizeof(MlpSmem) : (size_t)80 * 1024; }
+
+// Bounded waits of one thread; the first wait that ran out is remembered so
+// that it can be retried once before TMEM is released (no copy or MMA of the
+// CTA is then left in flight).
+struct WaitState {
+    uint64_t* fail_bar = nullptr;
+    uint32_t fail_par = 0;
+};
+__device__ __forceinline__ bool wait_bar(WaitState& ws, uint64_t* bar, uint32_t par) {
+    const bool done = mbar_wait(bar, par, kMaxPolls);
+    if (!done && !ws.fail_bar) {
+        ws.fail_bar = bar;
+        ws.fail_par = par;
+    }
+    return done;
+}
+
+// CTA prologue: barriers, TMEM (256 columns, warp 0) and the weight image.
+__device__ __forceinline__ uint32_t mlp_cta_setup(MlpSmem& S, const uint8_t* img, WaitState& ws, uint32_t& ph_load,
+                                                  int32_t* err) {
+    const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         mbar_init(&S.bar_load, 1);
         mbar_init(&S.bar_mma, 1);
@@ -203,146 +220,156 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_tc(int n, int ntiles, const
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = S.tmem_base;
-    uint32_t ph_load = 0, ph_mma = 0;
-    // a wait that ran out is retried once (bounded) before TMEM is released, so
-    // no copy or MMA of this CTA is left in flight
-    uint64_t* fail_bar = nullptr;
-    uint32_t fail_par = 0;
-    auto wait = [&](uint64_t* bar, uint32_t par) {
-        const bool done = mbar_wait(bar, par, kMaxPolls);
-        if (!done && !fail_bar) {
-            fail_bar = bar;
-            fail_par = par;
-        }
-        return done;
-    };
-    // weights once per CTA
     if (threadIdx.x == 0) {
         mbar_expect_tx(&S.bar_load, kImgBytes);
         bulk_g2s(S.w, img, kImgBytes, &S.bar_load);
     }
-    if (!wait(&S.bar_load, ph_load)) {
+    if (!wait_bar(ws, &S.bar_load, ph_load)) {
         S.stop = 1;
         if (err) atomicExch(err, 1);
     }
     ph_load ^= 1;
-    const float* bias = reinterpret_cast<const float*>(S.w + kImgB);
-    const uint32_t id64 = umma_idesc_bf16(kMlpTile, kMlpHid), id16 = umma_idesc_bf16(kMlpTile, kMlpOutPad);
+    return S.tmem_base;
+}
+
+// CTA epilogue: retry a timed-out wait once, then release TMEM.
+__device__ __forceinline__ void mlp_cta_teardown(MlpSmem& S, uint32_t tmem, WaitState& ws) {
+    if (ws.fail_bar) mbar_wait(ws.fail_bar, ws.fail_par, kMaxPolls);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// Hidden layer epilogue: gelu(D + bias) from TMEM columns [col, col+64) of this
+// thread's row -> BF16 into S.h (K-major interleaved, K = 64).
+__device__ __forceinline__ void mlp_hidden_epilogue(MlpSmem& S, uint32_t taddr, const float* bias, int row_in_tile) {
+#pragma unroll
+    for (int c = 0; c < kMlpHid; c += 16) {
+        float v[16];
+        tmem_ld16(taddr + c, v);
+        tmem_wait_ld();
+        uint32_t packed[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const __nv_bfloat162 two = __floats2bfloat162_rn(gelu(v[2 * i] + bias[c + 2 * i]),
+                                                             gelu(v[2 * i + 1] + bias[c + 2 * i + 1]));
+            packed[i] = *reinterpret_cast<const uint32_t*>(&two);
+        }
+        uint8_t* base = S.h + interleaved_offset(row_in_tile, c, kMlpHid);
+        *reinterpret_cast<uint4*>(base) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(base + 128) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+    }
+}
+
+// The three layers on the feature tile in S.x (which the caller has made
+// visible to the async proxy and synchronised); y receives this thread's row.
+// Returns false when a wait ran out.
+__device__ __forceinline__ bool mlp_tile_layers(MlpSmem& S, uint32_t tmem, uint32_t& ph_mma, WaitState& ws, bool ok,
+                                                float (&y)[3]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row_in_tile = warp * 32 + lane;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const float* bias = reinterpret_cast<const float*>(S.w + kImgB);
+    const uint32_t id64 = umma_idesc_bf16(kMlpTile, kMlpHid), id16 = umma_idesc_bf16(kMlpTile, kMlpOutPad);
+    // layer 1: D1 = X W1^T (K = 16: one MMA)
+    tc_fence_after();
+    if (threadIdx.x == 0 && ok) {
+        umma_bf16(tmem + 0, umma_desc(S.x, 128, 256), umma_desc(S.w + kImgW1, 128, 256), id64, 0);
+        umma_commit(&S.bar_mma);
+    }
+    ok = ok && wait_bar(ws, &S.bar_mma, ph_mma);
+    ph_mma ^= 1;
+    tc_fence_after();
+    mlp_hidden_epilogue(S, tmem + lane_base + 0, bias, row_in_tile);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // layer 2: D2 = H1 W2^T (K = 64: four MMAs)
+    if (threadIdx.x == 0 && ok) {
+#pragma unroll
+        for (int k = 0; k < kMlpHid / 16; ++k)
+            umma_bf16(tmem + 64, umma_desc(S.h + k * 256, 128, 1024), umma_desc(S.w + kImgW2 + k * 256, 128, 1024), id64,
+                      k > 0 ? 1u : 0u);
+        umma_commit(&S.bar_mma);
+    }
+    ok = ok && wait_bar(ws, &S.bar_mma, ph_mma);
+    ph_mma ^= 1;
+    tc_fence_after();
+    // H2 overwrites H1: layer 2 has finished reading it
+    mlp_hidden_epilogue(S, tmem + lane_base + 64, bias + kMlpHid, row_in_tile);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // layer 3: D3 = H2 W3^T (N = 16, 3 used)
+    if (threadIdx.x == 0 && ok) {
+#pragma unroll
+        for (int k = 0; k < kMlpHid / 16; ++k)
+            umma_bf16(tmem + 128, umma_desc(S.h + k * 256, 128, 1024), umma_desc(S.w + kImgW3 + k * 256, 128, 1024),
+                      id16, k > 0 ? 1u : 0u);
+        umma_commit(&S.bar_mma);
+    }
+    ok = ok && wait_bar(ws, &S.bar_mma, ph_mma);
+    ph_mma ^= 1;
+    tc_fence_after();
+    float v[16];
+    tmem_ld16(tmem + lane_base + 128, v);
+    tmem_wait_ld();
+    tc_fence_before();
+    y[0] = v[0] + bias[2 * kMlpHid];
+    y[1] = v[1] + bias[2 * kMlpHid + 1];
+    y[2] = v[2] + bias[2 * kMlpHid + 2];
+    return ok;
+}
+
+// Inference over feature tiles in global memory: one CTA (4 warps) per
+// 128-row tile, grid-strided.
+//   out_mode 0: y[row] = (y0, y1, y2, 0)
+//   out_mode 1: e[row] += scale[row] * (y0, y1, y2)
+// err (optional): set to 1 when a bounded wait ran out; the kernel then stops.
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_tc(int n, int ntiles, const uint8_t* __restrict__ tiles,
+                                                        const uint8_t* __restrict__ img, int out_mode,
+                                                        float4* __restrict__ y, float4* __restrict__ e,
+                                                        const float* __restrict__ scale, int32_t* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw);
+    WaitState ws;
+    uint32_t ph_load = 0, ph_mma = 0;
+    const uint32_t tmem = mlp_cta_setup(S, img, ws, ph_load, err);
+    const int row_in_tile = threadIdx.x;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         __syncthreads();
         if (S.stop) break;
-        // ---- feature tile
         if (threadIdx.x == 0) {
             mbar_expect_tx(&S.bar_load, kTileBytes);
             bulk_g2s(S.x, tiles + (size_t)tile * kTileBytes, kTileBytes, &S.bar_load);
         }
-        bool ok = wait(&S.bar_load, ph_load);
+        bool ok = wait_bar(ws, &S.bar_load, ph_load);
         ph_load ^= 1;
-        // ---- layer 1: D1 = X W1^T  (K = 16: one MMA)
-        tc_fence_after();
-        if (threadIdx.x == 0 && ok) {
-            umma_bf16(tmem + 0, umma_desc(S.x, 128, 256), umma_desc(S.w + kImgW1, 128, 256), id64, 0);
-            umma_commit(&S.bar_mma);
-        }
-        ok = ok && wait(&S.bar_mma, ph_mma);
-        ph_mma ^= 1;
-        tc_fence_after();
-        // ---- epilogue 1: H1 = gelu(D1 + b1) -> shared (bf16, K-major interleaved, K = 64)
-#pragma unroll
-        for (int c = 0; c < kMlpHid; c += 16) {
-            float v[16];
-            tmem_ld16(tmem + lane_base + c, v);
-            tmem_wait_ld();
-            uint32_t packed[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const __nv_bfloat162 two = __floats2bfloat162_rn(gelu(v[2 * i] + bias[c + 2 * i]),
-                                                                 gelu(v[2 * i + 1] + bias[c + 2 * i + 1]));
-                packed[i] = *reinterpret_cast<const uint32_t*>(&two);
-            }
-            uint8_t* base = S.h + interleaved_offset(row_in_tile, c, kMlpHid);
-            *reinterpret_cast<uint4*>(base) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-            *reinterpret_cast<uint4*>(base + 128) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
-        }
-        fence_async_shared();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        // ---- layer 2: D2 = H1 W2^T  (K = 64: four MMAs)
-        if (threadIdx.x == 0 && ok) {
-#pragma unroll
-            for (int k = 0; k < kMlpHid / 16; ++k)
-                umma_bf16(tmem + 64, umma_desc(S.h + k * 256, 128, 1024), umma_desc(S.w + kImgW2 + k * 256, 128, 1024),
-                          id64, k > 0 ? 1u : 0u);
-            umma_commit(&S.bar_mma);
-        }
-        ok = ok && wait(&S.bar_mma, ph_mma);
-        ph_mma ^= 1;
-        tc_fence_after();
-        // ---- epilogue 2: H2 = gelu(D2 + b2) -> shared (overwrites H1: layer 2 has finished reading it)
-#pragma unroll
-        for (int c = 0; c < kMlpHid; c += 16) {
-            float v[16];
-            tmem_ld16(tmem + lane_base + 64 + c, v);
-            tmem_wait_ld();
-            uint32_t packed[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const __nv_bfloat162 two = __floats2bfloat162_rn(gelu(v[2 * i] + bias[kMlpHid + c + 2 * i]),
-                                                                 gelu(v[2 * i + 1] + bias[kMlpHid + c + 2 * i + 1]));
-                packed[i] = *reinterpret_cast<const uint32_t*>(&two);
-            }
-            uint8_t* base = S.h + interleaved_offset(row_in_tile, c, kMlpHid);
-            *reinterpret_cast<uint4*>(base) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-            *reinterpret_cast<uint4*>(base + 128) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
-        }
-        fence_async_shared();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        // ---- layer 3: D3 = H2 W3^T  (N = 16, 3 used)
-        if (threadIdx.x == 0 && ok) {
-#pragma unroll
-            for (int k = 0; k < kMlpHid / 16; ++k)
-                umma_bf16(tmem + 128, umma_desc(S.h + k * 256, 128, 1024), umma_desc(S.w + kImgW3 + k * 256, 128, 1024),
-                          id16, k > 0 ? 1u : 0u);
-            umma_commit(&S.bar_mma);
-        }
-        ok = ok && wait(&S.bar_mma, ph_mma);
-        ph_mma ^= 1;
-        tc_fence_after();
-        float v[16];
-        tmem_ld16(tmem + lane_base + 128, v);
-        tmem_wait_ld();
-        tc_fence_before();
+        float out[3];
+        ok = mlp_tile_layers(S, tmem, ph_mma, ws, ok, out);
         if (!ok) {
             S.stop = 1;
             if (err) atomicExch(err, 1);
         }
         const int row = tile * kMlpTile + row_in_tile;
         if (ok && row < n) {
-            const float y0 = v[0] + bias[2 * kMlpHid], y1 = v[1] + bias[2 * kMlpHid + 1], y2 = v[2] + bias[2 * kMlpHid + 2];
             if (out_mode == 0) {
-                y[row] = make_float4(y0, y1, y2, 0.f);
+                y[row] = make_float4(out[0], out[1], out[2], 0.f);
             } else {
-                const float s = scale[row];
+                const float sc = scale[row];
                 float4 q = e[row];
-                q.x += s * y0;
-                q.y += s * y1;
-                q.z += s * y2;
+                q.x += sc * out[0];
+                q.y += sc * out[1];
+                q.z += sc * out[2];
                 e[row] = q;
             }
         }
     }
-    if (fail_bar) mbar_wait(fail_bar, fail_par, kMaxPolls);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    mlp_cta_teardown(S, tmem, ws);
 }
 
 // ---------------------------------------------------------------------------

@@ -69,7 +69,7 @@ mgsb_status mlp_err(mgsb_mlp* h, mgsb_status s, const char* fmt, ...) {
         if (s_ != MGSB_OK) return s_;      \
     } while (0)
 
-size_t mlp_tc_smem() { return std::max(sizeof(MlpSmem), (size_t)80 * 1024); }   // <= 2 CTAs (and TMEM users) per SM
+size_t mlp_tc_smem() { return mlp_tc_smem_bytes(); }
 
 mgsb_status ensure_data(mgsb_mlp* h, size_t n) {
     if (n <= h->data_cap) return MGSB_OK;

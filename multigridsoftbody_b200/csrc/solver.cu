@@ -14,9 +14,11 @@
 #include "../../include/mgsb.h"
 #include "kernels.cuh"
 #include "kernels_diag.cuh"
+#include "kernels_learned.cuh"
 #include "kernels_mg.cuh"
 #include "kernels_mixed.cuh"
 #include "mesh.hpp"
+#include "mlp.hpp"
 #include "plan.hpp"
 #include "setup.hpp"
 
@@ -26,6 +28,8 @@ namespace {
 
 constexpr int kBlock = 256;
 inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
+// blocks of kBlock threads for a row-group kernel (32/S lanes per row, slices of S rows)
+inline int grid_rows(int n, int S) { return ((n + S - 1) / S * 32 + kBlock - 1) / kBlock; }
 
 // Device allocation owned by the solver.
 struct DevMem {
@@ -78,6 +82,7 @@ struct mgsb_solver {
     cudaGraph_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
+    bool capture_error = false;   // a graph-building step inside a capture failed
     int launches = 0;
     // per-launch CUDA events of a profiled (eager) frame
     bool profiling = false;
@@ -154,6 +159,22 @@ struct mgsb_solver {
     int max_coarsest = 0;
     // host copies of precompute for export
     std::vector<float> h_inv, h_ac, h_vol, h_mass, h_diag;
+    // learned smoother (multigrid kinds): network, guard ratio and level-0 buffers
+    const mgsb_mlp* ls_net = nullptr;
+    cudaStream_t aux_stream = nullptr;   // captures the bodies of conditional graph nodes
+    float ls_gamma = 0.5f;
+    int ls_ntiles = 0, ls_nblk = 0, sm_count = 148;
+    uint8_t* ls_tiles = nullptr;
+    float* ls_scale = nullptr;
+    float4 *ls_r = nullptr, *ls_save = nullptr;
+    float *ls_part0 = nullptr, *ls_part1 = nullptr;
+    int32_t *ls_gate = nullptr, *ls_werr = nullptr;
+    unsigned long long* ls_stats = nullptr;
+    // training-pair generation (allocated on first use)
+    float *ls_xf = nullptr, *ls_t = nullptr, *ls_s = nullptr;
+    uint8_t* ls_mask = nullptr;
+    float4 *ls_e1 = nullptr, *ls_e2 = nullptr, *ls_ec = nullptr;
+    std::vector<DevMem> pair_mem;
     ~mgsb_solver();
 };
 
@@ -164,6 +185,7 @@ mgsb_solver::~mgsb_solver() {
     if (graph) cudaGraphDestroy(graph);
     for (auto& m : derived_mem) cudaFree(m.p);
     for (auto& m : state_mem) cudaFree(m.p);
+    for (auto& m : pair_mem) cudaFree(m.p);
     delete[] bodies_host;
     delete spheres_host;
     for (int k = 0; k < kStage; ++k) {
@@ -171,6 +193,7 @@ mgsb_solver::~mgsb_solver() {
         if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
     }
     if (readback) cudaFreeHost(readback);
+    if (aux_stream) cudaStreamDestroy(aux_stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
@@ -238,7 +261,7 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs);
 void apply_tuning(mgsb_solver* h) {
     // Default: the distributed-shared-memory kernel with <= 256 level-1 rows per CTA.
     h->fuse_l0 = h->tune_fuse >= 0 ? h->tune_fuse : 0;
-    if (h->p.precision == MGSB_PRECISION_MIXED) h->fuse_l0 = 0;   // mixed precision runs the DSM kernel
+    if (h->p.precision == MGSB_PRECISION_MIXED || h->ls_net) h->fuse_l0 = 0;   // these run the DSM kernel
     if (h->tune_cluster > 0) {
         h->cluster = h->tune_cluster;
     } else if (h->fuse_l0) {
@@ -468,6 +491,26 @@ mgsb_status rebuild(mgsb_solver* h) {
         BD.v0_n = h->bodies[bi].V;
     }
     TRY(upload_normals_data(h, pool));
+    if (mg) {
+        // learned-smoother level-0 buffers (used when a network is attached)
+        h->ls_ntiles = (N0 + kMlpTile - 1) / kMlpTile;
+        h->ls_nblk = grid_rows(N0, h->lev[0].S);
+        TRY(dalloc(h, pool, &h->ls_tiles, (size_t)h->ls_ntiles * kTileBytes));
+        TRY(dalloc(h, pool, &h->ls_scale, (size_t)N0));
+        TRY(dalloc(h, pool, &h->ls_r, (size_t)N0));
+        TRY(dalloc(h, pool, &h->ls_save, (size_t)N0));
+        TRY(dalloc(h, pool, &h->ls_part0, (size_t)h->ls_nblk));
+        TRY(dalloc(h, pool, &h->ls_part1, (size_t)h->ls_nblk));
+        TRY(dalloc(h, pool, &h->ls_gate, 1));
+        TRY(dalloc(h, pool, &h->ls_werr, 1));
+        TRY(dalloc(h, pool, &h->ls_stats, 2));
+        CUDA_TRY(h, cudaMemset(h->ls_stats, 0, 2 * sizeof(unsigned long long)));
+        CUDA_TRY(h, cudaMemset(h->ls_gate, 0, sizeof(int32_t)));
+        CUDA_TRY(h, cudaMemset(h->ls_werr, 0, sizeof(int32_t)));
+        CUDA_TRY(h, cudaFuncSetAttribute(k_ls_sweep_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mlp_tc_smem_bytes()));
+        CUDA_TRY(h, cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device));
+    }
     TRY(dalloc(h, pool, &h->energy_part, (size_t)kEnergyBlocks * kEnergyTerms));
     TRY(dalloc(h, pool, &h->energy_out, kEnergyTerms));
     h->dirty = false;
@@ -579,7 +622,104 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
     return MGSB_OK;
 }
 
-inline int grid_rows(int n, int S) { return ((n + S - 1) / S * 32 + kBlock - 1) / kBlock; }
+// One learned V-cycle on level 0 for A d = b: d is the warm start, or zero
+// when from_zero.  Pre-smoothing: residual -> features -> tensor-core MLP
+// (d += scale * y).  Coarse correction as in the plain cycle.  Post-smoothing:
+// the same learned sweep.  Guard: a final residual; if |r| did not drop to
+// gamma |r_start| (or is not finite) the gate opens, d is restored and the
+// plain V-cycle runs (its kernels are launched gated and return at once when
+// the learned cycle passed).  dtmp: ping-pong buffer of the plain sweeps.
+void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float4* b, bool from_zero, CoarseArgs ca) {
+    const mgsb_params& p = h->p;
+    const int n0 = h->N0;
+    std::vector<LevelDev>& lv = h->lev;
+    const LevelDev& l0 = lv[0];
+    const int g0 = h->ls_nblk;
+    const uint8_t* img = mlp_device_image(h->ls_net);
+    const int mgrid = std::min(h->ls_ntiles, 2 * h->sm_count);
+    const size_t msmem = mlp_tc_smem_bytes();
+    float4* bw = const_cast<float4*>(b);
+    // pre-smoothing
+    LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
+           h->ls_r, from_zero ? nullptr : h->ls_save, h->ls_part0);
+    LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
+           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
+    // coarse correction
+    LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, d, b, l0.res, nullptr);
+    ca.d = d;
+    ca.gate = nullptr;
+    launch_coarse(h, ca);
+    LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, d, nullptr);
+    // post-smoothing
+    LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
+           h->ls_r, nullptr, nullptr);
+    LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
+           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
+    // guard.  Inside a CUDA graph the fallback is the body of a conditional IF
+    // node that the guard kernel switches on; eagerly (and while profiling, as
+    // event nodes may not sit in a conditional body) its kernels are launched
+    // gated and return at once when the learned cycle passed.
+    cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(h->stream, &cst);
+    const bool cond = cst == cudaStreamCaptureStatusActive && !h->profiling && h->aux_stream;
+    cudaGraphConditionalHandle hnd = 0;
+    cudaGraph_t cap_graph = nullptr;
+    if (cond) {
+        cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &cap_graph, nullptr, nullptr);
+        if (cudaGraphConditionalHandleCreate(&hnd, cap_graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+            h->capture_error = true;
+    }
+    LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
+           nullptr, nullptr, h->ls_part1);
+    LAUNCH(h, k_ls_guard, 1, kLsThreads, 0, g0, h->ls_part0, g0, h->ls_part1, h->ls_gamma * h->ls_gamma, h->ls_gate,
+           h->ls_stats, hnd, cond ? 1 : 0);
+    cudaStream_t main_stream = h->stream;
+    if (cond) {
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &cap_graph, &deps, &nd);
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = hnd;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        if (cudaGraphAddNode(&node, cap_graph, deps, nd, &np) != cudaSuccess ||
+            cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess ||
+            cudaStreamBeginCaptureToGraph(h->aux_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            h->capture_error = true;
+        } else {
+            h->stream = h->aux_stream;   // the fallback below is captured into the IF body
+        }
+    }
+    // fallback: the plain V-cycle from the same start
+    LAUNCH(h, k_ls_restore, grid_for(n0), kBlock, 0, n0, h->ls_gate, from_zero ? nullptr : h->ls_save, d);
+    float4* xa = d;
+    float4* xb = dtmp;
+    for (int k = 0; k < p.pre_sweeps; ++k) {
+        LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb, bw,
+               h->b0, h->slot_ptr, h->slots, 0, h->ls_gate);
+        std::swap(xa, xb);
+    }
+    LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, xa, b, l0.res,
+           h->ls_gate);
+    ca.d = xa;
+    ca.gate = h->ls_gate;
+    launch_coarse(h, ca);
+    LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, xa, h->ls_gate);
+    for (int k = 0; k < p.post_sweeps; ++k) {
+        LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb, bw,
+               h->b0, h->slot_ptr, h->slots, 0, h->ls_gate);
+        std::swap(xa, xb);
+    }
+    if (xa != d) LAUNCH(h, k_ls_copy, grid_for(n0), kBlock, 0, n0, h->ls_gate, xa, d);
+    if (h->stream != main_stream) {
+        cudaGraph_t body = nullptr;
+        if (cudaStreamEndCapture(h->stream, &body) != cudaSuccess) h->capture_error = true;
+        h->stream = main_stream;
+    }
+}
 
 void enqueue_mg_frame(mgsb_solver* h) {
     const mgsb_params& p = h->p;
@@ -630,6 +770,11 @@ void enqueue_mg_frame(mgsb_solver* h) {
     const int g0 = grid_rows(n0, lv[0].S);
     for (int it = 0; it < p.iterations; ++it) {
         LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
+        if (h->ls_net) {
+            LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
+            for (int pass = 0; pass < p.refinement_passes; ++pass) enqueue_learned_vcycle(h, xa, xb, h->b, false, ca);
+            continue;
+        }
         for (int pass = 0; pass < p.refinement_passes; ++pass) {
             bool gathered = pass > 0;
             for (int k = 0; k < p.pre_sweeps; ++k) {
@@ -720,7 +865,12 @@ void enqueue_mixed_frame(mgsb_solver* h) {
             float4* ea = h->d;
             float4* eb = h->d2;
             LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
-                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, p.pre_sweeps > 0 ? 1 : 0);
+                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !h->ls_net) ? 1 : 0);
+            if (h->ls_net) {
+                enqueue_learned_vcycle(h, ea, eb, h->r32, true, ca);
+                LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
+                continue;
+            }
             for (int k = 1; k < p.pre_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                        lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0);
@@ -778,8 +928,14 @@ mgsb_status step_once(mgsb_solver* h) {
     if (h->p.use_graph) {
         if (!h->graph_valid) {
             CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            h->capture_error = false;
             enqueue_frame(h);
             cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+            if (e == cudaSuccess && h->capture_error) {
+                cudaGraphDestroy(h->graph);
+                h->graph = nullptr;
+                return set_err(h, MGSB_CUDA_ERROR, "graph capture failed: could not build a conditional node");
+            }
             if (e != cudaSuccess) return set_err(h, MGSB_CUDA_ERROR, "graph capture failed: %s", cudaGetErrorString(e));
             CUDA_TRY(h, cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
             h->graph_valid = true;
@@ -883,6 +1039,7 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
         CUDA_TRY(hp, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         h->own_stream = true;
     }
+    CUDA_TRY(hp, cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking));
     CUDA_TRY(hp, cudaEventCreate(&h->ev0));
     CUDA_TRY(hp, cudaEventCreate(&h->ev1));
     h->bodies_host = new BodyDev[nbodies];
@@ -1437,7 +1594,8 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
         if (nb > 1 && c > 2) continue;   // many bodies: small clusters, one per body
         for (int blk : {256, 512, 1024}) {
             if (coarse_shape_feasible(h, c, blk, 0)) cands.push_back({c, blk, 0});
-            if (blk >= 512 && c >= 2 && h->p.precision != MGSB_PRECISION_MIXED && coarse_shape_feasible(h, c, blk, 1))
+            if (blk >= 512 && c >= 2 && h->p.precision != MGSB_PRECISION_MIXED && !h->ls_net &&
+                coarse_shape_feasible(h, c, blk, 1))
                 cands.push_back({c, blk, 1});
         }
     }
@@ -1692,5 +1850,227 @@ extern "C" mgsb_status mgsb_get_normals_noalloc(mgsb_solver* h, int32_t body, fl
         out[3 * i + 1] = vn[j].y;
         out[3 * i + 2] = vn[j].z;
     }
+    return MGSB_OK;
+}
+
+// ===========================================================================
+// Learned smoother: attach a network, counters, training pairs
+// ===========================================================================
+extern "C" mgsb_status mgsb_set_learned_smoother(mgsb_solver* h, const mgsb_mlp* net, float guard_ratio) {
+    if (!h) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the learned smoother needs the multigrid solver kind");
+    if (net && mlp_device(net) != h->device)
+        return set_err(h, MGSB_INVALID_ARG, "network on device %d, solver on device %d", mlp_device(net), h->device);
+    if (net && !(guard_ratio > 0.f && guard_ratio <= 10.f))
+        return set_err(h, MGSB_INVALID_ARG, "guard ratio %g outside (0, 10]", (double)guard_ratio);
+    TRY(sync_check(h));
+    h->ls_net = net;
+    if (net) h->ls_gamma = guard_ratio;
+    if (!h->dirty) {
+        apply_tuning(h);
+        CUDA_TRY(h, cudaMemsetAsync(h->ls_stats, 0, 2 * sizeof(unsigned long long), h->stream));
+    }
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
+extern "C" mgsb_status mgsb_learned_stats(mgsb_solver* h, uint64_t out[2]) {
+    if (!h || !out) return MGSB_INVALID_ARG;
+    out[0] = out[1] = 0;
+    if (!is_mg(h) || h->dirty || !h->ls_stats) return MGSB_OK;
+    TRY(sync_check(h));
+    unsigned long long tmp[2] = {0, 0};
+    CUDA_TRY(h, cudaMemcpy(tmp, h->ls_stats, sizeof tmp, cudaMemcpyDeviceToHost));
+    out[0] = tmp[0];
+    out[1] = tmp[1];
+    return MGSB_OK;
+}
+
+extern "C" mgsb_status mgsb_smoother_pairs(mgsb_solver* h, int32_t sweeps, float* x, float* t, int64_t cap,
+                                           int64_t* n) {
+    if (!h || !n || sweeps < 1) return MGSB_INVALID_ARG;
+    *n = 0;
+    if (!is_mg(h) || h->p.precision != MGSB_PRECISION_FP32)
+        return set_err(h, MGSB_NOT_SUPPORTED, "training pairs come from the plain FP32 multigrid solver");
+    if (h->dirty || !h->d_final) return set_err(h, MGSB_INVALID_ARG, "run a frame before generating pairs");
+    if (h->fuse_l0)
+        return set_err(h, MGSB_NOT_SUPPORTED, "pair generation uses the shared-memory coarse kernel (fuse_level0 = 0)");
+    TRY(sync_check(h));
+    const int n0 = h->N0;
+    auto& pool = h->pair_mem;
+    if (!h->ls_xf) {
+        TRY(dalloc(h, pool, &h->ls_xf, (size_t)n0 * kMlpIn));
+        TRY(dalloc(h, pool, &h->ls_t, (size_t)n0 * kMlpOut));
+        TRY(dalloc(h, pool, &h->ls_mask, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_e1, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_e2, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_ec, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_s, (size_t)n0));
+    }
+    std::vector<LevelDev>& lv = h->lev;
+    const LevelDev& l0 = lv[0];
+    const int g0 = h->ls_nblk;
+    cudaStream_t st = h->stream;
+    const mgsb_params& p = h->p;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    const int launches = h->launches;   // not part of a frame
+    CoarseArgs ca;
+    fill_coarse_args(h, ca);
+    std::vector<float> hx((size_t)n0 * kMlpIn), ht((size_t)n0 * kMlpOut), hs(n0);
+    std::vector<uint8_t> hm(n0);
+    int64_t cnt = 0;
+    // Jacobi sweeps from e = 0 on A e = rhs (ping-pong e1/e2); returns the result buffer
+    auto sweeps_from_zero = [&](const float4* rhs, int k_sweeps) {
+        float4* xa = h->ls_e1;
+        float4* xb = h->ls_e2;
+        cudaMemsetAsync(xa, 0, (size_t)n0 * sizeof(float4), st);
+        for (int k = 0; k < k_sweeps; ++k) {
+            k_l0_sweep_rg<<<g0, kBlock, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb,
+                                                 const_cast<float4*>(rhs), h->b0, h->slot_ptr, h->slots, 0, nullptr);
+            std::swap(xa, xb);
+        }
+        return xa;
+    };
+    // one set of pairs for residual r: features of r against `sweeps` Jacobi sweeps
+    auto collect = [&](const float4* r) -> mgsb_status {
+        k_ls_features<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->vdiag, h->fixf, r,
+                                                 nullptr, h->ls_scale, h->ls_xf);
+        const float4* ek = sweeps_from_zero(r, sweeps);
+        CUDA_TRY(h, cudaMemsetAsync(h->ls_ec, 0, (size_t)n0 * sizeof(float4), st));   // no coarse part
+        k_ls_targets<<<grid_for(n0), kBlock, 0, st>>>(n0, h->ls_scale, l0.dfull, ek, h->ls_ec, h->ls_t, h->ls_mask,
+                                                      h->ls_s);
+        CUDA_TRY(h, cudaGetLastError());
+        CUDA_TRY(h, cudaMemcpyAsync(hx.data(), h->ls_xf, hx.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaMemcpyAsync(ht.data(), h->ls_t, ht.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaMemcpyAsync(hm.data(), h->ls_mask, hm.size(), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaMemcpyAsync(hs.data(), h->ls_s, hs.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        // Rows whose residual is tiny next to the state's RMS carry no
+        // information for the smoother: keep rows with s_i >= 1e-2 RMS(s).
+        double ss = 0.0;
+        int64_t nm = 0;
+        for (int i = 0; i < n0; ++i)
+            if (hm[i]) {
+                ss += (double)hs[i] * hs[i];
+                ++nm;
+            }
+        const double s_min = nm ? 1e-2 * std::sqrt(ss / (double)nm) : 0.0;
+        for (int i = 0; i < n0; ++i) {
+            if (!hm[i] || hs[i] < s_min) continue;
+            if (x && t && cnt < cap) {
+                std::copy(&hx[(size_t)i * kMlpIn], &hx[(size_t)i * kMlpIn] + kMlpIn, x + cnt * kMlpIn);
+                std::copy(&ht[(size_t)i * kMlpOut], &ht[(size_t)i * kMlpOut] + kMlpOut, t + cnt * kMlpOut);
+            }
+            ++cnt;
+        }
+        return MGSB_OK;
+    };
+    // (1) the residual of the last global step, r = b - A d (a pre-smoothing input)
+    k_ls_residual<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, h->d_final,
+                                             h->b, h->ls_r, nullptr, nullptr);
+    TRY(collect(h->ls_r));
+    // (2) the residual after plain pre-smoothing and the coarse correction (a
+    //     post-smoothing input): e = sweeps(r) + P V_c(P^T (r - A e)), r2 = r - A e
+    float4* e = sweeps_from_zero(h->ls_r, p.pre_sweeps);
+    k_l0_residual_rg<<<g0, kBlock, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, e, h->ls_r, l0.res, nullptr);
+    ca.d = e;
+    TRY(launch_coarse(h, ca));
+    k_l0_prolong<<<grid_for(n0), kBlock, 0, st>>>(n0, lv[1].pid, lv[1].pw, lv[1].e, e, nullptr);
+    k_ls_residual<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, e, h->ls_r,
+                                             h->ls_save, nullptr, nullptr);
+    TRY(collect(h->ls_save));
+    h->launches = launches;
+    *n = cnt;
+    if (x && t && cnt > cap) return set_err(h, MGSB_INVALID_ARG, "pair buffer too small (%lld < %lld)", (long long)cap,
+                                             (long long)cnt);
+    return MGSB_OK;
+}
+
+// Convergence of V-cycles on the last global step's correction equation
+// A e = r (r = b - A d, e from zero), for the smoother comparison: mode 0 =
+// plain with the configured sweeps, 1 = plain with one sweep each side, 2 =
+// learned (no fallback).  out[0] = |r|, out[k] = |r - A e| after k cycles.
+extern "C" mgsb_status mgsb_vcycle_residuals(mgsb_solver* h, int32_t cycles, int32_t mode, double* out) {
+    if (!h || !out || cycles < 1 || mode < 0 || mode > 2) return MGSB_INVALID_ARG;
+    if (!is_mg(h) || h->p.precision != MGSB_PRECISION_FP32)
+        return set_err(h, MGSB_NOT_SUPPORTED, "V-cycle residuals are measured on the plain FP32 multigrid solver");
+    if (h->dirty || !h->d_final) return set_err(h, MGSB_INVALID_ARG, "run a frame first");
+    if (mode == 2 && !h->ls_net) return set_err(h, MGSB_INVALID_ARG, "no learned smoother attached");
+    if (h->fuse_l0) return set_err(h, MGSB_NOT_SUPPORTED, "needs the shared-memory coarse kernel (fuse_level0 = 0)");
+    TRY(sync_check(h));
+    const int n0 = h->N0;
+    auto& pool = h->pair_mem;
+    if (!h->ls_xf) {
+        TRY(dalloc(h, pool, &h->ls_xf, (size_t)n0 * kMlpIn));
+        TRY(dalloc(h, pool, &h->ls_t, (size_t)n0 * kMlpOut));
+        TRY(dalloc(h, pool, &h->ls_mask, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_e1, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_e2, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_ec, (size_t)n0));
+        TRY(dalloc(h, pool, &h->ls_s, (size_t)n0));
+    }
+    std::vector<LevelDev>& lv = h->lev;
+    const LevelDev& l0 = lv[0];
+    const int g0 = h->ls_nblk;
+    cudaStream_t st = h->stream;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    float4* rhs = h->ls_ec;   // r, kept for the whole measurement
+    k_ls_residual<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, h->d_final,
+                                             h->b, rhs, nullptr, nullptr);
+    float4* e = h->ls_e1;
+    float4* tmp = h->ls_e2;
+    CUDA_TRY(h, cudaMemsetAsync(e, 0, (size_t)n0 * sizeof(float4), st));
+    std::vector<float> part(g0);
+    auto norm = [&](double* dst) -> mgsb_status {
+        k_ls_residual<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, e, rhs,
+                                                 nullptr, nullptr, h->ls_part1);
+        CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->ls_part1, g0 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        double a = 0.0;
+        for (float v : part) a += v;
+        *dst = std::sqrt(a);
+        return MGSB_OK;
+    };
+    TRY(norm(out));
+    CoarseArgs ca;
+    fill_coarse_args(h, ca);
+    const mgsb_params& p = h->p;
+    const int pre = mode == 1 ? 1 : p.pre_sweeps, post = mode == 1 ? 1 : p.post_sweeps;
+    const bool prof = h->profiling;
+    const int launches = h->launches;   // this measurement is not part of a frame
+    h->profiling = false;
+    for (int c = 0; c < cycles; ++c) {
+        if (mode == 2) {
+            // the learned cycle without its fallback: open the gate never
+            const float g = h->ls_gamma;
+            h->ls_gamma = 1e18f;
+            enqueue_learned_vcycle(h, e, tmp, rhs, c == 0, ca);
+            h->ls_gamma = g;
+        } else {
+            float4* xa = e;
+            float4* xb = tmp;
+            for (int k = 0; k < pre; ++k) {
+                k_l0_sweep_rg<<<g0, kBlock, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb,
+                                                     rhs, h->b0, h->slot_ptr, h->slots, 0, nullptr);
+                std::swap(xa, xb);
+            }
+            k_l0_residual_rg<<<g0, kBlock, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, xa, rhs, l0.res,
+                                                    nullptr);
+            ca.d = xa;
+            ca.gate = nullptr;
+            TRY(launch_coarse(h, ca));
+            k_l0_prolong<<<grid_for(n0), kBlock, 0, st>>>(n0, lv[1].pid, lv[1].pw, lv[1].e, xa, nullptr);
+            for (int k = 0; k < post; ++k) {
+                k_l0_sweep_rg<<<g0, kBlock, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb,
+                                                     rhs, h->b0, h->slot_ptr, h->slots, 0, nullptr);
+                std::swap(xa, xb);
+            }
+            if (xa != e) CUDA_TRY(h, cudaMemcpyAsync(e, xa, (size_t)n0 * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        }
+        CUDA_TRY(h, cudaGetLastError());
+        TRY(norm(out + c + 1));
+    }
+    h->profiling = prof;
+    h->launches = launches;
     return MGSB_OK;
 }

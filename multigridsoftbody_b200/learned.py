@@ -72,3 +72,60 @@ class MLP:
         losses = np.empty(steps, np.float32)
         self._check(self._lib.mgsb_mlp_train(self.h, _fp(x), _fp(t), x.shape[0], steps, batch, lr, seed, _fp(losses)))
         return losses
+
+
+# ---------------------------------------------------------------------------
+# The learned-smoother scene (organ-like blob) and the training pipeline
+# ---------------------------------------------------------------------------
+def blob_scene(levels: int = 5, precision: int = L.PRECISION_FP32, refinement_passes: int = 1, **overrides):
+    """Blob from a 64x32x48 voxel grid (spacing 0.25) inside (x/6)^2+(y/3)^2+(z/4)^2 < 1 + 0.15 s(x,y,z)
+    (seed-3 value noise, period 2), 6 tets per voxel; fixed x < -5; E 3e4, nu 0.45; gravity -9.8 along z;
+    dt 1/60; multigrid with `levels` levels.  Returns (mesh, fixed mask, params)."""
+    from .api import blob_mesh, default_params
+    m = blob_mesh()
+    fixed = (m.positions[:, 0] < -5.0).astype(np.uint8)
+    p = default_params(L.SOLVER_MULTIGRID, levels=levels, gravity=(0.0, 0.0, -9.8), youngs_modulus=3e4,
+                       poisson_ratio=0.45, precision=precision, refinement_passes=refinement_passes, **overrides)
+    return m, fixed, p
+
+
+def blob_tool_path(frames: int, seed: int, start=(0.0, 0.0, 3.3), dz: float = -0.02, sigma: float = 0.005,
+                   half_length: float = 4.0):
+    """Capsule r 0.3 along x (segment length 8) above the blob, moving -z 0.02 per frame plus
+    N(0, sigma^2) jitter per axis (seeded)."""
+    rng = np.random.default_rng(seed)
+    c = np.array(start, np.float64)
+    out = []
+    for _ in range(frames):
+        c = c + np.array([0.0, 0.0, dz]) + rng.normal(0.0, sigma, 3)
+        out.append(((c - [half_length, 0, 0]).astype(np.float32), (c + [half_length, 0, 0]).astype(np.float32)))
+    return out
+
+
+def generate_pairs(runs: int = 32, frames: int = 40, every: int = 20, sweeps: int = 4, device: int = 0,
+                   first_seed: int = 100):
+    """Residual/correction pairs from the plain FP32 multigrid solver on `runs` seeded blob runs:
+    every `every` frames, the pairs of the state after the frame (mgsb_smoother_pairs)."""
+    from .api import Solver
+    m, fixed, p = blob_scene()
+    p.device = device
+    xs, ts = [], []
+    for r in range(runs):
+        s = Solver(m, p)
+        s.set_fixed(fixed)
+        path = blob_tool_path(frames, seed=first_seed + r)
+        for f in range(frames):
+            s.set_capsule(*path[f], 0.3)
+            s.step()
+            if (f + 1) % every == 0:
+                x, t = s.smoother_pairs(sweeps)
+                xs.append(x)
+                ts.append(t)
+        s.close()
+    return np.concatenate(xs), np.concatenate(ts)
+
+
+def train_smoother(x, t, steps: int = 20000, batch: int = 4096, lr: float = 2e-3, seed: int = 0, device: int = 0):
+    net = MLP(device=device, seed=seed)
+    losses = net.train(x, t, steps=steps, batch=batch, lr=lr, seed=seed + 1)
+    return net, losses

@@ -1,0 +1,122 @@
+"""The learned smoother inside the V-cycle: training pairs from the plain
+solver, training on the GPU, the gain over plain sweeps at equal sweep count,
+the residual guard with its plain fallback (eager and in a CUDA graph), and
+parity of the learned mixed-precision solver with the FP64 oracle."""
+import numpy as np
+import pytest
+
+import multigridsoftbody_b200 as mg
+from multigridsoftbody_b200.learned import MLP, NUM_PARAMS
+from oracle.binding import Oracle
+
+from .common import beam, capsule_path, mg_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _train_on_beam(frames=24, steps=1500, seed=0):
+    m, fixed = beam(4, 40, 4)
+    s = mg.Solver(m, mg_params(levels=3))
+    s.set_fixed(fixed)
+    xs, ts = [], []
+    for f, (a, b) in enumerate(capsule_path(frames, start=(0.0, 0.0, 1.3), seed=seed + 3)):
+        s.set_capsule(a, b, 0.3)
+        s.step()
+        if f % 4 == 3:
+            x, t = s.smoother_pairs(4)
+            xs.append(x)
+            ts.append(t)
+    s.close()
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    net = MLP(seed=seed)
+    losses = net.train(x, t, steps=steps, batch=2048, lr=2e-3, seed=seed + 1)
+    return net, x, t, losses
+
+
+@pytest.fixture(scope="module")
+def trained():
+    return _train_on_beam()
+
+
+def test_pairs_and_training(lib, trained):
+    net, x, t, losses = trained
+    assert x.shape[1] == 9 and t.shape[1] == 3 and x.shape[0] == t.shape[0] > 1000
+    assert np.isfinite(x).all() and np.isfinite(t).all()
+    assert losses[-100:].mean() < 0.05 * losses[:10].mean(), (losses[:10].mean(), losses[-100:].mean())
+
+
+def test_learned_sweep_gains_over_plain(lib, trained):
+    """Ablation at equal sweep count: one learned sweep before and after the
+    coarse correction against one Jacobi sweep each side (and, for scale,
+    the configured two)."""
+    net = trained[0]
+    m, fixed = beam(4, 40, 4)
+    s = mg.Solver(m, mg_params(levels=3))
+    s.set_fixed(fixed)
+    s.set_learned_smoother(net, 0.5)
+    facs = {0: [], 1: [], 2: []}
+    for f, (a, b) in enumerate(capsule_path(30, start=(0.0, 0.0, 1.3), seed=42)):
+        s.set_capsule(a, b, 0.3)
+        s.step()
+        if f % 10 == 9:
+            for mode in facs:
+                r = s.vcycle_residuals(4, mode)
+                facs[mode].append((r[-1] / r[0]) ** 0.25)
+    plain22, plain11, learned = (np.mean(facs[k]) for k in (0, 1, 2))
+    assert learned < 0.7 * plain11, (plain22, plain11, learned)
+    assert learned < 1.5 * plain22, (plain22, plain11, learned)
+    v, fb = s.learned_stats()
+    assert v > 0 and fb <= v // 10, (v, fb)
+    s.close()
+
+
+@pytest.mark.parametrize("graph", [1, 0])
+def test_guard_falls_back_to_plain(lib, graph):
+    """A network with wild weights fails the residual check on every V-cycle;
+    the fallback restores the start and runs the plain cycle, so the frame
+    equals the plain solver's."""
+    m, fixed = beam(4, 40, 4)
+    bad = MLP(seed=11)
+    bad.params = np.random.default_rng(0).normal(0.0, 30.0, NUM_PARAMS).astype(np.float32)
+    runs = {}
+    for learned in (False, True):
+        s = mg.Solver(m, mg_params(levels=3, use_graph=graph))
+        s.set_fixed(fixed)
+        if learned:
+            s.set_learned_smoother(bad, 0.5)
+        for a, b in capsule_path(12, start=(0.0, 0.0, 1.3)):
+            s.set_capsule(a, b, 0.3)
+            s.step()
+        runs[learned] = s.positions()
+        if learned:
+            v, fb = s.learned_stats()
+            assert v == 12 * 10 and fb == v, (v, fb)
+        s.close()
+    # the fallback gathers the right-hand side in a different order than the
+    # plain sweep, so agreement is to rounding, not bitwise
+    assert np.abs(runs[True] - runs[False]).max() < 1e-6 * m.bbox_diagonal()
+
+
+def test_learned_mixed_matches_oracle(lib, oracle_built, trained):
+    """Learned smoother + mixed precision (FP64 residual, 3 refinement passes)
+    against the FP64 oracle running plain V-cycles with the same passes: the
+    global steps converge, so the smoother does not show in the frames."""
+    net = trained[0]
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=3)
+    s = mg.Solver(m, p)
+    s.set_fixed(fixed)
+    s.set_learned_smoother(net, 0.5)
+    o = Oracle(m, p)
+    o.set_fixed(fixed)
+    path = capsule_path(60, start=(0.0, 0.0, 1.4))
+    for f in range(60):
+        for solver in (s, o):
+            solver.set_capsule(*path[f], 0.3)
+            solver.step()
+    err = np.abs(s.positions_f64() - o.positions()).max()
+    assert err < 1e-5 * m.bbox_diagonal(), err
+    assert np.array_equal(np.nonzero(s.contact_flags())[0], np.nonzero(o.contact_flags())[0])
+    v, fb = s.learned_stats()
+    assert v == 60 * 10 * 3 and fb <= v // 10, (v, fb)
+    s.close()
