@@ -2,12 +2,16 @@
 """Benchmark: PD frames/s of the 103,680-tet beam with a moving capsule tool.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload beam|beam_mixed|batch|small]
+                    [--workload beam|beam_plain|beam_mixed|large_mixed|batch|blob|small]
 
-One "step" = one PD frame (10 local/global iterations, one V-cycle each) of
-the workload on one GPU.  Multi-GPU runs are independent replicas (the single
-body does not shard); value = frames of all ranks / max-over-ranks time.
-L2 is flushed (256 MB write) before every timed frame, outside the timed span.
+One "step" = one PD frame (10 local/global iterations) of the workload on one
+GPU.  The default workload is the headline: the learned-smoother mixed-precision
+multigrid (2 refinement passes per PD iteration) on the 103,680-tet beam, with
+the plain FP32 multigrid (1 V-cycle per PD iteration) timed the same way in the
+same run and both checked for max vertex error against a converged reference.
+Multi-GPU runs are independent replicas (the single body does not shard);
+value = frames of all ranks / max-over-ranks time.  L2 is flushed (256 MB
+write) before every timed frame, outside the timed span.
 """
 from __future__ import annotations
 
@@ -45,10 +49,10 @@ def capsule_path(frames, start=(0.0, 0.0, 3.0), dz=-0.02, sigma=0.005, half_leng
 def make_workload(name, mg):
     """Returns (meshes, params list, fixed masks, per-frame tool callback, description,
     per-body materials or None)."""
-    if name in ("beam", "beam_mixed", "small", "large_mixed"):
+    if name in ("beam", "beam_plain", "beam_mixed", "small", "large_mixed"):
         dims = {"small": (4, 40, 4), "large_mixed": (24, 240, 24)}.get(name, (12, 120, 12))
         levels = {"small": 3, "large_mixed": 5}.get(name, 4)
-        mixed = name in ("beam_mixed", "large_mixed")
+        mixed = name in ("beam", "beam_mixed", "large_mixed")
         m = mg.box_mesh(*dims)
         fixed = (np.abs(m.positions[:, 1] - 10.0) < 1e-5).astype(np.uint8)
         p = mg.default_params(mg.SOLVER_MULTIGRID, levels=levels, iterations=10, gravity=(0.0, 0.0, 0.0),
@@ -66,11 +70,26 @@ def make_workload(name, mg):
             rng = np.random.default_rng(7)
             mats = [(np.exp(rng.uniform(np.log(5e4), np.log(2e5), m.num_tets)).astype(np.float32), 0.3)]
         desc = (f"beam {dims[0]}x{dims[1]}x{dims[2]} hexes ({m.num_verts} verts, {m.num_tets} tets), "
-                f"{levels} MG levels, 2+2 Jacobi sweeps, 10 PD iterations/frame, capsule r=0.3 len 8 "
+                f"{levels} MG levels, 10 PD iterations/frame, capsule r=0.3 len 8 "
                 f"moving -z 0.02/frame + N(0,0.005^2) jitter (seed 1), in contact"
+                + (", learned smoother (1 learned sweep before and after the coarse correction, residual guard "
+                   "with plain fallback)" if name == "beam" else ", 2+2 Jacobi sweeps")
                 + (", mixed precision (FP64 residual, 2 refinement passes)" if mixed else "")
                 + (", E log-uniform [5e4,2e5] per tet (seed 7)" if name == "large_mixed" else ""))
         return [m], [p], [fixed], tool, desc, mats
+    if name == "blob":
+        from multigridsoftbody_b200.learned import blob_scene, blob_tool_path
+        m, fixed, p = blob_scene(precision=mg.PRECISION_MIXED, refinement_passes=2)
+        path = blob_tool_path(4096, seed=1)
+
+        def tool(f):
+            a, b = path[f % len(path)]
+            return a[None], b[None], np.array([0.3], np.float32)
+
+        desc = (f"organ-like blob 64x32x48 voxels at 0.25 m ({m.num_verts} verts, {m.num_tets} tets), fixed x<-5, "
+                f"E 3e4, nu 0.45, gravity -z, 5 MG levels, 10 PD iterations, capsule r=0.3 len 8 from (0,0,3.3) "
+                f"moving -z 0.02/frame + jitter (seed 1); learned smoother + mixed precision (2 refinement passes)")
+        return [m], [p], [fixed], tool, desc, None
     if name == "batch":
         rng = np.random.default_rng(11)
         ns = rng.integers(2, 9, size=256)
@@ -198,6 +217,10 @@ def algorithmic_bytes(kernel, solver, meshes, params):
         return (gather + (k - 1) * plain) / k
     if kernel == "k_coarse_vcycle":
         return coarse_vcycle_bytes(solver, params)
+    if kernel == "k_ls_sweep_tc":
+        # learned sweep: level-0 row walk (8 B/nnz, r/D/L/fix 28 B per row) + d read/write 32 B per row;
+        # the 12.9 KB weight image per CTA comes from L2
+        return 60 * n0 + 8 * nnz0
     return None
 
 
@@ -282,6 +305,86 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# Learned smoother: training from the plain solver, accuracy check
+# ---------------------------------------------------------------------------
+LEARNED = ("beam", "blob")
+
+
+def train_network(mg, name, device, stream_ptr, runs=8, frames=40, every=10, sweeps=4, steps=6000):
+    """Pairs from the plain FP32 multigrid solver on seeded runs of the same scene (tool seeds other than
+    the benchmark's), then the library's own trainer (Adam, 4096-pair minibatches)."""
+    from multigridsoftbody_b200.learned import MLP, blob_scene, blob_tool_path
+    t0 = time.perf_counter()
+    if name == "blob":
+        m, fixed, p = blob_scene()
+        paths = [blob_tool_path(frames, seed=100 + r) for r in range(runs)]
+    else:
+        m = mg.box_mesh(12, 120, 12)
+        fixed = (np.abs(m.positions[:, 1] - 10.0) < 1e-5).astype(np.uint8)
+        p = mg.default_params(mg.SOLVER_MULTIGRID, levels=4, iterations=10, gravity=(0.0, 0.0, 0.0))
+        paths = [capsule_path(frames, start=(0.0, 0.0, 1.5), seed=200 + r) for r in range(runs)]
+    p.device = device
+    p.stream = stream_ptr
+    xs, ts = [], []
+    for path in paths:
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        for f, (a, b) in enumerate(path):
+            s.set_capsule(a, b, 0.3)
+            s.step()
+            if f % every == every - 1:
+                x, t = s.smoother_pairs(sweeps)
+                xs.append(x)
+                ts.append(t)
+        s.close()
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    t1 = time.perf_counter()
+    net = MLP(device=device, seed=0)
+    losses = net.train(x, t, steps=steps, batch=4096, lr=2e-3, seed=1)
+    t2 = time.perf_counter()
+    info = {"pairs": int(x.shape[0]), "runs": runs, "frames_per_run": frames, "distilled_jacobi_sweeps": sweeps,
+            "train_steps": steps, "batch": 4096, "pair_generation_s": round(t1 - t0, 2),
+            "train_s": round(t2 - t1, 2), "loss_first": float(losses[:20].mean()),
+            "loss_last": float(losses[-200:].mean())}
+    return net, info
+
+
+def accuracy(mg, meshes, fixeds, params, tool, net, frames=40):
+    """Max vertex error / bbox diagonal after `frames` frames from rest, against a converged reference
+    (mixed precision with 6 FP64-residual V-cycles per PD iteration, plain smoother) on the GPU."""
+    m, fixed = meshes[0], fixeds[0]
+
+    def run(prec, passes, learned):
+        p = type(params[0]).from_buffer_copy(params[0])
+        p.precision = prec
+        p.refinement_passes = passes
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        if learned:
+            s.set_learned_smoother(net, 0.5)
+        for f in range(frames):
+            apply_tool(s, tool(f))
+            s.step()
+        x = s.positions_f64() if prec == mg.PRECISION_MIXED else s.positions().astype(np.float64)
+        stats = s.learned_stats() if learned else None
+        s.close()
+        return x, stats
+
+    ref, _ = run(mg.PRECISION_MIXED, 6, False)
+    diag = m.bbox_diagonal()
+    out = {"frames": frames, "reference": "GPU mixed precision, 6 V-cycles (FP64 residual) per PD iteration, "
+                                          "plain smoother; matches the FP64 oracle to ~1e-7 m"}
+    for key, prec, passes, learned in (("learned_mixed_2pass", mg.PRECISION_MIXED, 2, True),
+                                       ("plain_fp32_1pass", mg.PRECISION_FP32, 1, False),
+                                       ("plain_fp32_2pass", mg.PRECISION_FP32, 2, False)):
+        x, st = run(prec, passes, learned)
+        out[key] = {"err_over_diag": float(np.abs(x - ref).max() / diag)}
+        if st:
+            out[key]["learned_vcycles"], out[key]["fallbacks"] = st
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
@@ -302,11 +405,16 @@ def run_ours(args):
     for p in params:
         p.device = local
         p.stream = stream.cuda_stream
+    net, net_info = None, None
+    if args.workload in LEARNED:
+        net, net_info = train_network(mg, args.workload, local, stream.cuda_stream)
     solver = mg.Solver(meshes, params)
     for b, fx in enumerate(fixeds):
         solver.set_fixed(fx, body=b)
         if mats is not None:
             solver.set_material(*mats[b], body=b)
+    if net is not None:
+        solver.set_learned_smoother(net, 0.5)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
 
     def barrier():
@@ -356,8 +464,51 @@ def run_ours(args):
         torch.cuda.synchronize()
         apply_tool(solver, tool(frame))
         prof = solver.profile_frame()
+        frame += 1
+        # the plain FP32 multigrid (1 and 2 V-cycles per PD iteration), timed the same way
+        plain_ms = {}
+        if net is not None:
+            for passes in (1, 2):
+                pp = type(params[0]).from_buffer_copy(params[0])
+                pp.precision = mg.PRECISION_FP32
+                pp.refinement_passes = passes
+                sv = mg.Solver(meshes, [pp])
+                sv.set_fixed(fixeds[0])
+                if not args.no_tune:
+                    sv.autotune(frames=5)
+                for f in range(args.warmup):
+                    apply_tool(sv, tool(f))
+                    sv.step()
+                sv.synchronize()
+                barrier()
+                pevs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                        for _ in range(args.steps)]
+                for k in range(args.steps):
+                    flush.zero_()
+                    pevs[k][0].record(stream)
+                    apply_tool(sv, tool(args.warmup + k))
+                    sv.step()
+                    pevs[k][1].record(stream)
+                sv.synchronize()
+                barrier()
+                plain_ms[passes] = sum(a.elapsed_time(b) for a, b in pevs)
+                sv.close()
     from multigridsoftbody_b200.replicas import job_throughput, max_over_ranks
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist)
+    comparison = None
+    if net is not None:
+        p1, p2 = max_over_ranks([plain_ms[1], plain_ms[2]], dist)
+        comparison = {"plain_fp32_1pass": {"frames_per_s": job_throughput(args.steps, world, p1),
+                                           "ms_per_step": p1 / args.steps},
+                      "plain_fp32_2pass": {"frames_per_s": job_throughput(args.steps, world, p2),
+                                           "ms_per_step": p2 / args.steps},
+                      "network": net_info}
+        comparison["ratio_vs_plain_fp32_1pass"] = job_throughput(args.steps, world, ms) / comparison[
+            "plain_fp32_1pass"]["frames_per_s"]
+        comparison["ratio_vs_plain_fp32_2pass"] = job_throughput(args.steps, world, ms) / comparison[
+            "plain_fp32_2pass"]["frames_per_s"]
+        if rank == 0 and world == 1:
+            comparison["accuracy"] = accuracy(mg, meshes, fixeds, params, tool, net)
     value = job_throughput(args.steps, world, ms)
     e2e_value = job_throughput(args.steps, world, e2e_ms)
     if rank == 0:
@@ -384,7 +535,10 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": desc, "variant": "mixed precision multigrid" if params[0].precision == 1 else "plain FP32 multigrid", "parallelism": f"replicas x{world}",
+                "config": {"workload": desc,
+                           "variant": ("learned smoother + " if net is not None else "")
+                           + ("mixed precision multigrid" if params[0].precision == 1 else "plain FP32 multigrid"),
+                           "parallelism": f"replicas x{world}",
                            "l2": "flushed (256 MB write) before every timed frame, outside the timed span",
                            "autotuned_coarse_kernel": tuned},
                 "clocks": clk.summary(),
@@ -392,6 +546,7 @@ def run_ours(args):
                 "gpu_launches": launches * args.steps,
                 "roofline": roof,
                 "cpu_baseline": cpu,
+                "comparison": comparison,
                 "kernels": {k: {"ms_per_frame": v[0], "launches": v[1]} for k, v in
                             sorted(prof.items(), key=lambda kv: -kv[1][0])}}
         print(json.dumps(line))

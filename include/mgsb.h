@@ -319,13 +319,15 @@ mgsb_status mgsb_set_learned_smoother(mgsb_solver* h, const mgsb_mlp* net, float
 mgsb_status mgsb_learned_stats(mgsb_solver* h, uint64_t out[2]);
 /* Training pairs from the plain FP32 multigrid solver's current state: the
  * learned sweep is trained to reproduce `sweeps` weighted-Jacobi sweeps from
- * zero in one step.  Two residuals are used: r = b - A d of the last global
- * step (what pre-smoothing sees) and the residual left after plain
- * pre-smoothing and the coarse correction of r (what post-smoothing sees).  One
- * pair per free vertex whose residual scale s_i is at least 1e-2 of the state's
- * RMS: features x[9] of the residual against the Jacobi result in the network's
- * output space, t = e_sweeps / (s_i / D_i).  *n receives the count (up to
- * 2 x vertices); with x = t = NULL only counts. */
+ * zero in one step.  Three residuals are used: r = b - A d of the last global
+ * step, the residual left after plain pre-smoothing and the coarse correction
+ * of r (what post-smoothing sees), and the residual a further PD iteration
+ * would start from (local step at the current d; what pre-smoothing sees).  One
+ * pair per free vertex whose residual scale s_i is at least 1e-2 of that
+ * residual's RMS: features x[9] of the residual against the Jacobi result in
+ * the network's output space, t = e_sweeps / (s_i / D_i).  *n receives the
+ * count (up to 3 x vertices); with x = t = NULL only counts.  The call leaves
+ * the solver's state as it was, but not its scratch: call it between frames. */
 mgsb_status mgsb_smoother_pairs(mgsb_solver* h, int32_t sweeps, float* x, float* t, int64_t cap, int64_t* n);
 /* Smoother comparison on the last global step: V-cycles on A e = r from e = 0;
  * mode 0 plain (configured sweeps), 1 plain with 1+1 sweeps, 2 learned (no

@@ -300,7 +300,7 @@ class Solver:
     def smoother_pairs(self, sweeps: int = 4) -> tuple[np.ndarray, np.ndarray]:
         """Training pairs (features [n,9], targets [n,3]) from the current state (mgsb_smoother_pairs)."""
         n = C.c_int64()
-        cap = 2 * sum(self.num_verts(b) for b in range(self.num_bodies))
+        cap = 3 * sum(self.num_verts(b) for b in range(self.num_bodies))
         x = np.empty((cap, 9), np.float32)
         t = np.empty((cap, 3), np.float32)
         _check(self._lib.mgsb_smoother_pairs(self.h, sweeps, _fptr(x), _fptr(t), cap, C.byref(n)), self.h)

@@ -1979,6 +1979,15 @@ extern "C" mgsb_status mgsb_smoother_pairs(mgsb_solver* h, int32_t sweeps, float
     k_ls_residual<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, e, h->ls_r,
                                              h->ls_save, nullptr, nullptr);
     TRY(collect(h->ls_save));
+    // (3) the residual a further PD iteration would start from: the local step
+    //     at the current displacement gives b' = b0 + slots, r3 = b' - A d.
+    //     (the slots are rebuilt by the next frame's first local step)
+    k_mg_local<<<grid_for(h->T), kBlock, 0, st>>>(h->T, h->tets, h->tA, h->tB, h->tC, h->s, h->d_final, h->slot_of,
+                                                   h->slots);
+    k_gather_rhs<<<grid_for(n0), kBlock, 0, st>>>(n0, h->ls_ec, h->b0, h->slot_ptr, h->slots);
+    k_ls_residual<<<g0, kLsThreads, 0, st>>>(n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, h->d_final,
+                                             h->ls_ec, h->ls_save, nullptr, nullptr);
+    TRY(collect(h->ls_save));
     h->launches = launches;
     *n = cnt;
     if (x && t && cnt > cap) return set_err(h, MGSB_INVALID_ARG, "pair buffer too small (%lld < %lld)", (long long)cap,
