@@ -36,22 +36,35 @@ __device__ __forceinline__ float block_sum_f(float v, float* red) {
 }
 
 // r = fix * (b - A d) on level 0; optionally dsave = d and part[block] = sum |r|^2.
+// With slots set, b is first assembled as b0 + the row's RHS slots and stored
+// to bgather (the right-hand side of the PD iteration, reused afterwards).
 __global__ void __launch_bounds__(kLsThreads) k_ls_residual(int n, const int32_t* __restrict__ sp,
                                                             const int32_t* __restrict__ col, const float* __restrict__ val,
                                                             const float* __restrict__ dfull, const float* __restrict__ fixf,
                                                             const float4* __restrict__ d, const float4* __restrict__ b,
                                                             float4* __restrict__ r, float4* __restrict__ dsave,
-                                                            float* __restrict__ part) {
+                                                            float* __restrict__ part, const float4* __restrict__ b0 = nullptr,
+                                                            const int32_t* __restrict__ slot_ptr = nullptr,
+                                                            const float4* __restrict__ slots = nullptr,
+                                                            float4* __restrict__ bgather = nullptr) {
     __shared__ float red[kLsThreads / 32];
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
+    float4 bg = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (slots) {
+        const int beg = valid ? __ldg(slot_ptr + row) : 0, end = valid ? __ldg(slot_ptr + row + 1) : 0;
+        const float4 sl = rg_slot_sum<G>(valid, lane, beg, end, slots);
+        const float4 bb = valid ? __ldg(b0 + row) : make_float4(0.f, 0.f, 0.f, 0.f);
+        bg = make_float4(bb.x + sl.x, bb.y + sl.y, bb.z + sl.z, 0.f);
+        if (valid && lane < S) bgather[row] = bg;
+    }
     const float4 off = rg_offdiag<G, false>(row, valid, lane, sp, col, val, d);
     float rr = 0.f;
     if (valid && lane < S) {
-        const float4 x = d[row], bi = b[row];
+        const float4 x = d[row], bi = slots ? bg : b[row];
         const float D = __ldg(dfull + row), fx = __ldg(fixf + row);
         const float4 q = make_float4(fx * (bi.x - fmaf(D, x.x, off.x)), fx * (bi.y - fmaf(D, x.y, off.y)),
                                      fx * (bi.z - fmaf(D, x.z, off.z)), 0.f);
@@ -167,18 +180,22 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
     MlpSmem& Sm = *reinterpret_cast<MlpSmem*>(smem_raw);
     WaitState ws;
     uint32_t ph_load = 0, ph_mma = 0;
-    const uint32_t tmem = mlp_cta_setup(Sm, img, ws, ph_load, err);
+    // the weight copy overlaps the first tile's feature gather
+    const uint32_t tmem = mlp_cta_setup(Sm, img, ws, ph_load, err, false);
+    bool weights_pending = true;
+    __shared__ float part[5][kMlpTile];   // second half's 1-ring sums
+    const int rt = threadIdx.x & (kMlpTile - 1), half = threadIdx.x >> 7;   // 2 threads per row
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         __syncthreads();
         if (Sm.stop) break;
-        const int row = tile * kMlpTile + (int)threadIdx.x;
-        float f[kMlpIn];
-        float sc = 0.f;
+        const int row = tile * kMlpTile + rt;
+        float sx = 0.f, sy = 0.f, sz = 0.f, sa = 0.f, sd = 0.f;
         if (row < n) {
-            float sx = 0.f, sy = 0.f, sz = 0.f, sa = 0.f, sd = 0.f;
+            // the two threads of a row take alternate entries of its sliced-ELL row
             const int slice = row / S;
             const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
-            for (int e = beg + (row - slice * S); e < end; e += S) {
+#pragma unroll 4
+            for (int e = beg + (row - slice * S) + half * S; e < end; e += 2 * S) {
                 const float a = fabsf(__ldg(val + e));
                 const int j = __ldg(col + e);
                 const float4 rj = r[j];
@@ -189,22 +206,43 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
                 sa += a;
                 sd = fmaf(a, __ldg(dfull + j), sd);
             }
-            sc = ls_row_features(row, sx, sy, sz, sa, sd, dfull, diag0, fixf, r, f);
-        } else {
-#pragma unroll
-            for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
         }
-        ls_store_tile_row(Sm.x, threadIdx.x, f);
+        if (half) {
+            part[0][rt] = sx;
+            part[1][rt] = sy;
+            part[2][rt] = sz;
+            part[3][rt] = sa;
+            part[4][rt] = sd;
+        }
+        __syncthreads();
+        float sc = 0.f;
+        if (!half) {
+            float f[kMlpIn];
+            if (row < n) {
+                sc = ls_row_features(row, sx + part[0][rt], sy + part[1][rt], sz + part[2][rt], sa + part[3][rt],
+                                     sd + part[4][rt], dfull, diag0, fixf, r, f);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+            }
+            ls_store_tile_row(Sm.x, rt, f);
+        }
         fence_async_shared();
         tc_fence_before();
         __syncthreads();
+        bool wok = true;
+        if (weights_pending) {
+            wok = mlp_wait_weights(Sm, ws, ph_load, err);
+            weights_pending = false;
+        }
         float out[3];
-        const bool ok = mlp_tile_layers(Sm, tmem, ph_mma, ws, true, out);
+        const bool ok = mlp_tile_layers(Sm, tmem, ph_mma, ws, wok, out);
         if (!ok) {
             Sm.stop = 1;
             if (err) atomicExch(err, 1);
         }
-        if (ok && row < n && sc != 0.f) {
+        // threads 0..127 hold row rt's outputs (warps 0-3 serve TMEM lanes 0..127)
+        if (ok && !half && row < n && sc != 0.f) {
             float4 q = d[row];
             q.x += sc * out[0];
             q.y += sc * out[1];
@@ -212,6 +250,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
             d[row] = q;
         }
     }
+    if (weights_pending) mlp_wait_weights(Sm, ws, ph_load, err);   // no copy may outlive the CTA
     mlp_cta_teardown(Sm, tmem, ws);
 }
 
@@ -236,6 +275,59 @@ __global__ void k_ls_guard(int n0, const float* __restrict__ p0, int n1, const f
         if (use_cond) cudaGraphSetConditional(cond, pass ? 0u : 1u);
         stats[0] += 1ull;
         if (!pass) stats[1] += 1ull;
+    }
+}
+
+// The guard's residual |b - A d|^2 fused with the decision: every block writes
+// its partial sum, the last block to finish (atomic ticket) sums both partial
+// sets in a fixed order, decides, and resets the ticket for the next launch.
+__global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
+    int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col, const float* __restrict__ val,
+    const float* __restrict__ dfull, const float* __restrict__ fixf, const float4* __restrict__ d,
+    const float4* __restrict__ b, float* __restrict__ part1, const float* __restrict__ part0, float gamma2,
+    int32_t* __restrict__ gate, unsigned long long* __restrict__ stats, cudaGraphConditionalHandle cond, int use_cond,
+    unsigned int* __restrict__ ticket) {
+    __shared__ float red[kLsThreads / 32];
+    __shared__ bool last;
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const float4 off = rg_offdiag<G, false>(row, valid, lane, sp, col, val, d);
+    float rr = 0.f;
+    if (valid && lane < S) {
+        const float4 x = d[row], bi = b[row];
+        const float Dg = __ldg(dfull + row), fx = __ldg(fixf + row);
+        const float qx = fx * (bi.x - fmaf(Dg, x.x, off.x)), qy = fx * (bi.y - fmaf(Dg, x.y, off.y)),
+                    qz = fx * (bi.z - fmaf(Dg, x.z, off.z));
+        rr = qx * qx + qy * qy + qz * qz;
+    }
+    const float t = block_sum_f(rr, red);
+    if (threadIdx.x == 0) {
+        part1[blockIdx.x] = t;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    float a = 0.f, c = 0.f;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        a += part0[i];
+        c += part1[i];
+    }
+    __syncthreads();
+    const float before = block_sum_f(a, red);
+    __syncthreads();
+    const float after = block_sum_f(c, red);
+    if (threadIdx.x == 0) {
+        const bool pass = isfinite(before) && isfinite(after) && after <= gamma2 * before;
+        *gate = pass ? 0 : 1;
+        if (use_cond) cudaGraphSetConditional(cond, pass ? 0u : 1u);
+        stats[0] += 1ull;
+        if (!pass) stats[1] += 1ull;
+        *ticket = 0u;
     }
 }
 

@@ -41,10 +41,23 @@ __host__ __device__ constexpr int interleaved_offset(int row, int k, int K) {
     return (row >> 3) * (K >> 3) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016):
+//   g(x) = x/2 (1 + tanh(u)),  u = sqrt(2/pi) (x + 0.044715 x^3),
+// with the hardware tanh.approx.f32 (well below the BF16 rounding of the
+// activations that follows), the same in inference and in training.
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+    const float t = tanh_hw(kGeluC * fmaf(kGeluA * x, x * x, x));
+    return 0.5f * x * (1.f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-    // d/dx x Phi(x) = Phi(x) + x phi(x)
-    return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+    const float t = tanh_hw(kGeluC * fmaf(kGeluA * x, x * x, x));
+    return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * kGeluC * fmaf(3.f * kGeluA, x * x, 1.f);
 }
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
@@ -168,7 +181,7 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 //   out_mode 1: e[row] += scale[row] * (y0, y1, y2)   (learned smoothing sweep)
 // err (optional): set to 1 when a bounded wait ran out; the kernel then stops.
 // ---------------------------------------------------------------------------
-constexpr int kMlpThreads = 128;
+constexpr int kMlpThreads = 256;   // 8 warps: warp w serves TMEM lanes 32 (w % 4).. and hidden columns 32 (w / 4)..
 constexpr int kTmemCols = 256;     // D1 cols [0,64), D2 [64,128), D3 [128,144)
 constexpr int kMaxPolls = 1 << 22;
 
@@ -202,8 +215,10 @@ __device__ __forceinline__ bool wait_bar(WaitState& ws, uint64_t* bar, uint32_t 
 }
 
 // CTA prologue: barriers, TMEM (256 columns, warp 0) and the weight image.
+// With wait_weights = false the copy is left in flight (the caller overlaps it
+// with other work and calls mlp_wait_weights before the first MMA).
 __device__ __forceinline__ uint32_t mlp_cta_setup(MlpSmem& S, const uint8_t* img, WaitState& ws, uint32_t& ph_load,
-                                                  int32_t* err) {
+                                                  int32_t* err, bool wait_weights = true) {
     const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         mbar_init(&S.bar_load, 1);
@@ -224,12 +239,25 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(MlpSmem& S, const uint8_t* img
         mbar_expect_tx(&S.bar_load, kImgBytes);
         bulk_g2s(S.w, img, kImgBytes, &S.bar_load);
     }
-    if (!wait_bar(ws, &S.bar_load, ph_load)) {
+    if (wait_weights) {
+        if (!wait_bar(ws, &S.bar_load, ph_load)) {
+            S.stop = 1;
+            if (err) atomicExch(err, 1);
+        }
+        ph_load ^= 1;
+    }
+    return S.tmem_base;
+}
+
+// Completes a weight copy left in flight by mlp_cta_setup(..., false).
+__device__ __forceinline__ bool mlp_wait_weights(MlpSmem& S, WaitState& ws, uint32_t& ph_load, int32_t* err) {
+    const bool ok = wait_bar(ws, &S.bar_load, ph_load);
+    ph_load ^= 1;
+    if (!ok) {
         S.stop = 1;
         if (err) atomicExch(err, 1);
     }
-    ph_load ^= 1;
-    return S.tmem_base;
+    return ok;
 }
 
 // CTA epilogue: retry a timed-out wait once, then release TMEM.
@@ -242,11 +270,13 @@ __device__ __forceinline__ void mlp_cta_teardown(MlpSmem& S, uint32_t tmem, Wait
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
-// Hidden layer epilogue: gelu(D + bias) from TMEM columns [col, col+64) of this
-// thread's row -> BF16 into S.h (K-major interleaved, K = 64).
-__device__ __forceinline__ void mlp_hidden_epilogue(MlpSmem& S, uint32_t taddr, const float* bias, int row_in_tile) {
+// Hidden layer epilogue: gelu(D + bias) of this warp's half of the 64 columns
+// (c0 = 0 or 32) of this thread's row, from TMEM -> BF16 into S.h (K-major
+// interleaved, K = 64).
+__device__ __forceinline__ void mlp_hidden_epilogue(MlpSmem& S, uint32_t taddr, const float* bias, int row_in_tile,
+                                                    int c0) {
 #pragma unroll
-    for (int c = 0; c < kMlpHid; c += 16) {
+    for (int c = c0; c < c0 + kMlpHid / 2; c += 16) {
         float v[16];
         tmem_ld16(taddr + c, v);
         tmem_wait_ld();
@@ -269,8 +299,9 @@ __device__ __forceinline__ void mlp_hidden_epilogue(MlpSmem& S, uint32_t taddr, 
 __device__ __forceinline__ bool mlp_tile_layers(MlpSmem& S, uint32_t tmem, uint32_t& ph_mma, WaitState& ws, bool ok,
                                                 float (&y)[3]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row_in_tile = warp * 32 + lane;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const int grp = warp & 3, c0 = (warp >> 2) * (kMlpHid / 2);
+    const int row_in_tile = grp * 32 + lane;
+    const uint32_t lane_base = (uint32_t)(grp * 32) << 16;
     const float* bias = reinterpret_cast<const float*>(S.w + kImgB);
     const uint32_t id64 = umma_idesc_bf16(kMlpTile, kMlpHid), id16 = umma_idesc_bf16(kMlpTile, kMlpOutPad);
     // layer 1: D1 = X W1^T (K = 16: one MMA)
@@ -282,7 +313,7 @@ __device__ __forceinline__ bool mlp_tile_layers(MlpSmem& S, uint32_t tmem, uint3
     ok = ok && wait_bar(ws, &S.bar_mma, ph_mma);
     ph_mma ^= 1;
     tc_fence_after();
-    mlp_hidden_epilogue(S, tmem + lane_base + 0, bias, row_in_tile);
+    mlp_hidden_epilogue(S, tmem + lane_base + 0, bias, row_in_tile, c0);
     fence_async_shared();
     tc_fence_before();
     __syncthreads();
@@ -299,7 +330,7 @@ __device__ __forceinline__ bool mlp_tile_layers(MlpSmem& S, uint32_t tmem, uint3
     ph_mma ^= 1;
     tc_fence_after();
     // H2 overwrites H1: layer 2 has finished reading it
-    mlp_hidden_epilogue(S, tmem + lane_base + 64, bias + kMlpHid, row_in_tile);
+    mlp_hidden_epilogue(S, tmem + lane_base + 64, bias + kMlpHid, row_in_tile, c0);
     fence_async_shared();
     tc_fence_before();
     __syncthreads();
@@ -316,7 +347,7 @@ __device__ __forceinline__ bool mlp_tile_layers(MlpSmem& S, uint32_t tmem, uint3
     ph_mma ^= 1;
     tc_fence_after();
     float v[16];
-    tmem_ld16(tmem + lane_base + 128, v);
+    tmem_ld16(tmem + lane_base + 128, v);   // every warp (the .sync.aligned load is warp-wide); warps 0-3 use it
     tmem_wait_ld();
     tc_fence_before();
     y[0] = v[0] + bias[2 * kMlpHid];
@@ -356,7 +387,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_tc(int n, int ntiles, const
             if (err) atomicExch(err, 1);
         }
         const int row = tile * kMlpTile + row_in_tile;
-        if (ok && row < n) {
+        if (ok && row_in_tile < kMlpTile && row < n) {
             if (out_mode == 0) {
                 y[row] = make_float4(out[0], out[1], out[2], 0.f);
             } else {

@@ -169,6 +169,7 @@ struct mgsb_solver {
     float4 *ls_r = nullptr, *ls_save = nullptr;
     float *ls_part0 = nullptr, *ls_part1 = nullptr;
     int32_t *ls_gate = nullptr, *ls_werr = nullptr;
+    unsigned int* ls_ticket = nullptr;   // last-block ticket of the guard kernel (self-resetting)
     unsigned long long* ls_stats = nullptr;
     // training-pair generation (allocated on first use)
     float *ls_xf = nullptr, *ls_t = nullptr, *ls_s = nullptr;
@@ -504,6 +505,8 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dalloc(h, pool, &h->ls_gate, 1));
         TRY(dalloc(h, pool, &h->ls_werr, 1));
         TRY(dalloc(h, pool, &h->ls_stats, 2));
+        TRY(dalloc(h, pool, &h->ls_ticket, 1));
+        CUDA_TRY(h, cudaMemset(h->ls_ticket, 0, sizeof(unsigned int)));
         CUDA_TRY(h, cudaMemset(h->ls_stats, 0, 2 * sizeof(unsigned long long)));
         CUDA_TRY(h, cudaMemset(h->ls_gate, 0, sizeof(int32_t)));
         CUDA_TRY(h, cudaMemset(h->ls_werr, 0, sizeof(int32_t)));
@@ -629,7 +632,8 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
 // gamma |r_start| (or is not finite) the gate opens, d is restored and the
 // plain V-cycle runs (its kernels are launched gated and return at once when
 // the learned cycle passed).  dtmp: ping-pong buffer of the plain sweeps.
-void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float4* b, bool from_zero, CoarseArgs ca) {
+void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float4* b, bool from_zero, CoarseArgs ca,
+                            bool gather_b = false) {
     const mgsb_params& p = h->p;
     const int n0 = h->N0;
     std::vector<LevelDev>& lv = h->lev;
@@ -639,9 +643,10 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     const int mgrid = std::min(h->ls_ntiles, 2 * h->sm_count);
     const size_t msmem = mlp_tc_smem_bytes();
     float4* bw = const_cast<float4*>(b);
-    // pre-smoothing
+    // pre-smoothing (with gather_b the right-hand side b = b0 + slots is assembled here first)
     LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-           h->ls_r, from_zero ? nullptr : h->ls_save, h->ls_part0);
+           h->ls_r, from_zero ? nullptr : h->ls_save, h->ls_part0, gather_b ? h->b0 : nullptr,
+           gather_b ? h->slot_ptr : nullptr, gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
     // coarse correction
@@ -669,10 +674,9 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
         if (cudaGraphConditionalHandleCreate(&hnd, cap_graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
             h->capture_error = true;
     }
-    LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-           nullptr, nullptr, h->ls_part1);
-    LAUNCH(h, k_ls_guard, 1, kLsThreads, 0, g0, h->ls_part0, g0, h->ls_part1, h->ls_gamma * h->ls_gamma, h->ls_gate,
-           h->ls_stats, hnd, cond ? 1 : 0);
+    LAUNCH(h, k_ls_guard_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d,
+           b, h->ls_part1, h->ls_part0, h->ls_gamma * h->ls_gamma, h->ls_gate, h->ls_stats, hnd, cond ? 1 : 0,
+           h->ls_ticket);
     cudaStream_t main_stream = h->stream;
     if (cond) {
         const cudaGraphNode_t* deps = nullptr;
@@ -771,8 +775,8 @@ void enqueue_mg_frame(mgsb_solver* h) {
     for (int it = 0; it < p.iterations; ++it) {
         LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
         if (h->ls_net) {
-            LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
-            for (int pass = 0; pass < p.refinement_passes; ++pass) enqueue_learned_vcycle(h, xa, xb, h->b, false, ca);
+            for (int pass = 0; pass < p.refinement_passes; ++pass)
+                enqueue_learned_vcycle(h, xa, xb, h->b, false, ca, pass == 0);
             continue;
         }
         for (int pass = 0; pass < p.refinement_passes; ++pass) {

@@ -1136,9 +1136,15 @@ double bf16_round(double v) {
     std::memcpy(&f, &b, 4);
     return (double)f;
 }
-double gelu64(double x) { return 0.5 * x * (1.0 + std::erf(x / std::sqrt(2.0))); }
+// GELU, tanh form (Hendrycks & Gimpel 2016): x/2 (1 + tanh(sqrt(2/pi)(x + 0.044715 x^3)))
+double gelu64(double x) {
+    const double c = std::sqrt(2.0 / M_PI);
+    return 0.5 * x * (1.0 + std::tanh(c * (x + 0.044715 * x * x * x)));
+}
 double gelu64_grad(double x) {
-    return 0.5 * (1.0 + std::erf(x / std::sqrt(2.0))) + x * std::exp(-0.5 * x * x) / std::sqrt(2.0 * M_PI);
+    const double c = std::sqrt(2.0 / M_PI);
+    const double t = std::tanh(c * (x + 0.044715 * x * x * x));
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * c * (1.0 + 3.0 * 0.044715 * x * x);
 }
 
 struct MlpPass {

@@ -67,7 +67,7 @@ int oracle_level_matrix(const oracle_solver* h, int level, double* diag, int32_t
 /* Vertex normals of a triangle surface: UpdateTriNormal + AvgOutsideTetVertNormal
  * (PDSolver.cu:394-460).  pos [3V], tris [3F]; out [3V], zero where no triangle. */
 void oracle_surface_normals(const double* pos, int32_t V, const int32_t* tris, int32_t F, double* out);
-/* Learned-smoother MLP 9 -> 64 -> 64 -> 3 (GELU), parameters in the libmgsb
+/* Learned-smoother MLP 9 -> 64 -> 64 -> 3 (GELU, tanh form), parameters in the libmgsb
  * layout W1[64][9] b1[64] W2[64][64] b2[64] W3[3][64] b3[3].  With bf16 != 0
  * the weights (not the biases), the inputs and the hidden activations are
  * rounded to BF16 (round to nearest even) as on the tensor cores, and the
