@@ -281,6 +281,39 @@ mgsb_status mgsb_mesh_free(mgsb_mesh_data* m);
 double mgsb_value_noise(double x, double y, double z, double period, uint64_t seed);
 
 /* ------------------------------------------------------------------------
+ * The reference's two-level nested-iteration schedule — PDSolver_MG
+ * (PDSolver_MG.cpp:5-253, updatePointInTet / updateMapping PDSolver.cu:724-793,
+ * DCDByTriangle_sphere_V2 PDSolver.cu:612-680).  Two reference-kind solvers
+ * (mgsb_default_params(MGSB_SOLVER_REFERENCE_JACOBI) params, `iterations`
+ * per level) on a coarse and a fine mesh of the same body.  Per frame: both
+ * predict; the coarse level iterates with sphere-vs-surface-triangle
+ * collision; fine positions are interpolated from the coarse tets that hold
+ * them; the fine level iterates with per-vertex sphere collision; coarse
+ * positions are averaged back from the fine tets; the fine-in-coarse weights
+ * are recomputed; velocities follow.  The whole frame is one CUDA graph.
+ * Level 0 = fine, 1 = coarse.
+ * ------------------------------------------------------------------------ */
+typedef struct mgsb_two_level mgsb_two_level;
+/* PDSolver_MG::Init: binds every fine vertex to the coarse tet holding it and
+ * every coarse vertex to the fine tet holding it (MGSB_INVALID_ARG if a vertex
+ * lies outside the other mesh). */
+mgsb_status mgsb_mg2_create(const mgsb_mesh* coarse, const mgsb_mesh* fine, const mgsb_params* params,
+                            mgsb_two_level** out);
+mgsb_status mgsb_mg2_destroy(mgsb_two_level* t);
+const char* mgsb_mg2_last_error(const mgsb_two_level* t);
+/* The level's solver handle for the getters (positions, contacts, energy, ...);
+ * owned by t. */
+mgsb_status mgsb_mg2_level(mgsb_two_level* t, int32_t level, mgsb_solver** out);
+/* SetFixedVert of both PDSolvers (NULL leaves a level unchanged). */
+mgsb_status mgsb_mg2_set_fixed(mgsb_two_level* t, const uint8_t* coarse_mask, const uint8_t* fine_mask);
+/* g_simulator->m_sphereColliders for both levels. */
+mgsb_status mgsb_mg2_set_tool_spheres(mgsb_two_level* t, int32_t count, const float* centers, const float* radii,
+                                      const uint8_t* active);
+/* PDSolver_MG::Step. */
+mgsb_status mgsb_mg2_step(mgsb_two_level* t);
+mgsb_status mgsb_mg2_get_positions(mgsb_two_level* t, int32_t level, float* out);
+
+/* ------------------------------------------------------------------------
  * Learned smoother network (config 4).  No counterpart in the reference: its
  * multigrid smoother is plain Jacobi (PDSolver.cu:192-235).
  * A per-vertex MLP 9 -> 64 -> 64 -> 3 with GELU, BF16 weights/activations and

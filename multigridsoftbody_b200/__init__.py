@@ -5,12 +5,12 @@ include/mgsb.h); this package is its Python host mirror.
 """
 from ._lib import (PRECISION_FP32, PRECISION_MIXED, SOLVER_MULTIGRID, SOLVER_REFERENCE_JACOBI, MgsbError, Params,
                    load)
-from .api import (Solver, TetMesh, blob_mesh, box_mesh, default_params, extract_surface, params_dict, read_msh,
-                  value_noise)
+from .api import (Solver, TetMesh, TwoLevel, blob_mesh, box_mesh, default_params, extract_surface, params_dict,
+                  read_msh, value_noise)
 from .pdsolver import PDSolver, SphereCollider, SphereFixer
 
 __all__ = [
     "PRECISION_FP32", "PRECISION_MIXED", "SOLVER_MULTIGRID", "SOLVER_REFERENCE_JACOBI", "MgsbError", "Params", "load",
-    "Solver", "TetMesh", "blob_mesh", "box_mesh", "default_params", "extract_surface", "params_dict", "read_msh",
+    "Solver", "TetMesh", "TwoLevel", "blob_mesh", "box_mesh", "default_params", "extract_surface", "params_dict", "read_msh",
     "value_noise", "PDSolver", "SphereCollider", "SphereFixer",
 ]

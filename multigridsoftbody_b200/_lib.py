@@ -115,6 +115,14 @@ SIGNATURES = [
     ("mgsb_learned_stats", C.c_int, [_P, C.POINTER(C.c_uint64)]),
     ("mgsb_smoother_pairs", C.c_int, [_P, C.c_int32, _FP, _FP, C.c_int64, C.POINTER(C.c_int64)]),
     ("mgsb_vcycle_residuals", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    ("mgsb_mg2_create", C.c_int, [C.POINTER(Mesh), C.POINTER(Mesh), C.POINTER(Params), C.POINTER(_P)]),
+    ("mgsb_mg2_destroy", C.c_int, [_P]),
+    ("mgsb_mg2_last_error", C.c_char_p, [_P]),
+    ("mgsb_mg2_level", C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
+    ("mgsb_mg2_set_fixed", C.c_int, [_P, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
+    ("mgsb_mg2_set_tool_spheres", C.c_int, [_P, C.c_int32, _FP, _FP, C.POINTER(C.c_uint8)]),
+    ("mgsb_mg2_step", C.c_int, [_P]),
+    ("mgsb_mg2_get_positions", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_mlp_num_params", C.c_int32, []),
     ("mgsb_mlp_create", C.c_int, [C.c_int32, C.c_uint64, C.POINTER(_P)]),
     ("mgsb_mlp_destroy", C.c_int, [_P]),

@@ -410,3 +410,75 @@ class Solver:
         z = C.c_int32()
         _check(self._lib.mgsb_level_size(self.h, level, C.byref(n), C.byref(z)), self.h)
         return n.value, z.value
+
+
+class _LevelSolver(Solver):
+    """A level of a TwoLevel handle: the Solver getters on a handle it does not own."""
+
+    def __init__(self, lib, h, mesh, params):  # no Solver.__init__: the handle belongs to the TwoLevel
+        self._lib = lib
+        self.h = h
+        self.meshes = [mesh]
+        self.params = [params]
+
+    def close(self) -> None:
+        self.h = None
+
+
+class TwoLevel:
+    """The reference's two-level nested-iteration schedule (PDSolver_MG) on a coarse and a fine mesh of
+    one body; levels[0] = fine, levels[1] = coarse (Solver getters)."""
+
+    def __init__(self, coarse: TetMesh, fine: TetMesh, params: Params):
+        self._lib = L.load()
+        mc, kc = coarse.as_c()
+        mf, kf = fine.as_c()
+        h = C.c_void_p()
+        st = self._lib.mgsb_mg2_create(C.byref(mc), C.byref(mf), C.byref(params), C.byref(h))
+        if st != 0:
+            msg = self._lib.mgsb_mg2_last_error(h) if h else b""
+            raise MgsbError(st, "mgsb_mg2_create failed: " + (msg.decode() if msg else ""))
+        self.h = h
+        self.levels = []
+        for lvl, mesh in ((0, fine), (1, coarse)):
+            lh = C.c_void_p()
+            _check(self._lib.mgsb_mg2_level(self.h, lvl, C.byref(lh)))
+            self.levels.append(_LevelSolver(self._lib, lh, mesh, params))
+
+    def _chk(self, st):
+        if st != 0:
+            msg = self._lib.mgsb_mg2_last_error(self.h)
+            raise MgsbError(st, msg.decode() if msg else "")
+
+    def set_fixed(self, coarse_mask=None, fine_mask=None) -> None:
+        cm = np.ascontiguousarray(coarse_mask, np.uint8) if coarse_mask is not None else None
+        fm = np.ascontiguousarray(fine_mask, np.uint8) if fine_mask is not None else None
+        self._chk(self._lib.mgsb_mg2_set_fixed(self.h, _u8ptr(cm) if cm is not None else None,
+                                               _u8ptr(fm) if fm is not None else None))
+
+    def set_spheres(self, centers, radii, active=None) -> None:
+        c = np.ascontiguousarray(centers, np.float32).reshape(-1, 3)
+        r = np.ascontiguousarray(radii, np.float32).reshape(-1)
+        a = np.ascontiguousarray(active, np.uint8) if active is not None else None
+        self._chk(self._lib.mgsb_mg2_set_tool_spheres(self.h, c.shape[0], _fptr(c), _fptr(r),
+                                                      _u8ptr(a) if a is not None else None))
+
+    def step(self, n: int = 1) -> None:
+        for _ in range(n):
+            self._chk(self._lib.mgsb_mg2_step(self.h))
+
+    def positions(self, level: int = 0) -> np.ndarray:
+        return self.levels[level].positions()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            for lv in self.levels:
+                lv.close()
+            self._lib.mgsb_mg2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

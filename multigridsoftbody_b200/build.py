@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
               "-Xptxas", "-v"]
 
-SOURCES = ["solver.cu", "mlp.cu", "plan.cpp", "setup.cpp", "mesh.cpp", "mesh_api.cpp"]
+SOURCES = ["solver.cu", "mlp.cu", "plan.cpp", "setup.cpp", "mesh.cpp", "mesh_api.cpp", "twolevel.cpp"]
 
 
 def _nvcc() -> str:

@@ -68,7 +68,7 @@ __global__ void k_ref_predict(int n, float4* __restrict__ x, float4* __restrict_
 __global__ void __launch_bounds__(256) k_ref_local(int T, const int4* __restrict__ tets, const float4* __restrict__ invA,
                                                    const float4* __restrict__ invB, const float2* __restrict__ invC,
                                                    const float4* __restrict__ x, const int4* __restrict__ slot_of,
-                                                   float4* __restrict__ slots, float stiffness) {
+                                                   float4* __restrict__ slots, float stiffness, int drop_small = 1) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const int4 id = __ldg(tets + t);
@@ -109,7 +109,9 @@ __global__ void __launch_bounds__(256) k_ref_local(int T, const int4* __restrict
             if (isnan(val)) val = 0.f;
             val = fminf(10.0f, fmaxf(-10.0f, val));
             float res = val * vol * stiffness;
-            if ((double)fabsf(res) < 1e-5) res = 0.f;
+            // the single-kernel calculateIF of the two-level schedule (PDSolver.cu:128-183)
+            // keeps small contributions; getTetFRV2/calTetIFV1 drop |c| < 1e-5
+            if (drop_small && (double)fabsf(res) < 1e-5) res = 0.f;
             out[i] = res;
         }
         slots[sid[j]] = make_float4(out[0], out[1], out[2], 0.f);
@@ -125,7 +127,8 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
     float4* __restrict__ v, const float* __restrict__ fixf, const float* __restrict__ mass, const float* __restrict__ vdiag,
     const int32_t* __restrict__ slot_ptr, const float4* __restrict__ slots, const SphereSet* __restrict__ spheres,
     float kc, float dt, float omega, double relax, int last_iter, int32_t* __restrict__ cflag, float* __restrict__ cdepth,
-    float* __restrict__ cenergy, int32_t* __restrict__ nonfinite) {
+    float* __restrict__ cenergy, int32_t* __restrict__ nonfinite, const int32_t* __restrict__ tri_ptr = nullptr,
+    const int32_t* __restrict__ tri_idx = nullptr, const float4* __restrict__ tri_push = nullptr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float fx = 0.f, fy = 0.f, fz = 0.f;
@@ -139,7 +142,25 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
     float cd[3] = {0.f, 0.f, 0.f}, cf[3] = {0.f, 0.f, 0.f};
     int flag = 0;
     float depth = 0.f, ce = 0.f;
-    const int nsph = spheres->count;
+    if (tri_push) {
+        // collision from the surface triangles around this vertex (the coarse level of
+        // the two-level schedule): k_c per contact on every axis, k_c (c - hit) as force
+        float cnt = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+        const int t1 = __ldg(tri_ptr + i + 1);
+        for (int e = __ldg(tri_ptr + i); e < t1; ++e) {
+            const float4 q = tri_push[__ldg(tri_idx + e)];
+            mx += q.x;
+            my += q.y;
+            mz += q.z;
+            cnt += q.w;
+        }
+        cd[0] = cd[1] = cd[2] = kc * cnt;
+        cf[0] = kc * mx;
+        cf[1] = kc * my;
+        cf[2] = kc * mz;
+        flag = (int)cnt;
+    }
+    const int nsph = tri_push ? 0 : spheres->count;
     for (int q = 0; q < nsph; ++q) {
         if (!spheres->active[q]) continue;
         const float cx = spheres->cx[q], cy = spheres->cy[q], cz = spheres->cz[q];
@@ -191,9 +212,12 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
     prev[i] = p4;
     const float4 xn = make_float4(nx[0], nx[1], nx[2], 0.f);
     x[i] = xn;
-    if (last_iter) {
+    // last_iter: bit 0 = velocity, bit 1 = contact outputs and the finiteness check
+    if (last_iter & 1) {
         const float4 l4 = __ldg(last + i);
         v[i] = make_float4((xn.x - l4.x) / dt, (xn.y - l4.y) / dt, (xn.z - l4.z) / dt, 0.f);
+    }
+    if (last_iter & 2) {
         cflag[i] = flag;
         cdepth[i] = depth;
         cenergy[i] = ce;

@@ -15,12 +15,14 @@
 #include "kernels.cuh"
 #include "kernels_diag.cuh"
 #include "kernels_learned.cuh"
+#include "kernels_twolevel.cuh"
 #include "kernels_mg.cuh"
 #include "kernels_mixed.cuh"
 #include "mesh.hpp"
 #include "mlp.hpp"
 #include "plan.hpp"
 #include "setup.hpp"
+#include "twolevel.hpp"
 
 using namespace mgsb;
 
@@ -553,7 +555,7 @@ void enqueue_ref_frame(mgsb_solver* h) {
         omega = 4 / (4 - p.cheb_rho * p.cheb_rho * omega);
         LAUNCH(h, k_ref_vertex, grid_for(n), kBlock, 0, n, h->x, h->prev, h->s, h->last, h->v, h->fixf, h->mass,
                h->vdiag, h->slot_ptr, h->slots, h->spheres_dev, p.collision_stiffness, p.dt, omega,
-               (double)p.relaxation, it == p.iterations - 1 ? 1 : 0, h->cflag, h->cdepth, h->cenergy,
+               (double)p.relaxation, it == p.iterations - 1 ? 3 : 0, h->cflag, h->cdepth, h->cenergy,
                h->nonfinite);
     }
     if (p.iterations == 0) {
@@ -2087,3 +2089,240 @@ extern "C" mgsb_status mgsb_vcycle_residuals(mgsb_solver* h, int32_t cycles, int
     h->launches = launches;
     return MGSB_OK;
 }
+
+// ===========================================================================
+// The reference's two-level schedule (PDSolver_MG, PDSolver_MG.cpp:5-253)
+// ===========================================================================
+// Two reference-kind solvers share one stream: per frame both predict, the
+// coarse level runs its Jacobi/Chebyshev iterations with sphere-vs-surface-
+// triangle collision, the fine positions are interpolated from the coarse
+// mesh, the fine level iterates with per-vertex sphere collision, the coarse
+// positions are averaged back from the fine mesh, the fine-in-coarse weights are
+// recomputed from the current shapes, and both velocities follow.
+struct mgsb_two_level {
+    mgsb_solver* coarse = nullptr;
+    mgsb_solver* fine = nullptr;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    std::vector<DevMem> mem;
+    int nf = 0, nc = 0, ntri = 0;
+    int4* f_ids = nullptr;     // fine vertex -> coarse tet ids
+    float4* f_w = nullptr;     //   and weights (recomputed every frame)
+    int4* c_ids = nullptr;     // coarse vertex -> fine tet ids
+    float4* c_w = nullptr;
+    int4* tris = nullptr;      // coarse surface triangles
+    int32_t *tri_ptr = nullptr, *tri_idx = nullptr;   // coarse vertex -> its triangles
+    float4* push = nullptr;    // per-triangle push sum and contact count
+    bool graph_valid = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~mgsb_two_level() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        delete coarse;
+        delete fine;
+        cudaSetDevice(device);
+        for (auto& m : mem) cudaFree(m.p);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+mgsb_status tl_err(mgsb_two_level* t, mgsb_status s, const char* msg) {
+    if (t) t->err = msg;
+    return s;
+}
+
+template <typename T>
+mgsb_status tl_upload(mgsb_two_level* t, T** out, const T* src, size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return tl_err(t, MGSB_OUT_OF_MEMORY, "cudaMalloc failed");
+    t->mem.push_back({p, n * sizeof(T)});
+    *out = static_cast<T*>(p);
+    if (n && cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        return tl_err(t, MGSB_CUDA_ERROR, "cudaMemcpy failed");
+    return MGSB_OK;
+}
+
+void enqueue_two_level_frame(mgsb_two_level* t) {
+    mgsb_solver* C = t->coarse;
+    mgsb_solver* F = t->fine;
+    const mgsb_params& pc = C->p;
+    const mgsb_params& pf = F->p;
+    C->launches = F->launches = 0;
+    const BodyHost& BC = C->bodies[0];
+    const BodyHost& BF = F->bodies[0];
+    LAUNCH(C, k_ref_predict, grid_for(t->nc), kBlock, 0, t->nc, C->x, C->v, C->s, C->prev, C->last, C->fixf, BC.damping,
+           pc.dt, BC.gravity[0], BC.gravity[1], BC.gravity[2]);
+    LAUNCH(F, k_ref_predict, grid_for(t->nf), kBlock, 0, t->nf, F->x, F->v, F->s, F->prev, F->last, F->fixf, BF.damping,
+           pf.dt, BF.gravity[0], BF.gravity[1], BF.gravity[2]);
+    float omega = 1.0f;
+    for (int it = 0; it < pc.iterations; ++it) {
+        LAUNCH(C, k_ref_local, grid_for(C->T), kBlock, 0, C->T, C->tets, C->tA, C->tB, C->tC, C->x, C->slot_of, C->slots,
+               pc.volume_stiffness, 0);
+        LAUNCH(C, k_ref_tri_dcd, grid_for(t->ntri), kBlock, 0, t->ntri, t->tris, C->x, C->spheres_dev, t->push);
+        omega = 4 / (4 - pc.cheb_rho * pc.cheb_rho * omega);
+        LAUNCH(C, k_ref_vertex, grid_for(t->nc), kBlock, 0, t->nc, C->x, C->prev, C->s, C->last, C->v, C->fixf, C->mass,
+               C->vdiag, C->slot_ptr, C->slots, C->spheres_dev, pc.collision_stiffness, pc.dt, omega,
+               (double)pc.relaxation, it == pc.iterations - 1 ? 2 : 0, C->cflag, C->cdepth, C->cenergy, C->nonfinite,
+               t->tri_ptr, t->tri_idx, t->push);
+    }
+    LAUNCH(F, k_tl_transfer, grid_for(t->nf), kBlock, 0, t->nf, t->f_ids, t->f_w, C->x, F->x, F->prev);
+    omega = 1.0f;
+    for (int it = 0; it < pf.iterations; ++it) {
+        LAUNCH(F, k_ref_local, grid_for(F->T), kBlock, 0, F->T, F->tets, F->tA, F->tB, F->tC, F->x, F->slot_of, F->slots,
+               pf.volume_stiffness, 0);
+        omega = 4 / (4 - pf.cheb_rho * pf.cheb_rho * omega);
+        LAUNCH(F, k_ref_vertex, grid_for(t->nf), kBlock, 0, t->nf, F->x, F->prev, F->s, F->last, F->v, F->fixf, F->mass,
+               F->vdiag, F->slot_ptr, F->slots, F->spheres_dev, pf.collision_stiffness, pf.dt, omega,
+               (double)pf.relaxation, it == pf.iterations - 1 ? 2 : 0, F->cflag, F->cdepth, F->cenergy, F->nonfinite,
+               nullptr, nullptr, nullptr);
+    }
+    LAUNCH(C, k_tl_transfer, grid_for(t->nc), kBlock, 0, t->nc, t->c_ids, t->c_w, F->x, C->x, C->prev);
+    LAUNCH(F, k_tl_update_mapping, grid_for(t->nf), kBlock, 0, t->nf, F->x, t->f_ids, C->x, t->f_w);
+    LAUNCH(C, k_velocity, grid_for(t->nc), kBlock, 0, t->nc, C->x, C->last, C->v, pc.dt, C->nonfinite);
+    LAUNCH(F, k_velocity, grid_for(t->nf), kBlock, 0, t->nf, F->x, F->last, F->v, pf.dt, F->nonfinite);
+}
+
+}  // namespace
+
+extern "C" {
+
+mgsb_status mgsb_mg2_create(const mgsb_mesh* coarse, const mgsb_mesh* fine, const mgsb_params* params,
+                            mgsb_two_level** out) {
+    if (!out) return MGSB_INVALID_ARG;
+    *out = nullptr;
+    if (!coarse || !fine || !params) return MGSB_INVALID_ARG;
+    if (params->solver != MGSB_SOLVER_REFERENCE_JACOBI) return MGSB_NOT_SUPPORTED;
+    std::unique_ptr<mgsb_two_level> t(new mgsb_two_level());
+    t->device = params->device;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGSB_CUDA_ERROR;
+    mgsb_params p = *params;
+    if (!p.stream) {
+        cudaStream_t s = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return MGSB_CUDA_ERROR;
+        t->stream = s;
+        t->own_stream = true;
+        p.stream = s;
+    } else {
+        t->stream = (cudaStream_t)p.stream;
+    }
+    p.use_graph = 0;   // the two-level handle captures the whole frame itself
+    mgsb_status st = create_impl(1, coarse, &p, &t->coarse);
+    if (st != MGSB_OK) return st;
+    st = create_impl(1, fine, &p, &t->fine);
+    if (st != MGSB_OK) return st;
+    t->nc = coarse->num_verts;
+    t->nf = fine->num_verts;
+    // bindings on the rest shapes (PDSolver_MG::Init)
+    std::vector<int32_t> fid, cid;
+    std::vector<float> fw, cw;
+    std::string e;
+    if (!tl_bind_fine_to_coarse(fine->positions, t->nf, coarse->positions, coarse->tets, coarse->num_tets, fid, fw, e) ||
+        !tl_bind_coarse_to_fine(coarse->positions, t->nc, fine->positions, fine->tets, fine->num_tets, cid, cw, e)) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "two-level binding: %s", e.c_str());
+        t->err = buf;
+        return MGSB_INVALID_ARG;
+    }
+    TRY(tl_upload(t.get(), &t->f_ids, reinterpret_cast<const int4*>(fid.data()), (size_t)t->nf));
+    TRY(tl_upload(t.get(), &t->f_w, reinterpret_cast<const float4*>(fw.data()), (size_t)t->nf));
+    TRY(tl_upload(t.get(), &t->c_ids, reinterpret_cast<const int4*>(cid.data()), (size_t)t->nc));
+    TRY(tl_upload(t.get(), &t->c_w, reinterpret_cast<const float4*>(cw.data()), (size_t)t->nc));
+    // coarse surface triangles (TetFaceExtraction order) and the vertex -> triangle CSR
+    std::vector<int32_t> tris, opp;
+    extract_surface(coarse->tets, coarse->num_tets, tris, opp);
+    t->ntri = (int)(tris.size() / 3);
+    std::vector<int4> t4(t->ntri);
+    std::vector<int32_t> ptr(t->nc + 1, 0), idx;
+    for (int f = 0; f < t->ntri; ++f) {
+        t4[f] = int4{tris[3 * f], tris[3 * f + 1], tris[3 * f + 2], 0};
+        for (int q = 0; q < 3; ++q) ++ptr[tris[3 * f + q] + 1];
+    }
+    for (int v = 0; v < t->nc; ++v) ptr[v + 1] += ptr[v];
+    idx.resize(ptr[t->nc]);
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int f = 0; f < t->ntri; ++f)
+        for (int q = 0; q < 3; ++q) idx[fill[tris[3 * f + q]]++] = f;
+    TRY(tl_upload(t.get(), &t->tris, t4.data(), t4.size()));
+    TRY(tl_upload(t.get(), &t->tri_ptr, ptr.data(), ptr.size()));
+    TRY(tl_upload(t.get(), &t->tri_idx, idx.data(), idx.size()));
+    std::vector<float4> zero(std::max(t->ntri, 1), float4{0, 0, 0, 0});
+    TRY(tl_upload(t.get(), &t->push, zero.data(), (size_t)t->ntri));
+    *out = t.release();
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_mg2_destroy(mgsb_two_level* t) {
+    if (!t) return MGSB_INVALID_ARG;
+    delete t;
+    return MGSB_OK;
+}
+
+const char* mgsb_mg2_last_error(const mgsb_two_level* t) {
+    if (!t) return "null handle";
+    if (!t->err.empty()) return t->err.c_str();
+    if (t->coarse && !t->coarse->err.empty()) return t->coarse->err.c_str();
+    if (t->fine && !t->fine->err.empty()) return t->fine->err.c_str();
+    return "";
+}
+
+mgsb_status mgsb_mg2_level(mgsb_two_level* t, int32_t level, mgsb_solver** out) {
+    if (!t || !out || level < 0 || level > 1) return MGSB_INVALID_ARG;
+    *out = level == 0 ? t->fine : t->coarse;
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_mg2_set_fixed(mgsb_two_level* t, const uint8_t* coarse_mask, const uint8_t* fine_mask) {
+    if (!t) return MGSB_INVALID_ARG;
+    if (coarse_mask) TRY(mgsb_set_fixed(t->coarse, 0, coarse_mask));
+    if (fine_mask) TRY(mgsb_set_fixed(t->fine, 0, fine_mask));
+    t->graph_valid = false;
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_mg2_set_tool_spheres(mgsb_two_level* t, int32_t count, const float* centers, const float* radii,
+                                      const uint8_t* active) {
+    if (!t) return MGSB_INVALID_ARG;
+    TRY(mgsb_set_tool_spheres(t->coarse, count, centers, radii, active));
+    TRY(mgsb_set_tool_spheres(t->fine, count, centers, radii, active));
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_mg2_step(mgsb_two_level* t) {
+    if (!t) return MGSB_INVALID_ARG;
+    mgsb_solver* C = t->coarse;
+    mgsb_solver* F = t->fine;
+    if (C->dirty || F->dirty) t->graph_valid = false;
+    TRY(ensure_ready(C));
+    TRY(ensure_ready(F));
+    if (cudaSetDevice(t->device) != cudaSuccess) return tl_err(t, MGSB_CUDA_ERROR, "cudaSetDevice failed");
+    TRY(push_tool(C));
+    TRY(push_tool(F));
+    if (!t->graph_valid) {
+        if (t->exec) cudaGraphExecDestroy(t->exec);
+        if (t->graph) cudaGraphDestroy(t->graph);
+        t->exec = nullptr;
+        t->graph = nullptr;
+        if (cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return tl_err(t, MGSB_CUDA_ERROR, "graph capture could not start");
+        enqueue_two_level_frame(t);
+        if (cudaStreamEndCapture(t->stream, &t->graph) != cudaSuccess ||
+            cudaGraphInstantiate(&t->exec, t->graph, 0) != cudaSuccess)
+            return tl_err(t, MGSB_CUDA_ERROR, "graph capture of the two-level frame failed");
+        t->graph_valid = true;
+    }
+    if (cudaGraphLaunch(t->exec, t->stream) != cudaSuccess) return tl_err(t, MGSB_CUDA_ERROR, "graph launch failed");
+    C->timed = F->timed = false;
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_mg2_get_positions(mgsb_two_level* t, int32_t level, float* out) {
+    if (!t || !out || level < 0 || level > 1) return MGSB_INVALID_ARG;
+    return mgsb_get_positions(level == 0 ? t->fine : t->coarse, 0, out);
+}
+
+}  // extern "C"

@@ -53,6 +53,10 @@ def _load():
         "oracle_level_matrix": (C.c_int, [C.c_void_p, C.c_int, _DP, _IP, _IP, _DP]),
         "oracle_surface_normals": (None, [_DP, C.c_int32, _IP, C.c_int32, _DP]),
         "oracle_mlp_forward": (None, [_DP, _DP, C.c_int32, C.c_int32, _DP]),
+        "oracle_mg2_create": (C.c_void_p, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]),
+        "oracle_mg2_destroy": (None, [C.c_void_p]),
+        "oracle_mg2_level": (C.c_void_p, [C.c_void_p, C.c_int]),
+        "oracle_mg2_step": (None, [C.c_void_p]),
         "oracle_mlp_loss_grad": (C.c_double, [_DP, _DP, _DP, C.c_int32, C.c_int32, _DP]),
         "oracle_ref_rotation": (None, [_DP, _DP]),
         "oracle_svd_rotation": (None, [_DP, _DP]),
@@ -236,3 +240,62 @@ def mlp_loss_grad(params, x, t, bf16=True):
     g = np.empty(p.shape[0])
     loss = lib.oracle_mlp_loss_grad(_dp(p), _dp(x), _dp(t), x.shape[0], int(bf16), _dp(g))
     return float(loss), g
+
+
+class _Level(Oracle):
+    """One level of an OracleTwoLevel (borrowed handle)."""
+
+    def __init__(self, lib, h, mesh):  # noqa: D401 - no Oracle.__init__: the handle is owned by the pair
+        self._lib = lib
+        self.h = h
+        self.mesh = mesh
+        self.V = mesh.num_verts
+        self.T = mesh.num_tets
+
+    def close(self):
+        self.h = None
+
+
+class OracleTwoLevel:
+    """FP64 restatement of the reference's two-level schedule (PDSolver_MG); level 0 = fine, 1 = coarse."""
+
+    def __init__(self, coarse, fine, params):
+        self._lib = _load()
+        mc, self._kc = coarse.as_c()
+        mf, self._kf = fine.as_c()
+        err = C.create_string_buffer(256)
+        self._params = params
+        self.h = self._lib.oracle_mg2_create(C.byref(mc), C.byref(mf), C.byref(params), err, 256)
+        if not self.h:
+            raise RuntimeError("oracle_mg2_create: " + err.value.decode())
+        self.levels = [_Level(self._lib, self._lib.oracle_mg2_level(self.h, 0), fine),
+                       _Level(self._lib, self._lib.oracle_mg2_level(self.h, 1), coarse)]
+
+    def set_fixed(self, coarse_mask, fine_mask):
+        self.levels[1].set_fixed(coarse_mask)
+        self.levels[0].set_fixed(fine_mask)
+
+    def set_spheres(self, centers, radii, active=None):
+        for lv in self.levels:
+            lv.set_spheres(centers, radii, active)
+
+    def step(self, n=1):
+        for _ in range(n):
+            self._lib.oracle_mg2_step(self.h)
+
+    def positions(self, level=0):
+        return self.levels[level].positions()
+
+    def contact_flags(self, level=0):
+        return self.levels[level].contact_flags()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.oracle_mg2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

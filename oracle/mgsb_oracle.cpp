@@ -200,6 +200,13 @@ struct Sphere {
 
 struct Oracle {
     mgsb_params p;
+    // coarse level of the two-level schedule: sphere collision against the
+    // surface triangles (DCDByTriangle) instead of per vertex (DCDByPoint)
+    bool tri_dcd = false;
+    std::vector<int32_t> surf_tris;
+    // local step of PDSolver::Step (getTetFRV2 + calTetIFV1) drops |c| < 1e-5;
+    // calculateIF, used by the two-level schedule (PDSolver.cu:128-183), does not
+    bool drop_small = true;
     int V = 0, T = 0;
     std::vector<double> rest;
     std::vector<int> tets;
@@ -280,9 +287,12 @@ void build_surface(Oracle& o) {
         }
     }
     std::vector<char> on(o.V, 0);
+    o.surf_tris.clear();
     for (auto& kv : cnt)
-        if (kv.second == 1)
+        if (kv.second == 1) {
             for (int a : kv.first) on[a] = 1;
+            for (int a : kv.first) o.surf_tris.push_back(a);
+        }
     o.surface_verts.clear();
     for (int i = 0; i < o.V; ++i)
         if (on[i]) o.surface_verts.push_back(i);
@@ -465,6 +475,82 @@ void ref_predict(Oracle& o) {
     }
 }
 
+// Sphere vs surface triangles, every active sphere in order (UpdateTriNormal +
+// DCDByTriangle_sphere_V2 + DCDByTriangle_sphere_response, PDSolver.cu:394-425,
+// 462-501, 612-680): a contact of triangle (A, B, C) with a sphere adds k_c to
+// every axis of the diagonal of A, B and C, k_c (centre - hit) to their force,
+// and 1 to their contact count.
+void ref_triangle_dcd(Oracle& o, std::vector<V3>& cdiag, std::vector<V3>& cforce) {
+    auto sub = [](const V3& a, const V3& b) { return V3{a[0] - b[0], a[1] - b[1], a[2] - b[2]}; };
+    auto dot = [](const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    auto cross = [](const V3& a, const V3& b) {
+        return V3{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    };
+    auto length = [&](const V3& a) { return std::sqrt(dot(a, a)); };
+    const double k = o.p.collision_stiffness;
+    const int F = (int)(o.surf_tris.size() / 3);
+    for (const Sphere& sp : o.spheres) {
+        if (!sp.active) continue;
+        const V3 ctr = {sp.c[0], sp.c[1], sp.c[2]};
+        const double r = sp.r;
+        for (int f = 0; f < F; ++f) {
+            const int ia = o.surf_tris[3 * f], ib = o.surf_tris[3 * f + 1], ic = o.surf_tris[3 * f + 2];
+            const V3 A = o.x[ia], B = o.x[ib], C = o.x[ic];
+            V3 n = cross(sub(B, A), sub(C, A));
+            const double nl = length(n);
+            for (int c = 0; c < 3; ++c) n[c] /= nl;
+            const double sd = dot(n, sub(ctr, A));
+            const double dist = std::fabs(sd);
+            if (dist > r) continue;
+            const V3 proj = {ctr[0] - n[0] * sd, ctr[1] - n[1] * sd, ctr[2] - n[2] * sd};
+            V3 hit;
+            bool found = false;
+            {   // pointInTriangle, utils.cu:366-383
+                const V3 v0 = sub(C, A), v1 = sub(B, A), v2 = sub(proj, A);
+                const double d00 = dot(v0, v0), d01 = dot(v0, v1), d02 = dot(v0, v2), d11 = dot(v1, v1), d12 = dot(v1, v2);
+                const double inv = 1.0 / (d00 * d11 - d01 * d01);
+                const double u = (d11 * d02 - d01 * d12) * inv, v = (d00 * d12 - d01 * d02) * inv;
+                if (u >= 0 && v >= 0 && u + v <= 1.0) {
+                    const double sgn = sd < 0 ? -1.0 : 1.0;
+                    for (int c = 0; c < 3; ++c) hit[c] = ctr[c] + n[c] * (r - dist) * sgn;
+                    found = true;
+                }
+            }
+            const V3 tv[3] = {A, B, C};
+            for (int i = 0; i < 3 && !found; ++i) {
+                const V3& Bg = tv[i];
+                V3 ed = sub(tv[(i + 1) % 3], Bg);
+                const double el = length(ed);
+                for (int c = 0; c < 3; ++c) ed[c] /= el;
+                const double t = dot(sub(ctr, Bg), ed);
+                if (t < 0 || t > el) continue;
+                const V3 cl = {Bg[0] + ed[0] * t, Bg[1] + ed[1] * t, Bg[2] + ed[2] * t};
+                V3 rad = sub(ctr, cl);
+                const double rl = length(rad);
+                if (rl >= r) continue;
+                if (dot(cross(ed, sub(tv[(i + 2) % 3], Bg)), cross(ed, sub(proj, Bg))) >= 0) continue;
+                for (int c = 0; c < 3; ++c) hit[c] = cl[c] + rad[c] / rl * r;
+                found = true;
+            }
+            for (int i = 0; i < 3 && !found; ++i) {
+                const V3 vo = sub(ctr, tv[i]);
+                const double vl = length(vo);
+                if (vl > r) continue;
+                for (int c = 0; c < 3; ++c) hit[c] = tv[i][c] + vo[c] / vl * r;
+                found = true;
+            }
+            if (!found) continue;
+            for (int vid : {ia, ib, ic}) {
+                o.collided[vid] += 1;
+                for (int c = 0; c < 3; ++c) {
+                    cdiag[vid][c] += k;
+                    cforce[vid][c] += k * (ctr[c] - hit[c]);
+                }
+            }
+        }
+    }
+}
+
 void ref_iteration(Oracle& o, double omega, std::vector<V3>& force, std::vector<V3>& cdiag, std::vector<V3>& cforce) {
     const int V = o.V;
     std::fill(force.begin(), force.end(), V3{0, 0, 0});
@@ -473,36 +559,40 @@ void ref_iteration(Oracle& o, double omega, std::vector<V3>& force, std::vector<
     std::fill(o.collided.begin(), o.collided.end(), 0);
     std::fill(o.depth.begin(), o.depth.end(), 0.0);
     std::fill(o.cenergy.begin(), o.cenergy.end(), 0.0);
-    // DCDByPoint_sphere, PDSolver.cu:277-331, every active sphere in order
-    for (const Sphere& sp : o.spheres) {
-        if (!sp.active) continue;
-        const double k = o.p.collision_stiffness;
-        for (int i = 0; i < V; ++i) {
-            const V3 p = o.x[i];
-            const V3 cp = {p[0] - sp.c[0], p[1] - sp.c[1], p[2] - sp.c[2]};
-            const double dist = std::sqrt(cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2]);
-            const V3 dir = {cp[0] / dist, cp[1] / dist, cp[2] / dist};
-            const double R = sp.r * 1.5;
-            if (!(dist < R)) continue;
-            const double b = 2 * (cp[0] * dir[0] + cp[1] * dir[1] + cp[2] * dir[2]);
-            const double c = cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2] - R * R;
-            double t = (-b + std::sqrt(b * b - 4 * c)) / 2;
-            if (t > 0.5 * sp.r) {
-                o.collided[i] = 1;
-                o.depth[i] = t - 0.5 * sp.r;
+    if (o.tri_dcd) {
+        ref_triangle_dcd(o, cdiag, cforce);
+    } else {
+        // DCDByPoint_sphere, PDSolver.cu:277-331, every active sphere in order
+        for (const Sphere& sp : o.spheres) {
+            if (!sp.active) continue;
+            const double k = o.p.collision_stiffness;
+            for (int i = 0; i < V; ++i) {
+                const V3 p = o.x[i];
+                const V3 cp = {p[0] - sp.c[0], p[1] - sp.c[1], p[2] - sp.c[2]};
+                const double dist = std::sqrt(cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2]);
+                const V3 dir = {cp[0] / dist, cp[1] / dist, cp[2] / dist};
+                const double R = sp.r * 1.5;
+                if (!(dist < R)) continue;
+                const double b = 2 * (cp[0] * dir[0] + cp[1] * dir[1] + cp[2] * dir[2]);
+                const double c = cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2] - R * R;
+                double t = (-b + std::sqrt(b * b - 4 * c)) / 2;
+                if (t > 0.5 * sp.r) {
+                    o.collided[i] = 1;
+                    o.depth[i] = t - 0.5 * sp.r;
+                }
+                t = t / 2.0;
+                const V3 colP = {p[0] + dir[0] * t, p[1] + dir[1] * t, p[2] + dir[2] * t};
+                const V3 cc = {colP[0] - sp.c[0], colP[1] - sp.c[1], colP[2] - sp.c[2]};
+                const double lc = std::sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+                const V3 n = {cc[0] / lc, cc[1] / lc, cc[2] / lc};
+                const double nd = n[0] * dir[0] + n[1] * dir[1] + n[2] * dir[2];
+                for (int a = 0; a < 3; ++a) {
+                    cdiag[i][a] += k * n[a] * n[a];
+                    cforce[i][a] += k * t * nd * n[a];
+                }
+                const double pe = (p[0] - colP[0]) * n[0] + (p[1] - colP[1]) * n[1] + (p[2] - colP[2]) * n[2];
+                o.cenergy[i] += k * pe * pe;
             }
-            t = t / 2.0;
-            const V3 colP = {p[0] + dir[0] * t, p[1] + dir[1] * t, p[2] + dir[2] * t};
-            const V3 cc = {colP[0] - sp.c[0], colP[1] - sp.c[1], colP[2] - sp.c[2]};
-            const double lc = std::sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
-            const V3 n = {cc[0] / lc, cc[1] / lc, cc[2] / lc};
-            const double nd = n[0] * dir[0] + n[1] * dir[1] + n[2] * dir[2];
-            for (int a = 0; a < 3; ++a) {
-                cdiag[i][a] += k * n[a] * n[a];
-                cforce[i][a] += k * t * nd * n[a];
-            }
-            const double pe = (p[0] - colP[0]) * n[0] + (p[1] - colP[1]) * n[1] + (p[2] - colP[2]) * n[2];
-            o.cenergy[i] += k * pe * pe;
         }
     }
     // local step: getTetFRV2 + calTetIFV1 (PDSolverAc.cu:447-662)
@@ -526,7 +616,7 @@ void ref_iteration(Oracle& o, double omega, std::vector<V3>& force, std::vector<
                 if (std::isnan(val)) val = 0;
                 val = std::min(10.0, std::max(-10.0, val));
                 double res = val * o.vol[t] * kv;
-                if (std::fabs(res) < 1e-5) res = 0;
+                if (o.drop_small && std::fabs(res) < 1e-5) res = 0;   // calTetIFV1; calculateIF keeps them
                 contrib[12 * (size_t)t + j * 3 + i] = res;
             }
     }
@@ -1229,3 +1319,177 @@ double oracle_mlp_loss_grad(const double* params, const double* x, const double*
     if (grad) std::copy(g.begin(), g.end(), grad);
     return loss * inv;
 }
+
+
+// ---------------------------------------------------------------------------
+// Two-level schedule (PDSolver_MG, PDSolver_MG.cpp:5-253)
+// ---------------------------------------------------------------------------
+namespace {
+
+// barycentricCoordinate(point, A, B, C, D) (utils.cu:335-364) in FP64.
+void bary64(const double* p, const V3 v[4], double w[4], bool abs_volume = false) {
+    auto sub = [](const V3& a, const V3& b) { return V3{a[0] - b[0], a[1] - b[1], a[2] - b[2]}; };
+    auto dot = [](const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    auto cross = [](const V3& a, const V3& b) {
+        return V3{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    };
+    double Vol = dot(sub(v[1], v[0]), cross(sub(v[2], v[0]), sub(v[3], v[0]))) / 6.0;
+    if (abs_volume) Vol = std::fabs(Vol);   // the face-area form of PDSolver_MG::Init uses |V|
+    V3 ctr = {0, 0, 0};
+    for (int k = 0; k < 4; ++k)
+        for (int c = 0; c < 3; ++c) ctr[c] += 0.25 * v[k][c];
+    const V3 P = {p[0], p[1], p[2]};
+    for (int i = 0; i < 4; ++i) {
+        const V3& q = v[i];
+        const V3 &f0 = v[(i + 1) % 4], &f1 = v[(i + 2) % 4], &f2 = v[(i + 3) % 4];
+        V3 n = cross(sub(f1, f0), sub(f2, f0));
+        if (dot(n, sub(q, f0)) > 0)
+            for (int c = 0; c < 3; ++c) n[c] = -n[c];
+        const double l = std::sqrt(dot(n, n));
+        for (int c = 0; c < 3; ++c) n[c] /= l;
+        w[i] = 0.25 - dot(sub(P, ctr), n) * (0.5 * l) / (3 * Vol);
+    }
+}
+
+}  // namespace
+
+struct oracle_mg2 {
+    oracle_solver* c = nullptr;
+    oracle_solver* f = nullptr;
+    std::vector<int> fid, cid;        // fine -> coarse tet ids, coarse -> fine tet ids
+    std::vector<double> fw, cw;
+};
+
+extern "C" {
+
+oracle_mg2* oracle_mg2_create(const mgsb_mesh* coarse, const mgsb_mesh* fine, const mgsb_params* params, char* err,
+                              int errlen) {
+    auto fail = [&](const std::string& m, oracle_mg2* h) -> oracle_mg2* {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", m.c_str());
+        if (h) {
+            delete h->c;
+            delete h->f;
+            delete h;
+        }
+        return nullptr;
+    };
+    oracle_mg2* h = new oracle_mg2();
+    h->c = oracle_create(coarse, params, err, errlen);
+    h->f = oracle_create(fine, params, err, errlen);
+    if (!h->c || !h->f) return fail(err ? std::string(err) : "create failed", h);
+    Oracle& C = h->c->o;
+    Oracle& F = h->f->o;
+    build_surface(C);
+    C.tri_dcd = true;
+    C.drop_small = F.drop_small = false;
+    // PDSolver_MG::interpolate (PDSolver_MG.cpp:5-58): each fine vertex in the
+    // first coarse tet (index order) whose weights lie in [-1e-5, 1 + 1e-5]
+    h->fid.assign(4 * (size_t)F.V, -1);
+    h->fw.assign(4 * (size_t)F.V, 0.0);
+    for (int v = 0; v < F.V; ++v) {
+        const double* P = &F.rest[3 * (size_t)v];
+        bool found = false;
+        for (int t = 0; t < C.T && !found; ++t) {
+            const int* id = &C.tets[4 * t];
+            V3 tv[4];
+            for (int k = 0; k < 4; ++k) tv[k] = {C.rest[3 * id[k]], C.rest[3 * id[k] + 1], C.rest[3 * id[k] + 2]};
+            double w[4];
+            bary64(P, tv, w);
+            bool in = true;
+            for (int k = 0; k < 4; ++k)
+                if (w[k] < -1e-5 || w[k] > 1 + 1e-5) in = false;
+            if (!in) continue;
+            for (int k = 0; k < 4; ++k) {
+                h->fid[4 * (size_t)v + k] = id[k];
+                h->fw[4 * (size_t)v + k] = w[k];
+            }
+            found = true;
+        }
+        if (!found) return fail("fine vertex outside the coarse mesh", h);
+    }
+    // PDSolver_MG::Init (PDSolver_MG.cpp:120-167): each coarse vertex in the first
+    // fine tet whose four face planes (outward normals) it does not exceed by
+    // more than 1e-6; weights from the face areas and normals.
+    h->cid.assign(4 * (size_t)C.V, -1);
+    h->cw.assign(4 * (size_t)C.V, 0.0);
+    for (int v = 0; v < C.V; ++v) {
+        const double* P = &C.rest[3 * (size_t)v];
+        bool found = false;
+        for (int t = 0; t < F.T && !found; ++t) {
+            const int* id = &F.tets[4 * t];
+            V3 tv[4];
+            for (int k = 0; k < 4; ++k) tv[k] = {F.rest[3 * id[k]], F.rest[3 * id[k] + 1], F.rest[3 * id[k] + 2]};
+            bool in = true;
+            static const int face[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+            for (int k = 0; k < 4 && in; ++k) {
+                const V3 &A = tv[face[k][0]], &B = tv[face[k][1]], &Cc = tv[face[k][2]], &D = tv[k];
+                const V3 ab = {B[0] - A[0], B[1] - A[1], B[2] - A[2]}, ac = {Cc[0] - A[0], Cc[1] - A[1], Cc[2] - A[2]};
+                V3 n = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2], ab[0] * ac[1] - ab[1] * ac[0]};
+                if (n[0] * (D[0] - A[0]) + n[1] * (D[1] - A[1]) + n[2] * (D[2] - A[2]) > 0)
+                    for (int c = 0; c < 3; ++c) n[c] = -n[c];
+                const double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                const V3& Af = tv[(k + 1) % 4];
+                const double d = ((P[0] - Af[0]) * n[0] + (P[1] - Af[1]) * n[1] + (P[2] - Af[2]) * n[2]) / l;
+                if (d > 1e-6) in = false;
+            }
+            if (!in) continue;
+            double w[4];
+            bary64(P, tv, w, true);   // face-area form (utils.cu:313-333) with the tet's |V|
+            for (int k = 0; k < 4; ++k) {
+                h->cid[4 * (size_t)v + k] = id[k];
+                h->cw[4 * (size_t)v + k] = w[k];
+            }
+            found = true;
+        }
+        if (!found) return fail("coarse vertex outside the fine mesh", h);
+    }
+    return h;
+}
+
+void oracle_mg2_destroy(oracle_mg2* h) {
+    if (!h) return;
+    oracle_destroy(h->c);
+    oracle_destroy(h->f);
+    delete h;
+}
+
+oracle_solver* oracle_mg2_level(oracle_mg2* h, int level) { return level == 0 ? h->f : h->c; }
+
+// PDSolver_MG::Step (PDSolver_MG.cpp:183-253)
+void oracle_mg2_step(oracle_mg2* h) {
+    Oracle& C = h->c->o;
+    Oracle& F = h->f->o;
+    ref_predict(C);
+    ref_predict(F);
+    auto iterate = [](Oracle& o) {
+        std::vector<V3> force(o.V), cdiag(o.V), cforce(o.V);
+        float omega = 1.0f;
+        for (int it = 0; it < o.p.iterations; ++it) {
+            omega = 4 / (4 - o.p.cheb_rho * o.p.cheb_rho * omega);
+            ref_iteration(o, (double)omega, force, cdiag, cforce);
+        }
+    };
+    auto transfer = [](Oracle& dst, const Oracle& src, const std::vector<int>& id, const std::vector<double>& w) {
+        for (int v = 0; v < dst.V; ++v) {
+            V3 q = {0, 0, 0};
+            for (int k = 0; k < 4; ++k)
+                for (int c = 0; c < 3; ++c) q[c] += w[4 * (size_t)v + k] * src.x[id[4 * (size_t)v + k]][c];
+            dst.x[v] = q;
+            dst.prev[v] = q;
+        }
+    };
+    iterate(C);
+    transfer(F, C, h->fid, h->fw);        // runInterpolate
+    iterate(F);
+    transfer(C, F, h->cid, h->cw);        // runAverage
+    for (int v = 0; v < F.V; ++v) {       // runUpdateMapping
+        V3 tv[4];
+        for (int k = 0; k < 4; ++k) tv[k] = C.x[h->fid[4 * (size_t)v + k]];
+        bary64(F.x[v].data(), tv, &h->fw[4 * (size_t)v]);
+    }
+    for (Oracle* o : {&C, &F})
+        for (int i = 0; i < o->V; ++i)
+            for (int c = 0; c < 3; ++c) o->v[i][c] = (o->x[i][c] - o->last[i][c]) / o->p.dt;
+}
+
+}  // extern "C"

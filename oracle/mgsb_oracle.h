@@ -63,6 +63,16 @@ int oracle_level_size(const oracle_solver* h, int level, int32_t* n, int32_t* nn
 int oracle_level_prolongation(const oracle_solver* h, int level, int32_t* ids, double* w);
 int oracle_level_matrix(const oracle_solver* h, int level, double* diag, int32_t* ptr, int32_t* col, double* val);
 
+/* Two-level schedule of the reference (PDSolver_MG): a coarse and a fine
+ * reference-kind solver; level 0 = fine, 1 = coarse (use the oracle_solver
+ * calls on oracle_mg2_level for fixed sets, spheres and readback). */
+typedef struct oracle_mg2 oracle_mg2;
+oracle_mg2* oracle_mg2_create(const mgsb_mesh* coarse, const mgsb_mesh* fine, const mgsb_params* params, char* err,
+                              int errlen);
+void oracle_mg2_destroy(oracle_mg2* h);
+oracle_solver* oracle_mg2_level(oracle_mg2* h, int level);
+void oracle_mg2_step(oracle_mg2* h);
+
 /* Pure functions. */
 /* Vertex normals of a triangle surface: UpdateTriNormal + AvgOutsideTetVertNormal
  * (PDSolver.cu:394-460).  pos [3V], tris [3F]; out [3V], zero where no triangle. */

@@ -13,6 +13,7 @@
 
 #include "global.h"
 #include "PDSolver.h"
+#include "PDSolver_MG.h"
 #include "SoftObject.h"
 #include "Simulator.h"
 
@@ -167,6 +168,70 @@ int ref_run(const float* pos, int V, const int32_t* tets, int T, const uint8_t* 
             for (int i = 0; i < 3 * V; ++i) out_pos[(size_t)f * 3 * V + i] = sim->m_tetVertPos[i];
         if (out_flags)
             for (int i = 0; i < V; ++i) out_flags[(size_t)f * V + i] = sim->m_tetVertIsCollide[i];
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+// PDSolver_MG (the two-level schedule) on a coarse and a fine mesh of one body:
+// per frame the sphere pose, one Step, then the fine and coarse positions.
+int ref_mg2_run(const float* cpos, int cV, const int32_t* ctets, int cT, const float* fpos, int fV,
+                const int32_t* ftets, int fT, const uint8_t* cfixed, const uint8_t* ffixed, int frames,
+                const float* sphere, float* out_fine, float* out_coarse, float* ms) {
+    ensure_globals();
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return -1;
+    Simulator* sim = g_simulator;
+    sim->m_sphereFixers.clear();
+    sim->m_sphereColliders.clear();
+    sim->m_sphereColliders.push_back(std::shared_ptr<SphereCollider>(new SphereCollider({0.f, 0.f, 0.f}, 1.f)));
+    SoftObject co("coarse", "", "", "/dev/null"), fo("fine", "", "", "/dev/null");
+    co.m_tetVertPosORIG.assign(cpos, cpos + 3 * (size_t)cV);
+    co.m_tetIdxORIG.assign(ctets, ctets + 4 * (size_t)cT);
+    co.TetFaceExtraction();
+    fo.m_tetVertPosORIG.assign(fpos, fpos + 3 * (size_t)fV);
+    fo.m_tetIdxORIG.assign(ftets, ftets + 4 * (size_t)fT);
+    fo.TetFaceExtraction();
+    const int F = (int)(fo.m_tetFaceIdx.size() / 3);
+    sim->m_tetVertPos = fo.m_tetVertPosORIG;
+    sim->m_tetFaceIdx = fo.m_tetFaceIdx;
+    sim->m_normal.assign(3 * (size_t)fV, 0.f);
+    sim->m_tetVertIsCollide.assign(fV, 0);
+    sim->m_tetVertCollisionDepth.assign(fV, 0.f);
+    sim->m_triIsCollide.assign(F, 0);
+    sim->m_triMoveVec.assign(3 * (size_t)F, 0.f);
+    // PDSolver_MG::Step ends with runCalEnergy(..., true), which fills these per fine vertex
+    sim->m_tetVertEpDensity.assign(fV, 0.f);
+    sim->m_tetVertEpSum.assign(fV, 0.f);
+    sim->m_tetVertVSum.assign(fV, 0.f);
+    PDSolver_MG* mg = new PDSolver_MG();
+    mg->Init(co.m_tetVertPosORIG, co.m_tetIdxORIG, co.m_tetFaceIdx, co.m_tetFaceOppositeTetVertIdx, fo.m_tetVertPosORIG,
+             fo.m_tetIdxORIG, fo.m_tetFaceIdx, fo.m_tetFaceOppositeTetVertIdx);
+    auto set_fixed = [](PDSolver* s, const uint8_t* mask, int V) {
+        std::vector<float> fixf(V);
+        for (int i = 0; i < V; ++i) fixf[i] = mask && mask[i] ? 0.0f : 1.0f;
+        s->m_tetVertFixed = fixf;
+        cudaMemcpy(s->pdSolverData->tetVertFixed_d, fixf.data(), V * sizeof(float), cudaMemcpyHostToDevice);
+    };
+    set_fixed(mg->m_pdSolverCoarse, cfixed, cV);
+    set_fixed(mg->m_pdSolverFine, ffixed, fV);
+    cudaDeviceSynchronize();
+    for (int f = 0; f < frames; ++f) {
+        SphereCollider& sp = *sim->m_sphereColliders[0];
+        sp.m_position = Point3D(sphere[4 * f], sphere[4 * f + 1], sphere[4 * f + 2]);
+        sp.m_radius = sphere[4 * f + 3] > 0 ? sphere[4 * f + 3] : 1.f;
+        sp.m_active = sphere[4 * f + 3] > 0;
+        auto t0 = std::chrono::high_resolution_clock::now();
+        mg->Step();
+        cudaDeviceSynchronize();
+        auto t1 = std::chrono::high_resolution_clock::now();
+        if (ms) ms[f] = std::chrono::duration<float, std::milli>(t1 - t0).count();
+        if (out_fine)
+            cudaMemcpy(out_fine + (size_t)f * 3 * fV, mg->m_pdSolverFine->pdSolverData->tetVertPos_d,
+                       3 * (size_t)fV * sizeof(float), cudaMemcpyDeviceToHost);
+        if (out_coarse)
+            cudaMemcpy(out_coarse + (size_t)f * 3 * cV, mg->m_pdSolverCoarse->pdSolverData->tetVertPos_d,
+                       3 * (size_t)cV * sizeof(float), cudaMemcpyDeviceToHost);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : (int)e;

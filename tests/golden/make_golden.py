@@ -5,9 +5,10 @@ oracle/ref_build.sh into oracle/_ref/libmgsb_ref.so; this script calls it:
 
     python tests/golden/make_golden.py cpu     # precompute, polar, mesh I/O (no GPU)
     python tests/golden/make_golden.py gpu     # PDSolver::Step trajectories (needs a GPU)
+    python tests/golden/make_golden.py gpu_mg2 # PDSolver_MG::Step trajectories (needs a GPU)
 
 Inputs are generated here (seeded); no reference data file is copied.
-Outputs: ref_cpu.npz, ref_traj.npz (small, committed).
+Outputs: ref_cpu.npz, ref_traj.npz, ref_mg2_traj.npz (small, committed).
 """
 from __future__ import annotations
 
@@ -58,6 +59,9 @@ def _lib():
     lib.ref_extract_surface.restype = C.c_int
     lib.ref_run.argtypes = [fp, C.c_int, ip, C.c_int, C.POINTER(C.c_uint8), C.c_int, C.c_int, fp, fp, ip, fp]
     lib.ref_run.restype = C.c_int
+    u8 = C.POINTER(C.c_uint8)
+    lib.ref_mg2_run.argtypes = [fp, C.c_int, ip, C.c_int, fp, C.c_int, ip, C.c_int, u8, u8, C.c_int, fp, fp, fp, fp]
+    lib.ref_mg2_run.restype = C.c_int
     return lib
 
 
@@ -209,6 +213,48 @@ def make_gpu() -> None:
     print("wrote ref_traj.npz; mean Step() ms", float(ms[5:].mean()))
 
 
+# Two-level golden scene: the trajectory beam as the fine mesh and the same box
+# with half the hexes per axis as the coarse mesh (nested: every fine vertex lies
+# in a coarse tet and every coarse vertex is a fine vertex); top faces fixed.
+MG2_COARSE_DIMS = (2, 7, 2)
+MG2_FRAMES = 60
+MG2_KEEP = list(range(9, MG2_FRAMES, 10))
+
+
+def mg2_scene():
+    import multigridsoftbody_b200 as mg
+    fine = mg.box_mesh(*TRAJ_DIMS, TRAJ_LO, TRAJ_HI)
+    coarse = mg.box_mesh(*MG2_COARSE_DIMS, TRAJ_LO, TRAJ_HI)
+    ff = (np.abs(fine.positions[:, 1] - TRAJ_HI[1]) < 1e-5).astype(np.uint8)
+    cf = (np.abs(coarse.positions[:, 1] - TRAJ_HI[1]) < 1e-5).astype(np.uint8)
+    return coarse, fine, cf, ff
+
+
+def make_gpu_mg2() -> None:
+    lib = _lib()
+    coarse, fine, cf, ff = mg2_scene()
+    path = traj_sphere_path(MG2_FRAMES)
+    runs = []
+    for rep in range(2):
+        fpos = np.zeros((MG2_FRAMES, fine.num_verts, 3), np.float32)
+        cpos = np.zeros((MG2_FRAMES, coarse.num_verts, 3), np.float32)
+        ms = np.zeros(MG2_FRAMES, np.float32)
+        st = lib.ref_mg2_run(_f(np.ascontiguousarray(coarse.positions)), coarse.num_verts,
+                             _i(np.ascontiguousarray(coarse.tets)), coarse.num_tets,
+                             _f(np.ascontiguousarray(fine.positions)), fine.num_verts, _i(np.ascontiguousarray(fine.tets)),
+                             fine.num_tets, cf.ctypes.data_as(C.POINTER(C.c_uint8)),
+                             ff.ctypes.data_as(C.POINTER(C.c_uint8)), MG2_FRAMES, _f(path), _f(fpos), _f(cpos), _f(ms))
+        if st != 0:
+            raise SystemExit(f"ref_mg2_run failed with status {st}")
+        runs.append((fpos, cpos, ms))
+    rerun = np.abs(runs[0][0] - runs[1][0]).reshape(MG2_FRAMES, -1).max(1)
+    out_dir = sys.argv[2] if len(sys.argv) > 2 else HERE
+    np.savez_compressed(os.path.join(out_dir, "ref_mg2_traj.npz"), frames=np.array(MG2_KEEP),
+                        fine=runs[0][0][MG2_KEEP], coarse=runs[0][1][MG2_KEEP], ms=runs[0][2], rerun_maxdiff=rerun)
+    print("run-to-run max difference of the reference:", float(rerun.max()))
+    print("wrote ref_mg2_traj.npz; mean Step() ms", float(runs[0][2][5:].mean()))
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "cpu"
-    make_cpu() if what == "cpu" else make_gpu()
+    {"cpu": make_cpu, "gpu": make_gpu, "gpu_mg2": make_gpu_mg2}[what]()

@@ -177,3 +177,23 @@ def test_oracle_surface_normals_box():
     x = m.positions
     face = np.nonzero((x[:, 2] == 5.0) & (x[:, 0] == 1.0) & (x[:, 1] == 2.0))[0]
     assert np.allclose(n[face], [[0.0, 0.0, 1.0]])
+
+
+def test_oracle_two_level_binding_and_steps():
+    """The two-level restatement binds the nested golden meshes (every fine vertex
+    in a coarse tet, every coarse vertex in a fine tet) and steps finitely."""
+    from oracle.binding import OracleTwoLevel
+    from .golden.make_golden import mg2_scene, traj_sphere_path
+    coarse, fine, cf, ff = mg2_scene()
+    o = OracleTwoLevel(coarse, fine, mg.default_params(mg.SOLVER_REFERENCE_JACOBI))
+    o.set_fixed(cf, ff)
+    path = traj_sphere_path(5)
+    for f in range(5):
+        o.set_spheres(path[f, :3][None], [path[f, 3]])
+        o.step()
+    for lvl in (0, 1):
+        assert np.isfinite(o.positions(lvl)).all()
+    # fixed vertices stay at rest on both levels (the transfers rewrite them, as in the
+    # reference's updatePointInTet, so to rounding)
+    assert np.abs(o.positions(0)[ff == 1] - fine.positions[ff == 1]).max() < 1e-12
+    assert np.abs(o.positions(1)[cf == 1] - coarse.positions[cf == 1]).max() < 1e-12
