@@ -285,8 +285,31 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    meshes, params, fixeds, tool, desc, mats = make_workload(args.workload, mg)
     cores = os.cpu_count()
+    if args.workload == "twolevel":
+        from oracle.binding import OracleTwoLevel
+        coarse, fine, cf, ff, p, sphere, desc = twolevel_scene(mg)
+        o = OracleTwoLevel(coarse, fine, p)
+        o.set_fixed(cf, ff)
+        for f in range(args.warmup):
+            o.set_spheres(*sphere(f))
+            o.step()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            o.set_spheres(*sphere(args.warmup + k))
+            o.step()
+        dt = time.perf_counter() - t0
+        v = args.steps / dt
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": desc, "impl": "FP64 oracle restating PDSolver_MG::Step"},
+                          "impl": "reference",
+                          "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port",
+                                           "sample": f"{args.steps} frames after {args.warmup} warm-up frames"},
+                          "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    meshes, params, fixeds, tool, desc, mats = make_workload(args.workload, mg)
     os_ = make_oracles(meshes, params, fixeds, mats)
     oracle_frames(os_, tool, 0, args.warmup)
     t0 = time.perf_counter()
@@ -382,6 +405,110 @@ def accuracy(mg, meshes, fixeds, params, tool, net, frames=40):
         if st:
             out[key]["learned_vcycles"], out[key]["fallbacks"] = st
     return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's two-level schedule (PDSolver_MG) on the config-1 beam
+# ---------------------------------------------------------------------------
+def twolevel_scene(mg):
+    """Fine: the 12x120x12-hex beam (103,680 tets); coarse: the same box at 4x40x4 hexes (3,840 tets),
+    as the reference pairs cube120_12_12 with 40_4_4; top faces fixed; a sphere (r 0.8) swept along -x
+    through the beam; reference constants (20 Jacobi/Chebyshev iterations per level)."""
+    lo, hi = (-1.0, -10.0, -1.0), (1.0, 10.0, 1.0)
+    fine = mg.box_mesh(12, 120, 12, lo, hi)
+    coarse = mg.box_mesh(4, 40, 4, lo, hi)
+    ff = (np.abs(fine.positions[:, 1] - hi[1]) < 1e-5).astype(np.uint8)
+    cf = (np.abs(coarse.positions[:, 1] - hi[1]) < 1e-5).astype(np.uint8)
+    p = mg.default_params(mg.SOLVER_REFERENCE_JACOBI)
+
+    def sphere(f):
+        return np.array([[1.5 - 0.01 * (f % 300), -3.0, 0.2]], np.float32), np.array([0.8], np.float32)
+
+    desc = ("two-level schedule of the reference (PDSolver_MG): fine beam 12x120x12 hexes (20,449 verts, 103,680 "
+            "tets), coarse 4x40x4 (3,840 tets), 20 Jacobi/Chebyshev iterations per level, sphere r 0.8 swept -x")
+    return coarse, fine, cf, ff, p, sphere, desc
+
+
+def run_twolevel(args):
+    import torch
+    import multigridsoftbody_b200 as mg
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream(device=local)
+    coarse, fine, cf, ff, p, sphere, desc = twolevel_scene(mg)
+    p.device = local
+    p.stream = stream.cuda_stream
+    t = mg.TwoLevel(coarse, fine, p)
+    t.set_fixed(cf, ff)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    with torch.cuda.stream(stream):
+        for f in range(args.warmup):
+            t.set_spheres(*sphere(f))
+            t.step()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                evs[k][0].record(stream)
+                t.set_spheres(*sphere(args.warmup + k))
+                t.step()
+                evs[k][1].record(stream)
+            torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        e2e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            e2e[k][0].record(stream)
+            t.set_spheres(*sphere(args.warmup + args.steps + k))
+            t.step()
+            t.positions(0)
+            e2e[k][1].record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = sum(a.elapsed_time(b) for a, b in e2e)
+    from multigridsoftbody_b200.replicas import job_throughput, max_over_ranks
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist)
+    if rank == 0:
+        it = p.iterations
+        launches = 2 + 3 * it + 1 + 2 * it + 1 + 1 + 2
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            from oracle.binding import OracleTwoLevel
+            o = OracleTwoLevel(coarse, fine, p)
+            o.set_fixed(cf, ff)
+            o.set_spheres(*sphere(0))
+            o.step()
+            t0 = time.perf_counter()
+            nfr = max(1, args.cpu_frames)
+            for f in range(nfr):
+                o.set_spheres(*sphere(1 + f))
+                o.step()
+            dt = time.perf_counter() - t0
+            cpu = {"value": nfr / dt, "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"{nfr} frames of the same workload, FP64 oracle of the two-level schedule ({dt:.1f} s)"}
+        line = {"metric": METRIC, "value": job_throughput(args.steps, world, ms), "unit": "frames/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "parallelism": f"replicas x{world}",
+                           "l2": "flushed (256 MB write) before every timed frame, outside the timed span"},
+                "clocks": clk.summary(),
+                "e2e": {"value": job_throughput(args.steps, world, e2e_ms), "unit": "frames/s",
+                        "h2d_bytes_per_step": 2 * (88 + 164), "d2h_bytes_per_step": fine.num_verts * 16},
+                "gpu_launches": launches * args.steps, "roofline": None, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    t.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------
@@ -571,6 +698,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "twolevel":
+        run_twolevel(args)
     else:
         run_ours(args)
 
