@@ -224,14 +224,22 @@ mgsb_status mgsb_level_size(mgsb_solver* h, int32_t level, int32_t* num_verts, i
 mgsb_status mgsb_level_info(mgsb_solver* h, int32_t level, int32_t info[8]);
 
 /* Project-written autotuner: times `frames` frames for each candidate shape
- * of the coarse V-cycle kernel (cluster size, block size, level-0 fusion)
- * from the current state, keeps the fastest and restores the state.
+ * of the coarse V-cycle kernel (cluster size, block size, level-0 fusion,
+ * coarse split — read back with mgsb_get_coarse_split) from the current
+ * state, keeps the fastest and restores the state.
  * chosen (may be NULL): [cluster, block, fused].  No reference counterpart. */
 mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t chosen[3]);
 /* Set the coarse-kernel shape explicitly: cluster size (0 = by size, else
  * 1..16), block size (0 = keep, 256/512/1024), level-0 fusion (-1 = by size,
  * 0, 1).  No reference counterpart. */
 mgsb_status mgsb_set_kernel_shape(mgsb_solver* h, int32_t cluster, int32_t block, int32_t fuse_level0);
+/* Coarse-level split of the V-cycle: levels 1..split-1 run as grid-wide
+ * kernels over every SM, levels split..L-1 in the cluster kernel (split 1 =
+ * all coarse levels in the cluster kernel; 0 = by size: levels whose largest
+ * body has more than 4096 rows run grid-wide).  The autotuner also picks it.
+ * Same arithmetic either way.  No reference counterpart. */
+mgsb_status mgsb_set_coarse_split(mgsb_solver* h, int32_t split);
+mgsb_status mgsb_get_coarse_split(mgsb_solver* h, int32_t* split);
 
 /* Host-only (no GPU): build the multigrid hierarchy of one mesh exactly as
  * mgsb_create would and return level `level`: vertex count, off-diagonal

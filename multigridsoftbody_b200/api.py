@@ -400,10 +400,19 @@ class Solver:
         """Pick the coarse-kernel shape by timing candidates; the state is restored."""
         ch = np.zeros(3, np.int32)
         _check(self._lib.mgsb_autotune(self.h, frames, _iptr(ch)), self.h)
-        return {"cluster": int(ch[0]), "block": int(ch[1]), "fuse_l0": int(ch[2])}
+        return {"cluster": int(ch[0]), "block": int(ch[1]), "fuse_l0": int(ch[2]), "split": self.coarse_split()}
 
     def set_kernel_shape(self, cluster: int = 0, block: int = 0, fuse_level0: int = -1) -> None:
         _check(self._lib.mgsb_set_kernel_shape(self.h, cluster, block, fuse_level0), self.h)
+
+    def set_coarse_split(self, split: int = 0) -> None:
+        """Levels 1..split-1 grid-wide, the rest in the cluster kernel (0 = by size)."""
+        _check(self._lib.mgsb_set_coarse_split(self.h, split), self.h)
+
+    def coarse_split(self) -> int:
+        v = np.zeros(1, np.int32)
+        _check(self._lib.mgsb_get_coarse_split(self.h, _iptr(v)), self.h)
+        return int(v[0])
 
     def level_size(self, level: int) -> tuple[int, int]:
         n = C.c_int32()

@@ -42,6 +42,7 @@ struct CoarseArgs {
     int L;
     int pre, post;
     int fuse_l0;             // level-0 residual and prolongation inside the kernel
+    int first;               // shared-memory kernel: first level it owns (>= 1); input lv[first-1].res, output lv[first].e
     const int2* range;       // [nbody * L]: (first row, rows) of each body on each level
     const int32_t* dense_off;
     const float* Ainv;       // coarsest inverse blocks (row-major per body)
@@ -210,6 +211,88 @@ __global__ void k_l0_prolong(int n, const int4* __restrict__ pid, const float4* 
     vi.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
     vi.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
     v[i] = vi;
+}
+
+// ---------------------------------------------------------------------------
+// One coarse level as grid-wide kernels (levels below the cluster kernel's
+// first level when the hierarchy is split): every body's rows of the level in
+// one launch per phase, 8 lanes per row.  Same arithmetic per row as the
+// cluster kernel's phases.
+// ---------------------------------------------------------------------------
+
+// r = R res_fine (children of each row, CSR); e = dinv r (the first Jacobi
+// sweep from zero), or 0 when dinv is null (no pre-smoothing).
+__global__ void __launch_bounds__(256) k_lvl_restrict(int n, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rcol,
+                                                      const float* __restrict__ rw, const float4* __restrict__ res_fine,
+                                                      const float* __restrict__ dinv, float4* __restrict__ r,
+                                                      float4* __restrict__ e, const int32_t* __restrict__ gate) {
+    if (gate && __ldg(gate) == 0) return;
+    constexpr int G = kLanesC, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const int beg = valid ? __ldg(rptr + row) : 0, end = valid ? __ldg(rptr + row + 1) : 0;
+    const float4 s = rg_csr_sum<G>(valid, lane, beg, end, rcol, rw, res_fine);
+    if (!valid || lane >= S) return;
+    r[row] = s;
+    const float di = dinv ? __ldg(dinv + row) : 0.f;
+    e[row] = make_float4(di * s.x, di * s.y, di * s.z, 0.f);
+}
+
+// eout = ein + dinv (r - A ein)
+__global__ void __launch_bounds__(256) k_lvl_sweep(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                                   const float* __restrict__ val, const float* __restrict__ dfull,
+                                                   const float* __restrict__ dinv, const float4* __restrict__ r,
+                                                   const float4* __restrict__ ein, float4* __restrict__ eout,
+                                                   const int32_t* __restrict__ gate) {
+    if (gate && __ldg(gate) == 0) return;
+    constexpr int G = kLanesC, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, ein);
+    if (!valid || lane >= S) return;
+    const float4 x = __ldg(ein + row), ri = __ldg(r + row);
+    const float D = __ldg(dfull + row), w = __ldg(dinv + row);
+    eout[row] = make_float4(fmaf(w, ri.x - fmaf(D, x.x, off.x), x.x), fmaf(w, ri.y - fmaf(D, x.y, off.y), x.y),
+                            fmaf(w, ri.z - fmaf(D, x.z, off.z), x.z), 0.f);
+}
+
+// res = r - A e
+__global__ void __launch_bounds__(256) k_lvl_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                                      const float* __restrict__ val, const float* __restrict__ dfull,
+                                                      const float4* __restrict__ r, const float4* __restrict__ e,
+                                                      float4* __restrict__ res, const int32_t* __restrict__ gate) {
+    if (gate && __ldg(gate) == 0) return;
+    constexpr int G = kLanesC, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, e);
+    if (!valid || lane >= S) return;
+    const float4 x = __ldg(e + row), ri = __ldg(r + row);
+    const float D = __ldg(dfull + row);
+    res[row] = make_float4(ri.x - fmaf(D, x.x, off.x), ri.y - fmaf(D, x.y, off.y), ri.z - fmaf(D, x.z, off.z), 0.f);
+}
+
+// dst = cur + P ec (P: 4 coarse parents per row); dst may be cur.
+__global__ void k_lvl_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
+                              const float4* __restrict__ ec, const float4* cur, float4* dst,
+                              const int32_t* __restrict__ gate) {
+    if (gate && __ldg(gate) == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 id = __ldg(pid + i);
+    const float4 w = __ldg(pw + i);
+    const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
+    float4 v = cur[i];
+    v.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+    v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+    v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+    dst[i] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -390,8 +473,10 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle(const CoarseArgs A) {
 // and keeps r, e, e2, res of those rows in its shared memory; a row of
 // another CTA is read through the cluster shared-memory window.  Matrix and
 // transfer operators stay in global memory (read-only, L2-resident).
-// Inputs: level-0 residual (global).  Output: level-1 correction (global,
-// lv[1].e) for the level-0 prolongation kernel.
+// It owns levels F = A.first .. L-1 (F = 1: every coarse level; F > 1: the
+// levels below F run as the grid-wide k_lvl_* kernels).  Input: the level
+// F-1 residual (global).  Output: the level-F correction (global, lv[F].e)
+// for the prolongation kernel of level F-1.
 // ---------------------------------------------------------------------------
 struct SmemLevel {
     int off, n, B, base;   // first global row, rows, rows per CTA, float4 offset of [r|e|e2|res]
@@ -430,10 +515,11 @@ __device__ __forceinline__ float4 rg_offdiag_dsm(cg::cluster_group& cl, float4* 
     return make_float4(ax, ay, az, 0.f);
 }
 
-// Dynamic shared memory (float4 units) the kernel needs for a cluster size.
-__host__ __device__ inline int coarse_smem_float4(const int* nl, int L, int cs, int ncoarsest) {
+// Dynamic shared memory (float4 units) the kernel needs for a cluster size
+// when it owns levels first..L-1.
+__host__ __device__ inline int coarse_smem_float4(const int* nl, int L, int first, int cs, int ncoarsest) {
     int tot = 0;
-    for (int l = 1; l < L; ++l) tot += 4 * ((nl[l] + cs - 1) / cs);
+    for (int l = first; l < L; ++l) tot += 4 * ((nl[l] + cs - 1) / cs);
     return tot + ncoarsest;
 }
 
@@ -450,9 +536,10 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
     const int L = A.L;
     constexpr int Sc = 32 / kLanesC;
     constexpr int R = 0, E = 1, E2 = 2, RES = 3;
+    const int F = A.first;
     SmemLevel q[kMaxLevels];
     int base = 0;
-    for (int l = 1; l < L; ++l) {
+    for (int l = F; l < L; ++l) {
         const int2 rg = A.range[body * L + l];
         q[l].off = rg.x;
         q[l].n = rg.y;
@@ -467,10 +554,10 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
     auto loc = [&](int l, int vec, int i) -> float4& { return smv[q[l].base + vec * q[l].B + i]; };
 
     // ---- descend
-    for (int l = 1; l < L; ++l) {
+    for (int l = F; l < L; ++l) {
         const LevelView& C = A.lv[l];
         const int r0 = first_row(l), cnt = own_rows(l);
-        // restriction r = P^T res_{l-1} (level 0 residual from global memory)
+        // restriction r = P^T res_{l-1} (level F-1 residual from global memory)
         for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
             const int li = b0 + (lane % Sc);
             const bool valid = li < cnt;
@@ -482,7 +569,7 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
                 for (int k = beg + lane / Sc; k < end; k += kLanesC) {
                     const float w = __ldg(C.rw + k);
                     const int ch = __ldg(C.rcol + k);
-                    const float4 t = (l == 1) ? __ldg(A.lv[0].res + ch) : *dsm_ptr(cluster, smv, q[l - 1], RES, ch - q[l - 1].off);
+                    const float4 t = (l == F) ? __ldg(A.lv[l - 1].res + ch) : *dsm_ptr(cluster, smv, q[l - 1], RES, ch - q[l - 1].off);
                     ax = fmaf(w, t.x, ax);
                     ay = fmaf(w, t.y, ay);
                     az = fmaf(w, t.z, az);
@@ -586,7 +673,7 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
         cluster.sync();
     }
     // ---- ascend
-    for (int l = L - 2; l >= 1; --l) {
+    for (int l = L - 2; l >= F; --l) {
         const LevelView& C = A.lv[l];
         const LevelView& Cc = A.lv[l + 1];
         const int r0 = first_row(l), cnt = own_rows(l);
@@ -622,10 +709,10 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
             cluster.sync();
         }
     }
-    // ---- level-1 correction to global memory (own rows only: no remote access after the last barrier)
+    // ---- level-F correction to global memory (own rows only: no remote access after the last barrier)
     {
-        const int r0 = first_row(1), cnt = own_rows(1);
-        for (int li = threadIdx.x; li < cnt; li += blockDim.x) A.lv[1].e[q[1].off + r0 + li] = loc(1, ec[1], li);
+        const int r0 = first_row(F), cnt = own_rows(F);
+        for (int li = threadIdx.x; li < cnt; li += blockDim.x) A.lv[F].e[q[F].off + r0 + li] = loc(F, ec[F], li);
     }
 }
 

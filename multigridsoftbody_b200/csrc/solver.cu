@@ -151,9 +151,10 @@ struct mgsb_solver {
     int cluster = 1;
     int fuse_l0 = 1;
     int coarse_block = 512;
+    int split = 1;   // first level of the cluster kernel; levels 1..split-1 run grid-wide
     // autotuner overrides (0 / -1 = pick by size)
-    int tune_cluster = 0, tune_fuse = -1;
-    int maxv0 = 0, maxv1 = 0;   // largest body on levels 0 and 1
+    int tune_cluster = 0, tune_fuse = -1, tune_split = 0;
+    std::vector<int> maxv;   // largest body's rows on each level
     std::vector<int2> range_host;
     int max_smem_optin = 0;
     int32_t* fac_valid = nullptr;
@@ -259,19 +260,34 @@ bool is_mg(const mgsb_solver* h) { return h->p.solver == MGSB_SOLVER_MULTIGRID; 
 
 // Shape of the coarse V-cycle kernel: explicit tuning if set, else by size
 // (level-0 work fused for bodies up to 40k vertices; ~2.5k rows per CTA).
-size_t coarse_smem_bytes(const mgsb_solver* h, int cs);
+size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split);
+
+// Largest body's rows on a coarse level below which it stays in the cluster
+// kernel by default; larger levels run as grid-wide kernels over all SMs.
+constexpr int kClusterLevelRows = 4096;
 
 void apply_tuning(mgsb_solver* h) {
-    // Default: the distributed-shared-memory kernel with <= 256 level-1 rows per CTA.
+    // Default: the distributed-shared-memory kernel with <= 256 rows of its
+    // first level per CTA; levels above kClusterLevelRows rows run grid-wide.
+    const int L = h->p.levels;
+    if ((int)h->maxv.size() < L) return;   // before set-up
     h->fuse_l0 = h->tune_fuse >= 0 ? h->tune_fuse : 0;
     if (h->p.precision == MGSB_PRECISION_MIXED || h->ls_net) h->fuse_l0 = 0;   // these run the DSM kernel
+    if (h->fuse_l0) {
+        h->split = 1;
+    } else if (h->tune_split > 0) {
+        h->split = std::min(h->tune_split, L - 1);
+    } else {
+        h->split = 1;
+        while (h->split < L - 1 && h->maxv[h->split] > kClusterLevelRows) ++h->split;
+    }
     if (h->tune_cluster > 0) {
         h->cluster = h->tune_cluster;
     } else if (h->fuse_l0) {
-        h->cluster = std::min(16, std::max(1, (h->maxv0 + 2559) / 2560));
+        h->cluster = std::min(16, std::max(1, (h->maxv[0] + 2559) / 2560));
     } else {
-        h->cluster = std::min(16, std::max(1, (h->maxv1 + 255) / 256));
-        while (h->cluster < 16 && coarse_smem_bytes(h, h->cluster) > (size_t)h->max_smem_optin) ++h->cluster;
+        h->cluster = std::min(16, std::max(1, (h->maxv[h->split] + 255) / 256));
+        while (h->cluster < 16 && coarse_smem_bytes(h, h->cluster, h->split) > (size_t)h->max_smem_optin) ++h->cluster;
     }
 }
 
@@ -452,13 +468,12 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dupload(h, pool, &h->dense_off_d, P.dense_off));
         // cluster size of the coarse V-cycle kernel: sized by the rows one body
         // brings to it (level 0 when fused, else level 1)
-        int maxv0 = 0, maxv1 = 0;
-        for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
-            maxv0 = std::max(maxv0, P.range[bi * L].y);
-            maxv1 = std::max(maxv1, P.range[bi * L + 1].y);
-        }
-        h->maxv0 = maxv0;
-        h->maxv1 = maxv1;
+        h->maxv.assign(L, 0);
+        for (size_t bi = 0; bi < h->bodies.size(); ++bi)
+            for (int l = 0; l < L; ++l) h->maxv[l] = std::max(h->maxv[l], P.range[bi * L + l].y);
+        for (int l = 1; l < L; ++l)
+            if (h->lev[l].S != 32 / kLanesC)
+                return set_err(h, MGSB_NOT_SUPPORTED, "coarse level %d has slice height %d", l, h->lev[l].S);
         apply_tuning(h);
         CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
@@ -565,22 +580,22 @@ void enqueue_ref_frame(mgsb_solver* h) {
 }
 
 // Dynamic shared memory of the distributed-shared-memory coarse kernel: the
-// largest body's rows per CTA on every coarse level (4 vectors) + the whole
+// largest body's rows per CTA on every level it owns (4 vectors) + the whole
 // coarsest right-hand side.
-size_t coarse_smem_bytes(const mgsb_solver* h, int cs) {
+size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split) {
     const int L = h->p.levels;
     int best = 0;
     for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
         int nl[kMaxLevels] = {0};
         for (int l = 0; l < L; ++l) nl[l] = h->range_host[bi * L + l].y;
-        best = std::max(best, coarse_smem_float4(nl, L, cs, nl[L - 1]));
+        best = std::max(best, coarse_smem_float4(nl, L, split, cs, nl[L - 1]));
     }
     return (size_t)best * sizeof(float4);
 }
 
 // Can the device co-schedule one cluster of this shape?
-bool coarse_shape_feasible(mgsb_solver* h, int cs, int block, int fused) {
-    const size_t smem = fused ? 0 : coarse_smem_bytes(h, cs);
+bool coarse_shape_feasible(mgsb_solver* h, int cs, int block, int fused, int split) {
+    const size_t smem = fused ? 0 : coarse_smem_bytes(h, cs, split);
     if (smem > (size_t)h->max_smem_optin) return false;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)cs);
@@ -603,11 +618,54 @@ bool coarse_shape_feasible(mgsb_solver* h, int cs, int block, int fused) {
     return nclusters > 0;
 }
 
-mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args) {
+mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args);
+
+// Coarse part of one V-cycle: from the level-0 residual lv[0].res to the
+// level-1 correction lv[1].e.  Levels 1..split-1 run as grid-wide kernels
+// (restrict + first sweep, further pre-sweeps, residual going down;
+// prolongation and post-sweeps coming back up), the rest in one cluster
+// kernel per body.  The post-sweeps of a grid-wide level start in the buffer
+// that makes the last one land in lv[l].e.
+mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
+    CoarseArgs args = args_in;
+    const int F = h->fuse_l0 ? 1 : h->split;
+    args.first = F;
+    const int32_t* gate = args.gate;
+    float4* cur[kMaxLevels] = {};
+    for (int l = 1; l < F; ++l) {
+        const LevelView& C = args.lv[l];
+        const int g = grid_rows(C.n, 32 / kLanesC);
+        LAUNCH(h, k_lvl_restrict, g, kBlock, 0, C.n, C.rptr, C.rcol, C.rw, args.lv[l - 1].res,
+               args.pre > 0 ? C.dinv : nullptr, C.r, C.e, gate);
+        float4 *a = C.e, *b = C.e2;
+        for (int k = 1; k < args.pre; ++k) {
+            LAUNCH(h, k_lvl_sweep, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.dinv, C.r, a, b, gate);
+            std::swap(a, b);
+        }
+        LAUNCH(h, k_lvl_residual, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.r, a, C.res, gate);
+        cur[l] = a;
+    }
+    TRY(launch_coarse_cluster(h, args));
+    for (int l = F - 1; l >= 1; --l) {
+        const LevelView& C = args.lv[l];
+        const LevelView& Cc = args.lv[l + 1];
+        const int g = grid_rows(C.n, 32 / kLanesC);
+        float4* a = (args.post % 2 == 0) ? C.e : C.e2;
+        float4* b = (a == C.e) ? C.e2 : C.e;
+        LAUNCH(h, k_lvl_prolong, grid_for(C.n), kBlock, 0, C.n, Cc.pid, Cc.pw, Cc.e, cur[l], a, gate);
+        for (int k = 0; k < args.post; ++k) {
+            LAUNCH(h, k_lvl_sweep, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.dinv, C.r, a, b, gate);
+            std::swap(a, b);
+        }
+    }
+    return MGSB_OK;
+}
+
+mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(h->bodies.size() * h->cluster));
     cfg.blockDim = dim3((unsigned)h->coarse_block);
-    cfg.dynamicSmemBytes = h->fuse_l0 ? 0 : coarse_smem_bytes(h, h->cluster);
+    cfg.dynamicSmemBytes = h->fuse_l0 ? 0 : coarse_smem_bytes(h, h->cluster, args.first);
     cfg.stream = h->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1561,6 +1619,25 @@ mgsb_status mgsb_set_kernel_shape(mgsb_solver* h, int32_t cluster, int32_t block
     return MGSB_OK;
 }
 
+mgsb_status mgsb_set_coarse_split(mgsb_solver* h, int32_t split) {
+    if (!h) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the coarse split applies to the multigrid kind");
+    if (split < 0 || split >= h->p.levels)
+        return set_err(h, MGSB_INVALID_ARG, "split %d outside 0..%d", split, h->p.levels - 1);
+    h->tune_split = split;
+    apply_tuning(h);
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_get_coarse_split(mgsb_solver* h, int32_t* split) {
+    if (!h || !split) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the coarse split applies to the multigrid kind");
+    TRY(ensure_ready(h));
+    *split = h->fuse_l0 ? 1 : h->split;
+    return MGSB_OK;
+}
+
 mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     if (!h || frames < 1) return MGSB_INVALID_ARG;
     if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "autotuning applies to the multigrid kind");
@@ -1591,22 +1668,26 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
         }
     };
     struct Cand {
-        int cluster, block, fuse;
+        int cluster, block, fuse, split;
     };
     std::vector<Cand> cands;
     const int nb = (int)h->bodies.size();
+    const int L = h->p.levels;
     const int cls[] = {1, 2, 4, 8, 12, 16};
     for (int c : cls) {
         if (nb > 1 && c > 2) continue;   // many bodies: small clusters, one per body
         for (int blk : {256, 512, 1024}) {
-            if (coarse_shape_feasible(h, c, blk, 0)) cands.push_back({c, blk, 0});
+            // split: the cluster kernel's first level; skip clusters with < 32 of its rows per CTA
+            for (int sp = 1; sp < L; ++sp)
+                if ((c == 1 || h->maxv[sp] >= 32 * c) && coarse_shape_feasible(h, c, blk, 0, sp))
+                    cands.push_back({c, blk, 0, sp});
             if (blk >= 512 && c >= 2 && h->p.precision != MGSB_PRECISION_MIXED && !h->ls_net &&
-                coarse_shape_feasible(h, c, blk, 1))
-                cands.push_back({c, blk, 1});
+                coarse_shape_feasible(h, c, blk, 1, 1))
+                cands.push_back({c, blk, 1, 1});
         }
     }
     float best = 1e30f;
-    Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0};
+    Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0, h->split};
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -1614,6 +1695,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     for (const Cand& c : cands) {
         h->tune_cluster = c.cluster;
         h->tune_fuse = c.fuse;
+        h->tune_split = c.split;
         h->coarse_block = c.block;
         apply_tuning(h);
         invalidate_graph(h);
@@ -1646,6 +1728,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     cudaEventDestroy(b);
     h->tune_cluster = bestc.cluster;
     h->tune_fuse = bestc.fuse;
+    h->tune_split = bestc.split;
     h->coarse_block = bestc.block;
     apply_tuning(h);
     invalidate_graph(h);

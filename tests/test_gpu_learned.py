@@ -70,11 +70,12 @@ def test_learned_sweep_gains_over_plain(lib, trained):
     s.close()
 
 
-@pytest.mark.parametrize("graph", [1, 0])
-def test_guard_falls_back_to_plain(lib, graph):
+@pytest.mark.parametrize("graph,split", [(1, 1), (0, 1), (1, 2), (0, 2)])
+def test_guard_falls_back_to_plain(lib, graph, split):
     """A network with wild weights fails the residual check on every V-cycle;
     the fallback restores the start and runs the plain cycle, so the frame
-    equals the plain solver's."""
+    equals the plain solver's (also with level 1 run as grid-wide kernels,
+    whose launches the fallback gates)."""
     m, fixed = beam(4, 40, 4)
     bad = MLP(seed=11)
     bad.params = np.random.default_rng(0).normal(0.0, 30.0, NUM_PARAMS).astype(np.float32)
@@ -82,6 +83,7 @@ def test_guard_falls_back_to_plain(lib, graph):
     for learned in (False, True):
         s = mg.Solver(m, mg_params(levels=3, use_graph=graph))
         s.set_fixed(fixed)
+        s.set_coarse_split(split)
         if learned:
             s.set_learned_smoother(bad, 0.5)
         for a, b in capsule_path(12, start=(0.0, 0.0, 1.3)):

@@ -267,3 +267,49 @@ def test_coarsest_update_many_contacts(lib, oracle_built):
         err = np.abs(s.positions() - o.positions()).max()
         assert err < 1e-5 * m.bbox_diagonal(), (radius, err)
         s.close()
+
+
+@pytest.mark.parametrize("precision,graph", [(mg.PRECISION_FP32, 1), (mg.PRECISION_FP32, 0), (mg.PRECISION_MIXED, 1)])
+def test_coarse_split_same_frames(lib, oracle_built, precision, graph):
+    """Running the first coarse levels as grid-wide kernels instead of inside
+    the cluster kernel keeps every row's arithmetic (same lanes, same order),
+    so all splits give the same frames; the last split also matches the oracle."""
+    m, fixed = beam(8, 80, 8)
+    p = mg_params(levels=4, gravity=(0, 0, 0), precision=precision, refinement_passes=2, use_graph=graph)
+    path = capsule_path(20, start=(0.0, 0.0, 1.3))
+    runs = {}
+    for split in (1, 2, 3):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        s.set_coarse_split(split)
+        assert s.coarse_split() == split
+        for a, b in path:
+            s.set_capsule(a, b, 0.3)
+            s.step()
+        runs[split] = (s.positions_f64() if precision == mg.PRECISION_MIXED else s.positions().astype(np.float64),
+                       np.nonzero(s.contact_flags())[0])
+        s.close()
+    diag = m.bbox_diagonal()
+    for split in (2, 3):
+        assert np.abs(runs[split][0] - runs[1][0]).max() <= 1e-6 * diag, split
+        assert np.array_equal(runs[split][1], runs[1][1])
+    o = Oracle(m, p)
+    o.set_fixed(fixed)
+    for a, b in path:
+        o.set_capsule(a, b, 0.3)
+        o.step()
+    assert np.abs(runs[3][0] - o.positions()).max() < 1e-5 * diag
+    assert np.array_equal(runs[3][1], np.nonzero(o.contact_flags())[0])
+
+
+def test_coarse_split_default_by_size(lib):
+    """By size: coarse levels above 4096 rows run grid-wide (config 2's level 1
+    has 20,449), smaller ones stay in the cluster kernel."""
+    small = mg.Solver(beam(4, 40, 4)[0], mg_params(levels=3))
+    assert small.coarse_split() == 1
+    big = mg.Solver(beam(24, 240, 24)[0], mg_params(levels=5))
+    assert big.level_size(1)[0] == 20449 and big.coarse_split() == 2
+    with pytest.raises(mg.MgsbError):
+        big.set_coarse_split(5)
+    small.close()
+    big.close()
