@@ -236,10 +236,16 @@ mgsb_status mgsb_set_kernel_shape(mgsb_solver* h, int32_t cluster, int32_t block
 /* Coarse-level split of the V-cycle: levels 1..split-1 run as grid-wide
  * kernels over every SM, levels split..L-1 in the cluster kernel (split 1 =
  * all coarse levels in the cluster kernel; 0 = by size: levels whose largest
- * body has more than 4096 rows run grid-wide).  The autotuner also picks it.
+ * body has more than 1024 rows run grid-wide).  The autotuner also picks it.
  * Same arithmetic either way.  No reference counterpart. */
 mgsb_status mgsb_set_coarse_split(mgsb_solver* h, int32_t split);
 mgsb_status mgsb_get_coarse_split(mgsb_solver* h, int32_t* split);
+/* Programmatic dependent launch between the frame's consecutive kernels
+ * (default 1): the next kernel's blocks are scheduled while the previous one
+ * finishes and wait for its completion on the device, which hides most of
+ * the launch gap; 0 = plain stream order.  Same results either way.  No
+ * reference counterpart. */
+mgsb_status mgsb_set_launch_overlap(mgsb_solver* h, int32_t on);
 
 /* Host-only (no GPU): build the multigrid hierarchy of one mesh exactly as
  * mgsb_create would and return level `level`: vertex count, off-diagonal

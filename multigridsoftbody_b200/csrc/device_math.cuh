@@ -5,6 +5,17 @@
 
 namespace mgsb {
 
+// Programmatic dependent launch: allow the next kernel of the stream to be
+// scheduled now (its blocks become resident and wait), then wait until the
+// previous kernel has completed and its writes are visible.  Every kernel
+// that the solver launches with the programmatic-serialization attribute
+// calls this before touching global memory; without the attribute both
+// instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, 0.f); }
 __device__ __forceinline__ float4 f4sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, 0.f); }
 __device__ __forceinline__ float4 f4scale(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, 0.f); }

@@ -47,6 +47,7 @@ struct BodyDev {
 __global__ void k_ref_predict(int n, float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ s,
                               float4* __restrict__ prev, float4* __restrict__ last, const float* __restrict__ fixf,
                               float damping, float dt, float gx, float gy, float gz) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 p = x[i], vel = v[i];
@@ -69,6 +70,7 @@ __global__ void __launch_bounds__(256) k_ref_local(int T, const int4* __restrict
                                                    const float4* __restrict__ invB, const float2* __restrict__ invC,
                                                    const float4* __restrict__ x, const int4* __restrict__ slot_of,
                                                    float4* __restrict__ slots, float stiffness, int drop_small = 1) {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const int4 id = __ldg(tets + t);
@@ -129,6 +131,7 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
     float kc, float dt, float omega, double relax, int last_iter, int32_t* __restrict__ cflag, float* __restrict__ cdepth,
     float* __restrict__ cenergy, int32_t* __restrict__ nonfinite, const int32_t* __restrict__ tri_ptr = nullptr,
     const int32_t* __restrict__ tri_idx = nullptr, const float4* __restrict__ tri_push = nullptr) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float fx = 0.f, fy = 0.f, fz = 0.f;
@@ -234,6 +237,7 @@ __global__ void __launch_bounds__(256) k_ref_vertex(
 __global__ void k_mg_predict(int n, float4* __restrict__ x, float4* __restrict__ v, float4* __restrict__ s,
                              float4* __restrict__ last, const float* __restrict__ fixf, const int32_t* __restrict__ body_of,
                              const BodyDev* __restrict__ bodies, float dt) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const BodyDev& B = bodies[__ldg(body_of + i)];
@@ -284,6 +288,7 @@ __global__ void k_contact_all(int ns, const int32_t* __restrict__ surf, const in
                               const BodyDev* __restrict__ bodies, const float4* __restrict__ s,
                               const float* __restrict__ fixf, float kc, int32_t* __restrict__ cflag,
                               float* __restrict__ c0, float4* __restrict__ target) {
+    pdl_enter();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= ns) return;
     const int i = __ldg(surf + q);
@@ -302,6 +307,7 @@ __global__ void k_l0_frame(int n, const float4* __restrict__ s, const float* __r
                            const float4* __restrict__ target, const float* __restrict__ diag0,
                            const float* __restrict__ fixf, float omega, float4* __restrict__ b0, float* __restrict__ dfull,
                            float* __restrict__ dinv, float4* __restrict__ d) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float c = __ldg(c0 + i);
@@ -318,6 +324,7 @@ __global__ void k_l0_frame(int n, const float4* __restrict__ s, const float* __r
 // finiteness check of the new positions.
 __global__ void k_mg_finish(int n, const float4* __restrict__ s, const float4* __restrict__ d, float4* __restrict__ x,
                             float4* __restrict__ v, float inv_dt, int32_t* __restrict__ nonfinite) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 sv = __ldg(s + i), dv = __ldg(d + i);
@@ -336,6 +343,7 @@ __global__ void k_coarse_frame(int n, const int32_t* __restrict__ rptr, const in
                                const float* __restrict__ rw, const float* __restrict__ cfine,
                                const float* __restrict__ diag0, float omega, float* __restrict__ c,
                                float* __restrict__ dfull, float* __restrict__ dinv) {
+    pdl_enter();
     const int J = blockIdx.x * blockDim.x + threadIdx.x;
     if (J >= n) return;
     float acc = 0.f;
@@ -355,6 +363,7 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
                                                   const float4* __restrict__ gB, const float2* __restrict__ gC,
                                                   const float4* __restrict__ s, const float4* __restrict__ d,
                                                   const int4* __restrict__ slot_of, float4* __restrict__ slots) {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     const int4 id = __ldg(tets + t);
@@ -400,6 +409,7 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
 // RHS assembly alone: b = b0 + sum of the vertex's slots.
 __global__ void k_gather_rhs(int n, float4* __restrict__ b, const float4* __restrict__ b0,
                              const int32_t* __restrict__ slot_ptr, const float4* __restrict__ slots) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 bi = __ldg(b0 + i);
@@ -414,6 +424,7 @@ __global__ void k_gather_rhs(int n, float4* __restrict__ b, const float4* __rest
 // v = (x - last)/dt plus a finiteness check of the new positions.
 __global__ void k_velocity(int n, const float4* __restrict__ x, const float4* __restrict__ last, float4* __restrict__ v,
                            float dt, int32_t* __restrict__ nonfinite) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = __ldg(x + i), l = __ldg(last + i);

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_residual(int n, const int32_t
                                                             const int32_t* __restrict__ slot_ptr = nullptr,
                                                             const float4* __restrict__ slots = nullptr,
                                                             float4* __restrict__ bgather = nullptr) {
+    pdl_enter();
     __shared__ float red[kLsThreads / 32];
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_features(int n, const int32_t
                                                             const float* __restrict__ fixf, const float4* __restrict__ r,
                                                             uint8_t* __restrict__ tiles, float* __restrict__ scale,
                                                             float* __restrict__ xf) {
+    pdl_enter();
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -175,6 +177,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
                                                              const float* __restrict__ fixf, const float4* __restrict__ r,
                                                              const uint8_t* __restrict__ img, float4* __restrict__ d,
                                                              int32_t* __restrict__ err) {
+    pdl_enter();
     constexpr int S = 32 / kLanesL0;   // level-0 slice height
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     MlpSmem& Sm = *reinterpret_cast<MlpSmem*>(smem_raw);
@@ -262,6 +265,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
 __global__ void k_ls_guard(int n0, const float* __restrict__ p0, int n1, const float* __restrict__ p1, float gamma2,
                            int32_t* __restrict__ gate, unsigned long long* __restrict__ stats,
                            cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_enter();
     __shared__ float red[kLsThreads / 32];
     float a = 0.f, b = 0.f;
     for (int i = threadIdx.x; i < n0; i += blockDim.x) a += p0[i];
@@ -287,6 +291,7 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     const float4* __restrict__ b, float* __restrict__ part1, const float* __restrict__ part0, float gamma2,
     int32_t* __restrict__ gate, unsigned long long* __restrict__ stats, cudaGraphConditionalHandle cond, int use_cond,
     unsigned int* __restrict__ ticket) {
+    pdl_enter();
     __shared__ float red[kLsThreads / 32];
     __shared__ bool last;
     constexpr int G = kLanesL0, S = 32 / G;
@@ -334,6 +339,7 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
 // Fallback entry: d = dsave (or 0 when dsave is null) when the gate is set.
 __global__ void k_ls_restore(int n, const int32_t* __restrict__ gate, const float4* __restrict__ dsave,
                              float4* __restrict__ d) {
+    pdl_enter();
     if (__ldg(gate) == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -342,6 +348,7 @@ __global__ void k_ls_restore(int n, const int32_t* __restrict__ gate, const floa
 
 // Gated copy (fallback result back into the frame's displacement buffer).
 __global__ void k_ls_copy(int n, const int32_t* __restrict__ gate, const float4* __restrict__ src, float4* __restrict__ dst) {
+    pdl_enter();
     if (__ldg(gate) == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -354,6 +361,7 @@ __global__ void k_ls_copy(int n, const int32_t* __restrict__ gate, const float4*
 __global__ void k_ls_targets(int n, const float* __restrict__ scale, const float* __restrict__ dfull,
                              const float4* __restrict__ estar, const float4* __restrict__ ecoarse, float* __restrict__ t,
                              uint8_t* __restrict__ mask, float* __restrict__ snorm) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float s = scale[i];

@@ -155,6 +155,7 @@ __global__ void __launch_bounds__(256) k_l0_sweep_rg(int n, const int32_t* __res
                                                      const float4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
                                                      const float4* __restrict__ slots, int gather,
                                                      const int32_t* __restrict__ gate = nullptr) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;   // gated launches run only when the learned V-cycle was rejected
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(256) k_l0_residual_rg(int n, const int32_t* __
                                                         const float* __restrict__ val, const float* __restrict__ dfull,
                                                         const float4* __restrict__ dvec, const float4* __restrict__ b,
                                                         float4* __restrict__ res, const int32_t* __restrict__ gate = nullptr) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -200,6 +202,7 @@ __global__ void __launch_bounds__(256) k_l0_residual_rg(int n, const int32_t* __
 // Level-0 prolongation d += P e1 (used when the coarse kernel does not fuse it).
 __global__ void k_l0_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
                              const float4* __restrict__ ec, float4* __restrict__ v, const int32_t* __restrict__ gate = nullptr) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -226,6 +229,7 @@ __global__ void __launch_bounds__(256) k_lvl_restrict(int n, const int32_t* __re
                                                       const float* __restrict__ rw, const float4* __restrict__ res_fine,
                                                       const float* __restrict__ dinv, float4* __restrict__ r,
                                                       float4* __restrict__ e, const int32_t* __restrict__ gate) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     constexpr int G = kLanesC, S = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -246,6 +250,7 @@ __global__ void __launch_bounds__(256) k_lvl_sweep(int n, const int32_t* __restr
                                                    const float* __restrict__ dinv, const float4* __restrict__ r,
                                                    const float4* __restrict__ ein, float4* __restrict__ eout,
                                                    const int32_t* __restrict__ gate) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     constexpr int G = kLanesC, S = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -265,6 +270,7 @@ __global__ void __launch_bounds__(256) k_lvl_residual(int n, const int32_t* __re
                                                       const float* __restrict__ val, const float* __restrict__ dfull,
                                                       const float4* __restrict__ r, const float4* __restrict__ e,
                                                       float4* __restrict__ res, const int32_t* __restrict__ gate) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     constexpr int G = kLanesC, S = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -282,6 +288,7 @@ __global__ void __launch_bounds__(256) k_lvl_residual(int n, const int32_t* __re
 __global__ void k_lvl_prolong(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
                               const float4* __restrict__ ec, const float4* cur, float4* dst,
                               const int32_t* __restrict__ gate) {
+    pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -300,6 +307,7 @@ __global__ void k_lvl_prolong(int n, const int4* __restrict__ pid, const float4*
 // separated by cluster barriers (release/acquire on global memory).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_coarse_vcycle(const CoarseArgs A) {
+    pdl_enter();
     if (A.gate && __ldg(A.gate) == 0) return;   // uniform over the cluster, before any barrier
     cg::cluster_group cluster = cg::this_cluster();
     const int cs = (int)cluster.num_blocks();
@@ -524,6 +532,7 @@ __host__ __device__ inline int coarse_smem_float4(const int* nl, int L, int firs
 }
 
 __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) {
+    pdl_enter();
     if (A.gate && __ldg(A.gate) == 0) return;   // uniform over the cluster, before any barrier
     extern __shared__ float4 smv[];
     cg::cluster_group cluster = cg::this_cluster();
@@ -801,6 +810,7 @@ __global__ void __launch_bounds__(1024) k_coarsest_update(const int2* __restrict
                                                           const T* __restrict__ A0, const T* __restrict__ B0,
                                                           const float* __restrict__ c, float* __restrict__ c_prev,
                                                           T* __restrict__ Ainv, int32_t* __restrict__ valid) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* sm = reinterpret_cast<T*>(sm_raw);
     __shared__ int changed, k;

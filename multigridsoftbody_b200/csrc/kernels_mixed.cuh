@@ -22,6 +22,7 @@ __global__ void k_mx_predict(int n, double4* __restrict__ x, double4* __restrict
                              double4* __restrict__ last, float4* __restrict__ s32, float4* __restrict__ x32,
                              const float* __restrict__ fixf, const int32_t* __restrict__ body_of,
                              const BodyDev* __restrict__ bodies, double dt) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const BodyDev& B = bodies[__ldg(body_of + i)];
@@ -75,6 +76,7 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
                                    float omega, int32_t* __restrict__ cflag, float* __restrict__ c0,
                                    double4* __restrict__ b0, float* __restrict__ dfull, float* __restrict__ dinv,
                                    double4* __restrict__ d64, float4* __restrict__ d32, float4* __restrict__ target) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int flag = 0;
@@ -97,6 +99,7 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
 // b = b0 + sum of the vertex's slots, accumulated in FP64.
 __global__ void __launch_bounds__(256) k_mx_rhs(int n, const double4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
                                                 const float4* __restrict__ slots, double4* __restrict__ b) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 acc = b0[i];
@@ -118,6 +121,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
                                                      const float* __restrict__ c, const double4* __restrict__ d, const double4* __restrict__ b,
                                                      const float* __restrict__ dinv, float4* __restrict__ r32,
                                                      float4* __restrict__ e, int first_sweep) {
+    pdl_enter();
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -153,6 +157,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
 
 // d += e (FP64), FP32 mirror for the local step.
 __global__ void k_mx_update(int n, const float4* __restrict__ e, double4* __restrict__ d, float4* __restrict__ d32) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 c = __ldg(e + i);
@@ -167,6 +172,7 @@ __global__ void k_mx_update(int n, const float4* __restrict__ e, double4* __rest
 // x = s + d, v = v_predicted + d/dt (FP64); FP32 mirror; finiteness check.
 __global__ void k_mx_finish(int n, const double4* __restrict__ s, const double4* __restrict__ d, double4* __restrict__ x,
                             double4* __restrict__ v, float4* __restrict__ x32, double inv_dt, int32_t* __restrict__ nonfinite) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double4 sv = s[i], dv = d[i];

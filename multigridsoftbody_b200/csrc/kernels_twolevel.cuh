@@ -20,6 +20,7 @@ namespace mgsb {
 // vertex kernel gathers the per-triangle sums through a vertex->triangle CSR.
 __global__ void __launch_bounds__(256) k_ref_tri_dcd(int nf, const int4* __restrict__ tris, const float4* __restrict__ x,
                                                      const SphereSet* __restrict__ spheres, float4* __restrict__ push) {
+    pdl_enter();
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
     const int4 t = __ldg(tris + f);
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(256) k_ref_tri_dcd(int nf, const int4* __restr
 // fine level from the coarse one (runInterpolate) and back (runAverage).
 __global__ void k_tl_transfer(int n, const int4* __restrict__ ids, const float4* __restrict__ w,
                               const float4* __restrict__ src, float4* __restrict__ x, float4* __restrict__ prev) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 id = __ldg(ids + i);
@@ -137,6 +139,7 @@ __global__ void k_tl_transfer(int n, const int4* __restrict__ ids, const float4*
 // tet (updateMapping, PDSolver.cu:764-793; barycentricCoordinate utils.cu:335-364).
 __global__ void k_tl_update_mapping(int n, const float4* __restrict__ xf, const int4* __restrict__ ids,
                                     const float4* __restrict__ xc, float4* __restrict__ w) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 id = __ldg(ids + i);

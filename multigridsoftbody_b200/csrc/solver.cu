@@ -152,6 +152,7 @@ struct mgsb_solver {
     int fuse_l0 = 1;
     int coarse_block = 512;
     int split = 1;   // first level of the cluster kernel; levels 1..split-1 run grid-wide
+    bool pdl = true;  // programmatic dependent launch between consecutive kernels
     // autotuner overrides (0 / -1 = pick by size)
     int tune_cluster = 0, tune_fuse = -1, tune_split = 0;
     std::vector<int> maxv;   // largest body's rows on each level
@@ -264,7 +265,7 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split);
 
 // Largest body's rows on a coarse level below which it stays in the cluster
 // kernel by default; larger levels run as grid-wide kernels over all SMs.
-constexpr int kClusterLevelRows = 4096;
+constexpr int kClusterLevelRows = 1024;
 
 void apply_tuning(mgsb_solver* h) {
     // Default: the distributed-shared-memory kernel with <= 256 rows of its
@@ -549,10 +550,31 @@ void prof_mark(mgsb_solver* h, const char* name) {
     if (name) h->prof_names.push_back(name);
 }
 
+// Kernel launch on the solver's stream.  With h->pdl the launch carries the
+// programmatic-serialization attribute: its blocks may be scheduled while the
+// previous kernel finishes, and wait in pdl_enter() until that kernel has
+// completed (every kernel launched here calls it first).  Arguments are
+// converted to the kernel's parameter types, so every parameter is passed.
+template <typename... KArgs, typename... Args>
+void launch_kernel(mgsb_solver* h, void (*kernel)(KArgs...), int grid, int block, size_t smem, Args&&... args) {
+    static_assert(sizeof...(KArgs) == sizeof...(Args), "pass every kernel parameter");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = h->pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 #define LAUNCH(h, kernel, grid, block, smem, ...)                                  \
     do {                                                                             \
         if ((h)->profiling) prof_mark((h), #kernel);                                 \
-        kernel<<<(grid), (block), (smem), (h)->stream>>>(__VA_ARGS__);              \
+        launch_kernel((h), kernel, (grid), (block), (smem), __VA_ARGS__);           \
         if ((h)->profiling) prof_mark((h), nullptr);                                 \
         ++(h)->launches;                                                             \
     } while (0)
@@ -566,12 +588,12 @@ void enqueue_ref_frame(mgsb_solver* h) {
     float omega = 1.0f;
     for (int it = 0; it < p.iterations; ++it) {
         LAUNCH(h, k_ref_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->x, h->slot_of, h->slots,
-               p.volume_stiffness);
+               p.volume_stiffness, 1);
         omega = 4 / (4 - p.cheb_rho * p.cheb_rho * omega);
         LAUNCH(h, k_ref_vertex, grid_for(n), kBlock, 0, n, h->x, h->prev, h->s, h->last, h->v, h->fixf, h->mass,
                h->vdiag, h->slot_ptr, h->slots, h->spheres_dev, p.collision_stiffness, p.dt, omega,
                (double)p.relaxation, it == p.iterations - 1 ? 3 : 0, h->cflag, h->cdepth, h->cenergy,
-               h->nonfinite);
+               h->nonfinite, nullptr, nullptr, nullptr);
     }
     if (p.iterations == 0) {
         // velocity only
@@ -667,13 +689,15 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
     cfg.blockDim = dim3((unsigned)h->coarse_block);
     cfg.dynamicSmemBytes = h->fuse_l0 ? 0 : coarse_smem_bytes(h, h->cluster, args.first);
     cfg.stream = h->stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = (unsigned)h->cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = h->pdl ? 2 : 1;
     if (h->profiling) prof_mark(h, "k_coarse_vcycle");
     // fused: global-memory kernel that also owns the level-0 residual and prolongation;
     // else the distributed-shared-memory kernel over levels >= 1
@@ -717,7 +741,7 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, d, nullptr);
     // post-smoothing
     LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-           h->ls_r, nullptr, nullptr);
+           h->ls_r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
     // guard.  Inside a CUDA graph the fallback is the body of a conditional IF
@@ -843,21 +867,21 @@ void enqueue_mg_frame(mgsb_solver* h) {
             bool gathered = pass > 0;
             for (int k = 0; k < p.pre_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1);
+                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1, nullptr);
                 gathered = true;
                 std::swap(xa, xb);
             }
             if (!gathered) LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
             if (!h->fuse_l0)
                 LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
-                       lv[0].dfull, xa, h->b, lv[0].res);
+                       lv[0].dfull, xa, h->b, lv[0].res, nullptr);
             ca.d = xa;
             launch_coarse(h, ca);
             if (!h->fuse_l0)   // the shared-memory kernel leaves the level-1 correction in lv[1].e
-                LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, xa);
+                LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, xa, nullptr);
             for (int k = 0; k < p.post_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0);
+                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0, nullptr);
                 std::swap(xa, xb);
             }
         }
@@ -937,16 +961,16 @@ void enqueue_mixed_frame(mgsb_solver* h) {
             }
             for (int k = 1; k < p.pre_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0);
+                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0, nullptr);
                 std::swap(ea, eb);
             }
             LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                   ea, h->r32, lv[0].res);
+                   ea, h->r32, lv[0].res, nullptr);
             launch_coarse(h, ca);
-            LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, ea);
+            LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, ea, nullptr);
             for (int k = 0; k < p.post_sweeps; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0);
+                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0, nullptr);
                 std::swap(ea, eb);
             }
             LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
@@ -1626,6 +1650,13 @@ mgsb_status mgsb_set_coarse_split(mgsb_solver* h, int32_t split) {
         return set_err(h, MGSB_INVALID_ARG, "split %d outside 0..%d", split, h->p.levels - 1);
     h->tune_split = split;
     apply_tuning(h);
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_set_launch_overlap(mgsb_solver* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
+    h->pdl = on != 0;
     invalidate_graph(h);
     return MGSB_OK;
 }

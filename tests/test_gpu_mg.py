@@ -303,13 +303,48 @@ def test_coarse_split_same_frames(lib, oracle_built, precision, graph):
 
 
 def test_coarse_split_default_by_size(lib):
-    """By size: coarse levels above 4096 rows run grid-wide (config 2's level 1
-    has 20,449), smaller ones stay in the cluster kernel."""
+    """By size: coarse levels above 1024 rows run grid-wide (config 2's levels
+    1 and 2 have 20,449 and 2,989), smaller ones stay in the cluster kernel."""
     small = mg.Solver(beam(4, 40, 4)[0], mg_params(levels=3))
     assert small.coarse_split() == 1
     big = mg.Solver(beam(24, 240, 24)[0], mg_params(levels=5))
-    assert big.level_size(1)[0] == 20449 and big.coarse_split() == 2
+    assert big.level_size(2)[0] == 2989 and big.coarse_split() == 3
     with pytest.raises(mg.MgsbError):
         big.set_coarse_split(5)
     small.close()
     big.close()
+
+
+@pytest.mark.parametrize("kind", ["fp32_graph", "fp32_eager", "mixed", "reference", "batch"])
+def test_launch_overlap_bitwise(lib, kind):
+    """Programmatic dependent launch only moves when a kernel's blocks are
+    scheduled; each still waits for its predecessor, so frames are bitwise
+    the same with it on and off."""
+    m, fixed = beam(4, 40, 4)
+    meshes, fixeds = m, [fixed]
+    if kind == "reference":
+        p = mg.default_params(mg.SOLVER_REFERENCE_JACOBI, iterations=10)
+    elif kind == "mixed":
+        p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=2)
+    else:
+        p = mg_params(levels=3, use_graph=0 if kind == "fp32_eager" else 1)
+    if kind == "batch":
+        m1, f1 = beam(3, 20, 5, half_len=5.0)
+        meshes, fixeds = [m, m1], [fixed, f1]
+    path = capsule_path(12, start=(0.0, 0.0, 1.3))
+    out = {}
+    for on in (True, False):
+        s = mg.Solver(meshes, p)
+        for b, f in enumerate(fixeds):
+            s.set_fixed(f, body=b)
+        s.set_launch_overlap(on)
+        for a, b in path:
+            if kind == "reference":
+                s.set_spheres(((a + b) / 2)[None], [0.6])
+            else:
+                s.set_capsule(a, b, 0.3)
+            s.step()
+        out[on] = [s.positions(b) for b in range(len(fixeds))]
+        s.close()
+    for x_on, x_off in zip(out[True], out[False]):
+        assert np.array_equal(x_on, x_off)
