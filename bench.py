@@ -6,9 +6,11 @@
 
 One "step" = one PD frame (10 local/global iterations) of the workload on one
 GPU.  The default workload is the headline: the learned-smoother mixed-precision
-multigrid (2 refinement passes per PD iteration) on the 103,680-tet beam, with
-the plain FP32 multigrid (1 V-cycle per PD iteration) timed the same way in the
-same run and both checked for max vertex error against a converged reference.
+multigrid (1 refinement pass per PD iteration) on the 103,680-tet beam, with
+the plain FP32 multigrid (1 and 2 V-cycles per PD iteration) timed the same way
+in the same run and all checked for max vertex error against a converged
+reference; the ratio that counts is against the plain form that meets the
+1e-5 x bbox-diagonal bar.
 Multi-GPU runs are independent replicas (the single body does not shard);
 value = frames of all ranks / max-over-ranks time.  L2 is flushed (256 MB
 write) before every timed frame, outside the timed span.
@@ -57,7 +59,7 @@ def make_workload(name, mg):
         fixed = (np.abs(m.positions[:, 1] - 10.0) < 1e-5).astype(np.uint8)
         p = mg.default_params(mg.SOLVER_MULTIGRID, levels=levels, iterations=10, gravity=(0.0, 0.0, 0.0),
                               precision=mg.PRECISION_MIXED if mixed else mg.PRECISION_FP32,
-                              refinement_passes=2 if mixed else 1)
+                              refinement_passes=(1 if name == "beam" else 2) if mixed else 1)
         # Start the tool 0.3 above the top face so every timed frame has contacts.
         path = capsule_path(4096, start=(0.0, 0.0, 1.5))
 
@@ -74,7 +76,9 @@ def make_workload(name, mg):
                 f"moving -z 0.02/frame + N(0,0.005^2) jitter (seed 1), in contact"
                 + (", learned smoother (1 learned sweep before and after the coarse correction, residual guard "
                    "with plain fallback)" if name == "beam" else ", 2+2 Jacobi sweeps")
-                + (", mixed precision (FP64 residual, 2 refinement passes)" if mixed else "")
+                + ((", mixed precision (FP64 residual, %d refinement pass%s)" % (p.refinement_passes,
+                                                                                "" if p.refinement_passes == 1 else "es"))
+                   if mixed else "")
                 + (", E log-uniform [5e4,2e5] per tet (seed 7)" if name == "large_mixed" else ""))
         return [m], [p], [fixed], tool, desc, mats
     if name == "blob":
@@ -177,29 +181,51 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # Algorithmic bytes per launch of the main kernels (FP32, each array once)
 # ---------------------------------------------------------------------------
-def coarse_vcycle_bytes(solver, params):
-    """Algorithmic bytes of one k_coarse_vcycle launch (every array of every
-    phase counted once; FP32 values, int32 indices, float4 vectors)."""
-    L, pre, post = params.levels, params.pre_sweeps, params.post_sweeps
-    lv = [solver.level_info(l) for l in range(L)]
-    n = [x["n"] for x in lv]
-    nnz = [x["nnz"] for x in lv]
-    nch = [x["nchild"] for x in lv]
-    fuse = lv[0]["fuse_l0"]
-    sweep = lambda l: 8 * nnz[l] + n[l] * (16 + 16 + 8 + 16)        # ELL + e_in, r, dfull/dinv, e_out
-    resid = lambda l: 8 * nnz[l] + n[l] * (16 + 16 + 4 + 16)
-    restrict = lambda l: 8 * nch[l] + 16 * n[l - 1] + n[l] * (4 + 16 + 4 + 16)
-    prolong = lambda l: n[l] * (16 + 16 + 16 + 16) + 16 * n[l + 1]
-    b = 0
-    if fuse:
-        b += 8 * nnz[0] + n[0] * (16 + 16 + 4 + 16)                     # level-0 residual
-        b += n[0] * (16 + 16 + 16 + 16) + 16 * n[1]                     # d += P e1
-    for l in range(1, L - 1):
-        b += restrict(l) + max(pre - 1, 0) * sweep(l) + resid(l) + prolong(l) + post * sweep(l)
-    c = L - 1
-    b += 8 * nch[c] + 16 * n[c - 1] + n[c] * 20                         # coarsest restriction
-    b += 4 * n[c] * n[c] + 32 * n[c]                                     # dense inverse x r
-    return float(b)
+class LevelBytes:
+    """Algorithmic bytes of one launch of each multigrid phase on level l
+    (every array counted once; FP32 values, int32 indices, float4 vectors)."""
+
+    def __init__(self, solver, params):
+        self.L, self.pre, self.post = params.levels, params.pre_sweeps, params.post_sweeps
+        lv = [solver.level_info(l) for l in range(self.L)]
+        self.n = [x["n"] for x in lv]
+        self.nnz = [x["nnz"] for x in lv]
+        self.nch = [x["nchild"] for x in lv]
+        self.fuse = lv[0]["fuse_l0"]
+        self.split = solver.coarse_split()
+
+    def sweep(self, l):      # ELL + e_in, r, dfull/dinv, e_out
+        return 8 * self.nnz[l] + self.n[l] * (16 + 16 + 8 + 16)
+
+    def resid(self, l):      # ELL + e, r, dfull, res
+        return 8 * self.nnz[l] + self.n[l] * (16 + 16 + 4 + 16)
+
+    def restrict(self, l):   # children (id, weight) + finer residual; r, e, dinv written/read
+        return 8 * self.nch[l] + 16 * self.n[l - 1] + self.n[l] * (4 + 16 + 4 + 16)
+
+    def prolong(self, l):    # level l: parents ids/weights, cur, dst; coarser correction
+        return self.n[l] * (16 + 16 + 16 + 16) + 16 * self.n[l + 1]
+
+    def grid_levels(self):
+        return range(1, self.split)
+
+    def coarse_vcycle(self):
+        """One launch of the cluster kernel: levels split..L-1."""
+        L, pre, post = self.L, self.pre, self.post
+        b = 0
+        if self.fuse:
+            b += self.resid(0) + self.prolong(0)
+        for l in range(self.split, L - 1):
+            b += self.restrict(l) + max(pre - 1, 0) * self.sweep(l) + self.resid(l) + self.prolong(l) + post * self.sweep(l)
+        c = L - 1
+        b += 8 * self.nch[c] + 16 * self.n[c - 1] + self.n[c] * 20       # coarsest restriction
+        b += 4 * self.n[c] * self.n[c] + 32 * self.n[c]                   # dense inverse x r
+        return float(b)
+
+    def mean_over_grid_levels(self, f, per_level):
+        tot = sum(per_level * f(l) for l in self.grid_levels())
+        cnt = per_level * len(self.grid_levels())
+        return float(tot / cnt) if cnt else None
 
 
 def algorithmic_bytes(kernel, solver, meshes, params):
@@ -215,8 +241,21 @@ def algorithmic_bytes(kernel, solver, meshes, params):
         gather = plain + 16 * n0 + 4 * n0 + 16 * 4 * T   # b0, slot_ptr, slots
         k = params.pre_sweeps + params.post_sweeps
         return (gather + (k - 1) * plain) / k
+    lb = LevelBytes(solver, params)
     if kernel == "k_coarse_vcycle":
-        return coarse_vcycle_bytes(solver, params)
+        return lb.coarse_vcycle()
+    if kernel == "k_l0_residual_rg":
+        return float(lb.resid(0))
+    if kernel == "k_l0_prolong":
+        return float(lb.prolong(0))
+    if kernel == "k_lvl_sweep":        # (pre - 1) + post sweeps on each grid-wide level
+        return lb.mean_over_grid_levels(lb.sweep, max(params.pre_sweeps - 1, 0) + params.post_sweeps)
+    if kernel == "k_lvl_residual":
+        return lb.mean_over_grid_levels(lb.resid, 1)
+    if kernel == "k_lvl_restrict":
+        return lb.mean_over_grid_levels(lb.restrict, 1)
+    if kernel == "k_lvl_prolong":
+        return lb.mean_over_grid_levels(lb.prolong, 1)
     if kernel == "k_ls_sweep_tc":
         # learned sweep: level-0 row walk (8 B/nnz, r/D/L/fix 28 B per row) + d read/write 32 B per row;
         # the 12.9 KB weight image per CTA comes from L2
@@ -333,7 +372,7 @@ def run_reference(args):
 LEARNED = ("beam", "blob")
 
 
-def train_network(mg, name, device, stream_ptr, runs=8, frames=40, every=10, sweeps=4, steps=6000):
+def train_network(mg, name, device, stream_ptr, runs=8, frames=40, every=10, sweeps=3, steps=20000):
     """Pairs from the plain FP32 multigrid solver on seeded runs of the same scene (tool seeds other than
     the benchmark's), then the library's own trainer (Adam, 4096-pair minibatches)."""
     from multigridsoftbody_b200.learned import MLP, blob_scene, blob_tool_path
@@ -397,7 +436,8 @@ def accuracy(mg, meshes, fixeds, params, tool, net, frames=40):
     diag = m.bbox_diagonal()
     out = {"frames": frames, "reference": "GPU mixed precision, 6 V-cycles (FP64 residual) per PD iteration, "
                                           "plain smoother; matches the FP64 oracle to ~1e-7 m"}
-    for key, prec, passes, learned in (("learned_mixed_2pass", mg.PRECISION_MIXED, 2, True),
+    for key, prec, passes, learned in (("learned_mixed_%dpass" % params[0].refinement_passes, mg.PRECISION_MIXED,
+                                        params[0].refinement_passes, True),
                                        ("plain_fp32_1pass", mg.PRECISION_FP32, 1, False),
                                        ("plain_fp32_2pass", mg.PRECISION_FP32, 2, False)):
         x, st = run(prec, passes, learned)
@@ -635,7 +675,18 @@ def run_ours(args):
         comparison["ratio_vs_plain_fp32_2pass"] = job_throughput(args.steps, world, ms) / comparison[
             "plain_fp32_2pass"]["frames_per_s"]
         if rank == 0 and world == 1:
-            comparison["accuracy"] = accuracy(mg, meshes, fixeds, params, tool, net)
+            acc = accuracy(mg, meshes, fixeds, params, tool, net)
+            comparison["accuracy"] = acc
+            # the headline ratio: against the cheapest plain FP32 form that meets the error bar
+            bar = 1e-5
+            key = "learned_mixed_%dpass" % params[0].refinement_passes
+            comparison["error_bar_over_diag"] = bar
+            comparison["learned_meets_bar"] = acc[key]["err_over_diag"] <= bar
+            for passes in (1, 2):
+                if acc["plain_fp32_%dpass" % passes]["err_over_diag"] <= bar:
+                    comparison["plain_fp32_at_bar"] = "plain_fp32_%dpass" % passes
+                    comparison["ratio_vs_plain_fp32_at_bar"] = comparison["ratio_vs_plain_fp32_%dpass" % passes]
+                    break
     value = job_throughput(args.steps, world, ms)
     e2e_value = job_throughput(args.steps, world, e2e_ms)
     if rank == 0:

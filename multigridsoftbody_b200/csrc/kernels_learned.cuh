@@ -23,18 +23,6 @@ namespace {
 constexpr int kLsThreads = 256;
 constexpr int kLsRowsPerBlock = kLsThreads / kLanesL0;   // 64 rows per block
 
-__device__ __forceinline__ float block_sum_f(float v, float* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    float t = 0.f;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-    return t;   // valid in thread 0
-}
-
 // r = fix * (b - A d) on level 0; optionally dsave = d and part[block] = sum |r|^2.
 // With slots set, b is first assembled as b0 + the row's RHS slots and stored
 // to bgather (the right-hand side of the PD iteration, reused afterwards).

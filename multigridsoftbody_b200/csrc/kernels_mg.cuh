@@ -55,6 +55,20 @@ struct CoarseArgs {
 
 __device__ __forceinline__ float4 f4z() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 
+// Block sum: warp xor-shuffles, then thread 0 adds the warp sums in order.
+// Every thread of the block calls it; the result is valid in thread 0.
+__device__ __forceinline__ float block_sum_f(float v, float* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    float t = 0.f;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    return t;
+}
+
 // Load of a vector that may have been written earlier in the same kernel by
 // another CTA of the cluster: a plain (coherent) load, never the read-only path.
 template <bool kReadOnly>

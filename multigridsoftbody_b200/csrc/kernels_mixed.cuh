@@ -96,37 +96,40 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
     d32[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-// b = b0 + sum of the vertex's slots, accumulated in FP64.
-__global__ void __launch_bounds__(256) k_mx_rhs(int n, const double4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
-                                                const float4* __restrict__ slots, double4* __restrict__ b) {
-    pdl_enter();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double4 acc = b0[i];
-    const int e1 = __ldg(slot_ptr + i + 1);
-    for (int e = __ldg(slot_ptr + i); e < e1; ++e) {
-        const float4 c = __ldg(slots + e);
-        acc.x += c.x;
-        acc.y += c.y;
-        acc.z += c.z;
-    }
-    b[i] = acc;
-}
-
 // Outer FP64 residual r = b - A d with A = diag + c + off-diagonal (FP64
 // values; c = this frame's contact stiffness), stored as FP32 for the correction V-cycle, fused with its first Jacobi
 // sweep from a zero guess: e = dinv r.  4 lanes per row.
+// With b0 set, b is first assembled as b0 + the row's slots (FP64, slot
+// order; the first pass of a PD iteration) and stored.  With ls_r set (the
+// learned V-cycle, which starts from zero), also ls_r = fix * r and
+// part[block] = sum |ls_r|^2: the starting residual of that cycle.
 __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
                                                      const double* __restrict__ val, const double* __restrict__ diag64,
-                                                     const float* __restrict__ c, const double4* __restrict__ d, const double4* __restrict__ b,
+                                                     const float* __restrict__ c, const double4* __restrict__ d, double4* __restrict__ b,
                                                      const float* __restrict__ dinv, float4* __restrict__ r32,
-                                                     float4* __restrict__ e, int first_sweep) {
+                                                     float4* __restrict__ e, int first_sweep,
+                                                     const double4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
+                                                     const float4* __restrict__ slots, const float* __restrict__ fixf,
+                                                     float4* __restrict__ ls_r, float* __restrict__ part) {
     pdl_enter();
+    __shared__ float red[8];
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
+    double4 bi = d4z();
+    if (b0 && valid && lane < S) {
+        bi = b0[row];
+        const int e1 = __ldg(slot_ptr + row + 1);
+        for (int q = __ldg(slot_ptr + row); q < e1; ++q) {
+            const float4 t = __ldg(slots + q);
+            bi.x += t.x;
+            bi.y += t.y;
+            bi.z += t.z;
+        }
+        b[row] = bi;
+    }
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (valid) {
         const int slice = row / S;
@@ -146,13 +149,26 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
         az += __shfl_xor_sync(0xffffffffu, az, o);
     }
-    if (!valid || lane >= S) return;
-    const double4 x = d[row], bi = b[row];
-    const double D = __ldg(diag64 + row) + (double)__ldg(c + row);
-    const float rx = (float)(bi.x - fma(D, x.x, ax)), ry = (float)(bi.y - fma(D, x.y, ay)), rz = (float)(bi.z - fma(D, x.z, az));
-    r32[row] = make_float4(rx, ry, rz, 0.f);
-    const float w = first_sweep ? __ldg(dinv + row) : 0.f;
-    e[row] = make_float4(w * rx, w * ry, w * rz, 0.f);
+    float rr = 0.f;
+    if (valid && lane < S) {
+        const double4 x = d[row];
+        if (!b0) bi = b[row];
+        const double D = __ldg(diag64 + row) + (double)__ldg(c + row);
+        const float rx = (float)(bi.x - fma(D, x.x, ax)), ry = (float)(bi.y - fma(D, x.y, ay)), rz = (float)(bi.z - fma(D, x.z, az));
+        r32[row] = make_float4(rx, ry, rz, 0.f);
+        const float w = first_sweep ? __ldg(dinv + row) : 0.f;
+        e[row] = make_float4(w * rx, w * ry, w * rz, 0.f);
+        if (ls_r) {
+            const float fx = __ldg(fixf + row);
+            const float4 q = make_float4(fx * rx, fx * ry, fx * rz, 0.f);
+            ls_r[row] = q;
+            rr = q.x * q.x + q.y * q.y + q.z * q.z;
+        }
+    }
+    if (ls_r) {   // uniform over the block
+        const float t = block_sum_f(rr, red);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
 }
 
 // d += e (FP64), FP32 mirror for the local step.

@@ -268,8 +268,8 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split);
 constexpr int kClusterLevelRows = 1024;
 
 void apply_tuning(mgsb_solver* h) {
-    // Default: the distributed-shared-memory kernel with <= 256 rows of its
-    // first level per CTA; levels above kClusterLevelRows rows run grid-wide.
+    // Default: the distributed-shared-memory kernel for the levels up to
+    // kClusterLevelRows rows; larger coarse levels run grid-wide.
     const int L = h->p.levels;
     if ((int)h->maxv.size() < L) return;   // before set-up
     h->fuse_l0 = h->tune_fuse >= 0 ? h->tune_fuse : 0;
@@ -287,7 +287,10 @@ void apply_tuning(mgsb_solver* h) {
     } else if (h->fuse_l0) {
         h->cluster = std::min(16, std::max(1, (h->maxv[0] + 2559) / 2560));
     } else {
-        h->cluster = std::min(16, std::max(1, (h->maxv[h->split] + 255) / 256));
+        // ~64 rows of the first owned level per CTA (one body: latency bound, so
+        // more CTAs shorten every phase); at most 2 CTAs per body in a batch
+        const int cap = h->bodies.size() > 1 ? 2 : 16;
+        h->cluster = std::min(cap, std::max(1, (h->maxv[h->split] + 63) / 64));
         while (h->cluster < 16 && coarse_smem_bytes(h, h->cluster, h->split) > (size_t)h->max_smem_optin) ++h->cluster;
     }
 }
@@ -717,7 +720,7 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
 // plain V-cycle runs (its kernels are launched gated and return at once when
 // the learned cycle passed).  dtmp: ping-pong buffer of the plain sweeps.
 void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float4* b, bool from_zero, CoarseArgs ca,
-                            bool gather_b = false) {
+                            bool gather_b = false, bool start_residual_ready = false) {
     const mgsb_params& p = h->p;
     const int n0 = h->N0;
     std::vector<LevelDev>& lv = h->lev;
@@ -727,10 +730,12 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     const int mgrid = std::min(h->ls_ntiles, 2 * h->sm_count);
     const size_t msmem = mlp_tc_smem_bytes();
     float4* bw = const_cast<float4*>(b);
-    // pre-smoothing (with gather_b the right-hand side b = b0 + slots is assembled here first)
-    LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-           h->ls_r, from_zero ? nullptr : h->ls_save, h->ls_part0, gather_b ? h->b0 : nullptr,
-           gather_b ? h->slot_ptr : nullptr, gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
+    // pre-smoothing (with gather_b the right-hand side b = b0 + slots is assembled here first;
+    // start_residual_ready: the previous kernel left ls_r and its block sums, d = 0)
+    if (!start_residual_ready)
+        LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
+               h->ls_r, from_zero ? nullptr : h->ls_save, h->ls_part0, gather_b ? h->b0 : nullptr,
+               gather_b ? h->slot_ptr : nullptr, gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
     // coarse correction
@@ -948,14 +953,18 @@ void enqueue_mixed_frame(mgsb_solver* h) {
     const int g0 = grid_rows(n0, lv[0].S);
     for (int it = 0; it < p.iterations; ++it) {
         LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, h->d32, h->slot_of, h->slots);
-        LAUNCH(h, k_mx_rhs, grid_for(n0), kBlock, 0, n0, h->b0_64, h->slot_ptr, h->slots, h->b64);
         for (int pass = 0; pass < p.refinement_passes; ++pass) {
             float4* ea = h->d;
             float4* eb = h->d2;
+            // the first pass also assembles b = b0 + slots; with the learned smoother it
+            // also leaves the learned cycle's starting residual (the cycle starts from e = 0)
+            const bool gather = pass == 0, learned = h->ls_net != nullptr;
             LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
-                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !h->ls_net) ? 1 : 0);
-            if (h->ls_net) {
-                enqueue_learned_vcycle(h, ea, eb, h->r32, true, ca);
+                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !learned) ? 1 : 0,
+                   gather ? h->b0_64 : nullptr, gather ? h->slot_ptr : nullptr, gather ? h->slots : nullptr, h->fixf,
+                   learned ? h->ls_r : nullptr, learned ? h->ls_part0 : nullptr);
+            if (learned) {
+                enqueue_learned_vcycle(h, ea, eb, h->r32, true, ca, false, true);
                 LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
                 continue;
             }
