@@ -582,6 +582,8 @@ def run_ours(args):
             solver.set_material(*mats[b], body=b)
     if net is not None:
         solver.set_learned_smoother(net, 0.5)
+    if args.broad_phase:
+        solver.set_broad_phase(True)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
 
     def barrier():
@@ -718,7 +720,8 @@ def run_ours(args):
                            + ("mixed precision multigrid" if params[0].precision == 1 else "plain FP32 multigrid"),
                            "parallelism": f"replicas x{world}",
                            "l2": "flushed (256 MB write) before every timed frame, outside the timed span",
-                           "autotuned_coarse_kernel": tuned},
+                           "autotuned_coarse_kernel": tuned,
+                           "contact_broad_phase": "uniform grid" if args.broad_phase else "all surface vertices"},
                 "clocks": clk.summary(),
                 "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches * args.steps,
@@ -744,6 +747,7 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--broad-phase", action="store_true", help="uniform-grid broad phase for the tool contact")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

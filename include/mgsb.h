@@ -246,6 +246,15 @@ mgsb_status mgsb_get_coarse_split(mgsb_solver* h, int32_t* split);
  * the launch gap; 0 = plain stream order.  Same results either way.  No
  * reference counterpart. */
 mgsb_status mgsb_set_launch_overlap(mgsb_solver* h, int32_t on);
+/* Tool-contact broad phase of the multigrid kinds (default 0 = every
+ * surface vertex against its body's capsule).  1: a uniform grid per body
+ * over the rest bounding box of its surface, rebuilt every frame from the
+ * predicted positions by a counting sort; each capsule tests only the
+ * vertices in the cells its swept box covers.  The contact set, stiffness
+ * and targets are the same either way; toggling clears the contact state
+ * until the next frame.  Replaces the all-vertex loop of DCDByPoint
+ * (PDSolver.cpp:228-233, PDSolver.cu:277-331). */
+mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on);
 
 /* Host-only (no GPU): build the multigrid hierarchy of one mesh exactly as
  * mgsb_create would and return level `level`: vertex count, off-diagonal

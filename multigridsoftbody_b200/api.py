@@ -409,6 +409,10 @@ class Solver:
         """Levels 1..split-1 grid-wide, the rest in the cluster kernel (0 = by size)."""
         _check(self._lib.mgsb_set_coarse_split(self.h, split), self.h)
 
+    def set_broad_phase(self, on: bool = True) -> None:
+        """Uniform-grid broad phase for the capsule contact (same contacts as the all-vertex test)."""
+        _check(self._lib.mgsb_set_broad_phase(self.h, 1 if on else 0), self.h)
+
     def set_launch_overlap(self, on: bool = True) -> None:
         """Programmatic dependent launch between the frame's kernels (default on)."""
         _check(self._lib.mgsb_set_launch_overlap(self.h, 1 if on else 0), self.h)

@@ -740,6 +740,305 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
 }
 
 // ---------------------------------------------------------------------------
+// Coarse part of the V-cycle, levels F = A.first .. L-1 of one body in ONE
+// CTA: every vector of those levels in shared memory, phases separated by
+// block barriers instead of cluster barriers, no remote loads.  Same lane
+// layout (8 lanes per row), per-row arithmetic and summation order as the
+// cluster kernel, so the two give the same bits.  Each warp carries
+// kCtaRowGroups row groups (4 rows each) at once, so the load chains of
+// several rows overlap.  Input: the level F-1 residual (global); output:
+// the level-F correction (global, lv[F].e).
+// ---------------------------------------------------------------------------
+constexpr int kCtaRowGroups = 4;
+
+struct CtaLevel {
+    int off, n, base;   // first global row, rows, float4 offset of [r | e | e2 | res] (n each)
+};
+
+// Off-diagonal products of P row groups of a coarse sliced-ELL level with x
+// in shared memory (body-local index col - off).  Every lane calls it.
+template <int P>
+__device__ __forceinline__ void cta_offdiag(const int (&row)[P], const bool (&valid)[P], int lane,
+                                            const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                            const float* __restrict__ val, const float4* xs, int off,
+                                            float4 (&out)[P]) {
+    constexpr int S = 32 / kLanesC;
+    int e[P], end[P];
+    float ax[P], ay[P], az[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        ax[p] = ay[p] = az[p] = 0.f;
+        e[p] = end[p] = 0;
+        if (valid[p]) {
+            const int slice = row[p] / S;
+            e[p] = __ldg(sp + slice) + (lane / S) * S + (row[p] - slice * S);
+            end[p] = __ldg(sp + slice + 1);
+        }
+    }
+    for (bool more = true; more;) {
+        more = false;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            if (e[p] < end[p]) {
+                const float a = __ldg(val + e[p]);
+                const float4 xv = xs[__ldg(col + e[p]) - off];
+                ax[p] = fmaf(a, xv.x, ax[p]);
+                ay[p] = fmaf(a, xv.y, ay[p]);
+                az[p] = fmaf(a, xv.z, az[p]);
+                e[p] += 32;
+                more = true;
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+        for (int o = S; o < 32; o <<= 1) {
+            ax[p] += __shfl_xor_sync(0xffffffffu, ax[p], o);
+            ay[p] += __shfl_xor_sync(0xffffffffu, ay[p], o);
+            az[p] += __shfl_xor_sync(0xffffffffu, az[p], o);
+        }
+        out[p] = make_float4(ax[p], ay[p], az[p], 0.f);
+    }
+}
+
+// Restriction r = sum_k w_k src[child_k - src_off] of P row groups (CSR over
+// the finer level's rows, kLanesC lanes per row).  src is the finer level's
+// residual in global memory (src_off 0) or in shared memory.
+template <int P>
+__device__ __forceinline__ void cta_restrict(const int (&row)[P], const bool (&valid)[P], int lane,
+                                             const int32_t* __restrict__ rptr, const int32_t* __restrict__ rcol,
+                                             const float* __restrict__ rw, const float4* src, int src_off,
+                                             float4 (&out)[P]) {
+    constexpr int S = 32 / kLanesC;
+    int k[P], end[P];
+    float ax[P], ay[P], az[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        ax[p] = ay[p] = az[p] = 0.f;
+        k[p] = end[p] = 0;
+        if (valid[p]) {
+            k[p] = __ldg(rptr + row[p]) + lane / S;
+            end[p] = __ldg(rptr + row[p] + 1);
+        }
+    }
+    for (bool more = true; more;) {
+        more = false;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            if (k[p] < end[p]) {
+                const float w = __ldg(rw + k[p]);
+                const float4 t = src[__ldg(rcol + k[p]) - src_off];
+                ax[p] = fmaf(w, t.x, ax[p]);
+                ay[p] = fmaf(w, t.y, ay[p]);
+                az[p] = fmaf(w, t.z, az[p]);
+                k[p] += kLanesC;
+                more = true;
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+        for (int o = S; o < 32; o <<= 1) {
+            ax[p] += __shfl_xor_sync(0xffffffffu, ax[p], o);
+            ay[p] += __shfl_xor_sync(0xffffffffu, ay[p], o);
+            az[p] += __shfl_xor_sync(0xffffffffu, az[p], o);
+        }
+        out[p] = make_float4(ax[p], ay[p], az[p], 0.f);
+    }
+}
+
+// Shared memory (float4 units) of the one-CTA kernel: 4 vectors of every level it owns.
+__host__ __device__ inline int coarse_cta_smem_float4(const int* nl, int L, int first) {
+    int tot = 0;
+    for (int l = first; l < L; ++l) tot += 4 * nl[l];
+    return tot;
+}
+
+__global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) {
+    pdl_enter();
+    if (A.gate && __ldg(A.gate) == 0) return;
+    extern __shared__ float4 smv[];
+    constexpr int P = kCtaRowGroups;
+    constexpr int Sc = 32 / kLanesC;
+    constexpr int R = 0, E = 1, E2 = 2, RES = 3;
+    const int body = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarp = blockDim.x >> 5;
+    const int L = A.L, F = A.first;
+    CtaLevel q[kMaxLevels];
+    int base = 0;
+    for (int l = F; l < L; ++l) {
+        const int2 rg = A.range[body * L + l];
+        q[l].off = rg.x;
+        q[l].n = rg.y;
+        q[l].base = base;
+        base += 4 * rg.y;
+    }
+    auto vec = [&](int l, int v) -> float4* { return smv + q[l].base + v * q[l].n; };
+    int ec[kMaxLevels];   // which of E / E2 holds the level's current correction
+
+    // One pass of a Jacobi sweep (dst = x + w (r - D x - off)) or of the
+    // residual (res = r - D x - off) over level l, P row groups per warp.
+    auto sweep_or_residual = [&](int l, int src, int dst, bool residual) {
+        const LevelView& C = A.lv[l];
+        const int n = q[l].n, off = q[l].off;
+        const int ngroups = (n + Sc - 1) / Sc;
+        const float4* xs = vec(l, src);
+        const float4* r = vec(l, R);
+        float4* out = vec(l, dst);
+        for (int g0 = warp; g0 < ngroups; g0 += nwarp * P) {
+            int li[P], row[P];
+            bool valid[P];
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                li[p] = (g0 + p * nwarp) * Sc + (lane % Sc);
+                valid[p] = li[p] < n;
+                row[p] = off + li[p];
+            }
+            float4 o[P];
+            cta_offdiag<P>(row, valid, lane, C.slice_ptr, C.col, C.val, xs, off, o);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                if (!valid[p] || lane >= Sc) continue;
+                const float4 x = xs[li[p]], ri = r[li[p]];
+                const float D = __ldg(C.dfull + row[p]);
+                if (residual) {
+                    out[li[p]] = make_float4(ri.x - fmaf(D, x.x, o[p].x), ri.y - fmaf(D, x.y, o[p].y),
+                                             ri.z - fmaf(D, x.z, o[p].z), 0.f);
+                } else {
+                    const float w = __ldg(C.dinv + row[p]);
+                    out[li[p]] = make_float4(fmaf(w, ri.x - fmaf(D, x.x, o[p].x), x.x),
+                                             fmaf(w, ri.y - fmaf(D, x.y, o[p].y), x.y),
+                                             fmaf(w, ri.z - fmaf(D, x.z, o[p].z), x.z), 0.f);
+                }
+            }
+        }
+    };
+
+    // ---- descend
+    for (int l = F; l < L; ++l) {
+        const LevelView& C = A.lv[l];
+        const int n = q[l].n, off = q[l].off;
+        const int ngroups = (n + Sc - 1) / Sc;
+        const float4* src = (l == F) ? A.lv[l - 1].res : vec(l - 1, RES);
+        const int src_off = (l == F) ? 0 : q[l - 1].off;
+        float4* r = vec(l, R);
+        float4* e = vec(l, E);
+        for (int g0 = warp; g0 < ngroups; g0 += nwarp * P) {
+            int li[P], row[P];
+            bool valid[P];
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                li[p] = (g0 + p * nwarp) * Sc + (lane % Sc);
+                valid[p] = li[p] < n;
+                row[p] = off + li[p];
+            }
+            float4 t[P];
+            cta_restrict<P>(row, valid, lane, C.rptr, C.rcol, C.rw, src, src_off, t);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                if (!valid[p] || lane >= Sc) continue;
+                r[li[p]] = t[p];
+                const float di = (l < L - 1 && A.pre > 0) ? __ldg(C.dinv + row[p]) : 0.f;
+                e[li[p]] = make_float4(di * t[p].x, di * t[p].y, di * t[p].z, 0.f);
+            }
+        }
+        ec[l] = E;
+        __syncthreads();
+        if (l == L - 1) break;
+        for (int k = 1; k < A.pre; ++k) {
+            const int dst = (ec[l] == E) ? E2 : E;
+            sweep_or_residual(l, ec[l], dst, false);
+            ec[l] = dst;
+            __syncthreads();
+        }
+        sweep_or_residual(l, ec[l], RES, true);
+        __syncthreads();
+    }
+    // ---- coarsest: e = A^-1 r (dense, warp per row)
+    {
+        const int l = L - 1;
+        const int n = q[l].n;
+        const float4* rf = vec(l, R);
+        float4* e = vec(l, E);
+        if (A.Ainv64) {
+            const double* Ai = A.Ainv64 + __ldg(A.dense_off + body);
+            for (int i = warp; i < n; i += nwarp) {
+                double ax = 0.0, ay = 0.0, az = 0.0;
+                for (int k = lane; k < n; k += 32) {
+                    const double a = __ldg(Ai + (size_t)i * n + k);
+                    const float4 r = rf[k];
+                    ax = fma(a, (double)r.x, ax);
+                    ay = fma(a, (double)r.y, ay);
+                    az = fma(a, (double)r.z, az);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                    az += __shfl_xor_sync(0xffffffffu, az, o);
+                }
+                if (lane == 0) e[i] = make_float4((float)ax, (float)ay, (float)az, 0.f);
+            }
+        } else {
+            const float* Ai = A.Ainv + __ldg(A.dense_off + body);
+            for (int i = warp; i < n; i += nwarp) {
+                float ax = 0.f, ay = 0.f, az = 0.f;
+                for (int k = lane; k < n; k += 32) {
+                    const float a = __ldg(Ai + (size_t)i * n + k);
+                    const float4 r = rf[k];
+                    ax = fmaf(a, r.x, ax);
+                    ay = fmaf(a, r.y, ay);
+                    az = fmaf(a, r.z, az);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                    az += __shfl_xor_sync(0xffffffffu, az, o);
+                }
+                if (lane == 0) e[i] = make_float4(ax, ay, az, 0.f);
+            }
+        }
+        ec[l] = E;
+        __syncthreads();
+    }
+    // ---- ascend
+    for (int l = L - 2; l >= F; --l) {
+        const LevelView& Cc = A.lv[l + 1];
+        const int n = q[l].n, off = q[l].off, coff = q[l + 1].off;
+        const float4* ecs = vec(l + 1, ec[l + 1]);
+        float4* v = vec(l, ec[l]);
+        for (int li = threadIdx.x; li < n; li += blockDim.x) {
+            const int row = off + li;
+            const int4 id = __ldg(Cc.pid + row);
+            const float4 w = __ldg(Cc.pw + row);
+            const float4 e0 = ecs[id.x - coff], e1 = ecs[id.y - coff], e2 = ecs[id.z - coff], e3 = ecs[id.w - coff];
+            float4 t = v[li];
+            t.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+            t.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+            t.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+            v[li] = t;
+        }
+        __syncthreads();
+        for (int k = 0; k < A.post; ++k) {
+            const int dst = (ec[l] == E) ? E2 : E;
+            sweep_or_residual(l, ec[l], dst, false);
+            ec[l] = dst;
+            __syncthreads();
+        }
+    }
+    // ---- level-F correction to global memory
+    {
+        const float4* ef = vec(F, ec[F]);
+        for (int li = threadIdx.x; li < q[F].n; li += blockDim.x) A.lv[F].e[q[F].off + li] = ef[li];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Coarsest level: explicit inverse of A = A0 + diag(c) per body, refreshed
 // only when the lumped contact stiffness c changed.  A0^-1 = B0 is computed
 // once at set-up; with k coarsest vertices in contact (K = {i : c_i != 0}) the

@@ -69,10 +69,12 @@ __device__ __forceinline__ void capsule_test64(const double4 sp, const BodyDev& 
 }
 
 // Contact on the FP64 prediction; b0 = c (p - s) in FP64; D, dinv (FP32, for
-// the correction V-cycle); d = 0 in both precisions.
+// the correction V-cycle); d = 0 in both precisions.  With cand set (the
+// broad phase ran), only the surface vertices it flagged are tested.
 __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const float* __restrict__ fixf,
                                    const int32_t* __restrict__ body_of, const BodyDev* __restrict__ bodies,
-                                   const uint8_t* __restrict__ is_surf, float kc, const float* __restrict__ diag0,
+                                   const uint8_t* __restrict__ is_surf, const uint8_t* __restrict__ cand, float kc,
+                                   const float* __restrict__ diag0,
                                    float omega, int32_t* __restrict__ cflag, float* __restrict__ c0,
                                    double4* __restrict__ b0, float* __restrict__ dfull, float* __restrict__ dinv,
                                    double4* __restrict__ d64, float4* __restrict__ d32, float4* __restrict__ target) {
@@ -82,7 +84,7 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
     int flag = 0;
     double4 tg = d4z();
     const double4 sv = s[i];
-    if (__ldg(is_surf + i)) capsule_test64(sv, bodies[__ldg(body_of + i)], flag, tg);
+    if (__ldg(is_surf + i) && (!cand || cand[i])) capsule_test64(sv, bodies[__ldg(body_of + i)], flag, tg);
     const bool free_v = __ldg(fixf + i) != 0.f;
     const float c = (flag && free_v) ? kc : 0.f;
     cflag[i] = flag;

@@ -18,6 +18,7 @@
 #include "kernels_twolevel.cuh"
 #include "kernels_mg.cuh"
 #include "kernels_mixed.cuh"
+#include "kernels_contact.cuh"
 #include "mesh.hpp"
 #include "mlp.hpp"
 #include "plan.hpp"
@@ -85,6 +86,7 @@ struct mgsb_solver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     bool capture_error = false;   // a graph-building step inside a capture failed
+    mgsb_status enqueue_status = MGSB_OK;   // first failed launch of the frame being enqueued (message in err)
     int launches = 0;
     // per-launch CUDA events of a profiled (eager) frame
     bool profiling = false;
@@ -132,6 +134,13 @@ struct mgsb_solver {
     float* c0 = nullptr;
     int32_t* surf = nullptr;
     int nsurf = 0;
+    // uniform-grid broad phase of the tool contact (multigrid kinds)
+    bool broad_phase = false;
+    BpGrid* bp_grids = nullptr;
+    int bp_ncells = 0;
+    int32_t *bp_counts = nullptr, *bp_start = nullptr, *bp_sorted = nullptr, *bp_list = nullptr, *bp_nlist = nullptr;
+    int2* bp_cellrank = nullptr;
+    uint8_t* bp_cand = nullptr;
     float4* d_final = nullptr;   // displacement buffer that holds the last frame's d (FP32 multigrid)
     // surface normals: triangles (global vertex ids), surface vertices, and the
     // vertex->triangle CSR (triangle ids local to the body); per body the
@@ -307,6 +316,55 @@ void invalidate_graph(mgsb_solver* h) {
     h->graph_valid = false;
 }
 
+// Uniform grids of the broad phase: per body, cells of about twice the
+// surface vertex spacing (sqrt(bbox area / surface vertices)), at most 128
+// per axis, over the rest bounding box of its surface plus one cell.
+mgsb_status setup_broad_phase(mgsb_solver* h, std::vector<DevMem>& pool) {
+    std::vector<BpGrid> grids;
+    int cells = 0, sorted = 0;
+    for (const BodyHost& B : h->bodies) {
+        double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        for (size_t k = 0; k < B.surface.size(); ++k)
+            for (int a = 0; a < 3; ++a) {
+                const double x = B.rest[3 * (size_t)B.surface[k] + a];
+                lo[a] = k ? std::min(lo[a], x) : x;
+                hi[a] = k ? std::max(hi[a], x) : x;
+            }
+        const double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+        const double area = 2.0 * (ext[0] * ext[1] + ext[1] * ext[2] + ext[0] * ext[2]);
+        double hc = 2.0 * std::sqrt(area / (double)std::max<size_t>(B.surface.size(), 1));
+        for (int a = 0; a < 3; ++a) hc = std::max(hc, ext[a] / 128.0);
+        if (!(hc > 0.0)) hc = 1.0;
+        BpGrid g;
+        g.ox = (float)(lo[0] - hc);
+        g.oy = (float)(lo[1] - hc);
+        g.oz = (float)(lo[2] - hc);
+        g.inv_h = (float)(1.0 / hc);
+        g.nx = (int)std::floor(ext[0] / hc) + 3;
+        g.ny = (int)std::floor(ext[1] / hc) + 3;
+        g.nz = (int)std::floor(ext[2] / hc) + 3;
+        g.cell_off = cells;
+        g.start_off = cells + (int)grids.size();
+        g.sorted_off = sorted;
+        cells += g.nx * g.ny * g.nz;
+        sorted += (int)B.surface.size();
+        grids.push_back(g);
+    }
+    if (sorted != h->nsurf) return set_err(h, MGSB_NOT_SUPPORTED, "surface lists disagree (%d vs %d)", sorted, h->nsurf);
+    h->bp_ncells = cells;
+    TRY(dupload(h, pool, &h->bp_grids, grids));
+    TRY(dalloc(h, pool, &h->bp_counts, (size_t)cells));
+    TRY(dalloc(h, pool, &h->bp_start, (size_t)cells + grids.size()));
+    TRY(dalloc(h, pool, &h->bp_sorted, (size_t)h->nsurf));
+    TRY(dalloc(h, pool, &h->bp_list, (size_t)h->nsurf));
+    TRY(dalloc(h, pool, &h->bp_nlist, 1));
+    TRY(dalloc(h, pool, &h->bp_cellrank, (size_t)h->nsurf));
+    TRY(dalloc(h, pool, &h->bp_cand, (size_t)h->N0));
+    CUDA_TRY(h, cudaMemset(h->bp_nlist, 0, sizeof(int32_t)));
+    CUDA_TRY(h, cudaMemset(h->bp_cand, 0, (size_t)h->N0));
+    return MGSB_OK;
+}
+
 // Surface triangles of every body (extract_surface order), the surface
 // vertices in ascending order and, per surface vertex, its triangles in
 // ascending order; plus the two scratch arrays the normals pass writes.
@@ -469,6 +527,8 @@ mgsb_status rebuild(mgsb_solver* h) {
         CUDA_TRY(h, cudaDeviceGetAttribute(&h->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
         CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle_dsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          h->max_smem_optin));
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         h->max_smem_optin));
         TRY(dupload(h, pool, &h->dense_off_d, P.dense_off));
         // cluster size of the coarse V-cycle kernel: sized by the rows one body
         // brings to it (level 0 when fused, else level 1)
@@ -506,6 +566,7 @@ mgsb_status rebuild(mgsb_solver* h) {
         }
         h->nsurf = (int)P.surf.size();
         TRY(dupload(h, pool, &h->surf, P.surf));
+        TRY(setup_broad_phase(h, pool));
     }
     for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
         BodyDev& BD = h->bodies_host[bi];
@@ -607,13 +668,16 @@ void enqueue_ref_frame(mgsb_solver* h) {
 // Dynamic shared memory of the distributed-shared-memory coarse kernel: the
 // largest body's rows per CTA on every level it owns (4 vectors) + the whole
 // coarsest right-hand side.
+// With a cluster of one CTA the one-CTA kernel runs instead: 4 vectors of
+// every level it owns.
 size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split) {
     const int L = h->p.levels;
     int best = 0;
     for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
         int nl[kMaxLevels] = {0};
         for (int l = 0; l < L; ++l) nl[l] = h->range_host[bi * L + l].y;
-        best = std::max(best, coarse_smem_float4(nl, L, split, cs, nl[L - 1]));
+        best = std::max(best, cs == 1 ? coarse_cta_smem_float4(nl, L, split)
+                                      : coarse_smem_float4(nl, L, split, cs, nl[L - 1]));
     }
     return (size_t)best * sizeof(float4);
 }
@@ -634,6 +698,15 @@ bool coarse_shape_feasible(mgsb_solver* h, int cs, int block, int fused, int spl
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
+    if (!fused && cs == 1) {   // the one-CTA kernel: an ordinary launch
+        int nblk = 0;
+        const cudaError_t e1 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, k_coarse_vcycle_cta, block, smem);
+        if (e1 != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return nblk > 0;
+    }
     const cudaError_t e = fused ? cudaOccupancyMaxActiveClusters(&nclusters, k_coarse_vcycle, &cfg)
                                 : cudaOccupancyMaxActiveClusters(&nclusters, k_coarse_vcycle_dsm, &cfg);
     if (e != cudaSuccess) {
@@ -691,6 +764,12 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
     cfg.gridDim = dim3((unsigned)(h->bodies.size() * h->cluster));
     cfg.blockDim = dim3((unsigned)h->coarse_block);
     cfg.dynamicSmemBytes = h->fuse_l0 ? 0 : coarse_smem_bytes(h, h->cluster, args.first);
+    if (cfg.dynamicSmemBytes > (size_t)h->max_smem_optin) {
+        h->enqueue_status = set_err(h, MGSB_NOT_SUPPORTED,
+                                    "coarse kernel shape (cluster %d, split %d) needs %zu B of shared memory per CTA (max %d)",
+                                    h->cluster, args.first, cfg.dynamicSmemBytes, h->max_smem_optin);
+        return h->enqueue_status;
+    }
     cfg.stream = h->stream;
     cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -701,14 +780,24 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
     attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = h->pdl ? 2 : 1;
+    const bool one_cta = !h->fuse_l0 && h->cluster == 1;
+    if (one_cta) {   // no cluster attribute: one CTA per body
+        cfg.attrs = attr + 1;
+        cfg.numAttrs = h->pdl ? 1 : 0;
+    }
     if (h->profiling) prof_mark(h, "k_coarse_vcycle");
     // fused: global-memory kernel that also owns the level-0 residual and prolongation;
-    // else the distributed-shared-memory kernel over levels >= 1
+    // one CTA: every owned level in one CTA's shared memory; else the
+    // distributed-shared-memory kernel over the cluster
     cudaError_t e = h->fuse_l0 ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle, args)
+                    : one_cta  ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle_cta, args)
                                : cudaLaunchKernelEx(&cfg, k_coarse_vcycle_dsm, args);
     if (h->profiling) prof_mark(h, nullptr);
     ++h->launches;
-    if (e != cudaSuccess) return set_err(h, MGSB_CUDA_ERROR, "coarse V-cycle launch failed: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        h->enqueue_status = set_err(h, MGSB_CUDA_ERROR, "coarse V-cycle launch failed: %s", cudaGetErrorString(e));
+        return h->enqueue_status;
+    }
     return MGSB_OK;
 }
 
@@ -814,6 +903,24 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     }
 }
 
+// Broad phase on the predicted positions spos: clear the previous
+// candidates, bin, scan, scatter, query.  narrow: the query also runs the
+// FP32 kind's narrow phase (contact flag, stiffness, target).
+void enqueue_broad_phase(mgsb_solver* h, const float4* spos, bool narrow) {
+    const int nb = (int)h->bodies.size();
+    const int gclear = std::max(1, std::min(grid_for(std::max(h->bp_ncells, h->nsurf)), 4 * h->sm_count));
+    LAUNCH(h, k_bp_clear, gclear, kBlock, 0, h->bp_ncells, h->bp_counts, h->bp_list, h->bp_nlist, h->bp_cand,
+           narrow ? h->cflag : nullptr, narrow ? h->c0 : nullptr, narrow ? h->target : nullptr);
+    LAUNCH(h, k_bp_bin, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bp_grids, spos, h->bp_counts,
+           h->bp_cellrank, h->bp_nlist);
+    LAUNCH(h, k_bp_scan, nb, kBpScanThreads, 0, h->bp_grids, h->bp_counts, h->bp_start);
+    LAUNCH(h, k_bp_scatter, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->bp_cellrank, h->bp_start,
+           h->bp_sorted);
+    LAUNCH(h, k_bp_query, nb, kBlock, 0, h->bp_grids, h->bodies_dev, h->bp_start, h->bp_sorted, spos, h->fixf,
+           h->p.contact_stiffness, h->bp_cand, h->bp_list, h->bp_nlist, narrow ? h->cflag : nullptr,
+           narrow ? h->c0 : nullptr, narrow ? h->target : nullptr);
+}
+
 void enqueue_mg_frame(mgsb_solver* h) {
     const mgsb_params& p = h->p;
     const int n0 = h->N0, T = h->T, L = p.levels;
@@ -821,7 +928,9 @@ void enqueue_mg_frame(mgsb_solver* h) {
     const float om = p.jacobi_omega;
     std::vector<LevelDev>& lv = h->lev;
     LAUNCH(h, k_mg_predict, grid_for(n0), kBlock, 0, n0, h->x, h->v, h->s, h->last, h->fixf, h->body_of, h->bodies_dev, p.dt);
-    if (h->nsurf > 0)
+    if (h->nsurf > 0 && h->broad_phase)
+        enqueue_broad_phase(h, h->s, true);
+    else if (h->nsurf > 0)
         LAUNCH(h, k_contact_all, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bodies_dev, h->s,
                h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target);
     float4* xa = h->d;    // displacement d = x - s (ping)
@@ -939,8 +1048,9 @@ void enqueue_mixed_frame(mgsb_solver* h) {
     std::vector<LevelDev>& lv = h->lev;
     LAUNCH(h, k_mx_predict, grid_for(n0), kBlock, 0, n0, h->x64, h->v64, h->s64, h->last64, h->s, h->x, h->fixf,
            h->body_of, h->bodies_dev, (double)p.dt);
+    if (h->nsurf > 0 && h->broad_phase) enqueue_broad_phase(h, h->s, false);
     LAUNCH(h, k_mx_contact_frame, grid_for(n0), kBlock, 0, n0, h->s64, h->fixf, h->body_of, h->bodies_dev, h->is_surf,
-           p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32,
+           h->broad_phase ? h->bp_cand : nullptr, p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32,
            h->target);
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
@@ -1026,8 +1136,14 @@ mgsb_status step_once(mgsb_solver* h) {
         if (!h->graph_valid) {
             CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
             h->capture_error = false;
+            h->enqueue_status = MGSB_OK;
             enqueue_frame(h);
             cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+            if (h->enqueue_status != MGSB_OK) {
+                if (e == cudaSuccess) cudaGraphDestroy(h->graph);
+                h->graph = nullptr;
+                return h->enqueue_status;
+            }
             if (e == cudaSuccess && h->capture_error) {
                 cudaGraphDestroy(h->graph);
                 h->graph = nullptr;
@@ -1039,7 +1155,9 @@ mgsb_status step_once(mgsb_solver* h) {
         }
         CUDA_TRY(h, cudaGraphLaunch(h->graph_exec, h->stream));
     } else {
+        h->enqueue_status = MGSB_OK;
         enqueue_frame(h);
+        if (h->enqueue_status != MGSB_OK) return h->enqueue_status;
         CUDA_TRY(h, cudaGetLastError());
     }
     CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
@@ -1660,6 +1778,23 @@ mgsb_status mgsb_set_coarse_split(mgsb_solver* h, int32_t split) {
     h->tune_split = split;
     apply_tuning(h);
     invalidate_graph(h);
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the broad phase applies to the multigrid kinds");
+    TRY(ensure_ready(h));
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    h->broad_phase = on != 0;
+    invalidate_graph(h);
+    // start from an empty contact state: the next frame recomputes it either way
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaMemset(h->cflag, 0, (size_t)h->N0 * sizeof(int32_t)));
+    CUDA_TRY(h, cudaMemset(h->c0, 0, (size_t)h->N0 * sizeof(float)));
+    CUDA_TRY(h, cudaMemset(h->target, 0, (size_t)h->N0 * sizeof(float4)));
+    CUDA_TRY(h, cudaMemset(h->bp_cand, 0, (size_t)h->N0));
+    CUDA_TRY(h, cudaMemset(h->bp_nlist, 0, sizeof(int32_t)));
     return MGSB_OK;
 }
 

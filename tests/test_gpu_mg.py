@@ -311,6 +311,12 @@ def test_coarse_split_default_by_size(lib):
     assert big.level_size(2)[0] == 2989 and big.coarse_split() == 3
     with pytest.raises(mg.MgsbError):
         big.set_coarse_split(5)
+    # one CTA cannot hold levels 1-4 (24,078 rows) in shared memory: a clear error, not a bad frame
+    big.set_kernel_shape(1, 1024, 0)
+    big.set_coarse_split(1)
+    with pytest.raises(mg.MgsbError) as err:
+        big.step()
+    assert err.value.status == 6
     small.close()
     big.close()
 
@@ -348,3 +354,26 @@ def test_launch_overlap_bitwise(lib, kind):
         s.close()
     for x_on, x_off in zip(out[True], out[False]):
         assert np.array_equal(x_on, x_off)
+
+
+@pytest.mark.parametrize("split", [1, 2, 3])
+def test_one_cta_kernel_equals_cluster_kernel(lib, split):
+    """A cluster of one CTA runs the one-CTA kernel (every owned level in
+    shared memory, block barriers); it keeps the cluster kernel's lanes and
+    summation order, so the frames are the same bit for bit."""
+    m, fixed = beam(8, 80, 8)
+    p = mg_params(levels=4, gravity=(0, 0, 0), use_graph=1)
+    path = capsule_path(10, start=(0.0, 0.0, 1.3))
+    out = {}
+    for cluster in (1, 4):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        s.set_kernel_shape(cluster, 512, 0)
+        s.set_coarse_split(split)
+        for a, b in path:
+            s.set_capsule(a, b, 0.3)
+            s.step()
+        assert s.level_info(0)["cluster"] == cluster
+        out[cluster] = s.positions()
+        s.close()
+    assert np.array_equal(out[1], out[4])
