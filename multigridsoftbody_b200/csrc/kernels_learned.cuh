@@ -165,14 +165,17 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
                                                              const float* __restrict__ fixf, const float4* __restrict__ r,
                                                              const uint8_t* __restrict__ img, float4* __restrict__ d,
                                                              int32_t* __restrict__ err) {
-    pdl_enter();
+    pdl_trigger();
     constexpr int S = 32 / kLanesL0;   // level-0 slice height
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     MlpSmem& Sm = *reinterpret_cast<MlpSmem*>(smem_raw);
     WaitState ws;
     uint32_t ph_load = 0, ph_mma = 0;
-    // the weight copy overlaps the first tile's feature gather
+    // Prologue before the wait for the previous kernel: TMEM, barriers and the
+    // weight copy (the weight image is not written by any kernel of a frame);
+    // the copy also overlaps the first tile's feature gather.
     const uint32_t tmem = mlp_cta_setup(Sm, img, ws, ph_load, err, false);
+    pdl_wait();
     bool weights_pending = true;
     __shared__ float part[5][kMlpTile];   // second half's 1-ring sums
     const int rt = threadIdx.x & (kMlpTile - 1), half = threadIdx.x >> 7;   // 2 threads per row
