@@ -146,8 +146,12 @@ class ClockSampler:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # start timing only once the sampler is running (its first line is out)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -573,8 +577,15 @@ def run_ours(args):
         p.device = local
         p.stream = stream.cuda_stream
     net, net_info = None, None
-    if args.workload in LEARNED:
+    if args.workload in LEARNED and args.load_weights:
+        from multigridsoftbody_b200.learned import MLP
+        net = MLP(device=local, seed=0)
+        net.params = np.load(args.load_weights)
+        net_info = {"weights": os.path.basename(args.load_weights), "trained": "earlier run (--save-weights)"}
+    elif args.workload in LEARNED:
         net, net_info = train_network(mg, args.workload, local, stream.cuda_stream)
+        if args.save_weights and rank == 0:
+            np.save(args.save_weights, net.params)
     solver = mg.Solver(meshes, params)
     for b, fx in enumerate(fixeds):
         solver.set_fixed(fx, body=b)
@@ -636,7 +647,7 @@ def run_ours(args):
         frame += 1
         # the plain FP32 multigrid (1 and 2 V-cycles per PD iteration), timed the same way
         plain_ms = {}
-        if net is not None:
+        if net is not None and not args.no_compare:
             for passes in (1, 2):
                 pp = type(params[0]).from_buffer_copy(params[0])
                 pp.precision = mg.PRECISION_FP32
@@ -665,7 +676,7 @@ def run_ours(args):
     from multigridsoftbody_b200.replicas import job_throughput, max_over_ranks
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist)
     comparison = None
-    if net is not None:
+    if net is not None and not args.no_compare:
         p1, p2 = max_over_ranks([plain_ms[1], plain_ms[2]], dist)
         comparison = {"plain_fp32_1pass": {"frames_per_s": job_throughput(args.steps, world, p1),
                                            "ms_per_step": p1 / args.steps},
@@ -748,6 +759,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--broad-phase", action="store_true", help="uniform-grid broad phase for the tool contact")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="learned workloads: skip the plain-solver timings and the accuracy runs (profiling)")
+    ap.add_argument("--save-weights", default="", help="learned workloads: save the trained network (.npy)")
+    ap.add_argument("--load-weights", default="", help="learned workloads: use these weights instead of training")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

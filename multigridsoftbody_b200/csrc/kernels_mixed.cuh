@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
     if (b0 && valid && lane < S) {
         bi = b0[row];
         const int e1 = __ldg(slot_ptr + row + 1);
+#pragma unroll 4
         for (int q = __ldg(slot_ptr + row); q < e1; ++q) {
             const float4 t = __ldg(slots + q);
             bi.x += t.x;
