@@ -9,6 +9,15 @@ oracle/ref_build.sh into oracle/_ref/libmgsb_ref.so; this script calls it:
 
 Inputs are generated here (seeded); no reference data file is copied.
 Outputs: ref_cpu.npz, ref_traj.npz, ref_mg2_traj.npz (small, committed).
+
+beam_smoother.npy in this folder is not from the reference: it is the
+headline's learned-smoother network (4,995 float32 parameters), trained on a
+B200 by the library's own trainer and written by
+
+    python bench.py --steps 50 --warmup 5 --no-cpu --save-weights tests/golden/beam_smoother.npy
+
+The profiling commands in profiles/ load it (--load-weights) so that a
+profiled frame needs no training run.
 """
 from __future__ import annotations
 
