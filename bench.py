@@ -83,7 +83,7 @@ def make_workload(name, mg):
         return [m], [p], [fixed], tool, desc, mats
     if name == "blob":
         from multigridsoftbody_b200.learned import blob_scene, blob_tool_path
-        m, fixed, p = blob_scene(precision=mg.PRECISION_MIXED, refinement_passes=2)
+        m, fixed, p = blob_scene(precision=mg.PRECISION_MIXED, refinement_passes=1)
         path = blob_tool_path(4096, seed=1)
 
         def tool(f):
@@ -92,7 +92,7 @@ def make_workload(name, mg):
 
         desc = (f"organ-like blob 64x32x48 voxels at 0.25 m ({m.num_verts} verts, {m.num_tets} tets), fixed x<-5, "
                 f"E 3e4, nu 0.45, gravity -z, 5 MG levels, 10 PD iterations, capsule r=0.3 len 8 from (0,0,3.3) "
-                f"moving -z 0.02/frame + jitter (seed 1); learned smoother + mixed precision (2 refinement passes)")
+                f"moving -z 0.02/frame + jitter (seed 1); learned smoother + mixed precision (1 refinement pass)")
         return [m], [p], [fixed], tool, desc, None
     if name == "batch":
         rng = np.random.default_rng(11)
