@@ -199,6 +199,51 @@ __device__ __forceinline__ void svd_rotation(const float F[9], float R[9]) {
         for (int j = 0; j < 3; ++j) R[i * 3 + j] = u1[i] * V[j * 3 + 0] + u2[i] * V[j * 3 + 1] + u3[i] * V[j * 3 + 2];
 }
 
+// Orthogonal polar factor of F for det F > 0 by the scaled Newton iteration
+// of Higham (1986), "Computing the polar decomposition - with applications":
+// X <- (g X + X^-T / g) / 2 from X = F, with g = (|X^-1|_F / |X|_F)^(1/2) and
+// X^-T = cof(X) / det X.  For det F > 0 the polar factor is the rotation
+// U V^T of the SVD, the same matrix svd_rotation returns.  Stops when
+// |X_new - X|_F < 1e-6 (the error of X_new is then ~1e-12 by quadratic
+// convergence; 4-6 steps up to condition number 1e4); returns false if det X
+// <= 0 or no convergence in 8 steps (the caller falls back to the SVD).
+__device__ __forceinline__ bool polar_newton(const float F[9], float R[9]) {
+    float X[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) X[q] = F[q];
+#pragma unroll 1
+    for (int it = 0; it < 8; ++it) {
+        const float C[9] = {X[4] * X[8] - X[5] * X[7], X[5] * X[6] - X[3] * X[8], X[3] * X[7] - X[4] * X[6],
+                            X[2] * X[7] - X[1] * X[8], X[0] * X[8] - X[2] * X[6], X[1] * X[6] - X[0] * X[7],
+                            X[1] * X[5] - X[2] * X[4], X[2] * X[3] - X[0] * X[5], X[0] * X[4] - X[1] * X[3]};
+        const float det = X[0] * C[0] + X[1] * C[1] + X[2] * C[2];
+        if (!(det > 0.f)) return false;
+        float nx = 0.f, nc = 0.f;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            nx = fmaf(X[q], X[q], nx);
+            nc = fmaf(C[q], C[q], nc);
+        }
+        const float g = sqrtf(sqrtf(nc / nx) / det);
+        const float a = 0.5f * g, b = 0.5f / (det * g);
+        float d = 0.f;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const float xn = fmaf(a, X[q], b * C[q]);
+            const float t = xn - X[q];
+            d = fmaf(t, t, d);
+            X[q] = xn;
+        }
+        if (!(d == d)) return false;   // NaN
+        if (d < 1e-12f) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) R[q] = X[q];
+            return true;
+        }
+    }
+    return false;
+}
+
 // Closest point on segment [a, b] to p; returns the segment parameter.
 __device__ __forceinline__ float closest_on_segment(const float p[3], const float a[3], const float b[3], float q[3]) {
     const float ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};

@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
             F[r * 3 + q] = (e1[r] + f1[r]) * g1[q] + (e2[r] + f2[r]) * g2[q] + (e3[r] + f3[r]) * g3[q];
         }
     float R[9];
-    svd_rotation(F, R);
+    if (!polar_newton(F, R)) svd_rotation(F, R);   // the SVD only for inverted / degenerate tets
 #pragma unroll
     for (int q = 0; q < 9; ++q) R[q] -= Fs[q];
     float o1[3], o2[3], o3[3];

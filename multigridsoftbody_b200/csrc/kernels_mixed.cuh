@@ -101,8 +101,8 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
 // Outer FP64 residual r = b - A d with A = diag + c + off-diagonal (FP64
 // values; c = this frame's contact stiffness), stored as FP32 for the correction V-cycle, fused with its first Jacobi
 // sweep from a zero guess: e = dinv r.  4 lanes per row.
-// With b0 set, b is first assembled as b0 + the row's slots (FP64, slot
-// order; the first pass of a PD iteration) and stored.  With ls_r set (the
+// With b0 set, b is first assembled as b0 + the row's slots (FP64, the slots
+// split over the row's lanes; the first pass of a PD iteration) and stored.  With ls_r set (the
 // learned V-cycle, which starts from zero), also ls_r = fix * r and
 // part[block] = sum |ls_r|^2: the starting residual of that cycle.
 __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
@@ -121,17 +121,31 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
     double4 bi = d4z();
-    if (b0 && valid && lane < S) {
-        bi = b0[row];
-        const int e1 = __ldg(slot_ptr + row + 1);
+    if (b0) {   // uniform over the block: the row's slots split over its G lanes, FP64 sums
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        if (valid) {
+            const int e1 = __ldg(slot_ptr + row + 1);
 #pragma unroll 4
-        for (int q = __ldg(slot_ptr + row); q < e1; ++q) {
-            const float4 t = __ldg(slots + q);
-            bi.x += t.x;
-            bi.y += t.y;
-            bi.z += t.z;
+            for (int q = __ldg(slot_ptr + row) + lane / S; q < e1; q += G) {
+                const float4 t = __ldg(slots + q);
+                sx += t.x;
+                sy += t.y;
+                sz += t.z;
+            }
         }
-        b[row] = bi;
+#pragma unroll
+        for (int o = S; o < 32; o <<= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            sz += __shfl_xor_sync(0xffffffffu, sz, o);
+        }
+        if (valid && lane < S) {
+            bi = b0[row];
+            bi.x += sx;
+            bi.y += sy;
+            bi.z += sz;
+            b[row] = bi;
+        }
     }
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (valid) {
