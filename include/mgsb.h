@@ -246,6 +246,13 @@ mgsb_status mgsb_get_coarse_split(mgsb_solver* h, int32_t* split);
  * the launch gap; 0 = plain stream order.  Same results either way.  No
  * reference counterpart. */
 mgsb_status mgsb_set_launch_overlap(mgsb_solver* h, int32_t on);
+/* Prolongation fused with the first post-smoothing sweep (default 1): with
+ * OP = Off * P precomputed per level, A (d + P e) = (b - res) + D P e + OP e,
+ * so the sweep after the prolongation needs no neighbour of the prolonged
+ * vector and both run as one kernel (in the learned cycle: the prolongation
+ * and the post-smoothing residual).  0 = separate launches.  The same
+ * V-cycle; results agree to rounding.  No reference counterpart. */
+mgsb_status mgsb_set_fused_prolongation(mgsb_solver* h, int32_t on);
 /* Tool-contact broad phase of the multigrid kinds (default 0 = every
  * surface vertex against its body's capsule).  1: a uniform grid per body
  * over the rest bounding box of its surface, rebuilt every frame from the

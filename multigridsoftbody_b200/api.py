@@ -413,6 +413,10 @@ class Solver:
         """Uniform-grid broad phase for the capsule contact (same contacts as the all-vertex test)."""
         _check(self._lib.mgsb_set_broad_phase(self.h, 1 if on else 0), self.h)
 
+    def set_fused_prolongation(self, on: bool = True) -> None:
+        """Prolongation + first post-smoothing sweep as one kernel (default on)."""
+        _check(self._lib.mgsb_set_fused_prolongation(self.h, 1 if on else 0), self.h)
+
     def set_launch_overlap(self, on: bool = True) -> None:
         """Programmatic dependent launch between the frame's kernels (default on)."""
         _check(self._lib.mgsb_set_launch_overlap(self.h, 1 if on else 0), self.h)

@@ -36,6 +36,9 @@ struct LevelView {
     const int32_t* rptr;  // restriction: children in the next finer level
     const int32_t* rcol;
     const float* rw;
+    const int32_t* op_slice_ptr;   // OP = Off * P(next coarser level), sliced ELL
+    const int32_t* op_col;
+    const float* op_val;
 };
 
 struct CoarseArgs {
@@ -314,6 +317,58 @@ __global__ void k_lvl_prolong(int n, const int4* __restrict__ pid, const float4*
     v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
     v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
     dst[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Prolongation fused with the first post-smoothing sweep.  With the level's
+// operator A = D + Off, pe = P e_c (this row's 4 parents on the coarser level)
+// and OP = Off P precomputed,
+//     A (d + pe) = (b - res) + D pe + OP e_c,
+// where res = b - A d is the residual the descent already formed, so
+//     dout = d + pe + dinv (res - D pe - OP e_c)
+// needs no neighbour of the prolonged vector: one launch instead of two.
+// G lanes per row over OP's sliced-ELL row; dout may be din.  With ls_r set
+// (the learned cycle) the output is instead the post-smoothing residual
+// ls_r = fix (res - D pe - OP e_c), and d += pe in place.
+// ---------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(256) k_prolong_sweep(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
+                                                       const float4* __restrict__ ec, const int32_t* __restrict__ sp,
+                                                       const int32_t* __restrict__ col, const float* __restrict__ val,
+                                                       const float* __restrict__ dfull, const float* __restrict__ dinv,
+                                                       const float4* __restrict__ res, const float4* din, float4* dout,
+                                                       const float* __restrict__ fixf, float4* __restrict__ ls_r,
+                                                       const int32_t* __restrict__ gate) {
+    pdl_enter();
+    if (gate && __ldg(gate) == 0) return;
+    constexpr int S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const float4 q = rg_offdiag<G>(row, valid, lane, sp, col, val, ec);
+    if (!valid || lane >= S) return;
+    const int4 id = __ldg(pid + row);
+    const float4 w = __ldg(pw + row);
+    const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
+    const float4 pe = make_float4(w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x,
+                                  w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y,
+                                  w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z, 0.f);
+    const float4 r0 = __ldg(res + row);
+    const float D = __ldg(dfull + row);
+    const float rx = r0.x - fmaf(D, pe.x, q.x), ry = r0.y - fmaf(D, pe.y, q.y), rz = r0.z - fmaf(D, pe.z, q.z);
+    float4 x = din[row];
+    x.x += pe.x;
+    x.y += pe.y;
+    x.z += pe.z;
+    if (ls_r) {
+        const float fx = __ldg(fixf + row);
+        ls_r[row] = make_float4(fx * rx, fx * ry, fx * rz, 0.f);
+        dout[row] = x;
+    } else {
+        const float wi = __ldg(dinv + row);
+        dout[row] = make_float4(fmaf(wi, rx, x.x), fmaf(wi, ry, x.y), fmaf(wi, rz, x.z), 0.f);
+    }
 }
 
 // ---------------------------------------------------------------------------

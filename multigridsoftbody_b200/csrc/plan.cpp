@@ -45,7 +45,8 @@ mgsb_status make_body(const mgsb_mesh& m, const mgsb_params& p, bool multigrid, 
 }
 
 void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col, const std::vector<double>& val, int n,
-               int S, std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval) {
+               int S, std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval,
+               const std::vector<int32_t>* pad_col) {
     const int ns = (n + S - 1) / S;
     sptr.assign(ns + 1, 0);
     for (int s = 0; s < ns; ++s) {
@@ -65,8 +66,8 @@ void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col,
                     ecol[e] = col[ptr[r] + k];
                     eval[e] = (float)val[ptr[r] + k];
                 } else {
-                    // padding: a zero coefficient on the row itself (always a valid index)
-                    ecol[e] = r < n ? r : 0;
+                    // padding: a zero coefficient on a valid column (the row itself by default)
+                    ecol[e] = r < n ? (pad_col ? (*pad_col)[r] : r) : (pad_col ? (*pad_col)[n - 1] : 0);
                     eval[e] = 0.f;
                 }
             }
@@ -184,6 +185,10 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
     }
     if (!mg) return true;
 
+    // CSR of the off-diagonal part of the level built last, and the first row
+    // of each body on it (for OP = Off * P of that level)
+    std::vector<int32_t> prev_ptr, prev_col, prev_body;
+    std::vector<double> prev_val;
     // ---- level 0 matrix (off-diagonal, global ids)
     {
         PlanLevel l0;
@@ -218,6 +223,10 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
         l0.nnz = (int)col.size();
         l0.diag0 = P.diag;
         P.levels.push_back(std::move(l0));
+        prev_ptr = std::move(ptr);
+        prev_col = std::move(col);
+        prev_val = std::move(val);
+        prev_body = P.body_of;
     }
     // ---- coarse levels
     std::vector<int> loff(bodies.size(), 0);
@@ -289,7 +298,61 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
         ld.S = kSliceCoarse;
         build_ell(ptr, col, val, n, ld.S, ld.slice_ptr, ld.ell_col, ld.ell_val);
         ld.nnz = (int)col.size();
+        {
+            // OP of the finer level: row i = sum over its neighbours j of a_ij * (prolongation row j),
+            // accumulated in FP64 (weights as stored), columns ascending; padding on the body's
+            // first row of this level; every column checked to lie in the row's body
+            PlanLevel& fl = P.levels[l - 1];
+            std::vector<int32_t> optr(nfin + 1, 0), ocol, pad(nfin, 0);
+            std::vector<double> oval, acc(n, 0.0);
+            std::vector<uint8_t> mark(n, 0);
+            std::vector<int32_t> touched;
+            for (int i = 0; i < nfin; ++i) {
+                touched.clear();
+                for (int q = prev_ptr[i]; q < prev_ptr[i + 1]; ++q) {
+                    const int j = prev_col[q];
+                    const int ids[4] = {ld.pid[j].x, ld.pid[j].y, ld.pid[j].z, ld.pid[j].w};
+                    const float ws[4] = {ld.pw[j].x, ld.pw[j].y, ld.pw[j].z, ld.pw[j].w};
+                    for (int a = 0; a < 4; ++a) {
+                        if (ws[a] == 0.f) continue;
+                        const int c = ids[a];
+                        if (!mark[c]) {
+                            mark[c] = 1;
+                            touched.push_back(c);
+                        }
+                        acc[c] += prev_val[q] * (double)ws[a];
+                    }
+                }
+                std::sort(touched.begin(), touched.end());
+                for (int c : touched) {
+                    ocol.push_back(c);
+                    oval.push_back(acc[c]);
+                    acc[c] = 0.0;
+                    mark[c] = 0;
+                }
+                optr[i + 1] = (int32_t)ocol.size();
+                pad[i] = loff[prev_body[i]];
+            }
+            build_ell(optr, ocol, oval, nfin, fl.S, fl.op_slice_ptr, fl.op_col, fl.op_val, &pad);
+            std::vector<int32_t> body_of_level(n, 0);
+            for (size_t bi = 0; bi < bodies.size(); ++bi)
+                for (int J = loff[bi]; J < loff[bi] + bodies[bi].levels[l - 1].n; ++J) body_of_level[J] = (int32_t)bi;
+            const int fS = fl.S;
+            for (int sl = 0; sl + 1 < (int)fl.op_slice_ptr.size(); ++sl)
+                for (int e = fl.op_slice_ptr[sl]; e < fl.op_slice_ptr[sl + 1]; ++e) {
+                    const int i = sl * fS + (e - fl.op_slice_ptr[sl]) % fS;
+                    if (i < nfin && body_of_level[fl.op_col[e]] != prev_body[i]) {
+                        err = "prolonged operator column outside its body (level " + std::to_string(l - 1) + ")";
+                        return false;
+                    }
+                }
+            fl.op_nnz = (int)ocol.size();
+            prev_body = body_of_level;
+        }
         P.levels.push_back(std::move(ld));
+        prev_ptr = std::move(ptr);
+        prev_col = std::move(col);
+        prev_val = std::move(val);
     }
     // ---- per-body row ranges on every level
     P.range.assign(bodies.size() * L, int2{0, 0});

@@ -40,6 +40,15 @@ struct PlanLevel {
     // restriction CSR: children (finer vertices) of each vertex of this level
     std::vector<int32_t> rptr, rcol;
     std::vector<float> rw;
+    // OP = Off(this level) * P(next coarser level) as sliced ELL with this
+    // level's slice height; columns index the next coarser level (every level
+    // but the coarsest).  With it the product A (d + P e) = A d + D (P e) + OP e
+    // needs no neighbour of the prolonged vector: the prolongation and the first
+    // post-smoothing sweep (or the learned cycle's post-smoothing residual) run
+    // as one kernel from the residual of d.
+    std::vector<int32_t> op_slice_ptr, op_col;
+    std::vector<float> op_val;
+    int op_nnz = 0;
 };
 
 struct Plan {
@@ -67,8 +76,11 @@ struct Plan {
 
 // Sliced ELL (slices of S rows, column-major inside a slice: entry k of row r
 // at sptr[r / S] + k * S + r % S) from CSR rows.
+// Padding entries get a zero coefficient and column pad_col[r] (default: the
+// row itself, valid when rows and columns index the same level).
 void build_ell(const std::vector<int32_t>& ptr, const std::vector<int32_t>& col, const std::vector<double>& val, int n,
-               int S, std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval);
+               int S, std::vector<int32_t>& sptr, std::vector<int32_t>& ecol, std::vector<float>& eval,
+               const std::vector<int32_t>* pad_col = nullptr);
 
 constexpr int kSliceL0 = 8;       // 4 lanes per row at level 0
 constexpr int kSliceCoarse = 4;   // 8 lanes per row on coarse levels

@@ -63,6 +63,10 @@ struct LevelDev {
     // prolongation rows of the next finer level (this level = coarse side)
     int4* pid = nullptr;
     float4* pw = nullptr;
+    // OP = Off(this level) * P(next coarser level), sliced ELL (this level's slice height)
+    int32_t* op_slice_ptr = nullptr;
+    int32_t* op_col = nullptr;
+    float* op_val = nullptr;
     // restriction CSR (children in the finer level)
     int32_t* rptr = nullptr;
     int32_t* rcol = nullptr;
@@ -162,6 +166,7 @@ struct mgsb_solver {
     int coarse_block = 512;
     int split = 1;   // first level of the cluster kernel; levels 1..split-1 run grid-wide
     bool pdl = true;  // programmatic dependent launch between consecutive kernels
+    bool fuse_prolong = true;   // prolongation + first post-sweep as one kernel (k_prolong_sweep)
     // autotuner overrides (0 / -1 = pick by size)
     int tune_cluster = 0, tune_fuse = -1, tune_split = 0;
     std::vector<int> maxv;   // largest body's rows on each level
@@ -469,6 +474,11 @@ mgsb_status rebuild(mgsb_solver* h) {
             TRY(dupload(h, pool, &ld.slice_ptr, pl.slice_ptr));
             TRY(dupload(h, pool, &ld.ell_col, pl.ell_col));
             TRY(dupload(h, pool, &ld.ell_val, pl.ell_val));
+            if (!pl.op_slice_ptr.empty()) {
+                TRY(dupload(h, pool, &ld.op_slice_ptr, pl.op_slice_ptr));
+                TRY(dupload(h, pool, &ld.op_col, pl.op_col));
+                TRY(dupload(h, pool, &ld.op_val, pl.op_val));
+            }
             TRY(dalloc(h, pool, &ld.dfull, pl.n));
             TRY(dalloc(h, pool, &ld.dinv, pl.n));
             TRY(dalloc(h, pool, &ld.res, pl.n));
@@ -748,6 +758,18 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
         const LevelView& C = args.lv[l];
         const LevelView& Cc = args.lv[l + 1];
         const int g = grid_rows(C.n, 32 / kLanesC);
+        if (h->fuse_prolong && args.post > 0) {
+            // prolongation + first post-sweep in one launch (from the residual C.res of the descent)
+            float4* a = ((args.post - 1) % 2 == 0) ? C.e : C.e2;
+            float4* b = (a == C.e) ? C.e2 : C.e;
+            LAUNCH(h, k_prolong_sweep<kLanesC>, g, kBlock, 0, C.n, Cc.pid, Cc.pw, Cc.e, C.op_slice_ptr, C.op_col,
+                   C.op_val, C.dfull, C.dinv, C.res, cur[l], a, nullptr, nullptr, gate);
+            for (int k = 1; k < args.post; ++k) {
+                LAUNCH(h, k_lvl_sweep, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.dinv, C.r, a, b, gate);
+                std::swap(a, b);
+            }
+            continue;
+        }
         float4* a = (args.post % 2 == 0) ? C.e : C.e2;
         float4* b = (a == C.e) ? C.e2 : C.e;
         LAUNCH(h, k_lvl_prolong, grid_for(C.n), kBlock, 0, C.n, Cc.pid, Cc.pw, Cc.e, cur[l], a, gate);
@@ -801,6 +823,32 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
     return MGSB_OK;
 }
 
+// Level-0 prolongation d += P e1 and the post-smoothing sweeps (ping-pong
+// xa -> xb; on return xa holds the result): the first sweep fused with the
+// prolongation (k_prolong_sweep, from the level-0 residual lv[0].res of the
+// descent) unless disabled.  b: the right-hand side of the sweeps.
+void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const int32_t* gate) {
+    const mgsb_params& p = h->p;
+    const int n0 = h->N0;
+    const LevelDev& l0 = h->lev[0];
+    const LevelDev& l1 = h->lev[1];
+    const int g0 = grid_rows(n0, l0.S);
+    int k0 = 0;
+    if (h->fuse_prolong && p.post_sweeps > 0) {
+        LAUNCH(h, k_prolong_sweep<kLanesL0>, g0, kBlock, 0, n0, l1.pid, l1.pw, l1.e, l0.op_slice_ptr, l0.op_col,
+               l0.op_val, l0.dfull, l0.dinv, l0.res, xa, xb, nullptr, nullptr, gate);
+        std::swap(xa, xb);
+        k0 = 1;
+    } else {
+        LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, l1.pid, l1.pw, l1.e, xa, gate);
+    }
+    for (int k = k0; k < p.post_sweeps; ++k) {
+        LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb, b,
+               h->b0, h->slot_ptr, h->slots, 0, gate);
+        std::swap(xa, xb);
+    }
+}
+
 // One learned V-cycle on level 0 for A d = b: d is the warm start, or zero
 // when from_zero.  Pre-smoothing: residual -> features -> tensor-core MLP
 // (d += scale * y).  Coarse correction as in the plain cycle.  Post-smoothing:
@@ -832,10 +880,15 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     ca.d = d;
     ca.gate = nullptr;
     launch_coarse(h, ca);
-    LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, d, nullptr);
-    // post-smoothing
-    LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-           h->ls_r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    // post-smoothing: d += P e1 and the residual the learned sweep starts from
+    if (h->fuse_prolong) {
+        LAUNCH(h, k_prolong_sweep<kLanesL0>, g0, kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, l0.op_slice_ptr,
+               l0.op_col, l0.op_val, l0.dfull, l0.dinv, l0.res, d, d, h->fixf, h->ls_r, nullptr);
+    } else {
+        LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, d, nullptr);
+        LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
+               h->ls_r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    }
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
     // guard.  Inside a CUDA graph the fallback is the body of a conditional IF
@@ -889,12 +942,7 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     ca.d = xa;
     ca.gate = h->ls_gate;
     launch_coarse(h, ca);
-    LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, xa, h->ls_gate);
-    for (int k = 0; k < p.post_sweeps; ++k) {
-        LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb, bw,
-               h->b0, h->slot_ptr, h->slots, 0, h->ls_gate);
-        std::swap(xa, xb);
-    }
+    enqueue_l0_post(h, xa, xb, bw, h->ls_gate);
     if (xa != d) LAUNCH(h, k_ls_copy, grid_for(n0), kBlock, 0, n0, h->ls_gate, xa, d);
     if (h->stream != main_stream) {
         cudaGraph_t body = nullptr;
@@ -968,6 +1016,9 @@ void enqueue_mg_frame(mgsb_solver* h) {
         v.rptr = lv[l].rptr;
         v.rcol = lv[l].rcol;
         v.rw = lv[l].rw;
+        v.op_slice_ptr = lv[l].op_slice_ptr;
+        v.op_col = lv[l].op_col;
+        v.op_val = lv[l].op_val;
     }
     const int g0 = grid_rows(n0, lv[0].S);
     for (int it = 0; it < p.iterations; ++it) {
@@ -991,12 +1042,14 @@ void enqueue_mg_frame(mgsb_solver* h) {
                        lv[0].dfull, xa, h->b, lv[0].res, nullptr);
             ca.d = xa;
             launch_coarse(h, ca);
-            if (!h->fuse_l0)   // the shared-memory kernel leaves the level-1 correction in lv[1].e
-                LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, xa, nullptr);
-            for (int k = 0; k < p.post_sweeps; ++k) {
-                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0, nullptr);
-                std::swap(xa, xb);
+            if (!h->fuse_l0) {   // the shared-memory kernel leaves the level-1 correction in lv[1].e
+                enqueue_l0_post(h, xa, xb, h->b, nullptr);
+            } else {
+                for (int k = 0; k < p.post_sweeps; ++k) {
+                    LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
+                           lv[0].dfull, lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0, nullptr);
+                    std::swap(xa, xb);
+                }
             }
         }
     }
@@ -1035,6 +1088,9 @@ void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
         v.rptr = lv[l].rptr;
         v.rcol = lv[l].rcol;
         v.rw = lv[l].rw;
+        v.op_slice_ptr = lv[l].op_slice_ptr;
+        v.op_col = lv[l].op_col;
+        v.op_val = lv[l].op_val;
     }
 }
 
@@ -1086,12 +1142,7 @@ void enqueue_mixed_frame(mgsb_solver* h) {
             LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                    ea, h->r32, lv[0].res, nullptr);
             launch_coarse(h, ca);
-            LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, ea, nullptr);
-            for (int k = 0; k < p.post_sweeps; ++k) {
-                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0, nullptr);
-                std::swap(ea, eb);
-            }
+            enqueue_l0_post(h, ea, eb, h->r32, nullptr);
             LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
         }
     }
@@ -1795,6 +1846,13 @@ mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on) {
     CUDA_TRY(h, cudaMemset(h->target, 0, (size_t)h->N0 * sizeof(float4)));
     CUDA_TRY(h, cudaMemset(h->bp_cand, 0, (size_t)h->N0));
     CUDA_TRY(h, cudaMemset(h->bp_nlist, 0, sizeof(int32_t)));
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_set_fused_prolongation(mgsb_solver* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
+    h->fuse_prolong = on != 0;
+    invalidate_graph(h);
     return MGSB_OK;
 }
 

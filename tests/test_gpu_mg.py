@@ -377,3 +377,34 @@ def test_one_cta_kernel_equals_cluster_kernel(lib, split):
         out[cluster] = s.positions()
         s.close()
     assert np.array_equal(out[1], out[4])
+
+
+@pytest.mark.parametrize("precision,split", [(mg.PRECISION_FP32, 2), (mg.PRECISION_FP32, 1), (mg.PRECISION_MIXED, 3)])
+def test_fused_prolongation_same_vcycle(lib, oracle_built, precision, split):
+    """Prolongation + first post-sweep as one kernel (from the descent's
+    residual and OP = Off P) is the same V-cycle: the frames agree with the
+    separate launches to rounding and both match the oracle."""
+    m, fixed = beam(8, 80, 8)
+    p = mg_params(levels=4, gravity=(0, 0, 0), precision=precision, refinement_passes=1)
+    path = capsule_path(20, start=(0.0, 0.0, 1.3))
+    runs = {}
+    for fused in (True, False):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        s.set_coarse_split(split)
+        s.set_fused_prolongation(fused)
+        for a, b in path:
+            s.set_capsule(a, b, 0.3)
+            s.step()
+        runs[fused] = (s.positions_f64() if precision == mg.PRECISION_MIXED else s.positions().astype(np.float64),
+                       np.nonzero(s.contact_flags())[0])
+        s.close()
+    diag = m.bbox_diagonal()
+    assert np.abs(runs[True][0] - runs[False][0]).max() < 1e-6 * diag
+    assert np.array_equal(runs[True][1], runs[False][1])
+    o = Oracle(m, p)
+    o.set_fixed(fixed)
+    for a, b in path:
+        o.set_capsule(a, b, 0.3)
+        o.step()
+    assert np.abs(runs[True][0] - o.positions()).max() < 1e-5 * diag
