@@ -46,6 +46,7 @@ struct CoarseArgs {
     int pre, post;
     int fuse_l0;             // level-0 residual and prolongation inside the kernel
     int first;               // shared-memory kernel: first level it owns (>= 1); input lv[first-1].res, output lv[first].e
+    int fuse_prolong;        // prolongation + first post-sweep in one phase (OP = Off P), as k_prolong_sweep
     const int2* range;       // [nbody * L]: (first row, rows) of each body on each level
     const int32_t* dense_off;
     const float* Ainv;       // coarsest inverse blocks (row-major per body)
@@ -755,21 +756,58 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_dsm(const CoarseArgs A) 
         const LevelView& C = A.lv[l];
         const LevelView& Cc = A.lv[l + 1];
         const int r0 = first_row(l), cnt = own_rows(l);
-        for (int li = threadIdx.x; li < cnt; li += blockDim.x) {
-            const int row = q[l].off + r0 + li;
-            const int4 id = __ldg(Cc.pid + row);
-            const float4 w = __ldg(Cc.pw + row);
-            const float4 e0 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.x - q[l + 1].off);
-            const float4 e1 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.y - q[l + 1].off);
-            const float4 e2 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.z - q[l + 1].off);
-            const float4 e3 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.w - q[l + 1].off);
-            float4& v = loc(l, ec[l], li);
-            v.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
-            v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
-            v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+        int k0 = 0;
+        if (A.fuse_prolong && A.post > 0) {
+            // prolongation + first post-sweep from the descent's residual (RES) and OP = Off P:
+            // no neighbour of the prolonged vector is read (the same arithmetic as k_prolong_sweep)
+            const int src = ec[l], dst = (src == E) ? E2 : E;
+            for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
+                const int li = b0 + (lane % Sc);
+                const bool valid = li < cnt;
+                const int row = q[l].off + r0 + li;
+                const float4 qv = rg_offdiag_dsm<kLanesC>(cluster, smv, q[l + 1], ec[l + 1], row, valid, lane,
+                                                          C.op_slice_ptr, C.op_col, C.op_val);
+                if (valid && lane < Sc) {
+                    const int4 id = __ldg(Cc.pid + row);
+                    const float4 w = __ldg(Cc.pw + row);
+                    const float4 e0 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.x - q[l + 1].off);
+                    const float4 e1 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.y - q[l + 1].off);
+                    const float4 e2 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.z - q[l + 1].off);
+                    const float4 e3 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.w - q[l + 1].off);
+                    const float4 pe = make_float4(w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x,
+                                                  w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y,
+                                                  w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z, 0.f);
+                    const float4 r0v = loc(l, RES, li);
+                    const float D = __ldg(C.dfull + row), wi = __ldg(C.dinv + row);
+                    const float rx = r0v.x - fmaf(D, pe.x, qv.x), ry = r0v.y - fmaf(D, pe.y, qv.y),
+                                rz = r0v.z - fmaf(D, pe.z, qv.z);
+                    float4 x = loc(l, src, li);
+                    x.x += pe.x;
+                    x.y += pe.y;
+                    x.z += pe.z;
+                    loc(l, dst, li) = make_float4(fmaf(wi, rx, x.x), fmaf(wi, ry, x.y), fmaf(wi, rz, x.z), 0.f);
+                }
+            }
+            ec[l] = dst;
+            cluster.sync();
+            k0 = 1;
+        } else {
+            for (int li = threadIdx.x; li < cnt; li += blockDim.x) {
+                const int row = q[l].off + r0 + li;
+                const int4 id = __ldg(Cc.pid + row);
+                const float4 w = __ldg(Cc.pw + row);
+                const float4 e0 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.x - q[l + 1].off);
+                const float4 e1 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.y - q[l + 1].off);
+                const float4 e2 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.z - q[l + 1].off);
+                const float4 e3 = *dsm_ptr(cluster, smv, q[l + 1], ec[l + 1], id.w - q[l + 1].off);
+                float4& v = loc(l, ec[l], li);
+                v.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+                v.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+                v.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+            }
+            cluster.sync();
         }
-        cluster.sync();
-        for (int k = 0; k < A.post; ++k) {
+        for (int k = k0; k < A.post; ++k) {
             const int src = ec[l], dst = (src == E) ? E2 : E;
             for (int b0 = warp * Sc; b0 < cnt; b0 += nwarp * Sc) {
                 const int li = b0 + (lane % Sc);
@@ -1063,23 +1101,69 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) 
     }
     // ---- ascend
     for (int l = L - 2; l >= F; --l) {
+        const LevelView& C = A.lv[l];
         const LevelView& Cc = A.lv[l + 1];
         const int n = q[l].n, off = q[l].off, coff = q[l + 1].off;
         const float4* ecs = vec(l + 1, ec[l + 1]);
-        float4* v = vec(l, ec[l]);
-        for (int li = threadIdx.x; li < n; li += blockDim.x) {
-            const int row = off + li;
-            const int4 id = __ldg(Cc.pid + row);
-            const float4 w = __ldg(Cc.pw + row);
-            const float4 e0 = ecs[id.x - coff], e1 = ecs[id.y - coff], e2 = ecs[id.z - coff], e3 = ecs[id.w - coff];
-            float4 t = v[li];
-            t.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
-            t.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
-            t.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
-            v[li] = t;
+        int k0 = 0;
+        if (A.fuse_prolong && A.post > 0) {
+            // prolongation + first post-sweep in one phase (as in the cluster kernel)
+            const int dst = (ec[l] == E) ? E2 : E;
+            const float4* xs = vec(l, ec[l]);
+            const float4* res = vec(l, RES);
+            float4* out = vec(l, dst);
+            const int ngroups = (n + Sc - 1) / Sc;
+            for (int g0 = warp; g0 < ngroups; g0 += nwarp * P) {
+                int li[P], row[P];
+                bool valid[P];
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    li[p] = (g0 + p * nwarp) * Sc + (lane % Sc);
+                    valid[p] = li[p] < n;
+                    row[p] = off + li[p];
+                }
+                float4 o[P];
+                cta_offdiag<P>(row, valid, lane, C.op_slice_ptr, C.op_col, C.op_val, ecs, coff, o);
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    if (!valid[p] || lane >= Sc) continue;
+                    const int4 id = __ldg(Cc.pid + row[p]);
+                    const float4 w = __ldg(Cc.pw + row[p]);
+                    const float4 e0 = ecs[id.x - coff], e1 = ecs[id.y - coff], e2 = ecs[id.z - coff],
+                                 e3 = ecs[id.w - coff];
+                    const float4 pe = make_float4(w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x,
+                                                  w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y,
+                                                  w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z, 0.f);
+                    const float4 r0v = res[li[p]];
+                    const float D = __ldg(C.dfull + row[p]), wi = __ldg(C.dinv + row[p]);
+                    const float rx = r0v.x - fmaf(D, pe.x, o[p].x), ry = r0v.y - fmaf(D, pe.y, o[p].y),
+                                rz = r0v.z - fmaf(D, pe.z, o[p].z);
+                    float4 x = xs[li[p]];
+                    x.x += pe.x;
+                    x.y += pe.y;
+                    x.z += pe.z;
+                    out[li[p]] = make_float4(fmaf(wi, rx, x.x), fmaf(wi, ry, x.y), fmaf(wi, rz, x.z), 0.f);
+                }
+            }
+            ec[l] = dst;
+            __syncthreads();
+            k0 = 1;
+        } else {
+            float4* v = vec(l, ec[l]);
+            for (int li = threadIdx.x; li < n; li += blockDim.x) {
+                const int row = off + li;
+                const int4 id = __ldg(Cc.pid + row);
+                const float4 w = __ldg(Cc.pw + row);
+                const float4 e0 = ecs[id.x - coff], e1 = ecs[id.y - coff], e2 = ecs[id.z - coff], e3 = ecs[id.w - coff];
+                float4 t = v[li];
+                t.x += w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x;
+                t.y += w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y;
+                t.z += w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z;
+                v[li] = t;
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        for (int k = 0; k < A.post; ++k) {
+        for (int k = k0; k < A.post; ++k) {
             const int dst = (ec[l] == E) ? E2 : E;
             sweep_or_residual(l, ec[l], dst, false);
             ec[l] = dst;

@@ -738,6 +738,7 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
     CoarseArgs args = args_in;
     const int F = h->fuse_l0 ? 1 : h->split;
     args.first = F;
+    args.fuse_prolong = h->fuse_prolong ? 1 : 0;
     const int32_t* gate = args.gate;
     float4* cur[kMaxLevels] = {};
     for (int l = 1; l < F; ++l) {
