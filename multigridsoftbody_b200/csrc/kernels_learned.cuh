@@ -253,26 +253,6 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
 // stats[0] = learned V-cycles, stats[1] = fallbacks.
 // In a CUDA graph the decision also sets the conditional handle of the IF node
 // that holds the fallback (use_cond != 0).
-__global__ void k_ls_guard(int n0, const float* __restrict__ p0, int n1, const float* __restrict__ p1, float gamma2,
-                           int32_t* __restrict__ gate, unsigned long long* __restrict__ stats,
-                           cudaGraphConditionalHandle cond, int use_cond) {
-    pdl_enter();
-    __shared__ float red[kLsThreads / 32];
-    float a = 0.f, b = 0.f;
-    for (int i = threadIdx.x; i < n0; i += blockDim.x) a += p0[i];
-    for (int i = threadIdx.x; i < n1; i += blockDim.x) b += p1[i];
-    const float before = block_sum_f(a, red);
-    __syncthreads();
-    const float after = block_sum_f(b, red);
-    if (threadIdx.x == 0) {
-        const bool pass = isfinite(before) && isfinite(after) && after <= gamma2 * before;
-        *gate = pass ? 0 : 1;
-        if (use_cond) cudaGraphSetConditional(cond, pass ? 0u : 1u);
-        stats[0] += 1ull;
-        if (!pass) stats[1] += 1ull;
-    }
-}
-
 // The guard's residual |b - A d|^2 fused with the decision: every block writes
 // its partial sum, the last block to finish (atomic ticket) sums both partial
 // sets in a fixed order, decides, and resets the ticket for the next launch.
