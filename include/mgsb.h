@@ -207,6 +207,17 @@ mgsb_status mgsb_last_frame_ms(mgsb_solver* h, float* ms);
  * PDSolver.cpp:244-292). */
 mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* total_ms, int32_t* launches,
                                int32_t* count);
+/* Device time of one kernel in the frame's own launch chain: one frame is
+ * captured with every launch of the kernel `name` (a name mgsb_profile_frame
+ * reports) repeated `reps` (1..1000) times back to back between two
+ * event-record nodes, so the time per launch carries no event overhead;
+ * us_per_launch = summed chain time / (reps x launches_per_frame).  The
+ * solver state is saved before that frame and restored after it, so the
+ * simulation does not advance.  The broad-phase kernels (k_bp_*) append to
+ * shared lists and are refused (MGSB_NOT_SUPPORTED).  No reference
+ * counterpart. */
+mgsb_status mgsb_time_kernel(mgsb_solver* h, const char* name, int32_t reps, float* us_per_launch,
+                             int32_t* launches_per_frame);
 /* Number of kernel launches one frame issues. */
 mgsb_status mgsb_launches_per_frame(const mgsb_solver* h, int32_t* n);
 

@@ -137,6 +137,7 @@ SIGNATURES = [
     ("mgsb_last_frame_ms", C.c_int, [_P, _FP]),
     ("mgsb_launches_per_frame", C.c_int, [_P, _IP]),
     ("mgsb_profile_frame", C.c_int, [_P, C.c_int32, C.c_char_p, _FP, _IP, _IP]),
+    ("mgsb_time_kernel", C.c_int, [_P, C.c_char_p, C.c_int32, _FP, _IP]),
     ("mgsb_get_precompute", C.c_int, [_P, _FP, _FP, _FP, _FP, _FP]),
     ("mgsb_level_size", C.c_int, [_P, C.c_int32, _IP, _IP]),
     ("mgsb_level_info", C.c_int, [_P, C.c_int32, _IP]),

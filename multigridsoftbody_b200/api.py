@@ -379,6 +379,16 @@ class Solver:
             out[nm] = (float(ms[k]), int(cnt[k]))
         return out
 
+    def time_kernel(self, name: str, reps: int = 20) -> tuple:
+        """Device time of one launch of kernel `name` inside the frame's
+        launch chain (each of its launches repeated `reps` times back to
+        back, no events in between): (us_per_launch, launches_per_frame).
+        The state is restored afterwards; the simulation does not advance."""
+        us = C.c_float()
+        k = C.c_int32()
+        _check(self._lib.mgsb_time_kernel(self.h, name.encode(), int(reps), C.byref(us), C.byref(k)), self.h)
+        return float(us.value), int(k.value)
+
     def precompute(self) -> dict:
         T, V = self.num_tets(0), self.num_verts(0)
         inv = np.empty(9 * T, np.float32)

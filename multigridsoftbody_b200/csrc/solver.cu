@@ -94,6 +94,11 @@ struct mgsb_solver {
     int launches = 0;
     // per-launch CUDA events of a profiled (eager) frame
     bool profiling = false;
+    // kernel replay (mgsb_time_kernel): while profiling with replay_name set,
+    // only the launches of that kernel get events, and each is repeated
+    // replay_reps times back to back between them
+    std::string replay_name;
+    int replay_reps = 1;
     std::vector<std::string> prof_names;
     std::vector<cudaEvent_t> prof_ev;
     std::vector<DevMem> state_mem, derived_mem;
@@ -624,6 +629,20 @@ void prof_mark(mgsb_solver* h, const char* name) {
     if (name) h->prof_names.push_back(name);
 }
 
+// Number of back-to-back launches of one kernel launch site in the frame
+// being enqueued (replay_reps for the kernel mgsb_time_kernel measures, else
+// 1), with an event-record node before them when profiling.
+int prof_begin(mgsb_solver* h, const char* name) {
+    if (!h->profiling) return 1;
+    if (!h->replay_name.empty() && h->replay_name != name) return 1;
+    prof_mark(h, name);
+    return h->replay_name.empty() ? 1 : h->replay_reps;
+}
+
+void prof_end(mgsb_solver* h, const char* name) {
+    if (h->profiling && (h->replay_name.empty() || h->replay_name == name)) prof_mark(h, nullptr);
+}
+
 // Kernel launch on the solver's stream.  With h->pdl the launch carries the
 // programmatic-serialization attribute: its blocks may be scheduled while the
 // previous kernel finishes, and wait in pdl_enter() until that kernel has
@@ -647,9 +666,10 @@ void launch_kernel(mgsb_solver* h, void (*kernel)(KArgs...), int grid, int block
 
 #define LAUNCH(h, kernel, grid, block, smem, ...)                                  \
     do {                                                                             \
-        if ((h)->profiling) prof_mark((h), #kernel);                                 \
-        launch_kernel((h), kernel, (grid), (block), (smem), __VA_ARGS__);           \
-        if ((h)->profiling) prof_mark((h), nullptr);                                 \
+        const int reps_ = prof_begin((h), #kernel);                                  \
+        for (int r_ = 0; r_ < reps_; ++r_)                                           \
+            launch_kernel((h), kernel, (grid), (block), (smem), __VA_ARGS__);       \
+        prof_end((h), #kernel);                                                      \
         ++(h)->launches;                                                             \
     } while (0)
 
@@ -808,14 +828,16 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
         cfg.attrs = attr + 1;
         cfg.numAttrs = h->pdl ? 1 : 0;
     }
-    if (h->profiling) prof_mark(h, "k_coarse_vcycle");
     // fused: global-memory kernel that also owns the level-0 residual and prolongation;
     // one CTA: every owned level in one CTA's shared memory; else the
     // distributed-shared-memory kernel over the cluster
-    cudaError_t e = h->fuse_l0 ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle, args)
-                    : one_cta  ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle_cta, args)
-                               : cudaLaunchKernelEx(&cfg, k_coarse_vcycle_dsm, args);
-    if (h->profiling) prof_mark(h, nullptr);
+    const int reps = prof_begin(h, "k_coarse_vcycle");
+    cudaError_t e = cudaSuccess;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r)
+        e = h->fuse_l0 ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle, args)
+            : one_cta  ? cudaLaunchKernelEx(&cfg, k_coarse_vcycle_cta, args)
+                       : cudaLaunchKernelEx(&cfg, k_coarse_vcycle_dsm, args);
+    prof_end(h, "k_coarse_vcycle");
     ++h->launches;
     if (e != cudaSuccess) {
         h->enqueue_status = set_err(h, MGSB_CUDA_ERROR, "coarse V-cycle launch failed: %s", cudaGetErrorString(e));
@@ -1757,17 +1779,14 @@ mgsb_status mgsb_last_frame_ms(mgsb_solver* h, float* ms) {
     return MGSB_OK;
 }
 
-mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* total_ms, int32_t* launches,
-                               int32_t* count) {
-    if (!h || !count || cap < 0 || (cap > 0 && (!names || !total_ms || !launches))) return MGSB_INVALID_ARG;
-    TRY(ensure_ready(h));
-    CUDA_TRY(h, cudaSetDevice(h->device));
-    TRY(push_tool(h));
-    // The frame is captured into its own graph with an event-record node on
-    // both sides of every kernel, so the timings contain no host launch gaps.
+// One frame captured into its own graph with an event-record node on both
+// sides of every profiled launch (so the timings contain no host launch
+// gaps), run to completion.  The events stay in prof_ev / prof_names.
+cudaError_t run_profiled_frame(mgsb_solver* h) {
     h->profiling = true;
     h->prof_names.clear();
     h->prof_ev.clear();
+    h->enqueue_status = MGSB_OK;
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
@@ -1776,11 +1795,23 @@ mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* 
         e = cudaStreamEndCapture(h->stream, &g);
     }
     h->profiling = false;
+    if (e == cudaSuccess && h->enqueue_status != MGSB_OK) e = cudaErrorInvalidConfiguration;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(ge, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (ge) cudaGraphExecDestroy(ge);
     if (g) cudaGraphDestroy(g);
+    return e;
+}
+
+mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* total_ms, int32_t* launches,
+                               int32_t* count) {
+    if (!h || !count || cap < 0 || (cap > 0 && (!names || !total_ms || !launches))) return MGSB_INVALID_ARG;
+    TRY(ensure_ready(h));
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    TRY(push_tool(h));
+    h->replay_name.clear();
+    const cudaError_t e = run_profiled_frame(h);
     std::vector<std::string> uniq;
     std::vector<float> tot;
     std::vector<int32_t> cnt;
@@ -1799,6 +1830,7 @@ mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* 
     }
     for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
     h->prof_ev.clear();
+    if (h->enqueue_status != MGSB_OK) return h->enqueue_status;
     if (e != cudaSuccess) return set_err(h, MGSB_CUDA_ERROR, "profiled frame failed: %s", cudaGetErrorString(e));
     *count = (int32_t)uniq.size();
     for (size_t u = 0; u < uniq.size() && (int32_t)u < cap; ++u) {
@@ -1806,6 +1838,63 @@ mgsb_status mgsb_profile_frame(mgsb_solver* h, int32_t cap, char* names, float* 
         total_ms[u] = tot[u];
         launches[u] = cnt[u];
     }
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_time_kernel(mgsb_solver* h, const char* name, int32_t reps, float* us_per_launch,
+                             int32_t* launches_per_frame) {
+    if (!h || !name || !us_per_launch || !launches_per_frame || reps < 1 || reps > 1000) return MGSB_INVALID_ARG;
+    if (std::strncmp(name, "k_bp_", 5) == 0)
+        return set_err(h, MGSB_NOT_SUPPORTED, "%s appends to the broad phase's candidate lists; it is not repeated", name);
+    TRY(ensure_ready(h));
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    TRY(push_tool(h));
+    // The repeated launches change the frame's result: the state (and the
+    // guard's statistics) are saved before it and put back after it.
+    std::vector<std::pair<void*, size_t>> keep;
+    for (const DevMem& m : h->state_mem) keep.emplace_back(m.p, m.bytes);
+    if (h->ls_stats) keep.emplace_back(h->ls_stats, 2 * sizeof(unsigned long long));
+    size_t total = 0;
+    for (auto& k : keep) total += (k.second + 255) / 256 * 256;
+    char* save = nullptr;
+    CUDA_TRY(h, cudaMalloc((void**)&save, std::max<size_t>(total, 256)));
+    cudaError_t e = cudaSuccess;
+    size_t off = 0;
+    for (auto& k : keep) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(save + off, k.first, k.second, cudaMemcpyDeviceToDevice, h->stream);
+        off += (k.second + 255) / 256 * 256;
+    }
+    if (e == cudaSuccess) {
+        h->replay_name = name;
+        h->replay_reps = reps;
+        e = run_profiled_frame(h);
+        h->replay_name.clear();
+        h->replay_reps = 1;
+    }
+    float ms = 0.f;
+    const int k_launches = (int)h->prof_names.size();
+    for (int k = 0; k < k_launches && e == cudaSuccess; ++k) {
+        float t = 0.f;
+        e = cudaEventElapsedTime(&t, h->prof_ev[2 * k], h->prof_ev[2 * k + 1]);
+        ms += t;
+    }
+    for (cudaEvent_t ev : h->prof_ev) cudaEventDestroy(ev);
+    h->prof_ev.clear();
+    h->prof_names.clear();
+    off = 0;
+    cudaError_t er = cudaSuccess;
+    for (auto& k : keep) {
+        if (er == cudaSuccess) er = cudaMemcpyAsync(k.first, save + off, k.second, cudaMemcpyDeviceToDevice, h->stream);
+        off += (k.second + 255) / 256 * 256;
+    }
+    if (er == cudaSuccess) er = cudaStreamSynchronize(h->stream);
+    cudaFree(save);
+    if (e == cudaSuccess) e = er;
+    if (h->enqueue_status != MGSB_OK) return h->enqueue_status;
+    if (e != cudaSuccess) return set_err(h, MGSB_CUDA_ERROR, "kernel replay failed: %s", cudaGetErrorString(e));
+    if (k_launches == 0) return set_err(h, MGSB_INVALID_ARG, "no launch of %s in a frame", name);
+    *us_per_launch = 1000.f * ms / (float)(reps * k_launches);
+    *launches_per_frame = k_launches;
     return MGSB_OK;
 }
 

@@ -122,3 +122,29 @@ def test_learned_mixed_matches_oracle(lib, oracle_built, trained):
     v, fb = s.learned_stats()
     assert v == 60 * 10 * 3 and fb <= v // 10, (v, fb)
     s.close()
+
+
+def test_time_kernel_learned_cycle_restores_state(lib, trained):
+    """Replay timing of the learned cycle's kernels (tensor-core sweep, guard)
+    leaves the frames and the guard's statistics as they were."""
+    net = trained[0]
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=1)
+    path = capsule_path(8, start=(0.0, 0.0, 1.4))
+    runs = []
+    for timed in (False, True):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        s.set_learned_smoother(net, 0.5)
+        for f, (a, b) in enumerate(path):
+            s.set_capsule(a, b, 0.3)
+            if timed and f == 4:
+                for name in ("k_ls_sweep_tc", "k_ls_guard_residual", "k_mx_residual", "k_coarse_vcycle"):
+                    us, k = s.time_kernel(name, 8)
+                    assert us > 0.0 and k >= 1, (name, us, k)
+                assert s.time_kernel("k_ls_sweep_tc", 1)[1] == 2 * p.iterations
+            s.step()
+        runs.append((s.positions_f64(), s.learned_stats()))
+        s.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1]

@@ -408,3 +408,47 @@ def test_fused_prolongation_same_vcycle(lib, oracle_built, precision, split):
         o.set_capsule(a, b, 0.3)
         o.step()
     assert np.abs(runs[True][0] - o.positions()).max() < 1e-5 * diag
+
+
+@pytest.mark.parametrize("precision", [mg.PRECISION_FP32, mg.PRECISION_MIXED])
+def test_time_kernel_replays_without_changing_the_run(lib, precision):
+    """Replay timing of every kernel of the frame: a positive time per launch,
+    the launch count the profiled frame reports, and a run that continues
+    bit for bit as if no replay had happened (the state is restored).  The
+    broad-phase kernels are refused."""
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3, gravity=(0, 0, 0), precision=precision, refinement_passes=1)
+    path = capsule_path(10, start=(0.0, 0.0, 1.3))
+
+    def make():
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        s.set_coarse_split(2)   # grid-wide level 1 and the cluster kernel
+        s.set_broad_phase(True)
+        return s
+
+    probe = make()
+    for a, b in path[:5]:
+        probe.set_capsule(a, b, 0.3)
+        probe.step()
+    prof = probe.profile_frame()
+    probe.close()
+    assert "k_coarse_vcycle" in prof and "k_lvl_residual" in prof
+    runs = []
+    for timed in (False, True):
+        s = make()
+        for f, (a, b) in enumerate(path):
+            s.set_capsule(a, b, 0.3)
+            if timed and f == 5:
+                for name, (_, count) in prof.items():
+                    if name.startswith("k_bp_"):
+                        with pytest.raises(mg.MgsbError):
+                            s.time_kernel(name, 4)
+                        continue
+                    us, k = s.time_kernel(name, 4)
+                    assert k == count and us > 0.0, (name, us, k, count)
+            s.step()
+        runs.append((s.positions(), s.contact_flags().copy()))
+        s.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
