@@ -383,13 +383,17 @@ mgsb_status mgsb_mlp_train(mgsb_mlp* h, const float* x, const float* t, int64_t 
 
 /* Attach (net != NULL) or detach the learned smoother of a multigrid solver.
  * Each V-cycle then smooths level 0 with one learned sweep before and one after
- * the coarse correction (in place of the Jacobi sweeps), and checks the
- * residual: unless |r_end| <= guard_ratio * |r_start| (finite), it restores the
- * start and runs the plain V-cycle instead.  The network must live on the
- * solver's device and outlive the attachment; retraining it updates the solver
- * in place.  No counterpart in the reference. */
+ * the coarse correction (in place of the Jacobi sweeps), and every V-cycle's
+ * residual is checked: it fails unless |r_end| <= guard_ratio * |r_start|
+ * (both finite).  When any V-cycle of a frame fails, the frame's global solve
+ * is repeated from its start with the plain V-cycle, so that frame equals
+ * the plain solver's frame (in a CUDA graph the repeat is the body of a
+ * conditional node; eagerly the host reads the decision after the solve).
+ * The network must live on the solver's device and outlive the attachment;
+ * retraining it updates the solver in place.  No counterpart in the
+ * reference. */
 mgsb_status mgsb_set_learned_smoother(mgsb_solver* h, const mgsb_mlp* net, float guard_ratio);
-/* Learned V-cycles run and fallbacks taken since the network was attached. */
+/* Learned V-cycles checked, and checks failed, since the network was attached. */
 mgsb_status mgsb_learned_stats(mgsb_solver* h, uint64_t out[2]);
 /* Training pairs from the plain FP32 multigrid solver's current state: the
  * learned sweep is trained to reproduce `sweeps` weighted-Jacobi sweeps from

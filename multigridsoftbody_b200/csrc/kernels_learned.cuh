@@ -248,20 +248,27 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
     mlp_cta_teardown(Sm, tmem, ws);
 }
 
-// Guard: the learned V-cycle passes when |r_after|^2 <= gamma^2 |r_before|^2
-// (and both are finite); gate = 1 selects the plain fallback.  Counters:
-// stats[0] = learned V-cycles, stats[1] = fallbacks.
-// In a CUDA graph the decision also sets the conditional handle of the IF node
-// that holds the fallback (use_cond != 0).
-// The guard's residual |b - A d|^2 fused with the decision: every block writes
+// Guard of one learned V-cycle: it passes when |r_after|^2 <= gamma^2
+// |r_before|^2 (and both are finite), with r_after = fix (b - A d).  A
+// failure is kept for the whole frame: gate[0] ORs the checks of the frame
+// so far; the frame's last check (final != 0) moves the result to gate[1]
+// (1 = some learned V-cycle of this frame failed: the frame's global solve
+// is repeated with the plain V-cycle), clears gate[0] for the next frame and,
+// in a CUDA graph, sets the condition of the IF node that holds that solve
+// (use_cond != 0).  Counters: stats[0] = learned V-cycles checked, stats[1] =
+// checks failed.
+// The residual |b - A d|^2 is fused with the decision: every block writes
 // its partial sum, the last block to finish (atomic ticket) sums both partial
 // sets in a fixed order, decides, and resets the ticket for the next launch.
+// With dd64 set (mixed precision) the kernel also applies the correction d to
+// the FP64 displacement (dd64 += d) and writes its FP32 mirror d32, the work
+// of k_mx_update.
 __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col, const float* __restrict__ val,
     const float* __restrict__ dfull, const float* __restrict__ fixf, const float4* __restrict__ d,
     const float4* __restrict__ b, float* __restrict__ part1, const float* __restrict__ part0, float gamma2,
     int32_t* __restrict__ gate, unsigned long long* __restrict__ stats, cudaGraphConditionalHandle cond, int use_cond,
-    unsigned int* __restrict__ ticket) {
+    unsigned int* __restrict__ ticket, int final, double4* __restrict__ dd64, float4* __restrict__ d32) {
     pdl_enter();
     __shared__ float red[kLsThreads / 32];
     __shared__ bool last;
@@ -278,6 +285,14 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
         const float qx = fx * (bi.x - fmaf(Dg, x.x, off.x)), qy = fx * (bi.y - fmaf(Dg, x.y, off.y)),
                     qz = fx * (bi.z - fmaf(Dg, x.z, off.z));
         rr = qx * qx + qy * qy + qz * qz;
+        if (dd64) {
+            double4 v = dd64[row];
+            v.x += x.x;
+            v.y += x.y;
+            v.z += x.z;
+            dd64[row] = v;
+            d32[row] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+        }
     }
     const float t = block_sum_f(rr, red);
     if (threadIdx.x == 0) {
@@ -299,28 +314,23 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     const float after = block_sum_f(c, red);
     if (threadIdx.x == 0) {
         const bool pass = isfinite(before) && isfinite(after) && after <= gamma2 * before;
-        *gate = pass ? 0 : 1;
-        if (use_cond) cudaGraphSetConditional(cond, pass ? 0u : 1u);
+        const int fail = (gate[0] != 0 || !pass) ? 1 : 0;
+        if (final) {
+            gate[1] = fail;
+            gate[0] = 0;
+            if (use_cond) cudaGraphSetConditional(cond, (unsigned)fail);
+        } else {
+            gate[0] = fail;
+        }
         stats[0] += 1ull;
         if (!pass) stats[1] += 1ull;
         *ticket = 0u;
     }
 }
 
-// Fallback entry: d = dsave (or 0 when dsave is null) when the gate is set.
-__global__ void k_ls_restore(int n, const int32_t* __restrict__ gate, const float4* __restrict__ dsave,
-                             float4* __restrict__ d) {
+// Copy of the fallback solve's result into the frame's displacement buffer.
+__global__ void k_ls_copy(int n, const float4* __restrict__ src, float4* __restrict__ dst) {
     pdl_enter();
-    if (__ldg(gate) == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    d[i] = dsave ? dsave[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-}
-
-// Gated copy (fallback result back into the frame's displacement buffer).
-__global__ void k_ls_copy(int n, const int32_t* __restrict__ gate, const float4* __restrict__ src, float4* __restrict__ dst) {
-    pdl_enter();
-    if (__ldg(gate) == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     dst[i] = src[i];

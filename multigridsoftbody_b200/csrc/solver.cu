@@ -191,6 +191,8 @@ struct mgsb_solver {
     float* ls_scale = nullptr;
     float4 *ls_r = nullptr, *ls_save = nullptr;
     float *ls_part0 = nullptr, *ls_part1 = nullptr;
+    // ls_gate[0]: some learned V-cycle of the frame so far failed its check;
+    // ls_gate[1]: the last frame's decision (its solve was repeated with plain V-cycles)
     int32_t *ls_gate = nullptr, *ls_werr = nullptr;
     unsigned int* ls_ticket = nullptr;   // last-block ticket of the guard kernel (self-resetting)
     unsigned long long* ls_stats = nullptr;
@@ -599,13 +601,13 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dalloc(h, pool, &h->ls_save, (size_t)N0));
         TRY(dalloc(h, pool, &h->ls_part0, (size_t)h->ls_nblk));
         TRY(dalloc(h, pool, &h->ls_part1, (size_t)h->ls_nblk));
-        TRY(dalloc(h, pool, &h->ls_gate, 1));
+        TRY(dalloc(h, pool, &h->ls_gate, 2));
         TRY(dalloc(h, pool, &h->ls_werr, 1));
         TRY(dalloc(h, pool, &h->ls_stats, 2));
         TRY(dalloc(h, pool, &h->ls_ticket, 1));
         CUDA_TRY(h, cudaMemset(h->ls_ticket, 0, sizeof(unsigned int)));
         CUDA_TRY(h, cudaMemset(h->ls_stats, 0, 2 * sizeof(unsigned long long)));
-        CUDA_TRY(h, cudaMemset(h->ls_gate, 0, sizeof(int32_t)));
+        CUDA_TRY(h, cudaMemset(h->ls_gate, 0, 2 * sizeof(int32_t)));
         CUDA_TRY(h, cudaMemset(h->ls_werr, 0, sizeof(int32_t)));
         CUDA_TRY(h, cudaFuncSetAttribute(k_ls_sweep_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)mlp_tc_smem_bytes()));
@@ -875,13 +877,10 @@ void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const 
 // One learned V-cycle on level 0 for A d = b: d is the warm start, or zero
 // when from_zero.  Pre-smoothing: residual -> features -> tensor-core MLP
 // (d += scale * y).  Coarse correction as in the plain cycle.  Post-smoothing:
-// the same learned sweep.  Guard: a final residual; if |r| did not drop to
-// gamma |r_start| (or is not finite) the gate opens, d is restored and the
-// plain V-cycle runs (its kernels are launched gated and return at once when
-// the learned cycle passed).  dtmp: ping-pong buffer of the plain sweeps.
-void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float4* b, bool from_zero, CoarseArgs ca,
+// the same learned sweep.  The residual check that judges the cycle is the
+// caller's next launch (enqueue_learned_guard).
+void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool from_zero, CoarseArgs ca,
                             bool gather_b = false, bool start_residual_ready = false) {
-    const mgsb_params& p = h->p;
     const int n0 = h->N0;
     std::vector<LevelDev>& lv = h->lev;
     const LevelDev& l0 = lv[0];
@@ -890,12 +889,13 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     const int mgrid = std::min(h->ls_ntiles, 2 * h->sm_count);
     const size_t msmem = mlp_tc_smem_bytes();
     float4* bw = const_cast<float4*>(b);
+    (void)from_zero;
     // pre-smoothing (with gather_b the right-hand side b = b0 + slots is assembled here first;
     // start_residual_ready: the previous kernel left ls_r and its block sums, d = 0)
     if (!start_residual_ready)
         LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-               h->ls_r, from_zero ? nullptr : h->ls_save, h->ls_part0, gather_b ? h->b0 : nullptr,
-               gather_b ? h->slot_ptr : nullptr, gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
+               h->ls_r, nullptr, h->ls_part0, gather_b ? h->b0 : nullptr, gather_b ? h->slot_ptr : nullptr,
+               gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
     // coarse correction
@@ -914,64 +914,95 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, float4* dtmp, const float
     }
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
-    // guard.  Inside a CUDA graph the fallback is the body of a conditional IF
-    // node that the guard kernel switches on; eagerly (and while profiling, as
-    // event nodes may not sit in a conditional body) its kernels are launched
-    // gated and return at once when the learned cycle passed.
+}
+
+// The residual check of the learned V-cycle just enqueued (d, b as given to
+// it).  final: the frame's last check, which takes the frame's decision
+// (with fb->cond, into the IF node's condition).  dd64 / d32: the mixed
+// kind's FP64 update, fused into the check.
+struct LearnedFallback {
+    bool cond = false;                      // inside a capture: the IF node's handle is valid
+    cudaGraphConditionalHandle hnd = 0;
+};
+
+void enqueue_learned_guard(mgsb_solver* h, const float4* d, const float4* b, bool final, const LearnedFallback& fb,
+                           double4* dd64 = nullptr, float4* d32 = nullptr) {
+    const LevelDev& l0 = h->lev[0];
+    LAUNCH(h, k_ls_guard_residual, h->ls_nblk, kLsThreads, 0, h->N0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull,
+           h->fixf, d, b, h->ls_part1, h->ls_part0, h->ls_gamma * h->ls_gamma, h->ls_gate, h->ls_stats, fb.hnd,
+           (final && fb.cond) ? 1 : 0, h->ls_ticket, final ? 1 : 0, dd64, d32);
+}
+
+// Frame-level fallback of the learned smoother, before the frame's learned
+// solve: inside a stream capture, the handle of the IF node that will hold
+// the plain solve (reset to 0 at every launch of the graph).
+LearnedFallback begin_learned_fallback(mgsb_solver* h) {
+    LearnedFallback fb;
     cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(h->stream, &cst);
-    const bool cond = cst == cudaStreamCaptureStatusActive && !h->profiling && h->aux_stream;
-    cudaGraphConditionalHandle hnd = 0;
-    cudaGraph_t cap_graph = nullptr;
-    if (cond) {
-        cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &cap_graph, nullptr, nullptr);
-        if (cudaGraphConditionalHandleCreate(&hnd, cap_graph, 0, cudaGraphCondAssignDefault) != cudaSuccess)
-            h->capture_error = true;
+    if (cst != cudaStreamCaptureStatusActive) return fb;
+    cudaGraph_t g = nullptr;
+    if (!h->aux_stream || cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&fb.hnd, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+        h->capture_error = true;
+        return fb;
     }
-    LAUNCH(h, k_ls_guard_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d,
-           b, h->ls_part1, h->ls_part0, h->ls_gamma * h->ls_gamma, h->ls_gate, h->ls_stats, hnd, cond ? 1 : 0,
-           h->ls_ticket);
-    cudaStream_t main_stream = h->stream;
-    if (cond) {
-        const cudaGraphNode_t* deps = nullptr;
-        size_t nd = 0;
-        cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &cap_graph, &deps, &nd);
-        cudaGraphNodeParams np = {};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = hnd;
-        np.conditional.type = cudaGraphCondTypeIf;
-        np.conditional.size = 1;
-        cudaGraphNode_t node = nullptr;
-        if (cudaGraphAddNode(&node, cap_graph, deps, nd, &np) != cudaSuccess ||
-            cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess ||
-            cudaStreamBeginCaptureToGraph(h->aux_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    fb.cond = true;
+    return fb;
+}
+
+// After the learned solve: the plain solve (body) runs when the frame's last
+// check found a failed learned V-cycle.  In a capture it becomes the body of
+// an IF node (captured on the auxiliary stream, without profiling events:
+// event nodes may not sit in a conditional body); eagerly the host reads the
+// decision and enqueues it.
+template <typename Body>
+void end_learned_fallback(mgsb_solver* h, const LearnedFallback& fb, Body&& body) {
+    cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(h->stream, &cst);
+    if (!fb.cond) {
+        if (cst != cudaStreamCaptureStatusNone) {
             h->capture_error = true;
-        } else {
-            h->stream = h->aux_stream;   // the fallback below is captured into the IF body
+            return;
         }
+        int32_t g[2] = {0, 0};
+        cudaError_t e = cudaMemcpyAsync(g, h->ls_gate, sizeof g, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) {
+            h->enqueue_status = set_err(h, MGSB_CUDA_ERROR, "learned-smoother check: %s", cudaGetErrorString(e));
+            return;
+        }
+        if (g[1]) body();
+        return;
     }
-    // fallback: the plain V-cycle from the same start
-    LAUNCH(h, k_ls_restore, grid_for(n0), kBlock, 0, n0, h->ls_gate, from_zero ? nullptr : h->ls_save, d);
-    float4* xa = d;
-    float4* xb = dtmp;
-    for (int k = 0; k < p.pre_sweeps; ++k) {
-        LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb, bw,
-               h->b0, h->slot_ptr, h->slots, 0, h->ls_gate);
-        std::swap(xa, xb);
+    cudaGraph_t cap_graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = fb.hnd;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &cap_graph, &deps, &nd) != cudaSuccess ||
+        cudaGraphAddNode(&node, cap_graph, deps, nd, &np) != cudaSuccess ||
+        cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess ||
+        cudaStreamBeginCaptureToGraph(h->aux_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        h->capture_error = true;
+        return;
     }
-    LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, xa, b, l0.res,
-           h->ls_gate);
-    ca.d = xa;
-    ca.gate = h->ls_gate;
-    launch_coarse(h, ca);
-    enqueue_l0_post(h, xa, xb, bw, h->ls_gate);
-    if (xa != d) LAUNCH(h, k_ls_copy, grid_for(n0), kBlock, 0, n0, h->ls_gate, xa, d);
-    if (h->stream != main_stream) {
-        cudaGraph_t body = nullptr;
-        if (cudaStreamEndCapture(h->stream, &body) != cudaSuccess) h->capture_error = true;
-        h->stream = main_stream;
-    }
+    cudaStream_t main_stream = h->stream;
+    const bool prof = h->profiling;
+    const int launches = h->launches;
+    h->stream = h->aux_stream;
+    h->profiling = false;
+    body();
+    h->profiling = prof;
+    h->launches = launches;   // launches_per_frame counts the frame that runs when every check passes
+    cudaGraph_t bg = nullptr;
+    if (cudaStreamEndCapture(h->stream, &bg) != cudaSuccess) h->capture_error = true;
+    h->stream = main_stream;
 }
 
 // Broad phase on the predicted positions spos: clear the previous
@@ -990,94 +1021,6 @@ void enqueue_broad_phase(mgsb_solver* h, const float4* spos, bool narrow) {
     LAUNCH(h, k_bp_query, nb, kBlock, 0, h->bp_grids, h->bodies_dev, h->bp_start, h->bp_sorted, spos, h->fixf,
            h->p.contact_stiffness, h->bp_cand, h->bp_list, h->bp_nlist, narrow ? h->cflag : nullptr,
            narrow ? h->c0 : nullptr, narrow ? h->target : nullptr);
-}
-
-void enqueue_mg_frame(mgsb_solver* h) {
-    const mgsb_params& p = h->p;
-    const int n0 = h->N0, T = h->T, L = p.levels;
-    const int nb = (int)h->bodies.size();
-    const float om = p.jacobi_omega;
-    std::vector<LevelDev>& lv = h->lev;
-    LAUNCH(h, k_mg_predict, grid_for(n0), kBlock, 0, n0, h->x, h->v, h->s, h->last, h->fixf, h->body_of, h->bodies_dev, p.dt);
-    if (h->nsurf > 0 && h->broad_phase)
-        enqueue_broad_phase(h, h->s, true);
-    else if (h->nsurf > 0)
-        LAUNCH(h, k_contact_all, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bodies_dev, h->s,
-               h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target);
-    float4* xa = h->d;    // displacement d = x - s (ping)
-    float4* xb = h->d2;   // pong
-    LAUNCH(h, k_l0_frame, grid_for(n0), kBlock, 0, n0, h->s, h->c0, h->target, h->vdiag, h->fixf, om, h->b0,
-           lv[0].dfull, lv[0].dinv, xa);
-    for (int l = 1; l < L; ++l)
-        LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
-               lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
-    LAUNCH(h, k_coarsest_update<float>, nb, 1024, h->factor_smem, h->range, L, h->dense_off_d, h->A0dense, h->B0dense,
-           lv[L - 1].c, h->c_prev, h->Lfac, h->fac_valid);
-    CoarseArgs ca = {};
-    ca.L = L;
-    ca.pre = p.pre_sweeps;
-    ca.post = p.post_sweeps;
-    ca.fuse_l0 = h->fuse_l0;
-    ca.range = h->range;
-    ca.dense_off = h->dense_off_d;
-    ca.Ainv = h->Lfac;
-    ca.b = h->b;
-    for (int l = 0; l < L; ++l) {
-        LevelView& v = ca.lv[l];
-        v.n = lv[l].n;
-        v.slice_ptr = lv[l].slice_ptr;
-        v.col = lv[l].ell_col;
-        v.val = lv[l].ell_val;
-        v.dfull = lv[l].dfull;
-        v.dinv = lv[l].dinv;
-        v.r = lv[l].r;
-        v.e = lv[l].e;
-        v.e2 = lv[l].e2;
-        v.res = lv[l].res;
-        v.pid = lv[l].pid;
-        v.pw = lv[l].pw;
-        v.rptr = lv[l].rptr;
-        v.rcol = lv[l].rcol;
-        v.rw = lv[l].rw;
-        v.op_slice_ptr = lv[l].op_slice_ptr;
-        v.op_col = lv[l].op_col;
-        v.op_val = lv[l].op_val;
-    }
-    const int g0 = grid_rows(n0, lv[0].S);
-    for (int it = 0; it < p.iterations; ++it) {
-        LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
-        if (h->ls_net) {
-            for (int pass = 0; pass < p.refinement_passes; ++pass)
-                enqueue_learned_vcycle(h, xa, xb, h->b, false, ca, pass == 0);
-            continue;
-        }
-        for (int pass = 0; pass < p.refinement_passes; ++pass) {
-            bool gathered = pass > 0;
-            for (int k = 0; k < p.pre_sweeps; ++k) {
-                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1, nullptr);
-                gathered = true;
-                std::swap(xa, xb);
-            }
-            if (!gathered) LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
-            if (!h->fuse_l0)
-                LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
-                       lv[0].dfull, xa, h->b, lv[0].res, nullptr);
-            ca.d = xa;
-            launch_coarse(h, ca);
-            if (!h->fuse_l0) {   // the shared-memory kernel leaves the level-1 correction in lv[1].e
-                enqueue_l0_post(h, xa, xb, h->b, nullptr);
-            } else {
-                for (int k = 0; k < p.post_sweeps; ++k) {
-                    LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
-                           lv[0].dfull, lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0, nullptr);
-                    std::swap(xa, xb);
-                }
-            }
-        }
-    }
-    LAUNCH(h, k_mg_finish, grid_for(n0), kBlock, 0, n0, h->s, xa, h->x, h->v, 1.0f / p.dt, h->nonfinite);
-    h->d_final = xa;
 }
 
 void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
@@ -1117,17 +1060,98 @@ void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
     }
 }
 
-// Mixed precision: FP64 state and outer residual, FP32 local step and
-// correction V-cycles (refinement_passes per PD iteration).
-void enqueue_mixed_frame(mgsb_solver* h) {
+// The FP32 multigrid kind's global solve of one frame, from the contact
+// state: right-hand side and diagonals, coarse-level data and the coarsest
+// inverse, then the PD iterations (local step, V-cycles).  Returns the
+// buffer that holds the final displacement.  learned: learned V-cycles, each
+// followed by its residual check.
+float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb) {
     const mgsb_params& p = h->p;
     const int n0 = h->N0, T = h->T, L = p.levels;
     const int nb = (int)h->bodies.size();
     const float om = p.jacobi_omega;
     std::vector<LevelDev>& lv = h->lev;
-    LAUNCH(h, k_mx_predict, grid_for(n0), kBlock, 0, n0, h->x64, h->v64, h->s64, h->last64, h->s, h->x, h->fixf,
-           h->body_of, h->bodies_dev, (double)p.dt);
-    if (h->nsurf > 0 && h->broad_phase) enqueue_broad_phase(h, h->s, false);
+    float4* xa = h->d;    // displacement d = x - s (ping)
+    float4* xb = h->d2;   // pong
+    LAUNCH(h, k_l0_frame, grid_for(n0), kBlock, 0, n0, h->s, h->c0, h->target, h->vdiag, h->fixf, om, h->b0,
+           lv[0].dfull, lv[0].dinv, xa);
+    for (int l = 1; l < L; ++l)
+        LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
+               lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
+    LAUNCH(h, k_coarsest_update<float>, nb, 1024, h->factor_smem, h->range, L, h->dense_off_d, h->A0dense, h->B0dense,
+           lv[L - 1].c, h->c_prev, h->Lfac, h->fac_valid);
+    CoarseArgs ca;
+    fill_coarse_args(h, ca);
+    const int g0 = grid_rows(n0, lv[0].S);
+    for (int it = 0; it < p.iterations; ++it) {
+        LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
+        if (learned) {
+            for (int pass = 0; pass < p.refinement_passes; ++pass) {
+                enqueue_learned_vcycle(h, xa, h->b, false, ca, pass == 0);
+                enqueue_learned_guard(h, xa, h->b, it == p.iterations - 1 && pass == p.refinement_passes - 1, fb);
+            }
+            continue;
+        }
+        for (int pass = 0; pass < p.refinement_passes; ++pass) {
+            bool gathered = pass > 0;
+            for (int k = 0; k < p.pre_sweeps; ++k) {
+                LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
+                       lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1, nullptr);
+                gathered = true;
+                std::swap(xa, xb);
+            }
+            if (!gathered) LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
+            if (!h->fuse_l0)
+                LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
+                       lv[0].dfull, xa, h->b, lv[0].res, nullptr);
+            ca.d = xa;
+            launch_coarse(h, ca);
+            if (!h->fuse_l0) {   // the shared-memory kernel leaves the level-1 correction in lv[1].e
+                enqueue_l0_post(h, xa, xb, h->b, nullptr);
+            } else {
+                for (int k = 0; k < p.post_sweeps; ++k) {
+                    LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
+                           lv[0].dfull, lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0, nullptr);
+                    std::swap(xa, xb);
+                }
+            }
+        }
+    }
+    return xa;
+}
+
+void enqueue_mg_frame(mgsb_solver* h) {
+    const mgsb_params& p = h->p;
+    const int n0 = h->N0;
+    LAUNCH(h, k_mg_predict, grid_for(n0), kBlock, 0, n0, h->x, h->v, h->s, h->last, h->fixf, h->body_of, h->bodies_dev, p.dt);
+    if (h->nsurf > 0 && h->broad_phase)
+        enqueue_broad_phase(h, h->s, true);
+    else if (h->nsurf > 0)
+        LAUNCH(h, k_contact_all, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bodies_dev, h->s,
+               h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target);
+    const bool learned = h->ls_net != nullptr;
+    const LearnedFallback fb = learned ? begin_learned_fallback(h) : LearnedFallback{};
+    float4* d = enqueue_mg_solve(h, learned, fb);
+    if (learned)   // a failed learned V-cycle: the frame's solve again with the plain V-cycle
+        end_learned_fallback(h, fb, [&] {
+            float4* dp = enqueue_mg_solve(h, false, fb);
+            if (dp != d) LAUNCH(h, k_ls_copy, grid_for(n0), kBlock, 0, n0, dp, d);
+        });
+    LAUNCH(h, k_mg_finish, grid_for(n0), kBlock, 0, n0, h->s, d, h->x, h->v, 1.0f / p.dt, h->nonfinite);
+    h->d_final = d;
+}
+
+// Mixed precision: FP64 state and outer residual, FP32 local step and
+// correction V-cycles (refinement_passes per PD iteration).  The global
+// solve of one frame, from the predicted FP64 positions: contact state,
+// right-hand side and diagonals, coarse-level data and the coarsest FP64
+// inverse, then the PD iterations; the displacement ends in dd64 / d32.
+void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb) {
+    const mgsb_params& p = h->p;
+    const int n0 = h->N0, T = h->T, L = p.levels;
+    const int nb = (int)h->bodies.size();
+    const float om = p.jacobi_omega;
+    std::vector<LevelDev>& lv = h->lev;
     LAUNCH(h, k_mx_contact_frame, grid_for(n0), kBlock, 0, n0, h->s64, h->fixf, h->body_of, h->bodies_dev, h->is_surf,
            h->broad_phase ? h->bp_cand : nullptr, p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32,
            h->target);
@@ -1147,14 +1171,15 @@ void enqueue_mixed_frame(mgsb_solver* h) {
             float4* eb = h->d2;
             // the first pass also assembles b = b0 + slots; with the learned smoother it
             // also leaves the learned cycle's starting residual (the cycle starts from e = 0)
-            const bool gather = pass == 0, learned = h->ls_net != nullptr;
+            const bool gather = pass == 0;
             LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
                    h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !learned) ? 1 : 0,
                    gather ? h->b0_64 : nullptr, gather ? h->slot_ptr : nullptr, gather ? h->slots : nullptr, h->fixf,
                    learned ? h->ls_r : nullptr, learned ? h->ls_part0 : nullptr);
-            if (learned) {
-                enqueue_learned_vcycle(h, ea, eb, h->r32, true, ca, false, true);
-                LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
+            if (learned) {   // the check also applies the correction (dd64 += e)
+                enqueue_learned_vcycle(h, ea, h->r32, true, ca, false, true);
+                enqueue_learned_guard(h, ea, h->r32, it == p.iterations - 1 && pass == p.refinement_passes - 1, fb,
+                                      h->dd64, h->d32);
                 continue;
             }
             for (int k = 1; k < p.pre_sweeps; ++k) {
@@ -1169,6 +1194,19 @@ void enqueue_mixed_frame(mgsb_solver* h) {
             LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
         }
     }
+}
+
+void enqueue_mixed_frame(mgsb_solver* h) {
+    const mgsb_params& p = h->p;
+    const int n0 = h->N0;
+    LAUNCH(h, k_mx_predict, grid_for(n0), kBlock, 0, n0, h->x64, h->v64, h->s64, h->last64, h->s, h->x, h->fixf,
+           h->body_of, h->bodies_dev, (double)p.dt);
+    if (h->nsurf > 0 && h->broad_phase) enqueue_broad_phase(h, h->s, false);
+    const bool learned = h->ls_net != nullptr;
+    const LearnedFallback fb = learned ? begin_learned_fallback(h) : LearnedFallback{};
+    enqueue_mixed_solve(h, learned, fb);
+    if (learned)   // a failed learned V-cycle: the frame's solve again with the plain V-cycle
+        end_learned_fallback(h, fb, [&] { enqueue_mixed_solve(h, false, fb); });
     LAUNCH(h, k_mx_finish, grid_for(n0), kBlock, 0, n0, h->s64, h->dd64, h->x64, h->v64, h->x, 1.0 / (double)p.dt,
            h->nonfinite);
 }
@@ -2462,11 +2500,7 @@ extern "C" mgsb_status mgsb_vcycle_residuals(mgsb_solver* h, int32_t cycles, int
     h->profiling = false;
     for (int c = 0; c < cycles; ++c) {
         if (mode == 2) {
-            // the learned cycle without its fallback: open the gate never
-            const float g = h->ls_gamma;
-            h->ls_gamma = 1e18f;
-            enqueue_learned_vcycle(h, e, tmp, rhs, c == 0, ca);
-            h->ls_gamma = g;
+            enqueue_learned_vcycle(h, e, rhs, c == 0, ca);   // the learned cycle alone, no check
         } else {
             float4* xa = e;
             float4* xb = tmp;

@@ -73,9 +73,9 @@ def test_learned_sweep_gains_over_plain(lib, trained):
 @pytest.mark.parametrize("graph,split", [(1, 1), (0, 1), (1, 2), (0, 2)])
 def test_guard_falls_back_to_plain(lib, graph, split):
     """A network with wild weights fails the residual check on every V-cycle;
-    the fallback restores the start and runs the plain cycle, so the frame
-    equals the plain solver's (also with level 1 run as grid-wide kernels,
-    whose launches the fallback gates)."""
+    each frame's solve is then repeated with the plain V-cycle, so every
+    frame equals the plain solver's bit for bit (also with level 1 run as
+    grid-wide kernels)."""
     m, fixed = beam(4, 40, 4)
     bad = MLP(seed=11)
     bad.params = np.random.default_rng(0).normal(0.0, 30.0, NUM_PARAMS).astype(np.float32)
@@ -94,9 +94,32 @@ def test_guard_falls_back_to_plain(lib, graph, split):
             v, fb = s.learned_stats()
             assert v == 12 * 10 and fb == v, (v, fb)
         s.close()
-    # the fallback gathers the right-hand side in a different order than the
-    # plain sweep, so agreement is to rounding, not bitwise
-    assert np.abs(runs[True] - runs[False]).max() < 1e-6 * m.bbox_diagonal()
+    assert np.array_equal(runs[True], runs[False])
+
+
+@pytest.mark.parametrize("graph", [1, 0])
+def test_guard_falls_back_to_plain_mixed(lib, graph):
+    """Mixed precision: with a network that fails every check, every frame
+    is the plain mixed-precision solver's frame, bit for bit."""
+    m, fixed = beam(4, 40, 4)
+    bad = MLP(seed=12)
+    bad.params = np.random.default_rng(1).normal(0.0, 30.0, NUM_PARAMS).astype(np.float32)
+    p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=2, use_graph=graph)
+    runs = {}
+    for learned in (False, True):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        if learned:
+            s.set_learned_smoother(bad, 0.5)
+        for a, b in capsule_path(10, start=(0.0, 0.0, 1.3)):
+            s.set_capsule(a, b, 0.3)
+            s.step()
+        runs[learned] = s.positions_f64()
+        if learned:
+            v, fb = s.learned_stats()
+            assert v == 10 * 10 * 2 and fb == v, (v, fb)
+        s.close()
+    assert np.array_equal(runs[True], runs[False])
 
 
 def test_learned_mixed_matches_oracle(lib, oracle_built, trained):
