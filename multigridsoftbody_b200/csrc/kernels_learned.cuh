@@ -248,35 +248,36 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
     mlp_cta_teardown(Sm, tmem, ws);
 }
 
-// Guard of one learned V-cycle: it passes when |r_after|^2 <= gamma^2
-// |r_before|^2 (and both are finite), with r_after = fix (b - A d).  A
-// failure is kept for the whole frame: gate[0] ORs the checks of the frame
-// so far; the frame's last check (final != 0) moves the result to gate[1]
-// (1 = some learned V-cycle of this frame failed: the frame's global solve
-// is repeated with the plain V-cycle), clears gate[0] for the next frame and,
-// in a CUDA graph, sets the condition of the IF node that holds that solve
-// (use_cond != 0).  Counters: stats[0] = learned V-cycles checked, stats[1] =
-// checks failed.
-// The residual |b - A d|^2 is fused with the decision: every block writes
-// its partial sum, the last block to finish (atomic ticket) sums both partial
-// sets in a fixed order, decides, and resets the ticket for the next launch.
+// Residual check of the learned V-cycles.  Cycle c of the frame passes when
+// |r_after|^2 <= gamma^2 |r_before|^2 (both finite), r_after = fix (b - A d)
+// after the cycle; the block sums of |r_before|^2 are part0_all[c * nblk +
+// block] (written where the cycle started), those of |r_after|^2 are written
+// here to part1_all[c * nblk + block].  The decision waits for the frame's
+// last check (final != 0): its last block to finish (atomic ticket) sums
+// every cycle's partials (one warp per cycle, fixed order), sets gate[0] = 1
+// when some cycle failed (the frame's global solve is then repeated with the
+// plain V-cycle), counts (stats[0] += cycles, stats[1] += failed cycles),
+// in a CUDA graph sets the condition of the IF node that holds that solve
+// (use_cond != 0), and resets the ticket for the next launch.
 // With dd64 set (mixed precision) the kernel also applies the correction d to
 // the FP64 displacement (dd64 += d) and writes its FP32 mirror d32, the work
 // of k_mx_update.
 __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col, const float* __restrict__ val,
     const float* __restrict__ dfull, const float* __restrict__ fixf, const float4* __restrict__ d,
-    const float4* __restrict__ b, float* __restrict__ part1, const float* __restrict__ part0, float gamma2,
-    int32_t* __restrict__ gate, unsigned long long* __restrict__ stats, cudaGraphConditionalHandle cond, int use_cond,
-    unsigned int* __restrict__ ticket, int final, double4* __restrict__ dd64, float4* __restrict__ d32) {
+    const float4* __restrict__ b, int cycle, int final, const float* __restrict__ part0_all, float* __restrict__ part1_all,
+    float gamma2, int32_t* __restrict__ gate, unsigned long long* __restrict__ stats, cudaGraphConditionalHandle cond,
+    int use_cond, unsigned int* __restrict__ ticket, double4* __restrict__ dd64, float4* __restrict__ d32) {
     pdl_enter();
     __shared__ float red[kLsThreads / 32];
     __shared__ bool last;
+    __shared__ int fails;
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
+    const int nblk = gridDim.x;
     const float4 off = rg_offdiag<G, false>(row, valid, lane, sp, col, val, d);
     float rr = 0.f;
     if (valid && lane < S) {
@@ -296,34 +297,38 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     }
     const float t = block_sum_f(rr, red);
     if (threadIdx.x == 0) {
-        part1[blockIdx.x] = t;
-        __threadfence();
-        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+        part1_all[(size_t)cycle * nblk + blockIdx.x] = t;
+        if (final) {
+            __threadfence();
+            last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+            fails = 0;
+        }
     }
+    if (!final) return;
     __syncthreads();
     if (!last) return;
     __threadfence();
-    float a = 0.f, c = 0.f;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-        a += part0[i];
-        c += part1[i];
+    const int wl = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int c = wl; c <= cycle; c += nw) {
+        float a = 0.f, q = 0.f;
+        for (int i = lane; i < nblk; i += 32) {
+            a += part0_all[(size_t)c * nblk + i];
+            q += part1_all[(size_t)c * nblk + i];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            q += __shfl_xor_sync(0xffffffffu, q, o);
+        }
+        if (lane == 0 && !(isfinite(a) && isfinite(q) && q <= gamma2 * a)) atomicAdd(&fails, 1);
     }
     __syncthreads();
-    const float before = block_sum_f(a, red);
-    __syncthreads();
-    const float after = block_sum_f(c, red);
     if (threadIdx.x == 0) {
-        const bool pass = isfinite(before) && isfinite(after) && after <= gamma2 * before;
-        const int fail = (gate[0] != 0 || !pass) ? 1 : 0;
-        if (final) {
-            gate[1] = fail;
-            gate[0] = 0;
-            if (use_cond) cudaGraphSetConditional(cond, (unsigned)fail);
-        } else {
-            gate[0] = fail;
-        }
-        stats[0] += 1ull;
-        if (!pass) stats[1] += 1ull;
+        const int fail = fails > 0 ? 1 : 0;
+        gate[0] = fail;
+        if (use_cond) cudaGraphSetConditional(cond, (unsigned)fail);
+        stats[0] += (unsigned long long)(cycle + 1);
+        stats[1] += (unsigned long long)fails;
         *ticket = 0u;
     }
 }

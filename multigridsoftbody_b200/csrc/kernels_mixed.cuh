@@ -100,12 +100,16 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
 
 // Outer FP64 residual r = b - A d with A = diag + c + off-diagonal (FP64
 // values; c = this frame's contact stiffness), stored as FP32 for the correction V-cycle, fused with its first Jacobi
-// sweep from a zero guess: e = dinv r.  4 lanes per row.
+// sweep from a zero guess: e = dinv r.  G lanes per row (kLanesMx), 64
+// rows per block (64 * G threads), so the blocks cover the rows the
+// level-0 kernels' 256-thread blocks cover.
 // With b0 set, b is first assembled as b0 + the row's slots (FP64, the slots
 // split over the row's lanes; the first pass of a PD iteration) and stored.  With ls_r set (the
 // learned V-cycle, which starts from zero), also ls_r = fix * r and
 // part[block] = sum |ls_r|^2: the starting residual of that cycle.
-__global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+constexpr int kLanesMx = 4;
+constexpr int kMxThreads = 64 * kLanesMx;
+__global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
                                                      const double* __restrict__ val, const double* __restrict__ diag64,
                                                      const float* __restrict__ c, const double4* __restrict__ d, double4* __restrict__ b,
                                                      const float* __restrict__ dinv, float4* __restrict__ r32,
@@ -114,11 +118,13 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
                                                      const float4* __restrict__ slots, const float* __restrict__ fixf,
                                                      float4* __restrict__ ls_r, float* __restrict__ part) {
     pdl_enter();
-    __shared__ float red[8];
-    constexpr int G = kLanesL0, S = 32 / G;
+    __shared__ float red[kMxThreads / 32];
+    constexpr int G = kLanesMx, RW = 32 / G;   // lanes per row, rows per warp
+    constexpr int SH = 32 / kLanesL0;           // slice height of the level-0 sliced ELL
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int row = warp * S + (lane % S);
+    const int row = warp * RW + (lane % RW);
+    const int j = lane / RW;                    // this lane's share of the row
     const bool valid = row < n;
     double4 bi = d4z();
     if (b0) {   // uniform over the block: the row's slots split over its G lanes, FP64 sums
@@ -126,7 +132,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
         if (valid) {
             const int e1 = __ldg(slot_ptr + row + 1);
 #pragma unroll 4
-            for (int q = __ldg(slot_ptr + row) + lane / S; q < e1; q += G) {
+            for (int q = __ldg(slot_ptr + row) + j; q < e1; q += G) {
                 const float4 t = __ldg(slots + q);
                 sx += t.x;
                 sy += t.y;
@@ -134,12 +140,12 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
             }
         }
 #pragma unroll
-        for (int o = S; o < 32; o <<= 1) {
+        for (int o = RW; o < 32; o <<= 1) {
             sx += __shfl_xor_sync(0xffffffffu, sx, o);
             sy += __shfl_xor_sync(0xffffffffu, sy, o);
             sz += __shfl_xor_sync(0xffffffffu, sz, o);
         }
-        if (valid && lane < S) {
+        if (valid && lane < RW) {
             bi = b0[row];
             bi.x += sx;
             bi.y += sy;
@@ -149,10 +155,10 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
     }
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (valid) {
-        const int slice = row / S;
+        const int slice = row / SH;
         const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
 #pragma unroll 2
-        for (int q = beg + (lane / S) * S + (row - slice * S); q < end; q += 32) {
+        for (int q = beg + j * SH + (row - slice * SH); q < end; q += G * SH) {
             const double a = __ldg(val + q);
             const double4 xv = d[__ldg(col + q)];
             ax = fma(a, xv.x, ax);
@@ -161,13 +167,13 @@ __global__ void __launch_bounds__(256) k_mx_residual(int n, const int32_t* __res
         }
     }
 #pragma unroll
-    for (int o = S; o < 32; o <<= 1) {
+    for (int o = RW; o < 32; o <<= 1) {
         ax += __shfl_xor_sync(0xffffffffu, ax, o);
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
         az += __shfl_xor_sync(0xffffffffu, az, o);
     }
     float rr = 0.f;
-    if (valid && lane < S) {
+    if (valid && lane < RW) {
         const double4 x = d[row];
         if (!b0) bi = b[row];
         const double D = __ldg(diag64 + row) + (double)__ldg(c + row);

@@ -191,9 +191,11 @@ struct mgsb_solver {
     float* ls_scale = nullptr;
     float4 *ls_r = nullptr, *ls_save = nullptr;
     float *ls_part0 = nullptr, *ls_part1 = nullptr;
-    // ls_gate[0]: some learned V-cycle of the frame so far failed its check;
-    // ls_gate[1]: the last frame's decision (its solve was repeated with plain V-cycles)
+    // ls_gate: the last frame's decision (1: a learned V-cycle failed its check and the
+    // frame's solve was repeated with plain V-cycles); ls_part0 / ls_part1: block sums of
+    // |r|^2 before / after each of the frame's ls_cycles learned V-cycles (ls_nblk each)
     int32_t *ls_gate = nullptr, *ls_werr = nullptr;
+    int ls_cycles = 1;
     unsigned int* ls_ticket = nullptr;   // last-block ticket of the guard kernel (self-resetting)
     unsigned long long* ls_stats = nullptr;
     // training-pair generation (allocated on first use)
@@ -599,15 +601,16 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dalloc(h, pool, &h->ls_scale, (size_t)N0));
         TRY(dalloc(h, pool, &h->ls_r, (size_t)N0));
         TRY(dalloc(h, pool, &h->ls_save, (size_t)N0));
-        TRY(dalloc(h, pool, &h->ls_part0, (size_t)h->ls_nblk));
-        TRY(dalloc(h, pool, &h->ls_part1, (size_t)h->ls_nblk));
-        TRY(dalloc(h, pool, &h->ls_gate, 2));
+        h->ls_cycles = std::max(1, h->p.iterations * std::max(1, h->p.refinement_passes));
+        TRY(dalloc(h, pool, &h->ls_part0, (size_t)h->ls_cycles * h->ls_nblk));
+        TRY(dalloc(h, pool, &h->ls_part1, (size_t)h->ls_cycles * h->ls_nblk));
+        TRY(dalloc(h, pool, &h->ls_gate, 1));
         TRY(dalloc(h, pool, &h->ls_werr, 1));
         TRY(dalloc(h, pool, &h->ls_stats, 2));
         TRY(dalloc(h, pool, &h->ls_ticket, 1));
         CUDA_TRY(h, cudaMemset(h->ls_ticket, 0, sizeof(unsigned int)));
         CUDA_TRY(h, cudaMemset(h->ls_stats, 0, 2 * sizeof(unsigned long long)));
-        CUDA_TRY(h, cudaMemset(h->ls_gate, 0, 2 * sizeof(int32_t)));
+        CUDA_TRY(h, cudaMemset(h->ls_gate, 0, sizeof(int32_t)));
         CUDA_TRY(h, cudaMemset(h->ls_werr, 0, sizeof(int32_t)));
         CUDA_TRY(h, cudaFuncSetAttribute(k_ls_sweep_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)mlp_tc_smem_bytes()));
@@ -878,8 +881,9 @@ void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const 
 // when from_zero.  Pre-smoothing: residual -> features -> tensor-core MLP
 // (d += scale * y).  Coarse correction as in the plain cycle.  Post-smoothing:
 // the same learned sweep.  The residual check that judges the cycle is the
-// caller's next launch (enqueue_learned_guard).
-void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool from_zero, CoarseArgs ca,
+// caller's next launch (enqueue_learned_guard); cycle: the cycle's index in
+// the frame (its starting residual's block sums go to ls_part0 there).
+void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool from_zero, CoarseArgs ca, int cycle,
                             bool gather_b = false, bool start_residual_ready = false) {
     const int n0 = h->N0;
     std::vector<LevelDev>& lv = h->lev;
@@ -894,7 +898,7 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
     // start_residual_ready: the previous kernel left ls_r and its block sums, d = 0)
     if (!start_residual_ready)
         LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
-               h->ls_r, nullptr, h->ls_part0, gather_b ? h->b0 : nullptr, gather_b ? h->slot_ptr : nullptr,
+               h->ls_r, nullptr, h->ls_part0 + (size_t)cycle * g0, gather_b ? h->b0 : nullptr, gather_b ? h->slot_ptr : nullptr,
                gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
@@ -916,21 +920,26 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
            l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
 }
 
-// The residual check of the learned V-cycle just enqueued (d, b as given to
-// it).  final: the frame's last check, which takes the frame's decision
-// (with fb->cond, into the IF node's condition).  dd64 / d32: the mixed
-// kind's FP64 update, fused into the check.
+// The residual check of the learned V-cycle `cycle` just enqueued (d, b as
+// given to it).  final: the frame's last check, which takes the frame's
+// decision (with fb.cond, into the IF node's condition).  dd64 / d32: the
+// mixed kind's FP64 update, fused into the check.
 struct LearnedFallback {
     bool cond = false;                      // inside a capture: the IF node's handle is valid
     cudaGraphConditionalHandle hnd = 0;
 };
 
-void enqueue_learned_guard(mgsb_solver* h, const float4* d, const float4* b, bool final, const LearnedFallback& fb,
-                           double4* dd64 = nullptr, float4* d32 = nullptr) {
+// The checks pair the block sums of k_mx_residual / k_ls_residual and of the
+// guard block by block: the same 64 rows per block.
+static_assert(kLsThreads == kBlock && kLsThreads / kLanesL0 == 64 && kMxThreads / kLanesMx == 64,
+              "learned-cycle block sums are paired block by block");
+
+void enqueue_learned_guard(mgsb_solver* h, const float4* d, const float4* b, int cycle, bool final,
+                           const LearnedFallback& fb, double4* dd64 = nullptr, float4* d32 = nullptr) {
     const LevelDev& l0 = h->lev[0];
     LAUNCH(h, k_ls_guard_residual, h->ls_nblk, kLsThreads, 0, h->N0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull,
-           h->fixf, d, b, h->ls_part1, h->ls_part0, h->ls_gamma * h->ls_gamma, h->ls_gate, h->ls_stats, fb.hnd,
-           (final && fb.cond) ? 1 : 0, h->ls_ticket, final ? 1 : 0, dd64, d32);
+           h->fixf, d, b, cycle, final ? 1 : 0, h->ls_part0, h->ls_part1, h->ls_gamma * h->ls_gamma, h->ls_gate,
+           h->ls_stats, fb.hnd, (final && fb.cond) ? 1 : 0, h->ls_ticket, dd64, d32);
 }
 
 // Frame-level fallback of the learned smoother, before the frame's learned
@@ -965,14 +974,14 @@ void end_learned_fallback(mgsb_solver* h, const LearnedFallback& fb, Body&& body
             h->capture_error = true;
             return;
         }
-        int32_t g[2] = {0, 0};
-        cudaError_t e = cudaMemcpyAsync(g, h->ls_gate, sizeof g, cudaMemcpyDeviceToHost, h->stream);
+        int32_t g = 0;
+        cudaError_t e = cudaMemcpyAsync(&g, h->ls_gate, sizeof g, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
             h->enqueue_status = set_err(h, MGSB_CUDA_ERROR, "learned-smoother check: %s", cudaGetErrorString(e));
             return;
         }
-        if (g[1]) body();
+        if (g) body();
         return;
     }
     cudaGraph_t cap_graph = nullptr;
@@ -1087,8 +1096,9 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
         LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
         if (learned) {
             for (int pass = 0; pass < p.refinement_passes; ++pass) {
-                enqueue_learned_vcycle(h, xa, h->b, false, ca, pass == 0);
-                enqueue_learned_guard(h, xa, h->b, it == p.iterations - 1 && pass == p.refinement_passes - 1, fb);
+                const int c = it * p.refinement_passes + pass;
+                enqueue_learned_vcycle(h, xa, h->b, false, ca, c, pass == 0);
+                enqueue_learned_guard(h, xa, h->b, c, c == h->ls_cycles - 1, fb);
             }
             continue;
         }
@@ -1172,14 +1182,14 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
             // the first pass also assembles b = b0 + slots; with the learned smoother it
             // also leaves the learned cycle's starting residual (the cycle starts from e = 0)
             const bool gather = pass == 0;
-            LAUNCH(h, k_mx_residual, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
+            const int c = it * p.refinement_passes + pass;
+            LAUNCH(h, k_mx_residual, g0, kMxThreads, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
                    h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !learned) ? 1 : 0,
                    gather ? h->b0_64 : nullptr, gather ? h->slot_ptr : nullptr, gather ? h->slots : nullptr, h->fixf,
-                   learned ? h->ls_r : nullptr, learned ? h->ls_part0 : nullptr);
+                   learned ? h->ls_r : nullptr, learned ? h->ls_part0 + (size_t)c * h->ls_nblk : nullptr);
             if (learned) {   // the check also applies the correction (dd64 += e)
-                enqueue_learned_vcycle(h, ea, h->r32, true, ca, false, true);
-                enqueue_learned_guard(h, ea, h->r32, it == p.iterations - 1 && pass == p.refinement_passes - 1, fb,
-                                      h->dd64, h->d32);
+                enqueue_learned_vcycle(h, ea, h->r32, true, ca, c, false, true);
+                enqueue_learned_guard(h, ea, h->r32, c, c == h->ls_cycles - 1, fb, h->dd64, h->d32);
                 continue;
             }
             for (int k = 1; k < p.pre_sweeps; ++k) {
@@ -2500,7 +2510,7 @@ extern "C" mgsb_status mgsb_vcycle_residuals(mgsb_solver* h, int32_t cycles, int
     h->profiling = false;
     for (int c = 0; c < cycles; ++c) {
         if (mode == 2) {
-            enqueue_learned_vcycle(h, e, rhs, c == 0, ca);   // the learned cycle alone, no check
+            enqueue_learned_vcycle(h, e, rhs, c == 0, ca, 0);   // the learned cycle alone, no check
         } else {
             float4* xa = e;
             float4* xb = tmp;
