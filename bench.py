@@ -260,6 +260,11 @@ def algorithmic_bytes(kernel, solver, meshes, params):
         return lb.mean_over_grid_levels(lb.restrict, 1)
     if kernel == "k_lvl_prolong":
         return lb.mean_over_grid_levels(lb.prolong, 1)
+    if kernel.startswith("k_ls_guard_residual"):
+        # residual check: e, b 32 B + D, fix 8 B per row, 8 B/nnz; mixed precision also updates the
+        # FP64 displacement (read + write 64 B) and its FP32 mirror (16 B)
+        mixed = params.precision == 1
+        return (40 + (80 if mixed else 0)) * n0 + 8 * nnz0
     if kernel == "k_ls_sweep_tc":
         # learned sweep: level-0 row walk (8 B/nnz, r/D/L/fix 28 B per row) + d read/write 32 B per row;
         # the 12.9 KB weight image per CTA comes from L2
@@ -654,7 +659,7 @@ def run_ours(args):
         # kernel-only device time per launch: every launch of a kernel repeated back to back
         # inside the frame's own chain (no event nodes between them); the state is restored
         replay = {}
-        for kname in prof:
+        for kname in ([] if args.no_replay else prof):
             if kname.startswith("k_bp_"):
                 continue
             try:
@@ -782,6 +787,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="beam")
+    ap.add_argument("--no-replay", action="store_true",
+                    help="roofline from the profiled frame only (no kernel replay frames: short ncu launch lists)")
     ap.add_argument("--cpu-frames", type=int, default=1000, help="most frames of the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="the CPU baseline runs frames until this much time has passed (at least 3 frames)")

@@ -261,7 +261,9 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
 // (use_cond != 0), and resets the ticket for the next launch.
 // With dd64 set (mixed precision) the kernel also applies the correction d to
 // the FP64 displacement (dd64 += d) and writes its FP32 mirror d32, the work
-// of k_mx_update.
+// of k_mx_update.  kSetCond: the instance that can set a conditional handle
+// (only the last check of a graph frame; profilers skip such kernels).
+template <bool kSetCond>
 __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col, const float* __restrict__ val,
     const float* __restrict__ dfull, const float* __restrict__ fixf, const float4* __restrict__ d,
@@ -326,7 +328,9 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_guard_residual(
     if (threadIdx.x == 0) {
         const int fail = fails > 0 ? 1 : 0;
         gate[0] = fail;
-        if (use_cond) cudaGraphSetConditional(cond, (unsigned)fail);
+        if constexpr (kSetCond) {
+            if (use_cond) cudaGraphSetConditional(cond, (unsigned)fail);
+        }
         stats[0] += (unsigned long long)(cycle + 1);
         stats[1] += (unsigned long long)fails;
         *ticket = 0u;

@@ -937,19 +937,26 @@ static_assert(kLsThreads == kBlock && kLsThreads / kLanesL0 == 64 && kMxThreads 
 void enqueue_learned_guard(mgsb_solver* h, const float4* d, const float4* b, int cycle, bool final,
                            const LearnedFallback& fb, double4* dd64 = nullptr, float4* d32 = nullptr) {
     const LevelDev& l0 = h->lev[0];
-    LAUNCH(h, k_ls_guard_residual, h->ls_nblk, kLsThreads, 0, h->N0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull,
-           h->fixf, d, b, cycle, final ? 1 : 0, h->ls_part0, h->ls_part1, h->ls_gamma * h->ls_gamma, h->ls_gate,
-           h->ls_stats, fb.hnd, (final && fb.cond) ? 1 : 0, h->ls_ticket, dd64, d32);
+    if (final && fb.cond)
+        LAUNCH(h, k_ls_guard_residual<true>, h->ls_nblk, kLsThreads, 0, h->N0, l0.slice_ptr, l0.ell_col, l0.ell_val,
+               l0.dfull, h->fixf, d, b, cycle, 1, h->ls_part0, h->ls_part1, h->ls_gamma * h->ls_gamma, h->ls_gate,
+               h->ls_stats, fb.hnd, 1, h->ls_ticket, dd64, d32);
+    else
+        LAUNCH(h, k_ls_guard_residual<false>, h->ls_nblk, kLsThreads, 0, h->N0, l0.slice_ptr, l0.ell_col, l0.ell_val,
+               l0.dfull, h->fixf, d, b, cycle, final ? 1 : 0, h->ls_part0, h->ls_part1, h->ls_gamma * h->ls_gamma,
+               h->ls_gate, h->ls_stats, fb.hnd, 0, h->ls_ticket, dd64, d32);
 }
 
 // Frame-level fallback of the learned smoother, before the frame's learned
 // solve: inside a stream capture, the handle of the IF node that will hold
-// the plain solve (reset to 0 at every launch of the graph).
+// the plain solve (reset to 0 at every launch of the graph).  A profiled
+// frame gets no IF node (profilers do not see the kernels of a graph that
+// holds conditional nodes): it is captured in two parts instead.
 LearnedFallback begin_learned_fallback(mgsb_solver* h) {
     LearnedFallback fb;
     cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(h->stream, &cst);
-    if (cst != cudaStreamCaptureStatusActive) return fb;
+    if (cst != cudaStreamCaptureStatusActive || h->profiling) return fb;
     cudaGraph_t g = nullptr;
     if (!h->aux_stream || cudaStreamGetCaptureInfo(h->stream, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess ||
         cudaGraphConditionalHandleCreate(&fb.hnd, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
@@ -962,16 +969,38 @@ LearnedFallback begin_learned_fallback(mgsb_solver* h) {
 
 // After the learned solve: the plain solve (body) runs when the frame's last
 // check found a failed learned V-cycle.  In a capture it becomes the body of
-// an IF node (captured on the auxiliary stream, without profiling events:
-// event nodes may not sit in a conditional body); eagerly the host reads the
-// decision and enqueues it.
+// an IF node (captured on the auxiliary stream); eagerly the host reads the
+// decision and enqueues it.  A profiled frame (capture, no IF node) ends its
+// first part here, runs it, reads the decision and captures the rest of the
+// frame (with the body when it is needed) as its second part on the same
+// stream.
 template <typename Body>
 void end_learned_fallback(mgsb_solver* h, const LearnedFallback& fb, Body&& body) {
     cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(h->stream, &cst);
     if (!fb.cond) {
-        if (cst != cudaStreamCaptureStatusNone) {
+        if (cst != cudaStreamCaptureStatusNone && !h->profiling) {
             h->capture_error = true;
+            return;
+        }
+        if (cst != cudaStreamCaptureStatusNone) {   // profiled frame: run the first part now
+            cudaGraph_t g1 = nullptr;
+            cudaGraphExec_t ge1 = nullptr;
+            cudaError_t e = cudaStreamEndCapture(h->stream, &g1);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&ge1, g1, 0);
+            if (e == cudaSuccess) e = cudaGraphLaunch(ge1, h->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+            if (ge1) cudaGraphExecDestroy(ge1);
+            if (g1) cudaGraphDestroy(g1);
+            int32_t g = 0;
+            if (e == cudaSuccess) e = cudaMemcpy(&g, h->ls_gate, sizeof g, cudaMemcpyDeviceToHost);
+            const cudaError_t eb = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) e = eb;
+            if (e != cudaSuccess) {
+                h->enqueue_status = set_err(h, MGSB_CUDA_ERROR, "profiled frame, first part: %s", cudaGetErrorString(e));
+                return;
+            }
+            if (g) body();
             return;
         }
         int32_t g = 0;
@@ -1002,12 +1031,9 @@ void end_learned_fallback(mgsb_solver* h, const LearnedFallback& fb, Body&& body
         return;
     }
     cudaStream_t main_stream = h->stream;
-    const bool prof = h->profiling;
     const int launches = h->launches;
     h->stream = h->aux_stream;
-    h->profiling = false;
     body();
-    h->profiling = prof;
     h->launches = launches;   // launches_per_frame counts the frame that runs when every check passes
     cudaGraph_t bg = nullptr;
     if (cudaStreamEndCapture(h->stream, &bg) != cudaSuccess) h->capture_error = true;

@@ -122,6 +122,38 @@ def test_guard_falls_back_to_plain_mixed(lib, graph):
     assert np.array_equal(runs[True], runs[False])
 
 
+@pytest.mark.parametrize("wild", [False, True])
+def test_profiled_frame_equals_graph_frame(lib, trained, wild):
+    """A profiled frame (captured in two parts around the learned solve's
+    decision, no conditional node) advances the run exactly as a frame of
+    the solver's own graph, with and without the plain fallback; the
+    profile lists the frame's kernels, the fallback's when it ran."""
+    m, fixed = beam(4, 40, 4)
+    net = trained[0]
+    if wild:
+        net = MLP(seed=13)
+        net.params = np.random.default_rng(2).normal(0.0, 30.0, NUM_PARAMS).astype(np.float32)
+    p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=1)
+    path = capsule_path(6, start=(0.0, 0.0, 1.3))
+    runs = []
+    for profiled in (False, True):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        s.set_learned_smoother(net, 0.5)
+        for f, (a, b) in enumerate(path):
+            s.set_capsule(a, b, 0.3)
+            if profiled and f == 4:
+                prof = s.profile_frame()
+                assert prof["k_ls_sweep_tc"][1] == 2 * p.iterations
+                assert ("k_mx_update" in prof) == wild   # the plain solve of the fallback
+            else:
+                s.step()
+        runs.append((s.positions_f64(), s.learned_stats()))
+        s.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1]
+
+
 def test_learned_mixed_matches_oracle(lib, oracle_built, trained):
     """Learned smoother + mixed precision (FP64 residual, 3 refinement passes)
     against the FP64 oracle running plain V-cycles with the same passes: the
@@ -162,7 +194,7 @@ def test_time_kernel_learned_cycle_restores_state(lib, trained):
         for f, (a, b) in enumerate(path):
             s.set_capsule(a, b, 0.3)
             if timed and f == 4:
-                for name in ("k_ls_sweep_tc", "k_ls_guard_residual", "k_mx_residual", "k_coarse_vcycle"):
+                for name in ("k_ls_sweep_tc", "k_ls_guard_residual<false>", "k_mx_residual", "k_coarse_vcycle"):
                     us, k = s.time_kernel(name, 8)
                     assert us > 0.0 and k >= 1, (name, us, k)
                 assert s.time_kernel("k_ls_sweep_tc", 1)[1] == 2 * p.iterations
