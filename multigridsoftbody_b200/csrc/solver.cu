@@ -1165,7 +1165,7 @@ void enqueue_mg_frame(mgsb_solver* h) {
     else if (h->nsurf > 0)
         LAUNCH(h, k_contact_all, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bodies_dev, h->s,
                h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target);
-    const bool learned = h->ls_net != nullptr;
+    const bool learned = h->ls_net != nullptr && h->p.iterations > 0 && h->p.refinement_passes > 0;
     const LearnedFallback fb = learned ? begin_learned_fallback(h) : LearnedFallback{};
     float4* d = enqueue_mg_solve(h, learned, fb);
     if (learned)   // a failed learned V-cycle: the frame's solve again with the plain V-cycle
@@ -1238,7 +1238,7 @@ void enqueue_mixed_frame(mgsb_solver* h) {
     LAUNCH(h, k_mx_predict, grid_for(n0), kBlock, 0, n0, h->x64, h->v64, h->s64, h->last64, h->s, h->x, h->fixf,
            h->body_of, h->bodies_dev, (double)p.dt);
     if (h->nsurf > 0 && h->broad_phase) enqueue_broad_phase(h, h->s, false);
-    const bool learned = h->ls_net != nullptr;
+    const bool learned = h->ls_net != nullptr && h->p.iterations > 0 && h->p.refinement_passes > 0;
     const LearnedFallback fb = learned ? begin_learned_fallback(h) : LearnedFallback{};
     enqueue_mixed_solve(h, learned, fb);
     if (learned)   // a failed learned V-cycle: the frame's solve again with the plain V-cycle
