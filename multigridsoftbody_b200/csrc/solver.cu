@@ -1422,7 +1422,8 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     }
     auto& pool = h->state_mem;
     const int N0 = h->N0;
-    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback, (size_t)std::max(N0, 1) * sizeof(float4)));
+    // N0 float4 + the non-finite flag that every readback fetches with its data
+    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback, (size_t)std::max(N0, 1) * sizeof(float4) + 16));
     TRY(dalloc(hp, pool, &h->x, N0));
     TRY(dalloc(hp, pool, &h->xb, N0));
     TRY(dalloc(hp, pool, &h->v, N0));
@@ -1465,13 +1466,25 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     return MGSB_OK;
 }
 
+// Device -> pinned readback buffer, together with the non-finite flag, in one
+// stream synchronisation: MGSB_DIVERGED when the flag is set (the caller then
+// writes nothing).
+mgsb_status readback_checked(mgsb_solver* h, const void* src, size_t bytes) {
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    int32_t* flag = reinterpret_cast<int32_t*>(h->readback + (size_t)std::max(h->N0, 1) * sizeof(float4));
+    CUDA_TRY(h, cudaMemcpyAsync(flag, h->nonfinite, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (bytes) CUDA_TRY(h, cudaMemcpyAsync(h->readback, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (*flag) return set_err(h, MGSB_DIVERGED, "non-finite positions detected");
+    return MGSB_OK;
+}
+
 template <typename F>
 mgsb_status copy_body_f4(mgsb_solver* h, int32_t body, const float4* src, F&& sink) {
     TRY(check_body(h, body));
     const BodyHost& B = h->bodies[body];
-    float4* tmp = reinterpret_cast<float4*>(h->readback);
-    CUDA_TRY(h, cudaMemcpyAsync(tmp, src + B.v_off, B.V * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    TRY(readback_checked(h, src + B.v_off, B.V * sizeof(float4)));
+    const float4* tmp = reinterpret_cast<const float4*>(h->readback);
     for (int i = 0; i < B.V; ++i) sink(i, tmp[i]);
     return MGSB_OK;
 }
@@ -1638,7 +1651,6 @@ mgsb_status mgsb_synchronize(mgsb_solver* h) {
 mgsb_status mgsb_get_positions(mgsb_solver* h, int32_t body, float* out) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
-    TRY(sync_check(h));
     return copy_body_f4(h, body, h->x, [&](int i, float4 v) {
         out[3 * i] = v.x;
         out[3 * i + 1] = v.y;
@@ -1670,10 +1682,8 @@ mgsb_status mgsb_get_velocities(mgsb_solver* h, int32_t body, float* out) {
 
 mgsb_status mgsb_get_all_positions(mgsb_solver* h, float* out) {
     if (!h || !out) return MGSB_INVALID_ARG;
-    TRY(sync_check(h));
+    TRY(readback_checked(h, h->x, h->N0 * sizeof(float4)));
     const float4* tmp = reinterpret_cast<const float4*>(h->readback);
-    CUDA_TRY(h, cudaMemcpyAsync(h->readback, h->x, h->N0 * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     for (int i = 0; i < h->N0; ++i) {
         out[3 * i] = tmp[i].x;
         out[3 * i + 1] = tmp[i].y;
@@ -1701,19 +1711,15 @@ mgsb_status mgsb_get_positions_f64(mgsb_solver* h, int32_t body, double* out) {
 mgsb_status mgsb_get_contact_flags(mgsb_solver* h, int32_t body, int32_t* out) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
-    TRY(sync_check(h));
     const BodyHost& B = h->bodies[body];
-    CUDA_TRY(h, cudaMemcpyAsync(h->readback, h->cflag + B.v_off, B.V * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    TRY(readback_checked(h, h->cflag + B.v_off, B.V * sizeof(int32_t)));
     std::memcpy(out, h->readback, B.V * sizeof(int32_t));
     return MGSB_OK;
 }
 
 mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out) {
     if (!h || !out) return MGSB_INVALID_ARG;
-    TRY(sync_check(h));
-    CUDA_TRY(h, cudaMemcpyAsync(h->readback, h->cflag, h->N0 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    TRY(readback_checked(h, h->cflag, h->N0 * sizeof(int32_t)));
     std::memcpy(out, h->readback, h->N0 * sizeof(int32_t));
     return MGSB_OK;
 }

@@ -122,8 +122,9 @@ def test_guard_falls_back_to_plain_mixed(lib, graph):
     assert np.array_equal(runs[True], runs[False])
 
 
+@pytest.mark.parametrize("precision", [mg.PRECISION_MIXED, mg.PRECISION_FP32])
 @pytest.mark.parametrize("wild", [False, True])
-def test_profiled_frame_equals_graph_frame(lib, trained, wild):
+def test_profiled_frame_equals_graph_frame(lib, trained, wild, precision):
     """A profiled frame (captured in two parts around the learned solve's
     decision, no conditional node) advances the run exactly as a frame of
     the solver's own graph, with and without the plain fallback; the
@@ -133,8 +134,9 @@ def test_profiled_frame_equals_graph_frame(lib, trained, wild):
     if wild:
         net = MLP(seed=13)
         net.params = np.random.default_rng(2).normal(0.0, 30.0, NUM_PARAMS).astype(np.float32)
-    p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=1)
+    p = mg_params(levels=3, precision=precision, refinement_passes=1)
     path = capsule_path(6, start=(0.0, 0.0, 1.3))
+    mixed = precision == mg.PRECISION_MIXED
     runs = []
     for profiled in (False, True):
         s = mg.Solver(m, p)
@@ -143,12 +145,17 @@ def test_profiled_frame_equals_graph_frame(lib, trained, wild):
         for f, (a, b) in enumerate(path):
             s.set_capsule(a, b, 0.3)
             if profiled and f == 4:
+                failed_before = s.learned_stats()[1]
                 prof = s.profile_frame()
                 assert prof["k_ls_sweep_tc"][1] == 2 * p.iterations
-                assert ("k_mx_update" in prof) == wild   # the plain solve of the fallback
+                # the plain solve of the fallback runs exactly when a check of this frame failed
+                plain_kernel = "k_mx_update" if mixed else "k_l0_sweep_rg"
+                assert (plain_kernel in prof) == (s.learned_stats()[1] > failed_before)
+                if wild:
+                    assert plain_kernel in prof
             else:
                 s.step()
-        runs.append((s.positions_f64(), s.learned_stats()))
+        runs.append((s.positions_f64() if mixed else s.positions(), s.learned_stats()))
         s.close()
     assert np.array_equal(runs[0][0], runs[1][0])
     assert runs[0][1] == runs[1][1]
