@@ -425,39 +425,98 @@ def train_network(mg, name, device, stream_ptr, runs=8, frames=40, every=10, swe
     return net, info
 
 
-def accuracy(mg, meshes, fixeds, params, tool, net, frames=40):
-    """Max vertex error / bbox diagonal after `frames` frames from rest, against a converged reference
-    (mixed precision with 6 FP64-residual V-cycles per PD iteration, plain smoother) on the GPU."""
+def accuracy(mg, meshes, fixeds, params, tool, net, variants, frames=40):
+    """Max vertex error / bbox diagonal after `frames` frames of the timed tool path from rest, against the
+    converged solver (mixed precision with 6 FP64-residual V-cycles per PD iteration, plain smoother), for
+    each (sweeps, passes, learned) variant."""
     m, fixed = meshes[0], fixeds[0]
-
-    def run(prec, passes, learned):
-        p = type(params[0]).from_buffer_copy(params[0])
-        p.precision = prec
-        p.refinement_passes = passes
-        s = mg.Solver(m, p)
-        s.set_fixed(fixed)
-        if learned:
-            s.set_learned_smoother(net, 0.5)
-        for f in range(frames):
-            apply_tool(s, tool(f))
-            s.step()
-        x = s.positions_f64() if prec == mg.PRECISION_MIXED else s.positions().astype(np.float64)
-        stats = s.learned_stats() if learned else None
-        s.close()
-        return x, stats
-
-    ref, _ = run(mg.PRECISION_MIXED, 6, False)
+    ref = converged_positions(mg, m, fixed, params[0], tool, frames)
     diag = m.bbox_diagonal()
     out = {"frames": frames, "reference": "GPU mixed precision, 6 V-cycles (FP64 residual) per PD iteration, "
                                           "plain smoother; matches the FP64 oracle to ~1e-7 m"}
-    for key, prec, passes, learned in (("learned_mixed_%dpass" % params[0].refinement_passes, mg.PRECISION_MIXED,
-                                        params[0].refinement_passes, True),
-                                       ("plain_fp32_1pass", mg.PRECISION_FP32, 1, False),
-                                       ("plain_fp32_2pass", mg.PRECISION_FP32, 2, False)):
-        x, st = run(prec, passes, learned)
+    for sweeps, passes, learned in variants:
+        key = variant_key(sweeps, passes, learned)
+        if key in out:
+            continue
+        p = variant_params(mg, params[0], sweeps, passes, learned)
+        x, st = run_positions(mg, m, fixed, p, net if learned else None, tool, frames)
         out[key] = {"err_over_diag": float(np.abs(x - ref).max() / diag)}
         if st:
-            out[key]["learned_vcycles"], out[key]["fallbacks"] = st
+            out[key]["learned_vcycles"], out[key]["failed_checks"] = st
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Sweep counts picked by accuracy, with the same search for both solver families
+# ---------------------------------------------------------------------------
+ERROR_BAR = 1e-5   # max vertex error / bbox diagonal after 40 frames
+LEARNED_CANDIDATES = (((2, 2), 1), ((1, 1), 1))                       # (pre/post sweeps, passes)
+PLAIN_CANDIDATES = (((2, 2), 1), ((2, 2), 2), ((1, 1), 1), ((1, 1), 2), ((1, 1), 3))
+
+
+def held_out_tool(name):
+    """The workload's tool motion with another seed: the selection never sees the timed path."""
+    from multigridsoftbody_b200.learned import blob_tool_path
+    path = blob_tool_path(64, seed=301) if name == "blob" else capsule_path(64, start=(0.0, 0.0, 1.5), seed=301)
+
+    def tool(f):
+        a, b = path[f % len(path)]
+        return a[None], b[None], np.array([0.3], np.float32)
+
+    return tool
+
+
+def variant_params(mg, base, sweeps, passes, learned):
+    p = type(base).from_buffer_copy(base)
+    p.pre_sweeps, p.post_sweeps = sweeps
+    p.refinement_passes = passes
+    p.precision = mg.PRECISION_MIXED if learned else mg.PRECISION_FP32
+    return p
+
+
+def variant_key(sweeps, passes, learned):
+    return "%s_%dpass_%d+%d" % ("learned_mixed" if learned else "plain_fp32", passes, sweeps[0], sweeps[1])
+
+
+def run_positions(mg, m, fixed, p, net, tool, frames):
+    s = mg.Solver(m, p)
+    s.set_fixed(fixed)
+    if net is not None:
+        s.set_learned_smoother(net, 0.5)
+    for f in range(frames):
+        apply_tool(s, tool(f))
+        s.step()
+    x = s.positions_f64() if p.precision == mg.PRECISION_MIXED else s.positions().astype(np.float64)
+    stats = s.learned_stats() if net is not None else None
+    s.close()
+    return x, stats
+
+
+def converged_positions(mg, m, fixed, base, tool, frames):
+    """Mixed precision, 6 FP64-residual V-cycles (2+2 sweeps) per PD iteration, plain smoother."""
+    return run_positions(mg, m, fixed, variant_params(mg, base, (2, 2), 6, True), None, tool, frames)[0]
+
+
+def select_sweeps(mg, meshes, fixeds, base, net, tool_sel, time_fn, frames=40):
+    """For each family (learned + mixed; plain FP32), every candidate's error after `frames` frames
+    of a held-out tool path against the converged solver, and the frame time (time_fn) of those within
+    the bar; the fastest of those is the family's choice (None when none qualifies)."""
+    m, fixed = meshes[0], fixeds[0]
+    ref = converged_positions(mg, m, fixed, base, tool_sel, frames)
+    diag = m.bbox_diagonal()
+    out = {"held_out_path": "same motion, tool seed 301", "frames": frames}
+    for fam, cands, learned in (("learned_mixed", LEARNED_CANDIDATES, True), ("plain_fp32", PLAIN_CANDIDATES, False)):
+        rows = []
+        for sweeps, passes in cands:
+            p = variant_params(mg, base, sweeps, passes, learned)
+            x, _ = run_positions(mg, m, fixed, p, net if learned else None, tool_sel, frames)
+            row = {"key": variant_key(sweeps, passes, learned), "sweeps": list(sweeps), "passes": passes,
+                   "err_over_diag": float(np.abs(x - ref).max() / diag)}
+            if row["err_over_diag"] <= ERROR_BAR:
+                row["ms_per_frame"] = time_fn(p, net if learned else None)
+            rows.append(row)
+        ok = [r for r in rows if "ms_per_frame" in r]
+        out[fam] = {"candidates": rows, "chosen": min(ok, key=lambda r: r["ms_per_frame"]) if ok else None}
     return out
 
 
@@ -597,6 +656,59 @@ def run_ours(args):
         net, net_info = train_network(mg, args.workload, local, stream.cuda_stream)
         if args.save_weights and rank == 0:
             np.save(args.save_weights, net.params)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def time_config(p, netx, tool_t, frames=60, warm=10):
+        """ms per frame of one solver configuration: autotuned shape, L2 flushed before every frame."""
+        sv = mg.Solver(meshes, [p])
+        sv.set_fixed(fixeds[0])
+        if netx is not None:
+            sv.set_learned_smoother(netx, 0.5)
+        if not args.no_tune:
+            sv.autotune(frames=5)
+        with torch.cuda.stream(stream):
+            for f in range(warm):
+                apply_tool(sv, tool_t(f))
+                sv.step()
+            sv.synchronize()
+            tev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+            for k in range(frames):
+                flush.zero_()
+                tev[k][0].record(stream)
+                apply_tool(sv, tool_t(warm + k))
+                sv.step()
+                tev[k][1].record(stream)
+            sv.synchronize()
+        sv.close()
+        return sum(a.elapsed_time(b) for a, b in tev) / frames
+
+    # sweep counts of the learned solver: picked by accuracy on a held-out tool path (the plain
+    # solver gets the same search for the comparison), or given, or the workload's
+    selection, sweeps_source = None, "workload default"
+    workload_params = [type(p).from_buffer_copy(p) for p in params]   # the CPU baseline runs these
+    if args.sweeps:
+        pre, post = (int(v) for v in args.sweeps.split(","))
+        for p in params:
+            p.pre_sweeps, p.post_sweeps = pre, post
+        sweeps_source = "--sweeps"
+    elif net is not None and not args.no_compare and len(meshes) == 1:
+        selection = select_sweeps(mg, meshes, fixeds, params[0], net, held_out_tool(args.workload),
+                                  lambda p, netx: time_config(p, netx, held_out_tool(args.workload)))
+        choice = selection["learned_mixed"]["chosen"]
+        if dist is not None:   # every rank runs rank 0's choice
+            box = [choice]
+            dist.broadcast_object_list(box, src=0)
+            choice = box[0]
+        if choice is not None:
+            params[0].pre_sweeps, params[0].post_sweeps = choice["sweeps"]
+            params[0].refinement_passes = choice["passes"]
+            sweeps_source = "selected by accuracy on a held-out tool path"
     solver = mg.Solver(meshes, params)
     for b, fx in enumerate(fixeds):
         solver.set_fixed(fx, body=b)
@@ -606,13 +718,6 @@ def run_ours(args):
         solver.set_learned_smoother(net, 0.5)
     if args.broad_phase:
         solver.set_broad_phase(True)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-            torch.cuda.synchronize()
 
     frame = 0
     tuned = solver.autotune(frames=5) if not args.no_tune else None
@@ -667,13 +772,22 @@ def run_ours(args):
             except mg.MgsbError:
                 continue
             replay[kname] = (us, cnt)
-        # the plain FP32 multigrid (1 and 2 V-cycles per PD iteration), timed the same way
-        plain_ms = {}
+        # the plain FP32 multigrid, timed the same way: the configured form (1 V-cycle, 2+2 sweeps)
+        # and every form that met the error bar in the selection
+        plain_ms, plain_forms = {}, {}
         if net is not None and not args.no_compare:
-            for passes in (1, 2):
-                pp = type(params[0]).from_buffer_copy(params[0])
-                pp.precision = mg.PRECISION_FP32
-                pp.refinement_passes = passes
+            forms = [((2, 2), 1)]
+            if selection:
+                forms += [(tuple(r["sweeps"]), r["passes"]) for r in selection["plain_fp32"]["candidates"]
+                          if "ms_per_frame" in r]
+            if dist is not None:   # every rank times rank 0's list
+                box = [forms]
+                dist.broadcast_object_list(box, src=0)
+                forms = box[0]
+            for sweeps, passes in forms:
+                plain_forms.setdefault(variant_key(sweeps, passes, False), (tuple(sweeps), passes))
+            for key, (sweeps, passes) in plain_forms.items():
+                pp = variant_params(mg, params[0], sweeps, passes, False)
                 sv = mg.Solver(meshes, [pp])
                 sv.set_fixed(fixeds[0])
                 if not args.no_tune:
@@ -693,39 +807,40 @@ def run_ours(args):
                     pevs[k][1].record(stream)
                 sv.synchronize()
                 barrier()
-                plain_ms[passes] = sum(a.elapsed_time(b) for a, b in pevs)
+                plain_ms[key] = sum(a.elapsed_time(b) for a, b in pevs)
                 sv.close()
     from multigridsoftbody_b200.replicas import job_throughput, max_over_ranks
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist)
     comparison = None
     if net is not None and not args.no_compare:
-        p1, p2 = max_over_ranks([plain_ms[1], plain_ms[2]], dist)
-        comparison = {"plain_fp32_1pass": {"frames_per_s": job_throughput(args.steps, world, p1),
-                                           "ms_per_step": p1 / args.steps},
-                      "plain_fp32_2pass": {"frames_per_s": job_throughput(args.steps, world, p2),
-                                           "ms_per_step": p2 / args.steps},
-                      "network": net_info}
-        comparison["ratio_vs_plain_fp32_1pass"] = job_throughput(args.steps, world, ms) / comparison[
-            "plain_fp32_1pass"]["frames_per_s"]
-        comparison["ratio_vs_plain_fp32_2pass"] = job_throughput(args.steps, world, ms) / comparison[
-            "plain_fp32_2pass"]["frames_per_s"]
+        keys = list(plain_ms)
+        times = max_over_ranks([plain_ms[k] for k in keys], dist)
+        learned_key = variant_key((params[0].pre_sweeps, params[0].post_sweeps), params[0].refinement_passes, True)
+        comparison = {"learned": learned_key, "sweeps_source": sweeps_source, "network": net_info,
+                      "error_bar_over_diag": ERROR_BAR, "selection": selection}
+        for k, t in zip(keys, times):
+            comparison[k] = {"frames_per_s": job_throughput(args.steps, world, t), "ms_per_step": t / args.steps,
+                             "ratio": job_throughput(args.steps, world, ms) / job_throughput(args.steps, world, t)}
         if rank == 0 and world == 1:
-            acc = accuracy(mg, meshes, fixeds, params, tool, net)
+            variants = [((params[0].pre_sweeps, params[0].post_sweeps), params[0].refinement_passes, True)]
+            variants += [(sw, ps, False) for sw, ps in plain_forms.values()]
+            acc = accuracy(mg, meshes, fixeds, params, tool, net, variants)
             comparison["accuracy"] = acc
-            # the headline ratio: against the cheapest plain FP32 form that meets the error bar
-            bar = 1e-5
-            key = "learned_mixed_%dpass" % params[0].refinement_passes
-            comparison["error_bar_over_diag"] = bar
-            comparison["learned_meets_bar"] = acc[key]["err_over_diag"] <= bar
-            for passes in (1, 2):
-                if acc["plain_fp32_%dpass" % passes]["err_over_diag"] <= bar:
-                    comparison["plain_fp32_at_bar"] = "plain_fp32_%dpass" % passes
-                    comparison["ratio_vs_plain_fp32_at_bar"] = comparison["ratio_vs_plain_fp32_%dpass" % passes]
-                    break
+            comparison["learned_meets_bar"] = acc[learned_key]["err_over_diag"] <= ERROR_BAR
+            # the headline ratio: against the fastest timed plain FP32 form that meets the bar on this path
+            at_bar = [k for k in keys if acc[k]["err_over_diag"] <= ERROR_BAR]
+            if at_bar:
+                best = min(at_bar, key=lambda k: comparison[k]["ms_per_step"])
+                comparison["plain_fp32_at_bar"] = best
+                comparison["ratio_vs_plain_fp32_at_bar"] = comparison[best]["ratio"]
     value = job_throughput(args.steps, world, ms)
     e2e_value = job_throughput(args.steps, world, e2e_ms)
     if rank == 0:
         launches = solver.launches_per_frame()
+        if net is not None and comparison is not None:
+            # every learned V-cycle this solver ran (warm-up, timed, e2e, profiled and replayed frames):
+            # checks, and checks failed (a frame with a failed check was recomputed with plain V-cycles)
+            comparison["learned_checks_this_solver"] = list(solver.learned_stats())
         if replay:   # dominant kernel by its kernel-only time per frame
             kname = max(replay, key=lambda k: replay[k][0] * replay[k][1])
             kavg_ms = replay[kname][0] / 1e3
@@ -748,10 +863,12 @@ def run_ours(args):
                     "avg_launch_ms_profiled": prof[kname][0] / max(prof[kname][1], 1)}
         cpu = None
         if world == 1 and not args.no_cpu:
-            fps, nfr, dt = cpu_frames_per_s(meshes, params, fixeds, tool, mats, frames=args.cpu_frames,
+            fps, nfr, dt = cpu_frames_per_s(meshes, workload_params, fixeds, tool, mats, frames=args.cpu_frames,
                                             seconds=args.cpu_seconds)
             cpu = {"value": fps, "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"{nfr} frames of the same workload, FP64 oracle ({dt:.1f} s)"}
+                   "sample": f"{nfr} frames of the same workload, FP64 oracle of its plain iteration "
+                             f"({workload_params[0].pre_sweeps}+{workload_params[0].post_sweeps} sweeps, "
+                             f"{workload_params[0].refinement_passes} pass; {dt:.1f} s)"}
         h2d = len(meshes) * 88 + 164          # body table (88 B per body) + sphere set per frame
         d2h = nverts * 16 + nverts * 4        # float4 positions + contact flags
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -763,7 +880,9 @@ def run_ours(args):
                            "parallelism": f"replicas x{world}",
                            "l2": "flushed (256 MB write) before every timed frame, outside the timed span",
                            "autotuned_coarse_kernel": tuned,
-                           "contact_broad_phase": "uniform grid" if args.broad_phase else "all surface vertices"},
+                           "contact_broad_phase": "uniform grid" if args.broad_phase else "all surface vertices",
+                           "sweeps_per_level": [params[0].pre_sweeps, params[0].post_sweeps],
+                           "refinement_passes": params[0].refinement_passes, "sweeps_source": sweeps_source},
                 "clocks": clk.summary(),
                 "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches * args.steps,
@@ -787,6 +906,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="beam")
+    ap.add_argument("--sweeps", default=None,
+                    help="PRE,POST sweeps per level (default: picked by accuracy for the learned workloads)")
     ap.add_argument("--no-replay", action="store_true",
                     help="roofline from the profiled frame only (no kernel replay frames: short ncu launch lists)")
     ap.add_argument("--cpu-frames", type=int, default=1000, help="most frames of the CPU baseline sample")
