@@ -1,0 +1,102 @@
+"""The bench's sweep-count selection (bench.py:select_sweeps) on a fake solver
+module, no GPU: each family gets the fastest candidate whose error against the
+converged solver stays within the bar, candidates outside the bar are not
+timed, and a family with no candidate within the bar gets no choice."""
+import ctypes
+
+import numpy as np
+
+import bench
+
+
+class FakeParams(ctypes.Structure):
+    _fields_ = [("pre_sweeps", ctypes.c_int32), ("post_sweeps", ctypes.c_int32),
+                ("refinement_passes", ctypes.c_int32), ("precision", ctypes.c_int32)]
+
+
+class FakeMesh:
+    def bbox_diagonal(self):
+        return 10.0
+
+
+def fake_mg(error_of):
+    """A module whose solvers end at positions error_of(params, learned) away from the converged ones."""
+
+    class Solver:
+        def __init__(self, mesh, p):
+            self.p = p
+            self.learned = False
+
+        def set_fixed(self, fixed):
+            pass
+
+        def set_learned_smoother(self, net, ratio):
+            self.learned = True
+
+        def set_capsule(self, a, b, r):
+            pass
+
+        def step(self):
+            pass
+
+        def _x(self):
+            converged = (self.p.refinement_passes == 6 and not self.learned)
+            return np.full((4, 3), 0.0 if converged else error_of(self.p, self.learned))
+
+        def positions_f64(self):
+            return self._x()
+
+        def positions(self):
+            return self._x().astype(np.float32)
+
+        def learned_stats(self):
+            return (1, 0)
+
+        def close(self):
+            pass
+
+    class M:
+        PRECISION_FP32 = 0
+        PRECISION_MIXED = 1
+
+    M.Solver = Solver
+    return M
+
+
+def tool(f):
+    z = np.zeros((1, 3), np.float32)
+    return z, z, np.array([0.3], np.float32)
+
+
+def test_fastest_candidate_within_the_bar():
+    def err(p, learned):   # error / diag = value / 10
+        if learned:
+            return 5e-5 if p.pre_sweeps == 1 else 4e-5              # both within 1e-5 * 10
+        return 2e-4 / (p.refinement_passes * p.pre_sweeps)          # within the bar from 2 x 2+2 / 3 x ... on
+
+    def cost(p, net):
+        return p.refinement_passes * (p.pre_sweeps + 1.0) + (0.5 if net is not None else 0.0)
+
+    timed = []
+
+    def time_fn(p, net):
+        timed.append((p.pre_sweeps, p.refinement_passes, net is not None))
+        return cost(p, net)
+
+    mg = fake_mg(err)
+    base = FakeParams(2, 2, 1, 1)
+    out = bench.select_sweeps(mg, [FakeMesh()], [None], base, object(), tool, time_fn, frames=2)
+    assert out["learned_mixed"]["chosen"]["key"] == "learned_mixed_1pass_1+1"
+    # plain: 2+2 x 1 pass has 1e-5 (bar met exactly: <=), 1+1 x 1 pass 2e-5 (not timed)
+    assert out["plain_fp32"]["chosen"]["key"] == "plain_fp32_1pass_2+2"
+    assert (1, 1, False) not in timed
+    for fam in ("learned_mixed", "plain_fp32"):
+        for r in out[fam]["candidates"]:
+            assert ("ms_per_frame" in r) == (r["err_over_diag"] <= bench.ERROR_BAR)
+
+
+def test_no_candidate_within_the_bar():
+    mg = fake_mg(lambda p, learned: 1.0)
+    out = bench.select_sweeps(mg, [FakeMesh()], [None], FakeParams(2, 2, 1, 1), object(), tool,
+                              lambda p, net: 1.0, frames=2)
+    assert out["learned_mixed"]["chosen"] is None and out["plain_fp32"]["chosen"] is None
