@@ -429,17 +429,18 @@ def accuracy(mg, meshes, fixeds, params, tool, net, variants, frames=40):
     """Max vertex error / bbox diagonal after `frames` frames of the timed tool path from rest, against the
     converged solver (mixed precision with 6 FP64-residual V-cycles per PD iteration, plain smoother), for
     each (sweeps, passes, learned) variant."""
+    from multigridsoftbody_b200 import sweeps as sw
     m, fixed = meshes[0], fixeds[0]
-    ref = converged_positions(mg, m, fixed, params[0], tool, frames)
+    ref = sw.converged_positions(m, fixed, params[0], tool, frames)
     diag = m.bbox_diagonal()
     out = {"frames": frames, "reference": "GPU mixed precision, 6 V-cycles (FP64 residual) per PD iteration, "
                                           "plain smoother; matches the FP64 oracle to ~1e-7 m"}
     for sweeps, passes, learned in variants:
-        key = variant_key(sweeps, passes, learned)
+        key = sw.variant_key(sweeps, passes, learned)
         if key in out:
             continue
-        p = variant_params(mg, params[0], sweeps, passes, learned)
-        x, st = run_positions(mg, m, fixed, p, net if learned else None, tool, frames)
+        p = sw.variant_params(params[0], sweeps, passes, learned)
+        x, st = sw.run_positions(m, fixed, p, net if learned else None, tool, frames)
         out[key] = {"err_over_diag": float(np.abs(x - ref).max() / diag)}
         if st:
             out[key]["learned_vcycles"], out[key]["failed_checks"] = st
@@ -447,11 +448,9 @@ def accuracy(mg, meshes, fixeds, params, tool, net, variants, frames=40):
 
 
 # ---------------------------------------------------------------------------
-# Sweep counts picked by accuracy, with the same search for both solver families
+# Sweep counts picked by accuracy (multigridsoftbody_b200.sweeps), the same search for both families
 # ---------------------------------------------------------------------------
 ERROR_BAR = 1e-5   # max vertex error / bbox diagonal after 40 frames
-LEARNED_CANDIDATES = (((2, 2), 1), ((1, 1), 1))                       # (pre/post sweeps, passes)
-PLAIN_CANDIDATES = (((2, 2), 1), ((2, 2), 2), ((1, 1), 1), ((1, 1), 2), ((1, 1), 3))
 
 
 def held_out_tool(name):
@@ -464,60 +463,6 @@ def held_out_tool(name):
         return a[None], b[None], np.array([0.3], np.float32)
 
     return tool
-
-
-def variant_params(mg, base, sweeps, passes, learned):
-    p = type(base).from_buffer_copy(base)
-    p.pre_sweeps, p.post_sweeps = sweeps
-    p.refinement_passes = passes
-    p.precision = mg.PRECISION_MIXED if learned else mg.PRECISION_FP32
-    return p
-
-
-def variant_key(sweeps, passes, learned):
-    return "%s_%dpass_%d+%d" % ("learned_mixed" if learned else "plain_fp32", passes, sweeps[0], sweeps[1])
-
-
-def run_positions(mg, m, fixed, p, net, tool, frames):
-    s = mg.Solver(m, p)
-    s.set_fixed(fixed)
-    if net is not None:
-        s.set_learned_smoother(net, 0.5)
-    for f in range(frames):
-        apply_tool(s, tool(f))
-        s.step()
-    x = s.positions_f64() if p.precision == mg.PRECISION_MIXED else s.positions().astype(np.float64)
-    stats = s.learned_stats() if net is not None else None
-    s.close()
-    return x, stats
-
-
-def converged_positions(mg, m, fixed, base, tool, frames):
-    """Mixed precision, 6 FP64-residual V-cycles (2+2 sweeps) per PD iteration, plain smoother."""
-    return run_positions(mg, m, fixed, variant_params(mg, base, (2, 2), 6, True), None, tool, frames)[0]
-
-
-def select_sweeps(mg, meshes, fixeds, base, net, tool_sel, time_fn, frames=40):
-    """For each family (learned + mixed; plain FP32), every candidate's error after `frames` frames
-    of a held-out tool path against the converged solver, and the frame time (time_fn) of those within
-    the bar; the fastest of those is the family's choice (None when none qualifies)."""
-    m, fixed = meshes[0], fixeds[0]
-    ref = converged_positions(mg, m, fixed, base, tool_sel, frames)
-    diag = m.bbox_diagonal()
-    out = {"held_out_path": "same motion, tool seed 301", "frames": frames}
-    for fam, cands, learned in (("learned_mixed", LEARNED_CANDIDATES, True), ("plain_fp32", PLAIN_CANDIDATES, False)):
-        rows = []
-        for sweeps, passes in cands:
-            p = variant_params(mg, base, sweeps, passes, learned)
-            x, _ = run_positions(mg, m, fixed, p, net if learned else None, tool_sel, frames)
-            row = {"key": variant_key(sweeps, passes, learned), "sweeps": list(sweeps), "passes": passes,
-                   "err_over_diag": float(np.abs(x - ref).max() / diag)}
-            if row["err_over_diag"] <= ERROR_BAR:
-                row["ms_per_frame"] = time_fn(p, net if learned else None)
-            rows.append(row)
-        ok = [r for r in rows if "ms_per_frame" in r]
-        out[fam] = {"candidates": rows, "chosen": min(ok, key=lambda r: r["ms_per_frame"]) if ok else None}
-    return out
 
 
 # ---------------------------------------------------------------------------
@@ -631,6 +576,7 @@ def run_twolevel(args):
 def run_ours(args):
     import torch
     import multigridsoftbody_b200 as mg
+    from multigridsoftbody_b200 import sweeps as swp
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -698,8 +644,10 @@ def run_ours(args):
             p.pre_sweeps, p.post_sweeps = pre, post
         sweeps_source = "--sweeps"
     elif net is not None and not args.no_compare and len(meshes) == 1:
-        selection = select_sweeps(mg, meshes, fixeds, params[0], net, held_out_tool(args.workload),
-                                  lambda p, netx: time_config(p, netx, held_out_tool(args.workload)))
+        selection = swp.select_sweeps(meshes[0], fixeds[0], params[0], net, held_out_tool(args.workload),
+                                         time_fn=lambda p, netx: time_config(p, netx, held_out_tool(args.workload)),
+                                         bar=ERROR_BAR)
+        selection["held_out_path"] = "the workload's tool motion with tool seed 301"
         choice = selection["learned_mixed"]["chosen"]
         if dist is not None:   # every rank runs rank 0's choice
             box = [choice]
@@ -785,9 +733,9 @@ def run_ours(args):
                 dist.broadcast_object_list(box, src=0)
                 forms = box[0]
             for sweeps, passes in forms:
-                plain_forms.setdefault(variant_key(sweeps, passes, False), (tuple(sweeps), passes))
+                plain_forms.setdefault(swp.variant_key(sweeps, passes, False), (tuple(sweeps), passes))
             for key, (sweeps, passes) in plain_forms.items():
-                pp = variant_params(mg, params[0], sweeps, passes, False)
+                pp = swp.variant_params(params[0], sweeps, passes, False)
                 sv = mg.Solver(meshes, [pp])
                 sv.set_fixed(fixeds[0])
                 if not args.no_tune:
@@ -815,7 +763,8 @@ def run_ours(args):
     if net is not None and not args.no_compare:
         keys = list(plain_ms)
         times = max_over_ranks([plain_ms[k] for k in keys], dist)
-        learned_key = variant_key((params[0].pre_sweeps, params[0].post_sweeps), params[0].refinement_passes, True)
+        learned_key = swp.variant_key((params[0].pre_sweeps, params[0].post_sweeps), params[0].refinement_passes,
+                                         True)
         comparison = {"learned": learned_key, "sweeps_source": sweeps_source, "network": net_info,
                       "error_bar_over_diag": ERROR_BAR, "selection": selection}
         for k, t in zip(keys, times):

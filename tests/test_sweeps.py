@@ -1,12 +1,12 @@
-"""The bench's sweep-count selection (bench.py:select_sweeps) on a fake solver
-module, no GPU: each family gets the fastest candidate whose error against the
-converged solver stays within the bar, candidates outside the bar are not
-timed, and a family with no candidate within the bar gets no choice."""
+"""The sweep-count selection (multigridsoftbody_b200.sweeps.select_sweeps) on a
+fake solver class, no GPU: each family gets the fastest candidate whose error
+against the converged solver stays within the bar, candidates outside the bar
+are not timed, and a family with no candidate within the bar gets no choice."""
 import ctypes
 
 import numpy as np
 
-import bench
+from multigridsoftbody_b200 import sweeps
 
 
 class FakeParams(ctypes.Structure):
@@ -19,8 +19,8 @@ class FakeMesh:
         return 10.0
 
 
-def fake_mg(error_of):
-    """A module whose solvers end at positions error_of(params, learned) away from the converged ones."""
+def fake_solver(error_of):
+    """A solver class that ends at positions error_of(params, learned) away from the converged ones."""
 
     class Solver:
         def __init__(self, mesh, p):
@@ -55,12 +55,7 @@ def fake_mg(error_of):
         def close(self):
             pass
 
-    class M:
-        PRECISION_FP32 = 0
-        PRECISION_MIXED = 1
-
-    M.Solver = Solver
-    return M
+    return Solver
 
 
 def tool(f):
@@ -83,20 +78,24 @@ def test_fastest_candidate_within_the_bar():
         timed.append((p.pre_sweeps, p.refinement_passes, net is not None))
         return cost(p, net)
 
-    mg = fake_mg(err)
     base = FakeParams(2, 2, 1, 1)
-    out = bench.select_sweeps(mg, [FakeMesh()], [None], base, object(), tool, time_fn, frames=2)
+    out = sweeps.select_sweeps(FakeMesh(), None, base, object(), tool, time_fn, frames=2, solver_cls=fake_solver(err))
     assert out["learned_mixed"]["chosen"]["key"] == "learned_mixed_1pass_1+1"
     # plain: 2+2 x 1 pass has 1e-5 (bar met exactly: <=), 1+1 x 1 pass 2e-5 (not timed)
     assert out["plain_fp32"]["chosen"]["key"] == "plain_fp32_1pass_2+2"
     assert (1, 1, False) not in timed
     for fam in ("learned_mixed", "plain_fp32"):
         for r in out[fam]["candidates"]:
-            assert ("ms_per_frame" in r) == (r["err_over_diag"] <= bench.ERROR_BAR)
+            assert ("ms_per_frame" in r) == (r["err_over_diag"] <= sweeps.ERROR_BAR)
 
 
 def test_no_candidate_within_the_bar():
-    mg = fake_mg(lambda p, learned: 1.0)
-    out = bench.select_sweeps(mg, [FakeMesh()], [None], FakeParams(2, 2, 1, 1), object(), tool,
-                              lambda p, net: 1.0, frames=2)
+    out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), object(), tool, lambda p, net: 1.0,
+                               frames=2, solver_cls=fake_solver(lambda p, learned: 1.0))
     assert out["learned_mixed"]["chosen"] is None and out["plain_fp32"]["chosen"] is None
+
+
+def test_without_a_network_only_the_plain_family():
+    out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), None, tool, lambda p, net: 1.0,
+                               frames=2, solver_cls=fake_solver(lambda p, learned: 0.0))
+    assert "learned_mixed" not in out and out["plain_fp32"]["chosen"] is not None
