@@ -210,3 +210,29 @@ def test_time_kernel_learned_cycle_restores_state(lib, trained):
         s.close()
     assert np.array_equal(runs[0][0], runs[1][0])
     assert runs[0][1] == runs[1][1]
+
+
+def test_select_sweeps_on_the_gpu(lib, trained):
+    """The sweep-count tuner with the real solver and its default timer: every
+    candidate within the bar is timed, the choice is the fastest of them, and
+    the choice's error is the one measured."""
+    from multigridsoftbody_b200 import sweeps
+
+    net = trained[0]
+    m, fixed = beam(4, 40, 4)
+    p = mg_params(levels=3, precision=mg.PRECISION_MIXED, refinement_passes=1)
+    path = capsule_path(20, start=(0.0, 0.0, 1.3), seed=5)
+
+    def tool(f):
+        a, b = path[f % len(path)]
+        return a[None], b[None], np.array([0.3], np.float32)
+
+    out = sweeps.select_sweeps(m, fixed, p, net, tool, frames=10, bar=1e-3)
+    for fam in ("learned_mixed", "plain_fp32"):
+        rows = out[fam]["candidates"]
+        timed = [r for r in rows if "ms_per_frame" in r]
+        assert all(r["ms_per_frame"] > 0.0 for r in timed)
+        assert all(("ms_per_frame" in r) == (r["err_over_diag"] <= 1e-3) for r in rows)
+        if timed:
+            assert out[fam]["chosen"] == min(timed, key=lambda r: r["ms_per_frame"])
+    assert out["learned_mixed"]["chosen"] is not None
