@@ -128,6 +128,21 @@ mgsb_status mgsb_num_tets(const mgsb_solver* h, int32_t body, int32_t* n);
  * No reference counterpart (single scalar k, PDSolver.cpp:170). */
 mgsb_status mgsb_set_material(mgsb_solver* h, int32_t body, const float* youngs, const float* poisson);
 
+/* Change the solver's parameters between frames: the reference's public fields
+ * m_iterNum, m_dt, m_damping, m_volumnStiffness, m_collisionStiffness, m_rho,
+ * m_gravity{X,Y,Z} (PDSolver.h:72-81), which callers assign after Init, plus
+ * the multigrid kind's density, contact weight, levels, sweep counts, Jacobi
+ * factor, refinement passes and graph use.  Gravity and damping apply to every
+ * body of a batch.  A changed youngs_modulus / poisson_ratio sets every tet of
+ * every body to it (replacing mgsb_set_material); unchanged ones keep the
+ * per-tet material.  The solver kind, precision, device and stream are fixed
+ * at create (MGSB_NOT_SUPPORTED).  Invalid values: MGSB_INVALID_ARG, nothing
+ * changed.  Waits for the solver's stream; the next step rebuilds the derived
+ * data and the frame's CUDA graph.  Positions and velocities are kept. */
+mgsb_status mgsb_set_params(mgsb_solver* h, const mgsb_params* params);
+/* The parameters in force (the reference's public fields, read back). */
+mgsb_status mgsb_get_params(const mgsb_solver* h, mgsb_params* out);
+
 /* Fixed-vertex mask, 1 = fixed.  Replaces PDSolver::SetFixedVert
  * (PDSolver.cpp:134-162; flag 0.0f = fixed there). */
 mgsb_status mgsb_set_fixed(mgsb_solver* h, int32_t body, const uint8_t* mask);
@@ -185,9 +200,10 @@ mgsb_status mgsb_get_normals(mgsb_solver* h, int32_t body, float* out /* [3*V] *
  * triangles and 65,536 surface vertices, else MGSB_NOT_SUPPORTED.  A pending
  * set-up (after mgsb_set_fixed / mgsb_set_material) is not rebuilt here:
  * MGSB_INVALID_ARG until a mgsb_step or mgsb_get_normals call has done it.  The
- * first call on a device looks up the scratch address; make it outside any
- * stream capture.  All calls on one device share the scratch, so calls that
- * overlap in time (other threads, other handles) race. */
+ * first call on a device (and the first after its context was reset) looks up
+ * the scratch address; make it outside any stream capture.  All calls on one
+ * device share the scratch, so calls that overlap in time (other threads, other
+ * handles) race. */
 mgsb_status mgsb_get_normals_noalloc(mgsb_solver* h, int32_t body, float* out /* [3*V] */);
 
 /* Checkpoint / resume: overwrite positions and velocities of a body. */
@@ -273,6 +289,22 @@ mgsb_status mgsb_set_fused_prolongation(mgsb_solver* h, int32_t on);
  * until the next frame.  Replaces the all-vertex loop of DCDByPoint
  * (PDSolver.cpp:228-233, PDSolver.cu:277-331). */
 mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on);
+
+/* Capsule narrow phase of the multigrid kinds.  MGSB_CONTACT_VERTICES (the
+ * default): surface vertices inside the capsule are contacts, projected to its
+ * surface.  MGSB_CONTACT_VERTICES_AND_TRIANGLES: in addition every surface
+ * triangle closer to the capsule's segment than its radius is in contact (a
+ * capsule entering a face between its vertices), and each vertex of such a
+ * triangle that is not itself inside the capsule becomes a contact whose
+ * target is its predicted position plus the mean push of its touching
+ * triangles; a triangle's push moves it out along its closest-point line to
+ * the segment by the penetration depth.  The capsule form of the reference's
+ * sphere test DCDByTriangle_sphere_V2 (PDSolver.cu:612-680, response
+ * :462-501), gathered per vertex instead of float atomics.  Evaluated once per
+ * frame in FP64 on the predicted positions; not combined with the broad phase
+ * (MGSB_NOT_SUPPORTED). */
+enum { MGSB_CONTACT_VERTICES = 0, MGSB_CONTACT_VERTICES_AND_TRIANGLES = 1 };
+mgsb_status mgsb_set_surface_contact(mgsb_solver* h, int32_t mode);
 
 /* Host-only (no GPU): build the multigrid hierarchy of one mesh exactly as
  * mgsb_create would and return level `level`: vertex count, off-diagonal

@@ -93,6 +93,8 @@ SIGNATURES = [
     ("mgsb_num_verts", C.c_int, [_P, C.c_int32, _IP]),
     ("mgsb_num_tets", C.c_int, [_P, C.c_int32, _IP]),
     ("mgsb_set_material", C.c_int, [_P, C.c_int32, _FP, _FP]),
+    ("mgsb_set_params", C.c_int, [_P, C.POINTER(Params)]),
+    ("mgsb_get_params", C.c_int, [_P, C.POINTER(Params)]),
     ("mgsb_set_fixed", C.c_int, [_P, C.c_int32, _U8P]),
     ("mgsb_set_tool_capsule", C.c_int, [_P, C.c_int32, _FP, _FP, C.c_float]),
     ("mgsb_set_tool_capsules", C.c_int, [_P, _FP, _FP, _FP]),
@@ -147,6 +149,7 @@ SIGNATURES = [
     ("mgsb_get_coarse_split", C.c_int, [_P, _IP]),
     ("mgsb_set_launch_overlap", C.c_int, [_P, C.c_int32]),
     ("mgsb_set_fused_prolongation", C.c_int, [_P, C.c_int32]),
+    ("mgsb_set_surface_contact", C.c_int, [_P, C.c_int32]),
     ("mgsb_set_broad_phase", C.c_int, [_P, C.c_int32]),
     ("mgsb_inspect_level", C.c_int, [C.POINTER(Mesh), C.POINTER(Params), _U8P, C.c_int32, _IP, _IP, _IP, _FP, _FP, _IP,
                                      _IP, _FP]),

@@ -225,6 +225,24 @@ class Solver:
         return n.value
 
     # -- inputs
+    def get_params(self) -> Params:
+        """The parameters in force (mgsb_get_params)."""
+        p = Params()
+        _check(self._lib.mgsb_get_params(self.h, C.byref(p)), self.h)
+        return p
+
+    def set_params(self, params: Params = None, **changes) -> None:
+        """Change parameters between frames (mgsb_set_params): a full Params, or keyword changes to the
+        ones in force (gravity as a 3-sequence)."""
+        p = Params.from_buffer_copy(params if params is not None else self.get_params())
+        for k, v in changes.items():
+            if k == "gravity":
+                for c in range(3):
+                    p.gravity[c] = float(v[c])
+            else:
+                setattr(p, k, v)
+        _check(self._lib.mgsb_set_params(self.h, C.byref(p)), self.h)
+
     def set_fixed(self, mask, body: int = 0) -> None:
         m = np.ascontiguousarray(mask, dtype=np.uint8)
         _check(self._lib.mgsb_set_fixed(self.h, body, _u8ptr(m)), self.h)
@@ -418,6 +436,10 @@ class Solver:
     def set_coarse_split(self, split: int = 0) -> None:
         """Levels 1..split-1 grid-wide, the rest in the cluster kernel (0 = by size)."""
         _check(self._lib.mgsb_set_coarse_split(self.h, split), self.h)
+
+    def set_surface_contact(self, triangles: bool = True) -> None:
+        """Capsule against the surface triangles too (mgsb_set_surface_contact), or vertices only."""
+        _check(self._lib.mgsb_set_surface_contact(self.h, 1 if triangles else 0), self.h)
 
     def set_broad_phase(self, on: bool = True) -> None:
         """Uniform-grid broad phase for the capsule contact (same contacts as the all-vertex test)."""

@@ -282,19 +282,202 @@ __device__ __forceinline__ void capsule_test(const float4 sp, const BodyDev& B, 
     target = make_float4((float)(q[0] + r * nrm[0]), (float)(q[1] + r * nrm[1]), (float)(q[2] + r * nrm[2]), 0.f);
 }
 
+// ---------------------------------------------------------------------------
+// Capsule against the surface triangles (FP64).  A triangle is in contact when
+// its distance to the capsule's segment is below the radius, so a capsule that
+// enters a face between its vertices is found although no vertex lies inside
+// it.  The push of a contacting triangle moves it out along the line of the
+// closest points: push = (h - q) / |h - q| * (r - |h - q|), h on the triangle,
+// q on the segment -- the capsule form of the face / edge half-cylinder /
+// vertex cases of the reference's sphere test DCDByTriangle_sphere_V2
+// (PDSolver.cu:612-680, response :462-501), whose push centre - hit is the
+// same vector for a sphere.  When the segment touches the triangle (|h - q| ~ 0)
+// the push is r along the inward normal.  Per vertex, the pushes of its
+// contacting triangles are averaged in ascending triangle order (a gather
+// instead of the reference's float atomics).
+// ---------------------------------------------------------------------------
+struct Dv3 {
+    double x, y, z;
+};
+__device__ __forceinline__ Dv3 dv3(double x, double y, double z) { return Dv3{x, y, z}; }
+__device__ __forceinline__ Dv3 dsub(Dv3 a, Dv3 b) { return dv3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ Dv3 dadd(Dv3 a, Dv3 b) { return dv3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ Dv3 dscale(Dv3 a, double s) { return dv3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double ddot(Dv3 a, Dv3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ Dv3 dcross(Dv3 a, Dv3 b) {
+    return dv3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// Closest point of triangle abc to p, by the Voronoi regions of its vertices,
+// edges and face (Ericson, Real-Time Collision Detection, sec. 5.1.5).
+__device__ __forceinline__ Dv3 tri_closest_point(Dv3 p, Dv3 a, Dv3 b, Dv3 c) {
+    const Dv3 ab = dsub(b, a), ac = dsub(c, a), ap = dsub(p, a);
+    const double d1 = ddot(ab, ap), d2 = ddot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) return a;
+    const Dv3 bp = dsub(p, b);
+    const double d3 = ddot(ab, bp), d4 = ddot(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) return b;
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) return dadd(a, dscale(ab, d1 / (d1 - d3)));
+    const Dv3 cp = dsub(p, c);
+    const double d5 = ddot(ab, cp), d6 = ddot(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) return c;
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return dadd(a, dscale(ac, d2 / (d2 - d6)));
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0)
+        return dadd(b, dscale(dsub(c, b), (d4 - d3) / ((d4 - d3) + (d5 - d6))));
+    const double den = 1.0 / (va + vb + vc);
+    return dadd(a, dadd(dscale(ab, vb * den), dscale(ac, vc * den)));
+}
+
+// Closest points c1 on segment p1q1 and c2 on segment p2q2 (Ericson sec. 5.1.9,
+// clamped parametric form); returns |c1 - c2|^2.
+__device__ __forceinline__ double seg_seg_closest(Dv3 p1, Dv3 q1, Dv3 p2, Dv3 q2, Dv3& c1, Dv3& c2) {
+    const Dv3 d1 = dsub(q1, p1), d2 = dsub(q2, p2), r = dsub(p1, p2);
+    const double a = ddot(d1, d1), e = ddot(d2, d2), f = ddot(d2, r);
+    double s = 0.0, t = 0.0;
+    if (a <= 1e-300 && e <= 1e-300) {
+        s = t = 0.0;
+    } else if (a <= 1e-300) {
+        t = fmin(fmax(f / e, 0.0), 1.0);
+    } else {
+        const double c = ddot(d1, r);
+        if (e <= 1e-300) {
+            s = fmin(fmax(-c / a, 0.0), 1.0);
+        } else {
+            const double b = ddot(d1, d2), den = a * e - b * b;
+            s = den > 0.0 ? fmin(fmax((b * f - c * e) / den, 0.0), 1.0) : 0.0;
+            t = (b * s + f) / e;
+            if (t < 0.0) {
+                t = 0.0;
+                s = fmin(fmax(-c / a, 0.0), 1.0);
+            } else if (t > 1.0) {
+                t = 1.0;
+                s = fmin(fmax((b - c) / a, 0.0), 1.0);
+            }
+        }
+    }
+    c1 = dadd(p1, dscale(d1, s));
+    c2 = dadd(p2, dscale(d2, t));
+    const Dv3 w = dsub(c1, c2);
+    return ddot(w, w);
+}
+
+// Push of triangle (a, b, c) (o: the fourth vertex of its tet, inside the
+// body) out of the capsule (segment p0p1, radius r): true and push when the
+// triangle is in contact.
+__device__ __forceinline__ bool tri_capsule_push(Dv3 a, Dv3 b, Dv3 c, Dv3 o, Dv3 p0, Dv3 p1, double r, Dv3& push) {
+    double best = 1e300;
+    Dv3 q = p0, h = a;
+    {   // segment end points against the triangle
+        const Dv3 h0 = tri_closest_point(p0, a, b, c), h1 = tri_closest_point(p1, a, b, c);
+        const double e0 = ddot(dsub(p0, h0), dsub(p0, h0)), e1 = ddot(dsub(p1, h1), dsub(p1, h1));
+        if (e0 < best) { best = e0; q = p0; h = h0; }
+        if (e1 < best) { best = e1; q = p1; h = h1; }
+    }
+    const Dv3 ev[3][2] = {{a, b}, {b, c}, {c, a}};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {   // segment against the edges
+        Dv3 cs, ct;
+        const double e2 = seg_seg_closest(p0, p1, ev[k][0], ev[k][1], cs, ct);
+        if (e2 < best) { best = e2; q = cs; h = ct; }
+    }
+    const Dv3 n = dcross(dsub(b, a), dsub(c, a));
+    {   // segment through the face
+        const double s0 = ddot(n, dsub(p0, a)), s1 = ddot(n, dsub(p1, a));
+        if ((s0 <= 0.0 && s1 >= 0.0) || (s0 >= 0.0 && s1 <= 0.0)) {
+            if (s0 != s1) {
+                const Dv3 x = dadd(p0, dscale(dsub(p1, p0), s0 / (s0 - s1)));
+                const double u = ddot(dcross(dsub(b, a), dsub(x, a)), n), v = ddot(dcross(dsub(c, b), dsub(x, b)), n),
+                             w = ddot(dcross(dsub(a, c), dsub(x, c)), n);
+                if (u >= 0.0 && v >= 0.0 && w >= 0.0) { best = 0.0; q = x; h = x; }
+            }
+        }
+    }
+    if (!(best < r * r)) return false;
+    const double dist = sqrt(best);
+    if (dist > 1e-12) {
+        push = dscale(dsub(h, q), (r - dist) / dist);
+    } else {   // the segment touches the face: push r along the inward normal
+        const double nl = sqrt(ddot(n, n));
+        const double sgn = ddot(n, dsub(o, a)) > 0.0 ? 1.0 : -1.0;   // towards the inside of the body
+        push = nl > 0.0 ? dscale(n, sgn * r / nl) : dv3(0.0, 0.0, 0.0);
+    }
+    return true;
+}
+
+// Per surface triangle: push[f] = (push, 1) when triangle f touches its body's
+// capsule, else zero.  tris[f] = (a, b, c, o) global vertex ids, o the inner
+// vertex of the triangle's tet.  P = float4 (FP32 kind) or double4 (mixed).
+template <typename P>
+__global__ void k_tri_capsule(int nf, const int4* __restrict__ tris, const int32_t* __restrict__ body_of,
+                              const BodyDev* __restrict__ bodies, const P* __restrict__ s, double4* __restrict__ push) {
+    pdl_enter();
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const int4 t = __ldg(tris + f);
+    const BodyDev& B = bodies[__ldg(body_of + t.x)];
+    double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
+    const double r = B.cap_r;
+    if (r > 0.0) {
+        auto ld = [&](int i) {
+            const P v = s[i];
+            return dv3((double)v.x, (double)v.y, (double)v.z);
+        };
+        Dv3 pu;
+        if (tri_capsule_push(ld(t.x), ld(t.y), ld(t.z), ld(t.w), dv3(B.cap_a[0], B.cap_a[1], B.cap_a[2]),
+                             dv3(B.cap_b[0], B.cap_b[1], B.cap_b[2]), r, pu))
+            out = make_double4(pu.x, pu.y, pu.z, 1.0);
+    }
+    push[f] = out;
+}
+
+// Mean push of vertex i's contacting surface triangles (vt_ptr / vt_idx: its
+// triangles, ascending); false when none is in contact.
+__device__ __forceinline__ bool tri_contact_gather(int i, const int32_t* __restrict__ vt_ptr,
+                                                   const int32_t* __restrict__ vt_idx, const double4* __restrict__ push,
+                                                   Dv3& mean) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    int k = 0;
+    const int e1 = __ldg(vt_ptr + i + 1);
+    for (int e = __ldg(vt_ptr + i); e < e1; ++e) {
+        const double4 pu = push[__ldg(vt_idx + e)];
+        if (pu.w != 0.0) {
+            sx += pu.x;
+            sy += pu.y;
+            sz += pu.z;
+            ++k;
+        }
+    }
+    if (!k) return false;
+    mean = dv3(sx / k, sy / k, sz / k);
+    return true;
+}
+
 // Brute-force narrow phase over all surface vertices (used when the broad
 // phase is disabled).
+// With vt_ptr set (triangle contact on), a vertex outside the capsule whose
+// surface triangles touch it is a contact too, projected to s + their mean push.
 __global__ void k_contact_all(int ns, const int32_t* __restrict__ surf, const int32_t* __restrict__ body_of,
                               const BodyDev* __restrict__ bodies, const float4* __restrict__ s,
                               const float* __restrict__ fixf, float kc, int32_t* __restrict__ cflag,
-                              float* __restrict__ c0, float4* __restrict__ target) {
+                              float* __restrict__ c0, float4* __restrict__ target,
+                              const int32_t* __restrict__ vt_ptr = nullptr, const int32_t* __restrict__ vt_idx = nullptr,
+                              const double4* __restrict__ push = nullptr) {
     pdl_enter();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= ns) return;
     const int i = __ldg(surf + q);
     int flag;
     float4 tg;
-    capsule_test(__ldg(s + i), bodies[__ldg(body_of + i)], flag, tg);
+    const float4 sp = __ldg(s + i);
+    capsule_test(sp, bodies[__ldg(body_of + i)], flag, tg);
+    Dv3 mp;
+    if (!flag && vt_ptr && tri_contact_gather(i, vt_ptr, vt_idx, push, mp)) {
+        flag = 1;
+        tg = make_float4((float)((double)sp.x + mp.x), (float)((double)sp.y + mp.y), (float)((double)sp.z + mp.z), 0.f);
+    }
     cflag[i] = flag;
     c0[i] = (flag && __ldg(fixf + i) != 0.f) ? kc : 0.f;
     target[i] = tg;

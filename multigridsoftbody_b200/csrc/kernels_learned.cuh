@@ -158,13 +158,18 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_features(int n, const int32_t
 // One learned sweep in a single kernel: per 128-row tile, each thread forms its
 // row's features straight into the shared-memory operand tile, the tensor-core
 // MLP runs on the tile, and the same thread applies d_i += (s_i/D_i) y_i.
+// With dd64 set (the mixed kind's last sweep of a V-cycle whose residual check
+// is taken by the next outer residual), the finished correction is also applied
+// to the FP64 displacement, dd64_i += d_i, with its FP32 mirror d32_i: each row
+// belongs to one thread, so this is the work of k_mx_update for that row.
 __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, const int32_t* __restrict__ sp,
                                                              const int32_t* __restrict__ col, const float* __restrict__ val,
                                                              const float* __restrict__ dfull,
                                                              const float* __restrict__ diag0,
                                                              const float* __restrict__ fixf, const float4* __restrict__ r,
                                                              const uint8_t* __restrict__ img, float4* __restrict__ d,
-                                                             int32_t* __restrict__ err) {
+                                                             int32_t* __restrict__ err, double4* __restrict__ dd64,
+                                                             float4* __restrict__ d32) {
     pdl_trigger();
     constexpr int S = 32 / kLanesL0;   // level-0 slice height
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -236,12 +241,22 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
             if (err) atomicExch(err, 1);
         }
         // threads 0..127 hold row rt's outputs (warps 0-3 serve TMEM lanes 0..127)
-        if (ok && !half && row < n && sc != 0.f) {
+        if (ok && !half && row < n && (sc != 0.f || dd64)) {
             float4 q = d[row];
-            q.x += sc * out[0];
-            q.y += sc * out[1];
-            q.z += sc * out[2];
-            d[row] = q;
+            if (sc != 0.f) {
+                q.x += sc * out[0];
+                q.y += sc * out[1];
+                q.z += sc * out[2];
+                d[row] = q;
+            }
+            if (dd64) {
+                double4 v = dd64[row];
+                v.x += q.x;
+                v.y += q.y;
+                v.z += q.z;
+                dd64[row] = v;
+                d32[row] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+            }
         }
     }
     if (weights_pending) mlp_wait_weights(Sm, ws, ph_load, err);   // no copy may outlive the CTA

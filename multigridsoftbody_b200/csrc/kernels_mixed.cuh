@@ -77,7 +77,10 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
                                    const float* __restrict__ diag0,
                                    float omega, int32_t* __restrict__ cflag, float* __restrict__ c0,
                                    double4* __restrict__ b0, float* __restrict__ dfull, float* __restrict__ dinv,
-                                   double4* __restrict__ d64, float4* __restrict__ d32, float4* __restrict__ target) {
+                                   double4* __restrict__ d64, float4* __restrict__ d32, float4* __restrict__ target,
+                                   const int32_t* __restrict__ vt_ptr = nullptr,
+                                   const int32_t* __restrict__ vt_idx = nullptr,
+                                   const double4* __restrict__ push = nullptr) {
     pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -85,6 +88,11 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
     double4 tg = d4z();
     const double4 sv = s[i];
     if (__ldg(is_surf + i) && (!cand || cand[i])) capsule_test64(sv, bodies[__ldg(body_of + i)], flag, tg);
+    Dv3 mp;   // triangle contact (vt_ptr set): s + the mean push of the touching surface triangles
+    if (!flag && vt_ptr && tri_contact_gather(i, vt_ptr, vt_idx, push, mp)) {
+        flag = 1;
+        tg = make_double4(sv.x + mp.x, sv.y + mp.y, sv.z + mp.z, 0.0);
+    }
     const bool free_v = __ldg(fixf + i) != 0.f;
     const float c = (flag && free_v) ? kc : 0.f;
     cflag[i] = flag;
@@ -106,7 +114,12 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
 // With b0 set, b is first assembled as b0 + the row's slots (FP64, the slots
 // split over the row's lanes; the first pass of a PD iteration) and stored.  With ls_r set (the
 // learned V-cycle, which starts from zero), also ls_r = fix * r and
-// part[block] = sum |ls_r|^2: the starting residual of that cycle.
+// part[block] = sum |ls_r|^2: the starting residual of that cycle.  With
+// part_end set, the previous learned cycle's residual check rides on this
+// product: its correction is already in d (the cycle's last sweep applied it),
+// so its end residual is fix * (b_prev - A d) with b_prev the right-hand side
+// before this kernel's assembly (the same b when nothing is assembled), and
+// part_end[block] = sum |fix * (b_prev - A d)|^2.
 constexpr int kLanesMx = 4;
 constexpr int kMxThreads = 64 * kLanesMx;
 __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
@@ -116,7 +129,8 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
                                                      float4* __restrict__ e, int first_sweep,
                                                      const double4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
                                                      const float4* __restrict__ slots, const float* __restrict__ fixf,
-                                                     float4* __restrict__ ls_r, float* __restrict__ part) {
+                                                     float4* __restrict__ ls_r, float* __restrict__ part,
+                                                     float* __restrict__ part_end) {
     pdl_enter();
     __shared__ float red[kMxThreads / 32];
     constexpr int G = kLanesMx, RW = 32 / G;   // lanes per row, rows per warp
@@ -126,7 +140,7 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
     const int row = warp * RW + (lane % RW);
     const int j = lane / RW;                    // this lane's share of the row
     const bool valid = row < n;
-    double4 bi = d4z();
+    double4 bi = d4z(), bprev = d4z();
     if (b0) {   // uniform over the block: the row's slots split over its G lanes, FP64 sums
         double sx = 0.0, sy = 0.0, sz = 0.0;
         if (valid) {
@@ -146,6 +160,7 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
             sz += __shfl_xor_sync(0xffffffffu, sz, o);
         }
         if (valid && lane < RW) {
+            if (part_end) bprev = b[row];   // the previous iteration's right-hand side, before it is replaced
             bi = b0[row];
             bi.x += sx;
             bi.y += sy;
@@ -172,12 +187,19 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
         az += __shfl_xor_sync(0xffffffffu, az, o);
     }
-    float rr = 0.f;
+    float rr = 0.f, re = 0.f;
     if (valid && lane < RW) {
         const double4 x = d[row];
         if (!b0) bi = b[row];
         const double D = __ldg(diag64 + row) + (double)__ldg(c + row);
         const float rx = (float)(bi.x - fma(D, x.x, ax)), ry = (float)(bi.y - fma(D, x.y, ay)), rz = (float)(bi.z - fma(D, x.z, az));
+        if (part_end) {
+            const float fx = __ldg(fixf + row);
+            const float ex = b0 ? fx * (float)(bprev.x - fma(D, x.x, ax)) : fx * rx;
+            const float ey = b0 ? fx * (float)(bprev.y - fma(D, x.y, ay)) : fx * ry;
+            const float ez = b0 ? fx * (float)(bprev.z - fma(D, x.z, az)) : fx * rz;
+            re = ex * ex + ey * ey + ez * ez;
+        }
         r32[row] = make_float4(rx, ry, rz, 0.f);
         const float w = first_sweep ? __ldg(dinv + row) : 0.f;
         e[row] = make_float4(w * rx, w * ry, w * rz, 0.f);
@@ -191,6 +213,11 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
     if (ls_r) {   // uniform over the block
         const float t = block_sum_f(rr, red);
         if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+    if (part_end) {   // uniform over the block
+        __syncthreads();   // red is reused
+        const float t = block_sum_f(re, red);
+        if (threadIdx.x == 0) part_end[blockIdx.x] = t;
     }
 }
 

@@ -143,6 +143,14 @@ struct mgsb_solver {
     float* c0 = nullptr;
     int32_t* surf = nullptr;
     int nsurf = 0;
+    // capsule against the surface triangles (multigrid kinds): per triangle its
+    // vertices + the inner vertex of its tet, per vertex its triangles (CSR over
+    // all vertices, ascending), per triangle this frame's push
+    bool tri_contact = false;
+    int ctri_n = 0;
+    int4* ctri = nullptr;
+    int32_t *vt_ptr = nullptr, *vt_idx = nullptr;
+    double4* tri_push = nullptr;
     // uniform-grid broad phase of the tool contact (multigrid kinds)
     bool broad_phase = false;
     BpGrid* bp_grids = nullptr;
@@ -383,8 +391,9 @@ mgsb_status setup_broad_phase(mgsb_solver* h, std::vector<DevMem>& pool) {
 // vertices in ascending order and, per surface vertex, its triangles in
 // ascending order; plus the two scratch arrays the normals pass writes.
 mgsb_status upload_normals_data(mgsb_solver* h, std::vector<DevMem>& pool) {
-    std::vector<int4> tris_all;
+    std::vector<int4> tris_all, ctri_all;
     std::vector<int32_t> sv_all, ptr_all{0}, fidx_all;
+    std::vector<int32_t> vt_cnt(h->N0 + 1, 0), vt_idx_all;
     h->nrm_f_off.clear();
     h->nrm_nf.clear();
     h->nrm_sv_off.clear();
@@ -399,6 +408,8 @@ mgsb_status upload_normals_data(mgsb_solver* h, std::vector<DevMem>& pool) {
         std::vector<int32_t> cnt(B.V + 1, 0);
         for (int f = 0; f < nf; ++f) {
             tris_all.push_back(int4{tris[3 * f] + B.v_off, tris[3 * f + 1] + B.v_off, tris[3 * f + 2] + B.v_off, 0});
+            ctri_all.push_back(
+                int4{tris[3 * f] + B.v_off, tris[3 * f + 1] + B.v_off, tris[3 * f + 2] + B.v_off, opp[f] + B.v_off});
             for (int q = 0; q < 3; ++q) ++cnt[tris[3 * f + q] + 1];
         }
         std::vector<int32_t> start(B.V + 1, 0);
@@ -420,6 +431,28 @@ mgsb_status upload_normals_data(mgsb_solver* h, std::vector<DevMem>& pool) {
         h->nrm_max_f = std::max(h->nrm_max_f, nf);
         h->nrm_max_sv = std::max(h->nrm_max_sv, nsv);
     }
+    // vertex -> surface triangles over all vertices (global triangle ids, ascending)
+    for (const int4& t : ctri_all) {
+        ++vt_cnt[t.x + 1];
+        ++vt_cnt[t.y + 1];
+        ++vt_cnt[t.z + 1];
+    }
+    for (int i = 0; i < h->N0; ++i) vt_cnt[i + 1] += vt_cnt[i];
+    vt_idx_all.resize(vt_cnt[h->N0]);
+    {
+        std::vector<int32_t> fill(vt_cnt.begin(), vt_cnt.end() - 1);
+        for (int g = 0; g < (int)ctri_all.size(); ++g) {
+            vt_idx_all[fill[ctri_all[g].x]++] = g;
+            vt_idx_all[fill[ctri_all[g].y]++] = g;
+            vt_idx_all[fill[ctri_all[g].z]++] = g;
+        }
+    }
+    h->ctri_n = (int)ctri_all.size();
+    TRY(dupload(h, pool, &h->ctri, ctri_all));
+    TRY(dupload(h, pool, &h->vt_ptr, vt_cnt));
+    TRY(dupload(h, pool, &h->vt_idx, vt_idx_all));
+    TRY(dalloc(h, pool, &h->tri_push, (size_t)std::max(1, h->ctri_n)));
+    CUDA_TRY(h, cudaMemset(h->tri_push, 0, (size_t)std::max(1, h->ctri_n) * sizeof(double4)));
     h->nrm_sv_host = sv_all;
     TRY(dupload(h, pool, &h->nrm_tris, tris_all));
     TRY(dupload(h, pool, &h->nrm_sv, sv_all));
@@ -884,7 +917,8 @@ void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const 
 // caller's next launch (enqueue_learned_guard); cycle: the cycle's index in
 // the frame (its starting residual's block sums go to ls_part0 there).
 void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool from_zero, CoarseArgs ca, int cycle,
-                            bool gather_b = false, bool start_residual_ready = false) {
+                            bool gather_b = false, bool start_residual_ready = false, double4* dd64 = nullptr,
+                            float4* d32 = nullptr) {
     const int n0 = h->N0;
     std::vector<LevelDev>& lv = h->lev;
     const LevelDev& l0 = lv[0];
@@ -901,7 +935,7 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
                h->ls_r, nullptr, h->ls_part0 + (size_t)cycle * g0, gather_b ? h->b0 : nullptr, gather_b ? h->slot_ptr : nullptr,
                gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
-           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
+           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr, nullptr, nullptr);
     // coarse correction
     LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, d, b, l0.res, nullptr);
     ca.d = d;
@@ -916,8 +950,9 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
         LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
                h->ls_r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     }
+    // with dd64 (mixed kind, check taken by the next outer residual) the sweep also applies d to dd64
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
-           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr);
+           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr, dd64, d32);
 }
 
 // The residual check of the learned V-cycle `cycle` just enqueued (d, b as
@@ -1162,9 +1197,15 @@ void enqueue_mg_frame(mgsb_solver* h) {
     LAUNCH(h, k_mg_predict, grid_for(n0), kBlock, 0, n0, h->x, h->v, h->s, h->last, h->fixf, h->body_of, h->bodies_dev, p.dt);
     if (h->nsurf > 0 && h->broad_phase)
         enqueue_broad_phase(h, h->s, true);
-    else if (h->nsurf > 0)
+    else if (h->nsurf > 0) {
+        const bool tri = h->tri_contact && h->ctri_n > 0;
+        if (tri)
+            LAUNCH(h, k_tri_capsule<float4>, grid_for(h->ctri_n), kBlock, 0, h->ctri_n, h->ctri, h->body_of,
+                   h->bodies_dev, (const float4*)h->s, h->tri_push);
         LAUNCH(h, k_contact_all, grid_for(h->nsurf), kBlock, 0, h->nsurf, h->surf, h->body_of, h->bodies_dev, h->s,
-               h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target);
+               h->fixf, p.contact_stiffness, h->cflag, h->c0, h->target, tri ? h->vt_ptr : nullptr,
+               tri ? h->vt_idx : nullptr, tri ? (const double4*)h->tri_push : nullptr);
+    }
     const bool learned = h->ls_net != nullptr && h->p.iterations > 0 && h->p.refinement_passes > 0;
     const LearnedFallback fb = learned ? begin_learned_fallback(h) : LearnedFallback{};
     float4* d = enqueue_mg_solve(h, learned, fb);
@@ -1188,9 +1229,13 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
     const int nb = (int)h->bodies.size();
     const float om = p.jacobi_omega;
     std::vector<LevelDev>& lv = h->lev;
+    const bool tri = h->tri_contact && h->ctri_n > 0 && !h->broad_phase;
+    if (tri)
+        LAUNCH(h, k_tri_capsule<double4>, grid_for(h->ctri_n), kBlock, 0, h->ctri_n, h->ctri, h->body_of, h->bodies_dev,
+               (const double4*)h->s64, h->tri_push);
     LAUNCH(h, k_mx_contact_frame, grid_for(n0), kBlock, 0, n0, h->s64, h->fixf, h->body_of, h->bodies_dev, h->is_surf,
            h->broad_phase ? h->bp_cand : nullptr, p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32,
-           h->target);
+           h->target, tri ? h->vt_ptr : nullptr, tri ? h->vt_idx : nullptr, tri ? (const double4*)h->tri_push : nullptr);
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
                lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
@@ -1209,13 +1254,21 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
             // also leaves the learned cycle's starting residual (the cycle starts from e = 0)
             const bool gather = pass == 0;
             const int c = it * p.refinement_passes + pass;
+            // learned: the residual check of the previous cycle (its correction already in dd64) rides on
+            // this outer residual, against the right-hand side that cycle solved for
             LAUNCH(h, k_mx_residual, g0, kMxThreads, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
                    h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !learned) ? 1 : 0,
                    gather ? h->b0_64 : nullptr, gather ? h->slot_ptr : nullptr, gather ? h->slots : nullptr, h->fixf,
-                   learned ? h->ls_r : nullptr, learned ? h->ls_part0 + (size_t)c * h->ls_nblk : nullptr);
-            if (learned) {   // the check also applies the correction (dd64 += e)
-                enqueue_learned_vcycle(h, ea, h->r32, true, ca, c, false, true);
-                enqueue_learned_guard(h, ea, h->r32, c, c == h->ls_cycles - 1, fb, h->dd64, h->d32);
+                   learned ? h->ls_r : nullptr, learned ? h->ls_part0 + (size_t)c * h->ls_nblk : nullptr,
+                   (learned && c > 0) ? h->ls_part1 + (size_t)(c - 1) * h->ls_nblk : nullptr);
+            if (learned) {
+                // every cycle but the frame's last applies its correction in its last sweep (dd64 += e) and
+                // is checked by the next k_mx_residual; the last is checked (and applied) by the guard,
+                // which takes the frame's decision
+                const bool last = c == h->ls_cycles - 1;
+                enqueue_learned_vcycle(h, ea, h->r32, true, ca, c, false, true, last ? nullptr : h->dd64,
+                                       last ? nullptr : h->d32);
+                if (last) enqueue_learned_guard(h, ea, h->r32, c, true, fb, h->dd64, h->d32);
                 continue;
             }
             for (int k = 1; k < p.pre_sweeps; ++k) {
@@ -1492,8 +1545,11 @@ mgsb_status copy_body_f4(mgsb_solver* h, int32_t body, const float4* src, F&& si
 // Surface normals of one body from the current positions: triangle normals
 // into fscratch (>= the body's triangle count), vertex normals of the
 // surface vertices into vscratch (>= its surface-vertex count), then a copy
-// to the host and a scatter into out[3V] (zero for interior vertices).
-mgsb_status run_normals(mgsb_solver* h, int32_t body, float4* fscratch, float4* vscratch, float* out) {
+// to the host and a scatter into out[3V] (zero for interior vertices).  The
+// copy lands in host_stage (>= the surface-vertex count of float4) when one is
+// given, else in a temporary host vector.
+mgsb_status run_normals(mgsb_solver* h, int32_t body, float4* fscratch, float4* vscratch, float4* host_stage,
+                        float* out) {
     const BodyHost& B = h->bodies[body];
     const int nf = h->nrm_nf[body], nsv = h->nrm_nsv[body];
     const int f_off = h->nrm_f_off[body], sv_off = h->nrm_sv_off[body];
@@ -1503,9 +1559,13 @@ mgsb_status run_normals(mgsb_solver* h, int32_t body, float4* fscratch, float4* 
         k_vert_normals<<<(nsv + 255) / 256, 256, 0, h->stream>>>(nsv, h->nrm_ptr + sv_off, h->nrm_fidx, fscratch, vscratch);
         CUDA_TRY(h, cudaGetLastError());
     }
-    std::vector<float4> vn(nsv);
+    std::vector<float4> tmp;
+    if (!host_stage) {
+        tmp.resize(nsv);
+        host_stage = tmp.data();
+    }
     if (nsv > 0)
-        CUDA_TRY(h, cudaMemcpyAsync(vn.data(), vscratch, nsv * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(host_stage, vscratch, nsv * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     int32_t nf_flag = 0;
     CUDA_TRY(h, cudaMemcpy(&nf_flag, h->nonfinite, sizeof(int32_t), cudaMemcpyDeviceToHost));
@@ -1513,9 +1573,9 @@ mgsb_status run_normals(mgsb_solver* h, int32_t body, float4* fscratch, float4* 
     std::fill(out, out + 3 * (size_t)B.V, 0.f);
     for (int j = 0; j < nsv; ++j) {
         const int i = h->nrm_sv_host[sv_off + j] - B.v_off;
-        out[3 * i] = vn[j].x;
-        out[3 * i + 1] = vn[j].y;
-        out[3 * i + 2] = vn[j].z;
+        out[3 * i] = host_stage[j].x;
+        out[3 * i + 1] = host_stage[j].y;
+        out[3 * i + 2] = host_stage[j].z;
     }
     return MGSB_OK;
 }
@@ -1577,6 +1637,43 @@ mgsb_status mgsb_set_material(mgsb_solver* h, int32_t body, const float* youngs,
     B.youngs.assign(youngs, youngs + B.T);
     B.poisson.assign(poisson, poisson + B.T);
     h->dirty = true;
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_get_params(const mgsb_solver* h, mgsb_params* out) {
+    if (!h || !out) return MGSB_INVALID_ARG;
+    *out = h->p;
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_set_params(mgsb_solver* h, const mgsb_params* params) {
+    if (!h) return MGSB_INVALID_ARG;
+    if (!params) return set_err(h, MGSB_INVALID_ARG, "null params");
+    const mgsb_params& q = *params;
+    TRY(validate_params(h, q));
+    if (q.solver != h->p.solver)
+        return set_err(h, MGSB_NOT_SUPPORTED, "the solver kind is fixed at create (%d, asked %d)", h->p.solver, q.solver);
+    if (q.device != h->p.device || q.stream != h->p.stream)
+        return set_err(h, MGSB_NOT_SUPPORTED, "device and stream are fixed at create");
+    if (is_mg(h) && q.precision != h->p.precision)
+        return set_err(h, MGSB_NOT_SUPPORTED, "the precision is fixed at create (its state buffers are allocated there)");
+    if (!(q.density > 0.f) && is_mg(h)) return set_err(h, MGSB_INVALID_ARG, "density must be > 0");
+    const bool material = q.youngs_modulus != h->p.youngs_modulus || q.poisson_ratio != h->p.poisson_ratio;
+    if (material && is_mg(h) && (!(q.youngs_modulus > 0.f) || !(q.poisson_ratio > -1.f && q.poisson_ratio < 0.5f)))
+        return set_err(h, MGSB_INVALID_ARG, "bad material (E=%g, nu=%g)", q.youngs_modulus, q.poisson_ratio);
+    TRY(sync_check(h));
+    h->p = q;
+    for (size_t bi = 0; bi < h->bodies.size(); ++bi) {
+        BodyHost& B = h->bodies[bi];
+        BodyDev& BD = h->bodies_host[bi];
+        for (int c = 0; c < 3; ++c) B.gravity[c] = BD.gravity[c] = q.gravity[c];
+        B.damping = BD.damping = q.damping;
+        if (material) {
+            B.youngs.assign(B.T, q.youngs_modulus);
+            B.poisson.assign(B.T, q.poisson_ratio);
+        }
+    }
+    h->dirty = true;   // the next step rebuilds the plan, the hierarchy and the frame's graph
     return MGSB_OK;
 }
 
@@ -1761,7 +1858,7 @@ mgsb_status mgsb_get_normals(mgsb_solver* h, int32_t body, float* out) {
     if (!out) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
     TRY(ensure_ready(h));
-    return run_normals(h, body, h->nrm_face, h->nrm_out, out);
+    return run_normals(h, body, h->nrm_face, h->nrm_out, nullptr, out);
 }
 
 mgsb_status mgsb_set_state(mgsb_solver* h, int32_t body, const float* positions, const float* velocities) {
@@ -2002,9 +2099,21 @@ mgsb_status mgsb_set_coarse_split(mgsb_solver* h, int32_t split) {
     return MGSB_OK;
 }
 
+mgsb_status mgsb_set_surface_contact(mgsb_solver* h, int32_t mode) {
+    if (!h || (mode != MGSB_CONTACT_VERTICES && mode != MGSB_CONTACT_VERTICES_AND_TRIANGLES)) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the capsule contact applies to the multigrid kinds");
+    if (mode == MGSB_CONTACT_VERTICES_AND_TRIANGLES && h->broad_phase)
+        return set_err(h, MGSB_NOT_SUPPORTED, "the triangle test runs over all surface triangles: turn the broad phase off");
+    h->tri_contact = mode == MGSB_CONTACT_VERTICES_AND_TRIANGLES;
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
 mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on) {
     if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
     if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the broad phase applies to the multigrid kinds");
+    if (on && h->tri_contact)
+        return set_err(h, MGSB_NOT_SUPPORTED, "the broad phase bins vertices only: turn the triangle contact off first");
     TRY(ensure_ready(h));
     CUDA_TRY(h, cudaSetDevice(h->device));
     h->broad_phase = on != 0;
@@ -2277,24 +2386,48 @@ constexpr int kNoAllocMaxDevices = 64;
 // every triangle slot it reads and every vertex slot it copies out.
 static __device__ __align__(256) float4 g_noalloc_scratch[kNoAllocMaxTris + kNoAllocMaxSurfVerts];
 
-// Device address of the scratch on h's device, looked up once per device with
-// that device current (cudaGetSymbolAddress; no allocation).  The first call on
-// a device does this set-up, so make that first call outside any stream capture.
+// The driver's cuCtxGetCurrent, fetched through the runtime (no link against
+// libcuda): the context a cached symbol address belongs to.
+using CtxGetCurrentFn = int (*)(void**);
+
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    return fn;
+}
+
+// Device address of the scratch on h's device (cudaGetSymbolAddress; no
+// allocation), looked up with that device current once per device and context:
+// if the device's context is destroyed and created again (cudaDeviceReset by
+// the host or another library), the module may load at another address, so a
+// new context repeats the look-up.  The first call on a device (and the first
+// after such a reset) does this set-up, so make it outside any stream capture.
 mgsb_status noalloc_scratch(mgsb_solver* h, float4** out) {
     static std::mutex mu;
     static float4* ptr[kNoAllocMaxDevices] = {};
+    static void* ctx[kNoAllocMaxDevices] = {};
     if (h->device < 0 || h->device >= kNoAllocMaxDevices)
         return set_err(h, MGSB_NOT_SUPPORTED, "device %d: the allocation-free path supports devices 0..%d", h->device,
                        kNoAllocMaxDevices - 1);
     std::lock_guard<std::mutex> lock(mu);
-    if (!ptr[h->device]) {
-        CUDA_TRY(h, cudaSetDevice(h->device));
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    void* cur = nullptr;
+    const CtxGetCurrentFn get = ctx_get_current();
+    if (!get || get(&cur) != 0) cur = nullptr;   // unknown context: look the address up on every call
+    if (!ptr[h->device] || !cur || cur != ctx[h->device]) {
         float4* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return set_err(h, MGSB_CUDA_ERROR, "cudaGetSymbolAddress of the normals scratch failed on device %d: %s",
                            h->device, cudaGetErrorString(e));
         ptr[h->device] = p;
+        ctx[h->device] = cur;
     }
     *out = ptr[h->device];
     return MGSB_OK;
@@ -2317,32 +2450,8 @@ extern "C" mgsb_status mgsb_get_normals_noalloc(mgsb_solver* h, int32_t body, fl
                        body, nf, nsv, kNoAllocMaxTris, kNoAllocMaxSurfVerts);
     float4* scratch = nullptr;
     TRY(noalloc_scratch(h, &scratch));
-    float4* fscratch = scratch;
-    float4* vscratch = scratch + kNoAllocMaxTris;
-    const int f_off = h->nrm_f_off[body], sv_off = h->nrm_sv_off[body];
-    CUDA_TRY(h, cudaSetDevice(h->device));
-    if (nf > 0) {
-        k_tri_normals<<<(nf + 255) / 256, 256, 0, h->stream>>>(nf, h->nrm_tris + f_off, h->x, fscratch);
-        k_vert_normals<<<(nsv + 255) / 256, 256, 0, h->stream>>>(nsv, h->nrm_ptr + sv_off, h->nrm_fidx, fscratch, vscratch);
-        CUDA_TRY(h, cudaGetLastError());
-    }
     // the solver's pinned readback buffer (N0 float4, allocated at create) takes the copy
-    if (nsv > 0)
-        CUDA_TRY(h, cudaMemcpyAsync(h->readback, vscratch, nsv * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    int32_t nonfinite = 0;
-    CUDA_TRY(h, cudaMemcpy(&nonfinite, h->nonfinite, sizeof(int32_t), cudaMemcpyDeviceToHost));
-    if (nonfinite) return set_err(h, MGSB_DIVERGED, "non-finite positions detected");
-    const BodyHost& B = h->bodies[body];
-    const float4* vn = reinterpret_cast<const float4*>(h->readback);
-    std::fill(out, out + 3 * (size_t)B.V, 0.f);
-    for (int j = 0; j < nsv; ++j) {
-        const int i = h->nrm_sv_host[sv_off + j] - B.v_off;
-        out[3 * i] = vn[j].x;
-        out[3 * i + 1] = vn[j].y;
-        out[3 * i + 2] = vn[j].z;
-    }
-    return MGSB_OK;
+    return run_normals(h, body, scratch, scratch + kNoAllocMaxTris, reinterpret_cast<float4*>(h->readback), out);
 }
 
 // ===========================================================================

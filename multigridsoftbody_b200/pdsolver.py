@@ -91,8 +91,23 @@ class PDSolver:
         self.m_tetVertFixed = np.where(fixed > 0, 0.0, 1.0).astype(np.float32)  # reference flag: 0 = fixed
         self._solver.set_fixed(fixed)
 
+    def _sync_params(self) -> None:
+        """The reference reads its public fields at every Step, so assignments after Init take effect on
+        the next frame; here a changed field goes to the solver through mgsb_set_params."""
+        p = self._solver.get_params()
+        want = {"iterations": int(self.m_iterNum), "dt": float(self.m_dt), "damping": float(self.m_damping),
+                "volume_stiffness": float(self.m_volumnStiffness),
+                "collision_stiffness": float(self.m_collisionStiffness), "cheb_rho": float(self.m_rho)}
+        g = (float(self.m_gravityX), float(self.m_gravityY), float(self.m_gravityZ))
+        changed = {k: v for k, v in want.items() if getattr(p, k) != type(v)(np.float32(v) if isinstance(v, float) else v)}
+        if tuple(float(x) for x in p.gravity) != tuple(float(np.float32(x)) for x in g):
+            changed["gravity"] = g
+        if changed:
+            self._solver.set_params(**changed)
+
     # PDSolver::Step (PDSolver.cpp:243-293) incl. the render readback
     def Step(self) -> None:
+        self._sync_params()
         cols = [c for c in self.m_sphereColliders]
         if cols:
             self._solver.set_spheres(np.stack([c.m_position for c in cols]), [c.m_radius for c in cols],

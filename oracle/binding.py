@@ -37,6 +37,9 @@ def _load():
         "oracle_set_fixed": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
         "oracle_set_material": (C.c_int, [C.c_void_p, _FP, _FP]),
         "oracle_set_tool_capsule": (C.c_int, [C.c_void_p, _FP, _FP, C.c_float]),
+        "oracle_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "oracle_set_surface_contact": (C.c_int, [C.c_void_p, C.c_int]),
+        "oracle_segment_triangle": (C.c_double, [_DP, _DP, _DP, _DP]),
         "oracle_set_tool_spheres": (C.c_int, [C.c_void_p, C.c_int32, _FP, _FP, C.POINTER(C.c_uint8)]),
         "oracle_step": (C.c_int, [C.c_void_p]),
         "oracle_num_verts": (C.c_int, [C.c_void_p]),
@@ -48,6 +51,7 @@ def _load():
         "oracle_get_precompute": (None, [C.c_void_p, _DP, _DP, _DP, _DP, _DP]),
         "oracle_get_energy": (None, [C.c_void_p, _DP]),
         "oracle_last_residual": (C.c_double, [C.c_void_p]),
+        "oracle_set_threads": (C.c_int, [C.c_int]),
         "oracle_level_size": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP]),
         "oracle_level_prolongation": (C.c_int, [C.c_void_p, C.c_int, _IP, _DP]),
         "oracle_level_matrix": (C.c_int, [C.c_void_p, C.c_int, _DP, _IP, _IP, _DP]),
@@ -68,6 +72,11 @@ def _load():
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def set_threads(n: int = 0) -> int:
+    """Host threads of the oracle's OpenMP loops (0: all); returns the count in force."""
+    return int(_load().oracle_set_threads(int(n)))
 
 
 def _dp(a):
@@ -110,6 +119,15 @@ class Oracle:
         e = np.ascontiguousarray(np.broadcast_to(np.asarray(youngs, np.float32), (self.T,)))
         n = np.ascontiguousarray(np.broadcast_to(np.asarray(poisson, np.float32), (self.T,)))
         self._lib.oracle_set_material(self.h, e.ctypes.data_as(_FP), n.ctypes.data_as(_FP))
+
+    def set_params(self, params):
+        self._params = params
+        st = self._lib.oracle_set_params(self.h, C.byref(params))
+        if st != 0:
+            raise RuntimeError(f"oracle_set_params: status {st}")
+
+    def set_surface_contact(self, triangles=True):
+        self._lib.oracle_set_surface_contact(self.h, 1 if triangles else 0)
 
     def set_capsule(self, a, b, radius):
         aa = np.asarray(a, np.float32)
@@ -210,6 +228,17 @@ def svd_rotation(F):
     R = np.empty(9)
     lib.oracle_svd_rotation(_dp(F), _dp(R))
     return R.reshape(3, 3)
+
+
+def segment_triangle(p0, p1, a, b, c):
+    """Distance between segment p0p1 and triangle abc, and the closest points (on the segment, on the
+    triangle)."""
+    seg = np.ascontiguousarray(np.concatenate([p0, p1]), np.float64)
+    tri = np.ascontiguousarray(np.concatenate([a, b, c]), np.float64)
+    q = np.zeros(3)
+    h = np.zeros(3)
+    d = _load().oracle_segment_triangle(_dp(seg), _dp(tri), _dp(q), _dp(h))
+    return d, q, h
 
 
 def surface_normals(positions, tris):

@@ -226,6 +226,10 @@ struct Oracle {
     V3 cap_a{}, cap_b{};
     double cap_r = 0;
     std::vector<int> surface_verts;
+    // capsule against the surface triangles too (mgsb_set_surface_contact):
+    // per surface triangle its three vertices and the fourth vertex of its tet
+    bool tri_contact = false;
+    std::vector<std::array<int, 4>> cap_tris;
     std::vector<double> c0;      // contact weight per vertex
     std::vector<V3> target;
     std::vector<double> Ldiag;   // L diagonal at level 0
@@ -277,15 +281,21 @@ bool precompute(Oracle& o, std::string& err) {
 
 void build_surface(Oracle& o) {
     std::map<std::array<int, 3>, int> cnt;
+    std::map<std::array<int, 3>, std::array<int, 4>> face_of;   // a face and the tet vertex opposite it
     for (int t = 0; t < o.T; ++t) {
         const int* v = &o.tets[4 * t];
-        const int f[4][3] = {{v[0], v[2], v[1]}, {v[0], v[1], v[3]}, {v[0], v[3], v[2]}, {v[1], v[2], v[3]}};
+        const int f[4][4] = {{v[0], v[2], v[1], v[3]}, {v[0], v[1], v[3], v[2]}, {v[0], v[3], v[2], v[1]},
+                             {v[1], v[2], v[3], v[0]}};
         for (auto& ff : f) {
             std::array<int, 3> k = {ff[0], ff[1], ff[2]};
             std::sort(k.begin(), k.end());
             cnt[k]++;
+            face_of[k] = {ff[0], ff[1], ff[2], ff[3]};
         }
     }
+    o.cap_tris.clear();
+    for (auto& kv : cnt)
+        if (kv.second == 1) o.cap_tris.push_back(face_of[kv.first]);
     std::vector<char> on(o.V, 0);
     o.surf_tris.clear();
     for (auto& kv : cnt)
@@ -779,6 +789,128 @@ void vcycle(const Oracle& o, int l, const Vec& r, Vec& e) {
     for (int k = 0; k < o.p.post_sweeps; ++k) sweep();
 }
 
+// ---- capsule against the surface triangles --------------------------------
+// Distance from point p to segment [a, b], with the closest point.
+double point_segment(const V3& p, const V3& a, const V3& b, V3& cl) {
+    const V3 ab = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double l2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+    double t = 0;
+    if (l2 > 0) t = std::min(1.0, std::max(0.0, ((p[0] - a[0]) * ab[0] + (p[1] - a[1]) * ab[1] + (p[2] - a[2]) * ab[2]) / l2));
+    cl = {a[0] + t * ab[0], a[1] + t * ab[1], a[2] + t * ab[2]};
+    return std::sqrt((p[0] - cl[0]) * (p[0] - cl[0]) + (p[1] - cl[1]) * (p[1] - cl[1]) + (p[2] - cl[2]) * (p[2] - cl[2]));
+}
+
+// Closest points of triangle (A, B, C) and segment [P0, P1]: the minimum over
+// (i) each segment end point against the triangle -- its projection on the
+// plane when that lies inside the triangle, else the nearest edge point --,
+// (ii) each triangle edge against the segment -- the interior critical point
+// of the two-parameter distance when it lies inside both, else the four end
+// point / segment distances -- and (iii) the segment crossing the face.
+// Returns the distance; h on the triangle, q on the segment.
+double segment_triangle(const V3& P0, const V3& P1, const V3& A, const V3& B, const V3& C, V3& q, V3& h) {
+    auto sub = [](const V3& a, const V3& b) { return V3{a[0] - b[0], a[1] - b[1], a[2] - b[2]}; };
+    auto dot = [](const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    auto cross = [](const V3& a, const V3& b) {
+        return V3{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    };
+    auto dist = [&](const V3& a, const V3& b) { return std::sqrt(dot(sub(a, b), sub(a, b))); };
+    const V3 n = cross(sub(B, A), sub(C, A));
+    const double nn = dot(n, n);
+    auto inside = [&](const V3& x) {
+        return dot(cross(sub(B, A), sub(x, A)), n) >= 0 && dot(cross(sub(C, B), sub(x, B)), n) >= 0 &&
+               dot(cross(sub(A, C), sub(x, C)), n) >= 0;
+    };
+    const V3 E[3][2] = {{A, B}, {B, C}, {C, A}};
+    double best = 1e300;
+    auto take = [&](double dd, const V3& qq, const V3& hh) {
+        if (dd < best) {
+            best = dd;
+            q = qq;
+            h = hh;
+        }
+    };
+    for (const V3& P : {P0, P1}) {   // (i)
+        if (nn > 0) {
+            const double sd = dot(n, sub(P, A)) / nn;
+            const V3 pr = {P[0] - sd * n[0], P[1] - sd * n[1], P[2] - sd * n[2]};
+            if (inside(pr)) take(dist(P, pr), P, pr);
+        }
+        for (auto& e : E) {
+            V3 cl;
+            take(point_segment(P, e[0], e[1], cl), P, cl);
+        }
+    }
+    for (auto& e : E) {   // (ii)
+        const V3 u = sub(P1, P0), v = sub(e[1], e[0]), w = sub(P0, e[0]);
+        const double a = dot(u, u), b = dot(u, v), c = dot(v, v), d = dot(u, w), ee = dot(v, w);
+        const double den = a * c - b * b;
+        if (den > 1e-300 * std::max(1.0, a * c)) {
+            const double s = (b * ee - c * d) / den, t = (a * ee - b * d) / den;
+            if (s > 0 && s < 1 && t > 0 && t < 1) {
+                const V3 qs = {P0[0] + s * u[0], P0[1] + s * u[1], P0[2] + s * u[2]};
+                const V3 ht = {e[0][0] + t * v[0], e[0][1] + t * v[1], e[0][2] + t * v[2]};
+                take(dist(qs, ht), qs, ht);
+            }
+        }
+        for (const V3& X : {e[0], e[1]}) {   // edge end points against the segment
+            V3 cl;
+            take(point_segment(X, P0, P1, cl), cl, X);
+        }
+    }
+    if (nn > 0) {   // (iii)
+        const double s0 = dot(n, sub(P0, A)), s1 = dot(n, sub(P1, A));
+        if (((s0 <= 0 && s1 >= 0) || (s0 >= 0 && s1 <= 0)) && s0 != s1) {
+            const double t = s0 / (s0 - s1);
+            const V3 X = {P0[0] + t * (P1[0] - P0[0]), P0[1] + t * (P1[1] - P0[1]), P0[2] + t * (P1[2] - P0[2])};
+            if (inside(X)) take(0.0, X, X);
+        }
+    }
+    return best;
+}
+
+// Triangle contacts of the frame: every surface triangle closer to the
+// capsule's segment than its radius pushes its vertices out by
+// (h - q)/|h - q| (r - |h - q|) (r along the inward normal when the segment
+// touches the face); a surface vertex not itself inside the capsule but on
+// such triangles becomes a contact with target s + the mean of their pushes.
+// The capsule form of the reference's sphere test DCDByTriangle_sphere_V2
+// (PDSolver.cu:612-680) with its response (PDSolver.cu:462-501).
+void capsule_triangles(Oracle& o) {
+    const int F = (int)o.cap_tris.size();
+    std::vector<V3> psum(o.V, V3{0, 0, 0});
+    std::vector<int> pcnt(o.V, 0);
+    const V3 P0 = o.cap_a, P1 = o.cap_b;
+    const double r = o.cap_r;
+    for (int f = 0; f < F; ++f) {
+        const auto& t = o.cap_tris[f];
+        const V3 A = o.s[t[0]], B = o.s[t[1]], C = o.s[t[2]], D = o.s[t[3]];
+        V3 q, h;
+        const double d = segment_triangle(P0, P1, A, B, C, q, h);
+        if (!(d < r)) continue;
+        V3 push;
+        if (d > 1e-12) {
+            for (int c = 0; c < 3; ++c) push[c] = (h[c] - q[c]) / d * (r - d);
+        } else {
+            const V3 ab = {B[0] - A[0], B[1] - A[1], B[2] - A[2]}, ac = {C[0] - A[0], C[1] - A[1], C[2] - A[2]};
+            V3 n = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2], ab[0] * ac[1] - ab[1] * ac[0]};
+            const double nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            const double toward_d = n[0] * (D[0] - A[0]) + n[1] * (D[1] - A[1]) + n[2] * (D[2] - A[2]);
+            const double sg = toward_d > 0 ? 1.0 : -1.0;
+            for (int c = 0; c < 3; ++c) push[c] = nl > 0 ? sg * r * n[c] / nl : 0.0;
+        }
+        for (int k = 0; k < 3; ++k) {
+            for (int c = 0; c < 3; ++c) psum[t[k]][c] += push[c];
+            ++pcnt[t[k]];
+        }
+    }
+    for (int i : o.surface_verts) {
+        if (o.collided[i] || pcnt[i] == 0) continue;
+        o.collided[i] = 1;
+        o.c0[i] = o.fixed[i] ? 0.0 : (double)o.p.contact_stiffness;
+        for (int c = 0; c < 3; ++c) o.target[i][c] = o.s[i][c] + psum[i][c] / pcnt[i];
+    }
+}
+
 void mg_frame(Oracle& o) {
     const int V = o.V;
     const double dt = o.p.dt, ih2 = 1.0 / (dt * dt);
@@ -817,6 +949,7 @@ void mg_frame(Oracle& o) {
             o.c0[i] = o.fixed[i] ? 0.0 : (double)o.p.contact_stiffness;
             o.target[i] = {q[0] + o.cap_r * nrm[0], q[1] + o.cap_r * nrm[1], q[2] + o.cap_r * nrm[2]};
         }
+        if (o.tri_contact) capsule_triangles(o);
     }
     // lumped contact weights on the coarse levels, coarsest factorisation
     const int L = o.p.levels;
@@ -1001,6 +1134,39 @@ int oracle_set_material(oracle_solver* h, const float* youngs, const float* pois
     return 0;
 }
 
+int oracle_set_params(oracle_solver* h, const mgsb_params* params) {
+    Oracle& o = h->o;
+    if (!params || params->solver != o.p.solver) return MGSB_NOT_SUPPORTED;
+    const bool material = params->youngs_modulus != o.p.youngs_modulus || params->poisson_ratio != o.p.poisson_ratio;
+    o.p = *params;
+    if (material) {
+        o.youngs.assign(o.T, params->youngs_modulus);
+        o.poisson.assign(o.T, params->poisson_ratio);
+    }
+    std::string e;
+    if (!precompute(o, e)) return MGSB_INVALID_ARG;
+    if (o.p.solver == MGSB_SOLVER_MULTIGRID) assemble_L(o);
+    o.hierarchy_dirty = true;
+    return 0;
+}
+
+double oracle_segment_triangle(const double* p0p1, const double* abc, double* q, double* h) {
+    const V3 P0 = {p0p1[0], p0p1[1], p0p1[2]}, P1 = {p0p1[3], p0p1[4], p0p1[5]};
+    const V3 A = {abc[0], abc[1], abc[2]}, B = {abc[3], abc[4], abc[5]}, C = {abc[6], abc[7], abc[8]};
+    V3 qq, hh;
+    const double d = segment_triangle(P0, P1, A, B, C, qq, hh);
+    for (int c = 0; c < 3; ++c) {
+        q[c] = qq[c];
+        h[c] = hh[c];
+    }
+    return d;
+}
+
+int oracle_set_surface_contact(oracle_solver* h, int mode) {
+    h->o.tri_contact = mode == 1;
+    return 0;
+}
+
 int oracle_set_tool_capsule(oracle_solver* h, const float a[3], const float b[3], float radius) {
     Oracle& o = h->o;
     o.have_capsule = radius > 0;
@@ -1017,6 +1183,16 @@ int oracle_set_tool_spheres(oracle_solver* h, int32_t count, const float* center
     for (int i = 0; i < count; ++i)
         o.spheres.push_back({{centers[3 * i], centers[3 * i + 1], centers[3 * i + 2]}, radii[i], active ? active[i] != 0 : true});
     return 0;
+}
+
+int oracle_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
 }
 
 int oracle_step(oracle_solver* h) {

@@ -39,6 +39,14 @@ oracle_solver* oracle_create(const mgsb_mesh* mesh, const mgsb_params* params, c
 void oracle_destroy(oracle_solver* h);
 int oracle_set_fixed(oracle_solver* h, const uint8_t* mask);
 int oracle_set_material(oracle_solver* h, const float* youngs, const float* poisson);
+/* Capsule narrow phase: 0 vertices, 1 vertices and surface triangles
+ * (the rule of mgsb_set_surface_contact). */
+int oracle_set_surface_contact(oracle_solver* h, int mode);
+/* Distance between segment p0p1[6] and triangle abc[9], closest points q
+ * (segment) and h (triangle). */
+double oracle_segment_triangle(const double* p0p1, const double* abc, double* q, double* h);
+/* Parameters changed between frames (same rules as mgsb_set_params). */
+int oracle_set_params(oracle_solver* h, const mgsb_params* params);
 int oracle_set_tool_capsule(oracle_solver* h, const float a[3], const float b[3], float radius);
 int oracle_set_tool_spheres(oracle_solver* h, int32_t count, const float* centers, const float* radii,
                             const uint8_t* active);
@@ -56,6 +64,8 @@ void oracle_get_precompute(const oracle_solver* h, double* inv, double* ac, doub
 void oracle_get_energy(const oracle_solver* h, double out[5]);
 /* Fine-level residual norm of the PD global system after the last iteration. */
 double oracle_last_residual(const oracle_solver* h);
+/* Host threads of the OpenMP loops (n <= 0: all); returns the count in force. */
+int oracle_set_threads(int n);
 
 /* Hierarchy inspection (level >= 1): sizes, and the Galerkin matrix in CSR
  * with the diagonal first in each row. */

@@ -9,7 +9,8 @@
 # repository; only the built library lands in oracle/_ref/ (git-ignored).
 set -eu
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${MGSB_REFERENCE_DIR:-/root/reference}/MultiGridSoftBody/src
+# the reference checkout: MGSB_REFERENCE_DIR, else a directory "reference" beside the repository
+REF=${MGSB_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}/MultiGridSoftBody/src
 OUT="$HERE/_ref"
 if [ ! -d "$REF" ]; then
     echo "ref_build: reference sources not found at $REF; skipping" >&2

@@ -19,8 +19,8 @@ class FakeMesh:
         return 10.0
 
 
-def fake_solver(error_of):
-    """A solver class that ends at positions error_of(params, learned) away from the converged ones."""
+def fake_solver(error_of, axes=(1.0, 0.0, 0.0)):
+    """A solver class that ends at positions error_of(params, learned) x axes away from the converged ones."""
 
     class Solver:
         def __init__(self, mesh, p):
@@ -41,7 +41,8 @@ def fake_solver(error_of):
 
         def _x(self):
             converged = (self.p.refinement_passes == 6 and not self.learned)
-            return np.full((4, 3), 0.0 if converged else error_of(self.p, self.learned))
+            e = 0.0 if converged else error_of(self.p, self.learned)
+            return np.tile(np.asarray(axes, np.float64) * e, (4, 1))
 
         def positions_f64(self):
             return self._x()
@@ -86,7 +87,7 @@ def test_fastest_candidate_within_the_bar():
     assert (1, 1, False) not in timed
     for fam in ("learned_mixed", "plain_fp32"):
         for r in out[fam]["candidates"]:
-            assert ("ms_per_frame" in r) == (r["err_over_diag"] <= sweeps.ERROR_BAR)
+            assert ("ms_per_frame" in r) == (r["err_over_diag"] <= sweeps.ERROR_BAR) == r["within_bar"]
 
 
 def test_no_candidate_within_the_bar():
@@ -99,3 +100,29 @@ def test_without_a_network_only_the_plain_family():
     out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), None, tool, lambda p, net: 1.0,
                                frames=2, solver_cls=fake_solver(lambda p, learned: 0.0))
     assert "learned_mixed" not in out and out["plain_fp32"]["chosen"] is not None
+
+
+def test_error_is_the_vertex_distance():
+    """An error spread over all three axes counts with its Euclidean length: 0.8e-5 per axis is within a
+    1e-5 bar coordinate by coordinate, but the vertex is 1.39e-5 away, so no candidate qualifies."""
+    out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), object(), tool, lambda p, net: 1.0,
+                               frames=2, solver_cls=fake_solver(lambda p, learned: 0.8e-4, axes=(1.0, 1.0, 1.0)))
+    for fam in ("learned_mixed", "plain_fp32"):
+        assert out[fam]["chosen"] is None
+        for r in out[fam]["candidates"]:
+            assert abs(r["err_over_diag"] - 0.8e-5 * np.sqrt(3.0)) < 1e-12
+    assert sweeps.max_vertex_error(np.array([[3.0, 4.0, 0.0], [0.0, 0.0, 1.0]]), np.zeros((2, 3))) == 5.0
+
+
+def test_time_all_times_every_candidate():
+    """With time_all every candidate carries its frame time; the choice still comes from within the bar."""
+    def err(p, learned):
+        return 0.0 if p.refinement_passes >= 2 else 1.0
+
+    out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), None, tool,
+                               lambda p, net: 10.0 - p.refinement_passes, frames=2, solver_cls=fake_solver(err),
+                               time_all=True)
+    rows = out["plain_fp32"]["candidates"]
+    assert all("ms_per_frame" in r for r in rows)
+    assert out["plain_fp32"]["chosen"]["key"] == "plain_fp32_3pass_1+1"
+    assert not any(r["within_bar"] for r in rows if r["passes"] == 1)
