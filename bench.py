@@ -277,6 +277,15 @@ def algorithmic_bytes(kernel, solver, meshes, params):
         # FP64 displacement (read + write 64 B) and its FP32 mirror (16 B)
         mixed = params.precision == 1
         return (40 + (80 if mixed else 0)) * n0 + 8 * nnz0
+    if kernel == "k_mx_residual":
+        # FP64 outer residual: ELL value 8 + column 4 B per entry; per row the FP64 displacement (32), diagonal
+        # (8), contact weight, Jacobi weight, fix flag (12), r32 and e out (32), the learned start residual (16)
+        # and the right-hand side: read (32) or, in a PD iteration's first pass, assembled from b0 (32) and the
+        # row's slots (64 B per tet over the body) and written (32)
+        per_row = 32 + 8 + 12 + 32 + 16
+        first = 32 + 32 + 4 + 64 * T / max(n0, 1)
+        k = max(params.refinement_passes, 1)
+        return 12 * nnz0 + n0 * (per_row + (first + (k - 1) * 32) / k)
     if kernel == "k_ls_sweep_tc":
         # learned sweep: level-0 row walk (8 B/nnz, r/D/L/fix 28 B per row) + d read/write 32 B per row;
         # the 12.9 KB weight image per CTA comes from L2
@@ -439,9 +448,15 @@ def run_reference(args):
 LEARNED = ("beam", "blob")
 
 
-def train_network(mg, name, device, stream_ptr, runs=8, frames=40, every=10, sweeps=3, steps=20000):
+TRAIN_RUNS = {"beam": (8, 10), "blob": (32, 20)}   # seeded runs, pairs every k frames (40 frames per run)
+
+
+def train_network(mg, name, device, stream_ptr, runs=None, frames=40, every=None, sweeps=3, steps=20000):
     """Pairs from the plain FP32 multigrid solver on seeded runs of the same scene (tool seeds other than
-    the benchmark's), then the library's own trainer (Adam, 4096-pair minibatches)."""
+    the benchmark's), then the library's own trainer (Adam, 4096-pair minibatches).  The blob (config 4)
+    takes the configured 32 runs (~1M pairs); the beam headline 8 runs."""
+    default_runs, default_every = TRAIN_RUNS.get(name, (8, 10))
+    runs, every = runs or default_runs, every or default_every
     from multigridsoftbody_b200.learned import MLP, blob_scene, blob_tool_path
     t0 = time.perf_counter()
     if name == "blob":
@@ -657,7 +672,8 @@ def run_ours(args):
         net.params = np.load(args.load_weights)
         net_info = {"weights": os.path.basename(args.load_weights), "trained": "earlier run (--save-weights)"}
     elif args.workload in LEARNED:
-        net, net_info = train_network(mg, args.workload, local, stream.cuda_stream)
+        net, net_info = train_network(mg, args.workload, local, stream.cuda_stream,
+                                      runs=args.train_runs or None, every=args.train_every or None)
         if args.save_weights and rank == 0:
             np.save(args.save_weights, net.params)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
@@ -871,6 +887,20 @@ def run_ours(args):
                     "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kavg_ms,
                     "duration_source": source, "share_of_frame": share,
                     "avg_launch_ms_profiled": prof[kname][0] / max(prof[kname][1], 1)}
+            # whole frame: every launch of every kernel with an algorithmic-byte figure, over the frame time
+            fb, missing = 0.0, []
+            for k, (kms, cnt) in prof.items():
+                b = algorithmic_bytes(k, solver, meshes, params[0])
+                if b is None:
+                    missing.append(k)
+                else:
+                    fb += b * cnt
+            fms = ms / args.steps
+            roof["frame"] = {"algorithmic_bytes": fb, "ms": fms, "achieved_gbs": fb / (fms / 1e3) / 1e9,
+                             "frame_frac": fb / (fms / 1e3) / 1e9 / peak,
+                             "survey_estimate_bytes": params[0].iterations * (
+                                 168.0 * sum(m.num_tets for m in meshes) + 1139.0 * sum(m.num_verts for m in meshes)),
+                             "kernels_without_a_figure": sorted(missing)}
         cpu = None
         if world == 1 and not args.no_cpu:
             cpu = cpu_baseline(meshes, workload_params, fixeds, tool, mats, args,
@@ -928,6 +958,8 @@ def main():
     ap.add_argument("--broad-phase", action="store_true", help="uniform-grid broad phase for the tool contact")
     ap.add_argument("--no-compare", action="store_true",
                     help="learned workloads: skip the plain-solver timings and the accuracy runs (profiling)")
+    ap.add_argument("--train-runs", type=int, default=0, help="learned workloads: seeded training runs (0: workload's)")
+    ap.add_argument("--train-every", type=int, default=0, help="learned workloads: pairs every k frames (0: workload's)")
     ap.add_argument("--save-weights", default="", help="learned workloads: save the trained network (.npy)")
     ap.add_argument("--load-weights", default="", help="learned workloads: use these weights instead of training")
     args = ap.parse_args()
