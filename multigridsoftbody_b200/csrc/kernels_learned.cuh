@@ -155,6 +155,58 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_features(int n, const int32_t
         for (int k = 0; k < kMlpIn; ++k) xf[(size_t)row * kMlpIn + k] = f[k];
 }
 
+// Per-frame row constants of the learned sweep's features, from this frame's
+// diagonal D (contacts included): rc_i = (D_i / sa_i, (D_i - L_ii) / D_i,
+// D_i sa_i / sd_i, 1 / sa_i) with sa_i = sum_j |a_ij| and sd_i = sum_j |a_ij| D_j
+// over the level-0 off-diagonal row (4 lanes per row).  The sweep then needs
+// only |a_ij| r_j from each neighbour.
+__global__ void __launch_bounds__(kLsThreads) k_ls_row_consts(int n, const int32_t* __restrict__ sp,
+                                                              const int32_t* __restrict__ col,
+                                                              const float* __restrict__ val,
+                                                              const float* __restrict__ dfull,
+                                                              const float* __restrict__ diag0, float4* __restrict__ rc) {
+    pdl_enter();
+    constexpr int G = kLanesL0, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    float sa = 0.f, sd = 0.f;
+    if (valid) {
+        const int slice = row / S;
+        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
+        for (int e = beg + (lane / S) * S + (row - slice * S); e < end; e += 32) {
+            const float a = fabsf(__ldg(val + e));
+            sa += a;
+            sd = fmaf(a, __ldg(dfull + __ldg(col + e)), sd);
+        }
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sd += __shfl_xor_sync(0xffffffffu, sd, o);
+    }
+    if (!valid || lane >= S) return;
+    const float D = __ldg(dfull + row), L = __ldg(diag0 + row);
+    const float inv_a = sa > 0.f ? 1.f / sa : 0.f;
+    rc[row] = make_float4(D * inv_a, (D - L) / D, sd > 0.f ? D * sa / sd : 1.f, inv_a);
+}
+
+// Rows of the residual window of a 128-row tile that the learned sweep stages in
+// shared memory: [win.x, win.y) holds the tile's rows and every column of their
+// sliced-ELL entries (padding included); win.x == win.y: no window (gather from
+// global memory).
+constexpr int kLsWinRows = 3072;   // 48 KiB of float4
+constexpr int kLsPerThread = 8;    // ELL entries a thread loads ahead (2 threads per row: rows up to 16 wide)
+
+// Dynamic shared memory of k_ls_sweep_tc: the MLP's operands and barriers, then
+// the residual window; at least 80 KiB (two CTAs per SM at most, so that
+// tcgen05.alloc never waits).
+inline size_t ls_sweep_smem_bytes() {
+    const size_t b = ((sizeof(MlpSmem) + 127) / 128) * 128 + (size_t)kLsWinRows * sizeof(float4);
+    return b > 80 * 1024 ? b : (size_t)80 * 1024;
+}
+
 // One learned sweep in a single kernel: per 128-row tile, each thread forms its
 // row's features straight into the shared-memory operand tile, the tensor-core
 // MLP runs on the tile, and the same thread applies d_i += (s_i/D_i) y_i.
@@ -165,7 +217,7 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_features(int n, const int32_t
 __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, const int32_t* __restrict__ sp,
                                                              const int32_t* __restrict__ col, const float* __restrict__ val,
                                                              const float* __restrict__ dfull,
-                                                             const float* __restrict__ diag0,
+                                                             const float4* __restrict__ rc, const int2* __restrict__ win,
                                                              const float* __restrict__ fixf, const float4* __restrict__ r,
                                                              const uint8_t* __restrict__ img, float4* __restrict__ d,
                                                              int32_t* __restrict__ err, double4* __restrict__ dd64,
@@ -174,55 +226,101 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
     constexpr int S = 32 / kLanesL0;   // level-0 slice height
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     MlpSmem& Sm = *reinterpret_cast<MlpSmem*>(smem_raw);
+    float4* rwin = reinterpret_cast<float4*>(smem_raw + ((sizeof(MlpSmem) + 127) / 128) * 128);
     WaitState ws;
-    uint32_t ph_load = 0, ph_mma = 0;
+    uint32_t ph_load = 0, ph_mma = 0, ph_win = 0;
     // Prologue before the wait for the previous kernel: TMEM, barriers and the
     // weight copy (the weight image is not written by any kernel of a frame);
     // the copy also overlaps the first tile's feature gather.
     const uint32_t tmem = mlp_cta_setup(Sm, img, ws, ph_load, err, false);
     pdl_wait();
     bool weights_pending = true;
-    __shared__ float part[5][kMlpTile];   // second half's 1-ring sums
+    __shared__ float part[3][kMlpTile];   // second half's 1-ring sums
     const int rt = threadIdx.x & (kMlpTile - 1), half = threadIdx.x >> 7;   // 2 threads per row
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         __syncthreads();
         if (Sm.stop) break;
+        const int2 wv = __ldg(win + tile);
+        const bool use_win = wv.y > wv.x;
+        if (use_win && threadIdx.x == 0) {   // the residual rows this tile reads, in one bulk copy
+            mbar_expect_tx(&Sm.bar_win, (uint32_t)(wv.y - wv.x) * 16u);
+            bulk_g2s(rwin, r + wv.x, (uint32_t)(wv.y - wv.x) * 16u, &Sm.bar_win);
+        }
         const int row = tile * kMlpTile + rt;
-        float sx = 0.f, sy = 0.f, sz = 0.f, sa = 0.f, sd = 0.f;
+        // this thread's entries of the row (the two threads of a row take alternate entries), loaded
+        // while the window is in flight
+        int e0 = 0, end = 0;
+        int jc[kLsPerThread];
+        float av[kLsPerThread];
         if (row < n) {
-            // the two threads of a row take alternate entries of its sliced-ELL row
             const int slice = row / S;
-            const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
-#pragma unroll 4
-            for (int e = beg + (row - slice * S) + half * S; e < end; e += 2 * S) {
+            end = __ldg(sp + slice + 1);
+            e0 = __ldg(sp + slice) + (row - slice * S) + half * S;
+        }
+#pragma unroll
+        for (int k = 0; k < kLsPerThread; ++k) {
+            const int e = e0 + k * 2 * S;
+            const bool ok = e < end;
+            jc[k] = ok ? __ldg(col + e) : -1;
+            av[k] = ok ? fabsf(__ldg(val + e)) : 0.f;
+        }
+        bool win_ok = true;
+        if (use_win) {
+            win_ok = wait_bar(ws, &Sm.bar_win, ph_win);
+            ph_win ^= 1;
+            if (!win_ok) {
+                Sm.stop = 1;
+                if (err) atomicExch(err, 1);
+            }
+        }
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        if (win_ok) {
+#pragma unroll
+            for (int k = 0; k < kLsPerThread; ++k) {
+                if (jc[k] >= 0) {
+                    const float4 rj = use_win ? rwin[jc[k] - wv.x] : r[jc[k]];
+                    sx = fmaf(av[k], rj.x, sx);
+                    sy = fmaf(av[k], rj.y, sy);
+                    sz = fmaf(av[k], rj.z, sz);
+                }
+            }
+            for (int e = e0 + kLsPerThread * 2 * S; e < end; e += 2 * S) {   // rows wider than 2 x kLsPerThread
                 const float a = fabsf(__ldg(val + e));
                 const int j = __ldg(col + e);
-                const float4 rj = r[j];
-                const float fj = __ldg(fixf + j);
-                sx = fmaf(a * fj, rj.x, sx);
-                sy = fmaf(a * fj, rj.y, sy);
-                sz = fmaf(a * fj, rj.z, sz);
-                sa += a;
-                sd = fmaf(a, __ldg(dfull + j), sd);
+                const float4 rj = use_win ? rwin[j - wv.x] : r[j];
+                sx = fmaf(a, rj.x, sx);
+                sy = fmaf(a, rj.y, sy);
+                sz = fmaf(a, rj.z, sz);
             }
         }
         if (half) {
             part[0][rt] = sx;
             part[1][rt] = sy;
             part[2][rt] = sz;
-            part[3][rt] = sa;
-            part[4][rt] = sd;
         }
         __syncthreads();
         float sc = 0.f;
         if (!half) {
             float f[kMlpIn];
-            if (row < n) {
-                sc = ls_row_features(row, sx + part[0][rt], sy + part[1][rt], sz + part[2][rt], sa + part[3][rt],
-                                     sd + part[4][rt], dfull, diag0, fixf, r, f);
-            } else {
 #pragma unroll
-                for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+            for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+            if (row < n && win_ok) {
+                // r is zero at fixed vertices (every producer of the sweep's residual applies the fix mask)
+                const float4 ri = use_win ? rwin[row - wv.x] : r[row];
+                const float4 c = __ldg(rc + row);
+                const float bx = (sx + part[0][rt]) * c.w, by = (sy + part[1][rt]) * c.w, bz = (sz + part[2][rt]) * c.w;
+                const float s = sqrtf(ri.x * ri.x + ri.y * ri.y + ri.z * ri.z + bx * bx + by * by + bz * bz);
+                const float is = s > 0.f ? 1.f / s : 0.f;
+                f[0] = ri.x * is;
+                f[1] = ri.y * is;
+                f[2] = ri.z * is;
+                f[3] = c.x;
+                f[4] = c.y;
+                f[5] = c.z;
+                f[6] = bx * is;
+                f[7] = by * is;
+                f[8] = bz * is;
+                sc = (__ldg(fixf + row) != 0.f && s > 0.f) ? s / __ldg(dfull + row) : 0.f;
             }
             ls_store_tile_row(Sm.x, rt, f);
         }

@@ -189,7 +189,7 @@ struct MlpSmem {
     alignas(128) uint8_t x[kTileBytes];                          // 128 x 16 bf16
     alignas(128) uint8_t w[kImgBytes];                           // weights + biases
     alignas(128) uint8_t h[kMlpTile * kMlpHid * 2];              // 128 x 64 bf16 (layer 2 and 3 A operand)
-    alignas(8) uint64_t bar_load, bar_mma;
+    alignas(8) uint64_t bar_load, bar_mma, bar_win;   // bar_win: the learned sweep's residual window
     uint32_t tmem_base;
     int stop;
 };
@@ -223,6 +223,7 @@ __device__ __forceinline__ uint32_t mlp_cta_setup(MlpSmem& S, const uint8_t* img
     if (threadIdx.x == 0) {
         mbar_init(&S.bar_load, 1);
         mbar_init(&S.bar_mma, 1);
+        mbar_init(&S.bar_win, 1);
         S.stop = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }

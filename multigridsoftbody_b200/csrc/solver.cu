@@ -198,6 +198,8 @@ struct mgsb_solver {
     uint8_t* ls_tiles = nullptr;
     float* ls_scale = nullptr;
     float4 *ls_r = nullptr, *ls_save = nullptr;
+    float4* ls_rc = nullptr;    // per-frame row constants of the sweep's features (k_ls_row_consts)
+    int2* ls_win = nullptr;     // per 128-row tile: the residual rows the sweep stages in shared memory
     float *ls_part0 = nullptr, *ls_part1 = nullptr;
     // ls_gate: the last frame's decision (1: a learned V-cycle failed its check and the
     // frame's solve was repeated with plain V-cycles); ls_part0 / ls_part1: block sums of
@@ -633,6 +635,24 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dalloc(h, pool, &h->ls_tiles, (size_t)h->ls_ntiles * kTileBytes));
         TRY(dalloc(h, pool, &h->ls_scale, (size_t)N0));
         TRY(dalloc(h, pool, &h->ls_r, (size_t)N0));
+        TRY(dalloc(h, pool, &h->ls_rc, (size_t)N0));
+        {   // residual window per tile: the tile's rows and every column its rows' ELL entries name
+            const PlanLevel& pl = P.levels[0];
+            std::vector<int2> win(h->ls_ntiles);
+            for (int t = 0; t < h->ls_ntiles; ++t) {
+                const int r0 = t * kMlpTile, r1 = std::min(N0, r0 + kMlpTile);
+                int lo = r0, hi = r1;
+                for (int row = r0; row < r1; ++row) {
+                    const int slice = row / pl.S;
+                    for (int e = pl.slice_ptr[slice] + (row - slice * pl.S); e < pl.slice_ptr[slice + 1]; e += pl.S) {
+                        lo = std::min(lo, pl.ell_col[e]);
+                        hi = std::max(hi, pl.ell_col[e] + 1);
+                    }
+                }
+                win[t] = (hi - lo <= kLsWinRows) ? int2{lo, hi} : int2{0, 0};
+            }
+            TRY(dupload(h, pool, &h->ls_win, win));
+        }
         TRY(dalloc(h, pool, &h->ls_save, (size_t)N0));
         h->ls_cycles = std::max(1, h->p.iterations * std::max(1, h->p.refinement_passes));
         TRY(dalloc(h, pool, &h->ls_part0, (size_t)h->ls_cycles * h->ls_nblk));
@@ -646,7 +666,7 @@ mgsb_status rebuild(mgsb_solver* h) {
         CUDA_TRY(h, cudaMemset(h->ls_gate, 0, sizeof(int32_t)));
         CUDA_TRY(h, cudaMemset(h->ls_werr, 0, sizeof(int32_t)));
         CUDA_TRY(h, cudaFuncSetAttribute(k_ls_sweep_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)mlp_tc_smem_bytes()));
+                                         (int)ls_sweep_smem_bytes()));
         CUDA_TRY(h, cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device));
     }
     TRY(dalloc(h, pool, &h->energy_part, (size_t)kEnergyBlocks * kEnergyTerms));
@@ -925,7 +945,7 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
     const int g0 = h->ls_nblk;
     const uint8_t* img = mlp_device_image(h->ls_net);
     const int mgrid = std::min(h->ls_ntiles, 2 * h->sm_count);
-    const size_t msmem = mlp_tc_smem_bytes();
+    const size_t msmem = ls_sweep_smem_bytes();
     float4* bw = const_cast<float4*>(b);
     (void)from_zero;
     // pre-smoothing (with gather_b the right-hand side b = b0 + slots is assembled here first;
@@ -935,7 +955,8 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
                h->ls_r, nullptr, h->ls_part0 + (size_t)cycle * g0, gather_b ? h->b0 : nullptr, gather_b ? h->slot_ptr : nullptr,
                gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
-           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr, nullptr, nullptr);
+           l0.dfull, (const float4*)h->ls_rc, (const int2*)h->ls_win, h->fixf, h->ls_r, img, d, h->ls_werr, nullptr,
+           nullptr);
     // coarse correction
     LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, d, b, l0.res, nullptr);
     ca.d = d;
@@ -952,7 +973,15 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
     }
     // with dd64 (mixed kind, check taken by the next outer residual) the sweep also applies d to dd64
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
-           l0.dfull, h->vdiag, h->fixf, h->ls_r, img, d, h->ls_werr, dd64, d32);
+           l0.dfull, (const float4*)h->ls_rc, (const int2*)h->ls_win, h->fixf, h->ls_r, img, d, h->ls_werr, dd64, d32);
+}
+
+// The learned sweep's per-frame row constants, once the frame's level-0
+// diagonal (contacts included) is known.
+void enqueue_ls_row_consts(mgsb_solver* h) {
+    const LevelDev& l0 = h->lev[0];
+    LAUNCH(h, k_ls_row_consts, h->ls_nblk, kLsThreads, 0, h->N0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull,
+           h->vdiag, h->ls_rc);
 }
 
 // The residual check of the learned V-cycle `cycle` just enqueued (d, b as
@@ -1145,6 +1174,7 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
     float4* xb = h->d2;   // pong
     LAUNCH(h, k_l0_frame, grid_for(n0), kBlock, 0, n0, h->s, h->c0, h->target, h->vdiag, h->fixf, om, h->b0,
            lv[0].dfull, lv[0].dinv, xa);
+    if (learned) enqueue_ls_row_consts(h);
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
                lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
@@ -1236,6 +1266,7 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
     LAUNCH(h, k_mx_contact_frame, grid_for(n0), kBlock, 0, n0, h->s64, h->fixf, h->body_of, h->bodies_dev, h->is_surf,
            h->broad_phase ? h->bp_cand : nullptr, p.contact_stiffness, h->vdiag, om, h->cflag, h->c0, h->b0_64, lv[0].dfull, lv[0].dinv, h->dd64, h->d32,
            h->target, tri ? h->vt_ptr : nullptr, tri ? h->vt_idx : nullptr, tri ? (const double4*)h->tri_push : nullptr);
+    if (learned) enqueue_ls_row_consts(h);
     for (int l = 1; l < L; ++l)
         LAUNCH(h, k_coarse_frame, grid_for(lv[l].n), kBlock, 0, lv[l].n, lv[l].rptr, lv[l].rcol, lv[l].rw, lv[l - 1].c,
                lv[l].diag0, om, lv[l].c, lv[l].dfull, lv[l].dinv);
@@ -2649,6 +2680,7 @@ extern "C" mgsb_status mgsb_vcycle_residuals(mgsb_solver* h, int32_t cycles, int
     const bool prof = h->profiling;
     const int launches = h->launches;   // this measurement is not part of a frame
     h->profiling = false;
+    if (mode == 2) enqueue_ls_row_consts(h);
     for (int c = 0; c < cycles; ++c) {
         if (mode == 2) {
             enqueue_learned_vcycle(h, e, rhs, c == 0, ca, 0);   // the learned cycle alone, no check
