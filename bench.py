@@ -859,6 +859,14 @@ def run_ours(args):
                 best = min(at_bar, key=lambda k: comparison[k]["ms_per_step"])
                 comparison["plain_fp32_at_bar"] = best
                 comparison["ratio_vs_plain_fp32_at_bar"] = comparison[best]["ratio"]
+            # equal error in the strict sense: the fastest plain form at most as far from the converged
+            # frame as the learned solver (matters where every form is far inside the bar, e.g. the blob)
+            le = acc[learned_key]["err_over_diag"]
+            at_err = [k for k in keys if acc[k]["err_over_diag"] <= le]
+            comparison["plain_fp32_at_learned_error"] = (min(at_err, key=lambda k: comparison[k]["ms_per_step"])
+                                                         if at_err else None)
+            comparison["ratio_vs_plain_fp32_at_learned_error"] = (
+                comparison[comparison["plain_fp32_at_learned_error"]]["ratio"] if at_err else None)
     value = job_throughput(args.steps, world, ms)
     e2e_value = job_throughput(args.steps, world, e2e_ms)
     if rank == 0:

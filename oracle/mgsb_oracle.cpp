@@ -675,6 +675,7 @@ void spmv_level(const Oracle& o, int l, const Vec& xin, Vec& out) {
     const int n = (int)xin.size();
     out.assign(n, V3{0, 0, 0});
     const bool fine = (l == 0);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         const double d = fine ? (o.Ldiag[i] + o.c0[i]) : (o.lev[l].diag[i] + o.lev[l].c[i]);
         const Row& r = fine ? o.Loff[i] : o.lev[l].off[i];
@@ -760,6 +761,7 @@ void vcycle(const Oracle& o, int l, const Vec& r, Vec& e) {
     Vec Ae;
     auto sweep = [&]() {
         spmv_level(o, l, e, Ae);
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < n; ++i) {
             const double di = dinv_level(o, l, i);
             for (int c = 0; c < 3; ++c) e[i][c] += di * (r[i][c] - Ae[i][c]);
@@ -768,6 +770,7 @@ void vcycle(const Oracle& o, int l, const Vec& r, Vec& e) {
     for (int k = 0; k < o.p.pre_sweeps; ++k) sweep();
     spmv_level(o, l, e, Ae);
     Vec res(n);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i)
         for (int c = 0; c < 3; ++c) res[i][c] = r[i][c] - Ae[i][c];
     const OLevel& C = o.lev[l + 1];
@@ -780,6 +783,7 @@ void vcycle(const Oracle& o, int l, const Vec& r, Vec& e) {
         }
     Vec ec;
     vcycle(o, l + 1, rc, ec);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i)
         for (int a = 0; a < 4; ++a) {
             const double wgt = C.pw[i][a];
@@ -1011,9 +1015,11 @@ void mg_frame(Oracle& o) {
         }
         for (int pass = 0; pass < o.p.refinement_passes; ++pass) {
             spmv_level(o, 0, d, Ad);
+#pragma omp parallel for schedule(static)
             for (int i = 0; i < V; ++i)
                 for (int c = 0; c < 3; ++c) r[i][c] = b[i][c] - Ad[i][c];
             vcycle(o, 0, r, e);
+#pragma omp parallel for schedule(static)
             for (int i = 0; i < V; ++i)
                 for (int c = 0; c < 3; ++c) d[i][c] += e[i][c];
         }

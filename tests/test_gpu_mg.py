@@ -225,7 +225,10 @@ def test_mixed_precision_matches_oracle(lib, oracle_built):
 @pytest.mark.slow
 def test_config2_mixed_precision(lib, oracle_built):
     """Config 2: 24x240x24 hexes (829,440 tets), 5 levels, per-tet E log-uniform in
-    [5e4, 2e5] (seed 7), mixed precision with 2 refinement passes, config-1 tool path."""
+    [5e4, 2e5] (seed 7), mixed precision with 2 refinement passes, the config-1 tool
+    path started in contact, 100 frames: max vertex distance <= 1e-5 x diag at every
+    10th frame and contact sets bit-exact there."""
+    from multigridsoftbody_b200.sweeps import max_vertex_error
     m, fixed = beam(24, 240, 24)
     rng = np.random.default_rng(7)
     E = np.exp(rng.uniform(np.log(5e4), np.log(2e5), m.num_tets)).astype(np.float32)
@@ -233,15 +236,23 @@ def test_config2_mixed_precision(lib, oracle_built):
     s, o = _pair(m, fixed, p)
     s.set_material(E, 0.3)
     o.set_material(E, 0.3)
-    path = capsule_path(12, start=(0.0, 0.0, 1.25))
-    for f in range(12):
+    frames = 100
+    path = capsule_path(frames, start=(0.0, 0.0, 1.25))
+    tol = 1e-5 * m.bbox_diagonal()
+    worst, touched = 0.0, 0
+    for f in range(frames):
         for solver in (s, o):
             solver.set_capsule(*path[f], 0.3)
             solver.step()
-    xo = o.positions()
-    assert np.abs(s.positions_f64() - xo).max() < 1e-5 * m.bbox_diagonal()
-    assert np.array_equal(np.nonzero(s.contact_flags())[0], np.nonzero(o.contact_flags())[0])
-    assert o.contact_flags().sum() > 0
+        if f % 10 == 9:
+            worst = max(worst, max_vertex_error(s.positions_f64(), o.positions()))
+            cg, co = np.nonzero(s.contact_flags())[0], np.nonzero(o.contact_flags())[0]
+            assert np.array_equal(cg, co), (f, np.setxor1d(cg, co))
+            touched += len(co)
+    print(f"config 2, {frames} frames: max vertex distance {worst:.3e} m (tolerance {tol:.3e}), {touched} contacts")
+    assert worst < tol, (worst, tol)
+    assert touched > 0
+    s.close()
 
 
 def test_coarsest_update_many_contacts(lib, oracle_built):
