@@ -22,8 +22,8 @@ from . import _lib
 from .api import Solver
 
 ERROR_BAR = 1e-5                                                         # x bbox diagonal
-LEARNED_CANDIDATES = (((2, 2), 1), ((1, 1), 1))                          # ((pre, post), passes)
-PLAIN_CANDIDATES = (((2, 2), 1), ((2, 2), 2), ((1, 1), 1), ((1, 1), 2), ((1, 1), 3))
+LEARNED_CANDIDATES = (((2, 2), 1), ((1, 1), 1), ((1, 1), 2), ((2, 2), 2))  # ((pre, post), passes)
+PLAIN_CANDIDATES = (((2, 2), 1), ((2, 2), 2), ((1, 1), 1), ((1, 1), 2), ((1, 1), 3), ((2, 2), 3))
 
 
 def max_vertex_error(x, ref) -> float:
@@ -98,17 +98,20 @@ def time_frames(mesh, fixed, p, net, tool, frames=60, warm=10, tune=True, solver
 def select_sweeps(mesh, fixed, base, net, tool, time_fn=None, bar=ERROR_BAR, frames=100,
                   learned_candidates=LEARNED_CANDIDATES, plain_candidates=PLAIN_CANDIDATES, solver_cls=Solver,
                   time_all=False):
-    """For each family, every candidate's max vertex error / bbox diagonal after `frames` frames of
-    `tool` from rest against the converged solver, the frame time (time_fn(params, net) in ms; default
-    `time_frames`) of those within `bar` (of every candidate with `time_all`, so that the margins can be
-    read), and the fastest candidate within the bar as the family's choice (None when none is within
-    it).  `net` is the learned smoother (None skips that family)."""
+    """For each family, every candidate's max vertex error / bbox diagonal after `frames` frames from
+    rest against the converged solver -- the largest over the tool paths when `tool` is a list of tool
+    callbacks --, the frame time (time_fn(params, net) in ms; default `time_frames` on the first path)
+    of those within `bar` (of every candidate with `time_all`, so that the margins can be read), and the
+    fastest candidate within the bar as the family's choice (None when none is within it).  `net` is
+    the learned smoother (None skips that family)."""
+    tools = list(tool) if isinstance(tool, (list, tuple)) else [tool]
     if time_fn is None:
         def time_fn(p, netx):
-            return time_frames(mesh, fixed, p, netx, tool, solver_cls=solver_cls)
-    ref = converged_positions(mesh, fixed, base, tool, frames, solver_cls)
+            return time_frames(mesh, fixed, p, netx, tools[0], solver_cls=solver_cls)
+    refs = [converged_positions(mesh, fixed, base, t, frames, solver_cls) for t in tools]
     diag = mesh.bbox_diagonal()
-    out = {"frames": frames, "bar": bar, "error": "max over vertices of the Euclidean distance / bbox diagonal"}
+    out = {"frames": frames, "bar": bar, "paths": len(tools),
+           "error": "max over vertices of the Euclidean distance / bbox diagonal, worst over the paths"}
     families = [("plain_fp32", plain_candidates, False)]
     if net is not None:
         families.insert(0, ("learned_mixed", learned_candidates, True))
@@ -116,10 +119,13 @@ def select_sweeps(mesh, fixed, base, net, tool, time_fn=None, bar=ERROR_BAR, fra
         rows = []
         for sweeps, passes in cands:
             p = variant_params(base, sweeps, passes, learned)
-            x, _ = run_positions(mesh, fixed, p, net if learned else None, tool, frames, solver_cls)
-            err = max_vertex_error(x, ref) / diag
+            errs = []
+            for t, ref in zip(tools, refs):
+                x, _ = run_positions(mesh, fixed, p, net if learned else None, t, frames, solver_cls)
+                errs.append(max_vertex_error(x, ref) / diag)
+            err = max(errs)
             row = {"key": variant_key(sweeps, passes, learned), "sweeps": list(sweeps), "passes": passes,
-                   "err_over_diag": err, "within_bar": bool(err <= bar)}
+                   "err_over_diag": err, "err_per_path": errs, "within_bar": bool(err <= bar)}
             if row["within_bar"] or time_all:
                 row["ms_per_frame"] = float(time_fn(p, net if learned else None))
             rows.append(row)

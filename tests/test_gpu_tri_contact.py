@@ -15,9 +15,10 @@ from .common import beam, mg_params
 pytestmark = pytest.mark.gpu
 
 
-def _path(frames, y=0.5, z0=1.15, dz=-0.004):
+def _path(frames, y=0.5, z0=1.15, dz=-0.02):
     """Capsule along x (segment -3..3), radius 0.2, midway between two vertex rows of a coarse beam,
-    sinking slowly: its first frames touch the top faces but no vertex."""
+    sinking 0.02 per frame: its first frame touches the top faces but no vertex; the pushed surface
+    then moves away and the capsule catches up with it again."""
     return [(np.array([-3.0, y, z0 + dz * f], np.float32), np.array([3.0, y, z0 + dz * f], np.float32))
             for f in range(frames)]
 
@@ -50,7 +51,8 @@ def _run_pair(precision, frames=40):
 @pytest.mark.parametrize("precision", [mg.PRECISION_FP32, mg.PRECISION_MIXED])
 def test_triangle_contact_matches_oracle(lib, oracle_built, precision):
     worst, tol, ncontact = _run_pair(precision)
-    assert min(ncontact) > 0, ncontact
+    print(f"triangle contact, precision {precision}: contacts per frame {ncontact}, max error {worst:.3e} m")
+    assert ncontact[0] > 0 and sum(1 for c in ncontact if c) >= 5, ncontact
     assert worst < tol, (worst, tol)
 
 

@@ -4,6 +4,8 @@ against the converged solver stays within the bar, candidates outside the bar
 are not timed, and a family with no candidate within the bar gets no choice."""
 import ctypes
 
+import pytest
+
 import numpy as np
 
 from multigridsoftbody_b200 import sweeps
@@ -34,14 +36,14 @@ def fake_solver(error_of, axes=(1.0, 0.0, 0.0)):
             self.learned = True
 
         def set_capsule(self, a, b, r):
-            pass
+            self.scale = float(a[0]) if a[0] != 0 else 1.0   # a path can scale the error
 
         def step(self):
             pass
 
         def _x(self):
             converged = (self.p.refinement_passes == 6 and not self.learned)
-            e = 0.0 if converged else error_of(self.p, self.learned)
+            e = 0.0 if converged else error_of(self.p, self.learned) * getattr(self, "scale", 1.0)
             return np.tile(np.asarray(axes, np.float64) * e, (4, 1))
 
         def positions_f64(self):
@@ -126,3 +128,19 @@ def test_time_all_times_every_candidate():
     assert all("ms_per_frame" in r for r in rows)
     assert out["plain_fp32"]["chosen"]["key"] == "plain_fp32_3pass_1+1"
     assert not any(r["within_bar"] for r in rows if r["passes"] == 1)
+
+
+def test_worst_path_decides():
+    """With several tool paths a candidate's error is its worst one: 0.6e-5 on one path and 1.2e-5 on
+    another is outside a 1e-5 bar."""
+    def path(scale):
+        def tool(f):
+            a = np.array([[scale, 0.0, 0.0]], np.float32)
+            return a, a, np.array([0.3], np.float32)
+        return tool
+
+    out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), None, [path(1.0), path(2.0)],
+                               lambda p, net: 1.0, frames=2, solver_cls=fake_solver(lambda p, learned: 0.6e-4))
+    for r in out["plain_fp32"]["candidates"]:
+        assert r["err_per_path"] == pytest.approx([0.6e-5, 1.2e-5]) and not r["within_bar"]
+    assert out["plain_fp32"]["chosen"] is None and out["paths"] == 2
