@@ -140,18 +140,54 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
     const int row = warp * RW + (lane % RW);
     const int j = lane / RW;                    // this lane's share of the row
     const bool valid = row < n;
+    // Every load whose address is known is issued before the first sum: the row's slots (up to
+    // kMxSlotsAhead per lane) and its ELL entries (up to kMxEllAhead per lane), then the neighbour
+    // displacements; the sums then run in the order of the plain loops (same bits).  Rows with more
+    // entries finish in the tail loops.
+    constexpr int kMxSlotsAhead = 6, kMxEllAhead = 4;
+    int s_beg = 0, s_end = 0, q0 = 0, end = 0;
+    if (valid) {
+        if (b0) {
+            s_beg = __ldg(slot_ptr + row) + j;
+            s_end = __ldg(slot_ptr + row + 1);
+        }
+        const int slice = row / SH;
+        q0 = __ldg(sp + slice) + j * SH + (row - slice * SH);
+        end = __ldg(sp + slice + 1);
+    }
+    float4 sl[kMxSlotsAhead];
+    if (b0) {
+#pragma unroll
+        for (int k = 0; k < kMxSlotsAhead; ++k) {
+            const int q = s_beg + k * G;
+            sl[k] = q < s_end ? __ldg(slots + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+    int cj[kMxEllAhead];
+    double av[kMxEllAhead];
+#pragma unroll
+    for (int k = 0; k < kMxEllAhead; ++k) {
+        const int q = q0 + k * G * SH;
+        const bool ok = q < end;
+        cj[k] = ok ? __ldg(col + q) : -1;
+        av[k] = ok ? __ldg(val + q) : 0.0;
+    }
     double4 bi = d4z(), bprev = d4z();
     if (b0) {   // uniform over the block: the row's slots split over its G lanes, FP64 sums
         double sx = 0.0, sy = 0.0, sz = 0.0;
-        if (valid) {
-            const int e1 = __ldg(slot_ptr + row + 1);
-#pragma unroll 4
-            for (int q = __ldg(slot_ptr + row) + j; q < e1; q += G) {
-                const float4 t = __ldg(slots + q);
-                sx += t.x;
-                sy += t.y;
-                sz += t.z;
+#pragma unroll
+        for (int k = 0; k < kMxSlotsAhead; ++k) {
+            if (s_beg + k * G < s_end) {
+                sx += sl[k].x;
+                sy += sl[k].y;
+                sz += sl[k].z;
             }
+        }
+        for (int q = s_beg + kMxSlotsAhead * G; q < s_end; q += G) {
+            const float4 t = __ldg(slots + q);
+            sx += t.x;
+            sy += t.y;
+            sz += t.z;
         }
 #pragma unroll
         for (int o = RW; o < 32; o <<= 1) {
@@ -169,17 +205,21 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
         }
     }
     double ax = 0.0, ay = 0.0, az = 0.0;
-    if (valid) {
-        const int slice = row / SH;
-        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
-#pragma unroll 2
-        for (int q = beg + j * SH + (row - slice * SH); q < end; q += G * SH) {
-            const double a = __ldg(val + q);
-            const double4 xv = d[__ldg(col + q)];
-            ax = fma(a, xv.x, ax);
-            ay = fma(a, xv.y, ay);
-            az = fma(a, xv.z, az);
+#pragma unroll
+    for (int k = 0; k < kMxEllAhead; ++k) {
+        if (cj[k] >= 0) {
+            const double4 xv = d[cj[k]];
+            ax = fma(av[k], xv.x, ax);
+            ay = fma(av[k], xv.y, ay);
+            az = fma(av[k], xv.z, az);
         }
+    }
+    for (int q = q0 + kMxEllAhead * G * SH; q < end; q += G * SH) {
+        const double a = __ldg(val + q);
+        const double4 xv = d[__ldg(col + q)];
+        ax = fma(a, xv.x, ax);
+        ay = fma(a, xv.y, ay);
+        az = fma(a, xv.z, az);
     }
 #pragma unroll
     for (int o = RW; o < 32; o <<= 1) {
