@@ -264,6 +264,18 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
             jc[k] = ok ? __ldg(col + e) : -1;
             av[k] = ok ? fabsf(__ldg(val + e)) : 0.f;
         }
+        // the row's own data (its feature constants, fix flag, diagonal, displacement) does not depend on
+        // the window: loaded now, so that its latency overlaps the window copy
+        float4 rcv = make_float4(0.f, 0.f, 0.f, 0.f), dq = make_float4(0.f, 0.f, 0.f, 0.f);
+        float fxr = 0.f, Dr = 1.f;
+        double4 dv = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (!half && row < n) {
+            rcv = __ldg(rc + row);
+            fxr = __ldg(fixf + row);
+            Dr = __ldg(dfull + row);
+            dq = d[row];
+            if (dd64) dv = dd64[row];
+        }
         bool win_ok = true;
         if (use_win) {
             win_ok = wait_bar(ws, &Sm.bar_win, ph_win);
@@ -307,7 +319,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
             if (row < n && win_ok) {
                 // r is zero at fixed vertices (every producer of the sweep's residual applies the fix mask)
                 const float4 ri = use_win ? rwin[row - wv.x] : r[row];
-                const float4 c = __ldg(rc + row);
+                const float4 c = rcv;
                 const float bx = (sx + part[0][rt]) * c.w, by = (sy + part[1][rt]) * c.w, bz = (sz + part[2][rt]) * c.w;
                 const float s = sqrtf(ri.x * ri.x + ri.y * ri.y + ri.z * ri.z + bx * bx + by * by + bz * bz);
                 const float is = s > 0.f ? 1.f / s : 0.f;
@@ -320,7 +332,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
                 f[6] = bx * is;
                 f[7] = by * is;
                 f[8] = bz * is;
-                sc = (__ldg(fixf + row) != 0.f && s > 0.f) ? s / __ldg(dfull + row) : 0.f;
+                sc = (fxr != 0.f && s > 0.f) ? s / Dr : 0.f;
             }
             ls_store_tile_row(Sm.x, rt, f);
         }
@@ -340,7 +352,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
         }
         // threads 0..127 hold row rt's outputs (warps 0-3 serve TMEM lanes 0..127)
         if (ok && !half && row < n && (sc != 0.f || dd64)) {
-            float4 q = d[row];
+            float4 q = dq;
             if (sc != 0.f) {
                 q.x += sc * out[0];
                 q.y += sc * out[1];
@@ -348,7 +360,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
                 d[row] = q;
             }
             if (dd64) {
-                double4 v = dd64[row];
+                double4 v = dv;
                 v.x += q.x;
                 v.y += q.y;
                 v.z += q.z;

@@ -122,7 +122,7 @@ __global__ void k_mx_contact_frame(int n, const double4* __restrict__ s, const f
 // part_end[block] = sum |fix * (b_prev - A d)|^2.
 constexpr int kLanesMx = 4;
 constexpr int kMxThreads = 64 * kLanesMx;
-__global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+__global__ void __launch_bounds__(kMxThreads, 3) k_mx_residual(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
                                                      const double* __restrict__ val, const double* __restrict__ diag64,
                                                      const float* __restrict__ c, const double4* __restrict__ d, double4* __restrict__ b,
                                                      const float* __restrict__ dinv, float4* __restrict__ r32,
@@ -172,6 +172,12 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
         cj[k] = ok ? __ldg(col + q) : -1;
         av[k] = ok ? __ldg(val + q) : 0.0;
     }
+    // the row's own data, on the row's first lane
+    const bool own = valid && lane < RW;
+    const double4 xown = own ? d[row] : d4z();
+    const double Down = own ? __ldg(diag64 + row) + (double)__ldg(c + row) : 0.0;
+    const float fxown = own ? __ldg(fixf + row) : 0.f;
+    const float wown = (own && first_sweep) ? __ldg(dinv + row) : 0.f;
     double4 bi = d4z(), bprev = d4z();
     if (b0) {   // uniform over the block: the row's slots split over its G lanes, FP64 sums
         double sx = 0.0, sy = 0.0, sz = 0.0;
@@ -228,23 +234,23 @@ __global__ void __launch_bounds__(kMxThreads) k_mx_residual(int n, const int32_t
         az += __shfl_xor_sync(0xffffffffu, az, o);
     }
     float rr = 0.f, re = 0.f;
-    if (valid && lane < RW) {
-        const double4 x = d[row];
+    if (own) {
+        const double4 x = xown;
         if (!b0) bi = b[row];
-        const double D = __ldg(diag64 + row) + (double)__ldg(c + row);
+        const double D = Down;
         const float rx = (float)(bi.x - fma(D, x.x, ax)), ry = (float)(bi.y - fma(D, x.y, ay)), rz = (float)(bi.z - fma(D, x.z, az));
         if (part_end) {
-            const float fx = __ldg(fixf + row);
+            const float fx = fxown;
             const float ex = b0 ? fx * (float)(bprev.x - fma(D, x.x, ax)) : fx * rx;
             const float ey = b0 ? fx * (float)(bprev.y - fma(D, x.y, ay)) : fx * ry;
             const float ez = b0 ? fx * (float)(bprev.z - fma(D, x.z, az)) : fx * rz;
             re = ex * ex + ey * ey + ez * ez;
         }
         r32[row] = make_float4(rx, ry, rz, 0.f);
-        const float w = first_sweep ? __ldg(dinv + row) : 0.f;
+        const float w = wown;
         e[row] = make_float4(w * rx, w * ry, w * rz, 0.f);
         if (ls_r) {
-            const float fx = __ldg(fixf + row);
+            const float fx = fxown;
             const float4 q = make_float4(fx * rx, fx * ry, fx * rz, 0.f);
             ls_r[row] = q;
             rr = q.x * q.x + q.y * q.y + q.z * q.z;
