@@ -209,6 +209,8 @@ class LevelBytes:
         self.nch = [x["nchild"] for x in lv]
         self.fuse = lv[0]["fuse_l0"]
         self.split = solver.coarse_split()
+        # the coarsest level is a dense inverse per body: sum of the bodies' n^2
+        self.dense = sum(solver.body_level_size(b, self.L - 1) ** 2 for b in range(solver.num_bodies))
 
     def sweep(self, l):      # ELL + e_in, r, dfull/dinv, e_out
         return 8 * self.nnz[l] + self.n[l] * (16 + 16 + 8 + 16)
@@ -235,7 +237,7 @@ class LevelBytes:
             b += self.restrict(l) + max(pre - 1, 0) * self.sweep(l) + self.resid(l) + self.prolong(l) + post * self.sweep(l)
         c = L - 1
         b += 8 * self.nch[c] + 16 * self.n[c - 1] + self.n[c] * 20       # coarsest restriction
-        b += 4 * self.n[c] * self.n[c] + 32 * self.n[c]                   # dense inverse x r
+        b += 4 * self.dense + 32 * self.n[c]                             # dense inverses x r
         return float(b)
 
     def mean_over_grid_levels(self, f, per_level):

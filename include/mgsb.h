@@ -249,6 +249,9 @@ mgsb_status mgsb_level_size(mgsb_solver* h, int32_t level, int32_t* num_verts, i
  * stored ELL entries, coarse-kernel cluster size, its block size, level-0
  * fusion flag].  No reference counterpart. */
 mgsb_status mgsb_level_info(mgsb_solver* h, int32_t level, int32_t info[8]);
+/* Rows of one body on one multigrid level (a batch's bodies have levels of
+ * their own sizes).  No reference counterpart. */
+mgsb_status mgsb_body_level_size(mgsb_solver* h, int32_t body, int32_t level, int32_t* n);
 
 /* Project-written autotuner: times `frames` frames for each candidate shape
  * of the coarse V-cycle kernel (cluster size, block size, level-0 fusion,

@@ -142,6 +142,7 @@ SIGNATURES = [
     ("mgsb_time_kernel", C.c_int, [_P, C.c_char_p, C.c_int32, _FP, _IP]),
     ("mgsb_get_precompute", C.c_int, [_P, _FP, _FP, _FP, _FP, _FP]),
     ("mgsb_level_size", C.c_int, [_P, C.c_int32, _IP, _IP]),
+    ("mgsb_body_level_size", C.c_int, [_P, C.c_int32, C.c_int32, _IP]),
     ("mgsb_level_info", C.c_int, [_P, C.c_int32, _IP]),
     ("mgsb_autotune", C.c_int, [_P, C.c_int32, _IP]),
     ("mgsb_set_kernel_shape", C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),

@@ -424,6 +424,12 @@ class Solver:
         keys = ("n", "nnz", "nchild", "slice", "ell_entries", "cluster", "block", "fuse_l0")
         return {k: int(v) for k, v in zip(keys, info)}
 
+    def body_level_size(self, body: int, level: int) -> int:
+        """Rows of one body on one level (mgsb_body_level_size)."""
+        n = C.c_int32()
+        _check(self._lib.mgsb_body_level_size(self.h, body, level, C.byref(n)), self.h)
+        return n.value
+
     def autotune(self, frames: int = 5) -> dict:
         """Pick the coarse-kernel shape by timing candidates; the state is restored."""
         ch = np.zeros(3, np.int32)

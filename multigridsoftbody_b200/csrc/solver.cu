@@ -2376,6 +2376,16 @@ mgsb_status mgsb_level_info(mgsb_solver* h, int32_t level, int32_t info[8]) {
     return MGSB_OK;
 }
 
+mgsb_status mgsb_body_level_size(mgsb_solver* h, int32_t body, int32_t level, int32_t* n) {
+    if (!h || !n) return MGSB_INVALID_ARG;
+    TRY(check_body(h, body));
+    TRY(ensure_ready(h));
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "levels exist in the multigrid kinds only");
+    if (level < 0 || level >= h->p.levels) return set_err(h, MGSB_INVALID_ARG, "level %d out of range", level);
+    *n = h->range_host[(size_t)body * h->p.levels + level].y;
+    return MGSB_OK;
+}
+
 const char* mgsb_last_error_string(const mgsb_solver* h) { return h ? h->err.c_str() : "null handle"; }
 
 const char* mgsb_status_string(mgsb_status s) {
