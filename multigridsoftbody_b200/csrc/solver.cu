@@ -292,6 +292,10 @@ void free_pool(std::vector<DevMem>& pool) {
 
 bool is_mg(const mgsb_solver* h) { return h->p.solver == MGSB_SOLVER_MULTIGRID; }
 
+// Level-0 Jacobi sweeps (before and after the coarse correction) of a learned
+// solver's plain fallback at least: the configured plain multigrid's 2+2.
+constexpr int kFallbackL0Sweeps = 2;
+
 // Shape of the coarse V-cycle kernel: explicit tuning if set, else by size
 // (level-0 work fused for bodies up to 40k vertices; ~2.5k rows per CTA).
 size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split);
@@ -908,14 +912,15 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
 // xa -> xb; on return xa holds the result): the first sweep fused with the
 // prolongation (k_prolong_sweep, from the level-0 residual lv[0].res of the
 // descent) unless disabled.  b: the right-hand side of the sweeps.
-void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const int32_t* gate) {
+void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const int32_t* gate, int post = -1) {
     const mgsb_params& p = h->p;
+    if (post < 0) post = p.post_sweeps;
     const int n0 = h->N0;
     const LevelDev& l0 = h->lev[0];
     const LevelDev& l1 = h->lev[1];
     const int g0 = grid_rows(n0, l0.S);
     int k0 = 0;
-    if (h->fuse_prolong && p.post_sweeps > 0) {
+    if (h->fuse_prolong && post > 0) {
         LAUNCH(h, k_prolong_sweep<kLanesL0>, g0, kBlock, 0, n0, l1.pid, l1.pw, l1.e, l0.op_slice_ptr, l0.op_col,
                l0.op_val, l0.dfull, l0.dinv, l0.res, xa, xb, nullptr, nullptr, gate);
         std::swap(xa, xb);
@@ -923,7 +928,7 @@ void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const 
     } else {
         LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, l1.pid, l1.pw, l1.e, xa, gate);
     }
-    for (int k = k0; k < p.post_sweeps; ++k) {
+    for (int k = k0; k < post; ++k) {
         LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, l0.dinv, xa, xb, b,
                h->b0, h->slot_ptr, h->slots, 0, gate);
         std::swap(xa, xb);
@@ -1183,6 +1188,10 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
     CoarseArgs ca;
     fill_coarse_args(h, ca);
     const int g0 = grid_rows(n0, lv[0].S);
+    // a learned solver's plain fallback smooths level 0 with at least the configured 2+2 Jacobi sweeps
+    const bool fallback = !learned && h->ls_net != nullptr;
+    const int l0_pre = fallback ? std::max(p.pre_sweeps, kFallbackL0Sweeps) : p.pre_sweeps;
+    const int l0_post = fallback ? std::max(p.post_sweeps, kFallbackL0Sweeps) : p.post_sweeps;
     for (int it = 0; it < p.iterations; ++it) {
         LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, xa, h->slot_of, h->slots);
         if (learned) {
@@ -1195,7 +1204,7 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
         }
         for (int pass = 0; pass < p.refinement_passes; ++pass) {
             bool gathered = pass > 0;
-            for (int k = 0; k < p.pre_sweeps; ++k) {
+            for (int k = 0; k < l0_pre; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                        lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, gathered ? 0 : 1, nullptr);
                 gathered = true;
@@ -1208,9 +1217,9 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
             ca.d = xa;
             launch_coarse(h, ca);
             if (!h->fuse_l0) {   // the shared-memory kernel leaves the level-1 correction in lv[1].e
-                enqueue_l0_post(h, xa, xb, h->b, nullptr);
+                enqueue_l0_post(h, xa, xb, h->b, nullptr, l0_post);
             } else {
-                for (int k = 0; k < p.post_sweeps; ++k) {
+                for (int k = 0; k < l0_post; ++k) {
                     LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
                            lv[0].dfull, lv[0].dinv, xa, xb, h->b, h->b0, h->slot_ptr, h->slots, 0, nullptr);
                     std::swap(xa, xb);
@@ -1276,6 +1285,10 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
     fill_coarse_args(h, ca);
     ca.Ainv64 = h->Ainv64;
     const int g0 = grid_rows(n0, lv[0].S);
+    // a learned solver's plain fallback smooths level 0 with at least the configured 2+2 Jacobi sweeps
+    const bool fallback = !learned && h->ls_net != nullptr;
+    const int l0_pre = fallback ? std::max(p.pre_sweeps, kFallbackL0Sweeps) : p.pre_sweeps;
+    const int l0_post = fallback ? std::max(p.post_sweeps, kFallbackL0Sweeps) : p.post_sweeps;
     for (int it = 0; it < p.iterations; ++it) {
         LAUNCH(h, k_mg_local, grid_for(T), kBlock, 0, T, h->tets, h->tA, h->tB, h->tC, h->s, h->d32, h->slot_of, h->slots);
         for (int pass = 0; pass < p.refinement_passes; ++pass) {
@@ -1288,7 +1301,7 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
             // learned: the residual check of the previous cycle (its correction already in dd64) rides on
             // this outer residual, against the right-hand side that cycle solved for
             LAUNCH(h, k_mx_residual, g0, kMxThreads, 0, n0, lv[0].slice_ptr, lv[0].ell_col, h->ell_val64, h->diag64, h->c0,
-                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, (p.pre_sweeps > 0 && !learned) ? 1 : 0,
+                   h->dd64, h->b64, lv[0].dinv, h->r32, ea, (l0_pre > 0 && !learned) ? 1 : 0,
                    gather ? h->b0_64 : nullptr, gather ? h->slot_ptr : nullptr, gather ? h->slots : nullptr, h->fixf,
                    learned ? h->ls_r : nullptr, learned ? h->ls_part0 + (size_t)c * h->ls_nblk : nullptr,
                    (learned && c > 0) ? h->ls_part1 + (size_t)(c - 1) * h->ls_nblk : nullptr);
@@ -1302,7 +1315,7 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
                 if (last) enqueue_learned_guard(h, ea, h->r32, c, true, fb, h->dd64, h->d32);
                 continue;
             }
-            for (int k = 1; k < p.pre_sweeps; ++k) {
+            for (int k = 1; k < l0_pre; ++k) {
                 LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                        lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0, nullptr);
                 std::swap(ea, eb);
@@ -1310,7 +1323,7 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
             LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
                    ea, h->r32, lv[0].res, nullptr);
             launch_coarse(h, ca);
-            enqueue_l0_post(h, ea, eb, h->r32, nullptr);
+            enqueue_l0_post(h, ea, eb, h->r32, nullptr, l0_post);
             LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
         }
     }
