@@ -293,6 +293,18 @@ mgsb_status mgsb_set_fused_prolongation(mgsb_solver* h, int32_t on);
  * (PDSolver.cpp:228-233, PDSolver.cu:277-331). */
 mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on);
 
+/* Dense coarse operator (one body): the V-cycle of the levels from the coarse
+ * split down to the coarsest is a linear map M of the split level's
+ * right-hand side.  With 1, M is formed once per frame after the coarse
+ * diagonals and the coarsest inverse are refreshed (one CTA per column, each
+ * the one-CTA V-cycle on a unit vector) and every V-cycle applies it as one
+ * restriction + one dense product instead of the cluster kernel.  The same
+ * V-cycle up to rounding.  At most 1,024 rows on the split level
+ * (MGSB_NOT_SUPPORTED otherwise, and for batches).  The autotuner tries it at
+ * every eligible split.  No reference counterpart. */
+mgsb_status mgsb_set_coarse_dense(mgsb_solver* h, int32_t on);
+mgsb_status mgsb_get_coarse_dense(mgsb_solver* h, int32_t* on);
+
 /* Capsule narrow phase of the multigrid kinds.  MGSB_CONTACT_VERTICES (the
  * default): surface vertices inside the capsule are contacts, projected to its
  * surface.  MGSB_CONTACT_VERTICES_AND_TRIANGLES: in addition every surface

@@ -151,6 +151,8 @@ SIGNATURES = [
     ("mgsb_set_launch_overlap", C.c_int, [_P, C.c_int32]),
     ("mgsb_set_fused_prolongation", C.c_int, [_P, C.c_int32]),
     ("mgsb_set_surface_contact", C.c_int, [_P, C.c_int32]),
+    ("mgsb_set_coarse_dense", C.c_int, [_P, C.c_int32]),
+    ("mgsb_get_coarse_dense", C.c_int, [_P, _IP]),
     ("mgsb_set_broad_phase", C.c_int, [_P, C.c_int32]),
     ("mgsb_inspect_level", C.c_int, [C.POINTER(Mesh), C.POINTER(Params), _U8P, C.c_int32, _IP, _IP, _IP, _FP, _FP, _IP,
                                      _IP, _FP]),

@@ -434,7 +434,8 @@ class Solver:
         """Pick the coarse-kernel shape by timing candidates; the state is restored."""
         ch = np.zeros(3, np.int32)
         _check(self._lib.mgsb_autotune(self.h, frames, _iptr(ch)), self.h)
-        return {"cluster": int(ch[0]), "block": int(ch[1]), "fuse_l0": int(ch[2]), "split": self.coarse_split()}
+        return {"cluster": int(ch[0]), "block": int(ch[1]), "fuse_l0": int(ch[2]), "split": self.coarse_split(),
+                "dense_operator": self.coarse_dense()}
 
     def set_kernel_shape(self, cluster: int = 0, block: int = 0, fuse_level0: int = -1) -> None:
         _check(self._lib.mgsb_set_kernel_shape(self.h, cluster, block, fuse_level0), self.h)
@@ -446,6 +447,15 @@ class Solver:
     def set_surface_contact(self, triangles: bool = True) -> None:
         """Capsule against the surface triangles too (mgsb_set_surface_contact), or vertices only."""
         _check(self._lib.mgsb_set_surface_contact(self.h, 1 if triangles else 0), self.h)
+
+    def set_coarse_dense(self, on: bool = True) -> None:
+        """The dense coarse operator for the levels from the coarse split down (mgsb_set_coarse_dense)."""
+        _check(self._lib.mgsb_set_coarse_dense(self.h, 1 if on else 0), self.h)
+
+    def coarse_dense(self) -> bool:
+        n = C.c_int32()
+        _check(self._lib.mgsb_get_coarse_dense(self.h, C.byref(n)), self.h)
+        return bool(n.value)
 
     def set_broad_phase(self, on: bool = True) -> None:
         """Uniform-grid broad phase for the capsule contact (same contacts as the all-vertex test)."""

@@ -949,14 +949,18 @@ __host__ __device__ inline int coarse_cta_smem_float4(const int* nl, int L, int 
     return tot;
 }
 
-__global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) {
-    pdl_enter();
-    if (A.gate && __ldg(A.gate) == 0) return;
+// The one-CTA V-cycle of levels F..L-1 of `body`.  kOperator: instead of the
+// restricted level F-1 residual, the right-hand side on level F is the unit
+// vector of row `col` (every component 1), and the resulting level-F
+// correction is column `col` of the coarse operator M (row-major n_F x n_F):
+// the V-cycle of levels F..L-1 is linear in its right-hand side and acts on
+// the three components alike, so e_F = M r_F.
+template <bool kOperator>
+__device__ __forceinline__ void coarse_cta_vcycle(const CoarseArgs& A, int body, int col, float* __restrict__ M) {
     extern __shared__ float4 smv[];
     constexpr int P = kCtaRowGroups;
     constexpr int Sc = 32 / kLanesC;
     constexpr int R = 0, E = 1, E2 = 2, RES = 3;
-    const int body = blockIdx.x;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int nwarp = blockDim.x >> 5;
@@ -1030,7 +1034,13 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) 
                 row[p] = off + li[p];
             }
             float4 t[P];
-            cta_restrict<P>(row, valid, lane, C.rptr, C.rcol, C.rw, src, src_off, t);
+            if (kOperator && l == F) {
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+                    t[p] = li[p] == col ? make_float4(1.f, 1.f, 1.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                cta_restrict<P>(row, valid, lane, C.rptr, C.rcol, C.rw, src, src_off, t);
+            }
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 if (!valid[p] || lane >= Sc) continue;
@@ -1170,10 +1180,88 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) 
             __syncthreads();
         }
     }
-    // ---- level-F correction to global memory
+    // ---- level-F correction to global memory (kOperator: column `col` of M)
     {
         const float4* ef = vec(F, ec[F]);
-        for (int li = threadIdx.x; li < q[F].n; li += blockDim.x) A.lv[F].e[q[F].off + li] = ef[li];
+        const int nF = q[F].n;
+        for (int li = threadIdx.x; li < nF; li += blockDim.x) {
+            if constexpr (kOperator)
+                M[(size_t)li * nF + col] = ef[li].x;
+            else
+                A.lv[F].e[q[F].off + li] = ef[li];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) {
+    pdl_enter();
+    if (A.gate && __ldg(A.gate) == 0) return;
+    coarse_cta_vcycle<false>(A, blockIdx.x, 0, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Dense coarse operator (one body): the V-cycle of levels F..L-1 is a linear
+// map M of the level-F right-hand side, so it can be formed once per frame
+// (after the coarse diagonals and the coarsest inverse are refreshed) and
+// applied in every V-cycle as one restriction + one dense product, one launch
+// instead of the cluster kernel's chain of barrier-separated phases.
+//   k_coarse_operator: CTA j runs the one-CTA V-cycle on the unit vector of
+//                      row j and writes column j of M (n_F CTAs).
+//   k_coarse_apply:    every CTA restricts the level F-1 residual to level F
+//                      into shared memory, then its warps form rows of
+//                      e_F = M r_F (warp per row, lanes over the columns).
+// ---------------------------------------------------------------------------
+constexpr int kDenseOpMaxRows = 1024;   // M at most 4 MiB
+constexpr int kDenseApplyRows = 32;     // rows of M per CTA of k_coarse_apply
+constexpr int kDenseApplyThreads = 256;
+
+__global__ void __launch_bounds__(256) k_coarse_operator(const CoarseArgs A, float* __restrict__ M) {
+    pdl_enter();
+    coarse_cta_vcycle<true>(A, 0, blockIdx.x, M);
+}
+
+__global__ void __launch_bounds__(kDenseApplyThreads) k_coarse_apply(int nf, const int32_t* __restrict__ rptr,
+                                                                    const int32_t* __restrict__ rcol,
+                                                                    const float* __restrict__ rw,
+                                                                    const float4* __restrict__ src,
+                                                                    const float* __restrict__ M, float4* __restrict__ e,
+                                                                    const int32_t* __restrict__ gate) {
+    pdl_enter();
+    if (gate && __ldg(gate) == 0) return;
+    extern __shared__ float4 rs[];   // the level-F right-hand side, nf rows
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        const int k1 = __ldg(rptr + i + 1);
+#pragma unroll 4
+        for (int k = __ldg(rptr + i); k < k1; ++k) {
+            const float w = __ldg(rw + k);
+            const float4 t = __ldg(src + __ldg(rcol + k));
+            ax = fmaf(w, t.x, ax);
+            ay = fmaf(w, t.y, ay);
+            az = fmaf(w, t.z, az);
+        }
+        rs[i] = make_float4(ax, ay, az, 0.f);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int row0 = blockIdx.x * kDenseApplyRows;
+    for (int i = row0 + warp; i < min(nf, row0 + kDenseApplyRows); i += nwarp) {
+        const float* Mi = M + (size_t)i * nf;
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        for (int k = lane; k < nf; k += 32) {
+            const float a = __ldg(Mi + k);
+            const float4 t = rs[k];
+            ax = fmaf(a, t.x, ax);
+            ay = fmaf(a, t.y, ay);
+            az = fmaf(a, t.z, az);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(0xffffffffu, ax, o);
+            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+            az += __shfl_xor_sync(0xffffffffu, az, o);
+        }
+        if (lane == 0) e[i] = make_float4(ax, ay, az, 0.f);
     }
 }
 

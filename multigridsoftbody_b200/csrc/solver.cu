@@ -182,6 +182,12 @@ struct mgsb_solver {
     bool fuse_prolong = true;   // prolongation + first post-sweep as one kernel (k_prolong_sweep)
     // autotuner overrides (0 / -1 = pick by size)
     int tune_cluster = 0, tune_fuse = -1, tune_split = 0;
+    // dense coarse operator (one body): levels split..L-1 as M = their V-cycle's matrix,
+    // formed once per frame (k_coarse_operator) and applied per V-cycle (k_coarse_apply)
+    int tune_dense = 0;
+    bool dense_op = false;
+    float* dop_M = nullptr;
+    int dop_cap = 0;   // rows of the largest level M was allocated for
     std::vector<int> maxv;   // largest body's rows on each level
     std::vector<int2> range_host;
     int max_smem_optin = 0;
@@ -319,6 +325,9 @@ void apply_tuning(mgsb_solver* h) {
         h->split = 1;
         while (h->split < L - 1 && h->maxv[h->split] > kClusterLevelRows) ++h->split;
     }
+    h->dense_op = h->tune_dense && !h->fuse_l0 && h->bodies.size() == 1 && h->split >= 1 &&
+                  h->maxv[h->split] <= h->dop_cap && h->dop_M != nullptr &&
+                  coarse_smem_bytes(h, 1, h->split) <= (size_t)h->max_smem_optin;
     if (h->tune_cluster > 0) {
         h->cluster = h->tune_cluster;
     } else if (h->fuse_l0) {
@@ -593,10 +602,19 @@ mgsb_status rebuild(mgsb_solver* h) {
         h->maxv.assign(L, 0);
         for (size_t bi = 0; bi < h->bodies.size(); ++bi)
             for (int l = 0; l < L; ++l) h->maxv[l] = std::max(h->maxv[l], P.range[bi * L + l].y);
+        // the dense coarse operator's matrix, for the largest coarse level it may start at (one body)
+        h->dop_cap = 0;
+        h->dop_M = nullptr;
+        if (h->bodies.size() == 1)
+            for (int l = 1; l < L; ++l)
+                if (h->maxv[l] <= kDenseOpMaxRows) h->dop_cap = std::max(h->dop_cap, h->maxv[l]);
+        if (h->dop_cap > 0) TRY(dalloc(h, pool, &h->dop_M, (size_t)h->dop_cap * h->dop_cap));
         for (int l = 1; l < L; ++l)
             if (h->lev[l].S != 32 / kLanesC)
                 return set_err(h, MGSB_NOT_SUPPORTED, "coarse level %d has slice height %d", l, h->lev[l].S);
         apply_tuning(h);
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_operator, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         h->max_smem_optin));
         CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->fac_valid, h->bodies.size()));
@@ -836,7 +854,14 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
         LAUNCH(h, k_lvl_residual, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.r, a, C.res, gate);
         cur[l] = a;
     }
-    TRY(launch_coarse_cluster(h, args));
+    if (h->dense_op) {   // levels F..L-1: restriction + the dense operator, one launch
+        const LevelView& C = args.lv[F];
+        LAUNCH(h, k_coarse_apply, (C.n + kDenseApplyRows - 1) / kDenseApplyRows, kDenseApplyThreads,
+               (size_t)C.n * sizeof(float4), C.n, C.rptr, C.rcol, C.rw, (const float4*)args.lv[F - 1].res,
+               (const float*)h->dop_M, C.e, gate);
+    } else {
+        TRY(launch_coarse_cluster(h, args));
+    }
     for (int l = F - 1; l >= 1; --l) {
         const LevelView& C = args.lv[l];
         const LevelView& Cc = args.lv[l + 1];
@@ -1127,6 +1152,18 @@ void enqueue_broad_phase(mgsb_solver* h, const float4* spos, bool narrow) {
            narrow ? h->c0 : nullptr, narrow ? h->target : nullptr);
 }
 
+// The frame's dense coarse operator M (levels split..L-1 of the one body), once
+// the coarse diagonals and the coarsest inverse are refreshed: one CTA per
+// column, each the one-CTA V-cycle on a unit right-hand side.
+void enqueue_coarse_operator(mgsb_solver* h, const CoarseArgs& ca_in) {
+    if (!h->dense_op) return;
+    CoarseArgs ca = ca_in;
+    ca.first = h->split;
+    ca.fuse_prolong = h->fuse_prolong ? 1 : 0;
+    ca.gate = nullptr;
+    LAUNCH(h, k_coarse_operator, h->maxv[h->split], 256, coarse_smem_bytes(h, 1, h->split), ca, h->dop_M);
+}
+
 void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
     const mgsb_params& p = h->p;
     const int L = p.levels;
@@ -1187,6 +1224,7 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
            lv[L - 1].c, h->c_prev, h->Lfac, h->fac_valid);
     CoarseArgs ca;
     fill_coarse_args(h, ca);
+    enqueue_coarse_operator(h, ca);
     const int g0 = grid_rows(n0, lv[0].S);
     // a learned solver's plain fallback smooths level 0 with at least the configured 2+2 Jacobi sweeps
     const bool fallback = !learned && h->ls_net != nullptr;
@@ -1284,6 +1322,7 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
     CoarseArgs ca;
     fill_coarse_args(h, ca);
     ca.Ainv64 = h->Ainv64;
+    enqueue_coarse_operator(h, ca);
     const int g0 = grid_rows(n0, lv[0].S);
     // a learned solver's plain fallback smooths level 0 with at least the configured 2+2 Jacobi sweeps
     const bool fallback = !learned && h->ls_net != nullptr;
@@ -2186,6 +2225,29 @@ mgsb_status mgsb_set_launch_overlap(mgsb_solver* h, int32_t on) {
     return MGSB_OK;
 }
 
+mgsb_status mgsb_set_coarse_dense(mgsb_solver* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
+    if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the coarse operator applies to the multigrid kind");
+    TRY(ensure_ready(h));
+    if (on && (h->bodies.size() != 1 || h->fuse_l0 || h->maxv[h->split] > h->dop_cap ||
+               coarse_smem_bytes(h, 1, h->split) > (size_t)h->max_smem_optin))
+        return set_err(h, MGSB_NOT_SUPPORTED,
+                       "the dense coarse operator needs one body and at most %d rows on the coarse split's level "
+                       "(split %d has %d)",
+                       kDenseOpMaxRows, h->split, h->maxv[h->split]);
+    h->tune_dense = on;
+    apply_tuning(h);
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_get_coarse_dense(mgsb_solver* h, int32_t* on) {
+    if (!h || !on) return MGSB_INVALID_ARG;
+    TRY(ensure_ready(h));
+    *on = h->dense_op ? 1 : 0;
+    return MGSB_OK;
+}
+
 mgsb_status mgsb_get_coarse_split(mgsb_solver* h, int32_t* split) {
     if (!h || !split) return MGSB_INVALID_ARG;
     if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the coarse split applies to the multigrid kind");
@@ -2224,7 +2286,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
         }
     };
     struct Cand {
-        int cluster, block, fuse, split;
+        int cluster, block, fuse, split, dense;
     };
     std::vector<Cand> cands;
     const int nb = (int)h->bodies.size();
@@ -2236,14 +2298,19 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
             // split: the cluster kernel's first level; skip clusters with < 32 of its rows per CTA
             for (int sp = 1; sp < L; ++sp)
                 if ((c == 1 || h->maxv[sp] >= 32 * c) && coarse_shape_feasible(h, c, blk, 0, sp))
-                    cands.push_back({c, blk, 0, sp});
+                    cands.push_back({c, blk, 0, sp, 0});
             if (blk >= 512 && c >= 2 && h->p.precision != MGSB_PRECISION_MIXED && !h->ls_net &&
                 coarse_shape_feasible(h, c, blk, 1, 1))
-                cands.push_back({c, blk, 1, 1});
+                cands.push_back({c, blk, 1, 1, 0});
         }
     }
+    // the dense coarse operator at every split it can start at (one body)
+    if (nb == 1)
+        for (int sp = 1; sp < L; ++sp)
+            if (h->maxv[sp] <= h->dop_cap && coarse_smem_bytes(h, 1, sp) <= (size_t)h->max_smem_optin)
+                cands.push_back({1, 256, 0, sp, 1});
     float best = 1e30f;
-    Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0, h->split};
+    Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0, h->split, h->dense_op ? 1 : 0};
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -2252,6 +2319,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
         h->tune_cluster = c.cluster;
         h->tune_fuse = c.fuse;
         h->tune_split = c.split;
+        h->tune_dense = c.dense;
         h->coarse_block = c.block;
         apply_tuning(h);
         invalidate_graph(h);
@@ -2285,6 +2353,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     h->tune_cluster = bestc.cluster;
     h->tune_fuse = bestc.fuse;
     h->tune_split = bestc.split;
+    h->tune_dense = bestc.dense;
     h->coarse_block = bestc.block;
     apply_tuning(h);
     invalidate_graph(h);
