@@ -1207,12 +1207,13 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) 
 // instead of the cluster kernel's chain of barrier-separated phases.
 //   k_coarse_operator: CTA j runs the one-CTA V-cycle on the unit vector of
 //                      row j and writes column j of M (n_F CTAs).
-//   k_coarse_apply:    every CTA restricts the level F-1 residual to level F
-//                      into shared memory, then its warps form rows of
-//                      e_F = M r_F (warp per row, lanes over the columns).
+//   k_coarse_apply:    after k_lvl_restrict has formed the level-F right-hand
+//                      side r_F, every CTA stages r_F in shared memory and its
+//                      warps form 16 rows of e_F = M r_F (warp per row, lanes
+//                      over the columns).
 // ---------------------------------------------------------------------------
 constexpr int kDenseOpMaxRows = 1024;   // M at most 4 MiB
-constexpr int kDenseApplyRows = 32;     // rows of M per CTA of k_coarse_apply
+constexpr int kDenseApplyRows = 16;     // rows of M per CTA of k_coarse_apply
 constexpr int kDenseApplyThreads = 256;
 
 __global__ void __launch_bounds__(256) k_coarse_operator(const CoarseArgs A, float* __restrict__ M) {
@@ -1220,34 +1221,20 @@ __global__ void __launch_bounds__(256) k_coarse_operator(const CoarseArgs A, flo
     coarse_cta_vcycle<true>(A, 0, blockIdx.x, M);
 }
 
-__global__ void __launch_bounds__(kDenseApplyThreads) k_coarse_apply(int nf, const int32_t* __restrict__ rptr,
-                                                                    const int32_t* __restrict__ rcol,
-                                                                    const float* __restrict__ rw,
-                                                                    const float4* __restrict__ src,
+__global__ void __launch_bounds__(kDenseApplyThreads) k_coarse_apply(int nf, const float4* __restrict__ r,
                                                                     const float* __restrict__ M, float4* __restrict__ e,
                                                                     const int32_t* __restrict__ gate) {
     pdl_enter();
     if (gate && __ldg(gate) == 0) return;
     extern __shared__ float4 rs[];   // the level-F right-hand side, nf rows
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) {
-        float ax = 0.f, ay = 0.f, az = 0.f;
-        const int k1 = __ldg(rptr + i + 1);
-#pragma unroll 4
-        for (int k = __ldg(rptr + i); k < k1; ++k) {
-            const float w = __ldg(rw + k);
-            const float4 t = __ldg(src + __ldg(rcol + k));
-            ax = fmaf(w, t.x, ax);
-            ay = fmaf(w, t.y, ay);
-            az = fmaf(w, t.z, az);
-        }
-        rs[i] = make_float4(ax, ay, az, 0.f);
-    }
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) rs[i] = r[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int row0 = blockIdx.x * kDenseApplyRows;
     for (int i = row0 + warp; i < min(nf, row0 + kDenseApplyRows); i += nwarp) {
         const float* Mi = M + (size_t)i * nf;
         float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 4
         for (int k = lane; k < nf; k += 32) {
             const float a = __ldg(Mi + k);
             const float4 t = rs[k];

@@ -854,11 +854,12 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
         LAUNCH(h, k_lvl_residual, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.r, a, C.res, gate);
         cur[l] = a;
     }
-    if (h->dense_op) {   // levels F..L-1: restriction + the dense operator, one launch
+    if (h->dense_op) {   // levels F..L-1: the restriction to level F (grid-wide), then the dense operator
         const LevelView& C = args.lv[F];
+        LAUNCH(h, k_lvl_restrict, grid_rows(C.n, 32 / kLanesC), kBlock, 0, C.n, C.rptr, C.rcol, C.rw,
+               args.lv[F - 1].res, nullptr, C.r, C.e2, gate);
         LAUNCH(h, k_coarse_apply, (C.n + kDenseApplyRows - 1) / kDenseApplyRows, kDenseApplyThreads,
-               (size_t)C.n * sizeof(float4), C.n, C.rptr, C.rcol, C.rw, (const float4*)args.lv[F - 1].res,
-               (const float*)h->dop_M, C.e, gate);
+               (size_t)C.n * sizeof(float4), C.n, (const float4*)C.r, (const float*)h->dop_M, C.e, gate);
     } else {
         TRY(launch_coarse_cluster(h, args));
     }
