@@ -1209,11 +1209,11 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) 
 //                      row j and writes column j of M (n_F CTAs).
 //   k_coarse_apply:    after k_lvl_restrict has formed the level-F right-hand
 //                      side r_F, every CTA stages r_F in shared memory and its
-//                      warps form 16 rows of e_F = M r_F (warp per row, lanes
+//                      warps form 8 rows of e_F = M r_F (warp per row, lanes
 //                      over the columns).
 // ---------------------------------------------------------------------------
 constexpr int kDenseOpMaxRows = 1024;   // M at most 4 MiB
-constexpr int kDenseApplyRows = 16;     // rows of M per CTA of k_coarse_apply
+constexpr int kDenseApplyRows = 8;      // rows of M per CTA of k_coarse_apply
 constexpr int kDenseApplyThreads = 256;
 
 __global__ void __launch_bounds__(256) k_coarse_operator(const CoarseArgs A, float* __restrict__ M) {
