@@ -949,14 +949,10 @@ __host__ __device__ inline int coarse_cta_smem_float4(const int* nl, int L, int 
     return tot;
 }
 
-// The one-CTA V-cycle of levels F..L-1 of `body`.  kOperator: instead of the
-// restricted level F-1 residual, the right-hand side on level F is the unit
-// vector of row `col` (every component 1), and the resulting level-F
-// correction is column `col` of the coarse operator M (row-major n_F x n_F):
-// the V-cycle of levels F..L-1 is linear in its right-hand side and acts on
-// the three components alike, so e_F = M r_F.
-template <bool kOperator>
-__device__ __forceinline__ void coarse_cta_vcycle(const CoarseArgs& A, int body, int col, float* __restrict__ M) {
+__global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) {
+    pdl_enter();
+    if (A.gate && __ldg(A.gate) == 0) return;
+    const int body = blockIdx.x;
     extern __shared__ float4 smv[];
     constexpr int P = kCtaRowGroups;
     constexpr int Sc = 32 / kLanesC;
@@ -1034,13 +1030,7 @@ __device__ __forceinline__ void coarse_cta_vcycle(const CoarseArgs& A, int body,
                 row[p] = off + li[p];
             }
             float4 t[P];
-            if (kOperator && l == F) {
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-                    t[p] = li[p] == col ? make_float4(1.f, 1.f, 1.f, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                cta_restrict<P>(row, valid, lane, C.rptr, C.rcol, C.rw, src, src_off, t);
-            }
+            cta_restrict<P>(row, valid, lane, C.rptr, C.rcol, C.rw, src, src_off, t);
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 if (!valid[p] || lane >= Sc) continue;
@@ -1180,46 +1170,134 @@ __device__ __forceinline__ void coarse_cta_vcycle(const CoarseArgs& A, int body,
             __syncthreads();
         }
     }
-    // ---- level-F correction to global memory (kOperator: column `col` of M)
+    // ---- level-F correction to global memory
     {
         const float4* ef = vec(F, ec[F]);
-        const int nF = q[F].n;
-        for (int li = threadIdx.x; li < nF; li += blockDim.x) {
-            if constexpr (kOperator)
-                M[(size_t)li * nF + col] = ef[li].x;
-            else
-                A.lv[F].e[q[F].off + li] = ef[li];
-        }
+        for (int li = threadIdx.x; li < q[F].n; li += blockDim.x) A.lv[F].e[q[F].off + li] = ef[li];
     }
-}
-
-__global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) {
-    pdl_enter();
-    if (A.gate && __ldg(A.gate) == 0) return;
-    coarse_cta_vcycle<false>(A, blockIdx.x, 0, nullptr);
 }
 
 // ---------------------------------------------------------------------------
 // Dense coarse operator (one body): the V-cycle of levels F..L-1 is a linear
 // map M of the level-F right-hand side, so it can be formed once per frame
 // (after the coarse diagonals and the coarsest inverse are refreshed) and
-// applied in every V-cycle as one restriction + one dense product, one launch
-// instead of the cluster kernel's chain of barrier-separated phases.
-//   k_coarse_operator: CTA j runs the one-CTA V-cycle on the unit vector of
-//                      row j and writes column j of M (n_F CTAs).
-//   k_coarse_apply:    after k_lvl_restrict has formed the level-F right-hand
-//                      side r_F, every CTA stages r_F in shared memory and its
-//                      warps form 8 rows of e_F = M r_F (warp per row, lanes
-//                      over the columns).
+// applied in every V-cycle as one restriction + one dense product instead of
+// the cluster kernel's chain of barrier-separated phases.
+//   k_op_*:         the V-cycle applied to the identity, all columns at once
+//                   (below), leaves M in a scratch block.
+//   k_coarse_apply: after k_lvl_restrict has formed the level-F right-hand
+//                   side r_F, every CTA stages r_F in shared memory and its
+//                   warps form 8 rows of e_F = M r_F (warp per row, lanes over
+//                   the columns).
 // ---------------------------------------------------------------------------
 constexpr int kDenseOpMaxRows = 1024;   // M at most 4 MiB
 constexpr int kDenseApplyRows = 8;      // rows of M per CTA of k_coarse_apply
 constexpr int kDenseApplyThreads = 256;
 
-__global__ void __launch_bounds__(256) k_coarse_operator(const CoarseArgs A, float* __restrict__ M) {
+// ---- the operator built for all columns at once ------------------------------
+// M acts on the three components alike, so it is built as a scalar operator:
+// the V-cycle of levels F..L-1 applied to the n_F x n_F identity, every level's
+// vectors held as n_l x m row-major blocks (m = n_F columns).  One warp per
+// row, lanes over the columns; one launch per phase of the V-cycle.
+constexpr int kOpThreads = 256;
+
+// R = I (row i: 1 in column i), E = dinv R (the first Jacobi sweep from zero; 0 without dinv).
+__global__ void __launch_bounds__(kOpThreads) k_op_init(int n, int m, const float* __restrict__ dinv,
+                                                       float* __restrict__ R, float* __restrict__ E) {
     pdl_enter();
-    coarse_cta_vcycle<true>(A, 0, blockIdx.x, M);
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const float di = dinv ? __ldg(dinv + i) : 0.f;
+    for (int c = lane; c < m; c += 32) {
+        R[(size_t)i * m + c] = c == i ? 1.f : 0.f;
+        E[(size_t)i * m + c] = c == i ? di : 0.f;
+    }
 }
+
+// residual == 0: Xout = Xin + dinv (R - D Xin - Off Xin); residual != 0: Xout = R - D Xin - Off Xin.
+// Level of slice height 32 / kLanesC (coarse levels), off-diagonal sliced ELL.
+__global__ void __launch_bounds__(kOpThreads) k_op_sweep(int n, int m, const int32_t* __restrict__ sp,
+                                                        const int32_t* __restrict__ col,
+                                                        const float* __restrict__ val,
+                                                        const float* __restrict__ dfull,
+                                                        const float* __restrict__ dinv, const float* __restrict__ R,
+                                                        const float* __restrict__ Xin, float* __restrict__ Xout,
+                                                        int residual) {
+    pdl_enter();
+    constexpr int S = 32 / kLanesC;
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const int slice = i / S;
+    const int e0 = __ldg(sp + slice) + (i - slice * S), e1 = __ldg(sp + slice + 1);
+    const float D = __ldg(dfull + i), w = residual ? 0.f : __ldg(dinv + i);
+    for (int c = lane; c < m; c += 32) {
+        float acc = 0.f;
+        for (int e = e0; e < e1; e += S) acc = fmaf(__ldg(val + e), Xin[(size_t)__ldg(col + e) * m + c], acc);
+        const float x = Xin[(size_t)i * m + c];
+        const float r = R[(size_t)i * m + c] - fmaf(D, x, acc);
+        Xout[(size_t)i * m + c] = residual ? r : fmaf(w, r, x);
+    }
+}
+
+// Rc = restriction of Resf (children of each coarse row, CSR); Ec = dinv Rc (0 without dinv).
+__global__ void __launch_bounds__(kOpThreads) k_op_restrict(int n, int m, const int32_t* __restrict__ rptr,
+                                                           const int32_t* __restrict__ rcol,
+                                                           const float* __restrict__ rw,
+                                                           const float* __restrict__ Resf,
+                                                           const float* __restrict__ dinv, float* __restrict__ Rc,
+                                                           float* __restrict__ Ec) {
+    pdl_enter();
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const int k0 = __ldg(rptr + i), k1 = __ldg(rptr + i + 1);
+    const float di = dinv ? __ldg(dinv + i) : 0.f;
+    for (int c = lane; c < m; c += 32) {
+        float acc = 0.f;
+        for (int k = k0; k < k1; ++k) acc = fmaf(__ldg(rw + k), Resf[(size_t)__ldg(rcol + k) * m + c], acc);
+        Rc[(size_t)i * m + c] = acc;
+        Ec[(size_t)i * m + c] = di * acc;
+    }
+}
+
+// Coarsest level: E = Ainv R (dense inverse of the one body, FP64 when Ainv64 is set).
+__global__ void __launch_bounds__(kOpThreads) k_op_coarsest(int n, int m, const float* __restrict__ Ainv,
+                                                           const double* __restrict__ Ainv64,
+                                                           const float* __restrict__ R, float* __restrict__ E) {
+    pdl_enter();
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    for (int c = lane; c < m; c += 32) {
+        if (Ainv64) {
+            double acc = 0.0;
+            for (int k = 0; k < n; ++k) acc = fma(__ldg(Ainv64 + (size_t)i * n + k), (double)R[(size_t)k * m + c], acc);
+            E[(size_t)i * m + c] = (float)acc;
+        } else {
+            float acc = 0.f;
+            for (int k = 0; k < n; ++k) acc = fmaf(__ldg(Ainv + (size_t)i * n + k), R[(size_t)k * m + c], acc);
+            E[(size_t)i * m + c] = acc;
+        }
+    }
+}
+
+// Ef += P Ec (4 coarse parents per fine row).
+__global__ void __launch_bounds__(kOpThreads) k_op_prolong(int n, int m, const int4* __restrict__ pid,
+                                                          const float4* __restrict__ pw, const float* __restrict__ Ec,
+                                                          float* __restrict__ Ef) {
+    pdl_enter();
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const int4 id = __ldg(pid + i);
+    const float4 w = __ldg(pw + i);
+    for (int c = lane; c < m; c += 32)
+        Ef[(size_t)i * m + c] += w.x * Ec[(size_t)id.x * m + c] + w.y * Ec[(size_t)id.y * m + c] +
+                                 w.z * Ec[(size_t)id.z * m + c] + w.w * Ec[(size_t)id.w * m + c];
+}
+
 
 __global__ void __launch_bounds__(kDenseApplyThreads) k_coarse_apply(int nf, const float4* __restrict__ r,
                                                                     const float* __restrict__ M, float4* __restrict__ e,

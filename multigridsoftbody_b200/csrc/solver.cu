@@ -183,11 +183,13 @@ struct mgsb_solver {
     // autotuner overrides (0 / -1 = pick by size)
     int tune_cluster = 0, tune_fuse = -1, tune_split = 0;
     // dense coarse operator (one body): levels split..L-1 as M = their V-cycle's matrix,
-    // formed once per frame (k_coarse_operator) and applied per V-cycle (k_coarse_apply)
+    // formed once per frame (k_op_* kernels) and applied per V-cycle (k_coarse_apply)
     int tune_dense = 0;
     bool dense_op = false;
-    float* dop_M = nullptr;
-    int dop_cap = 0;   // rows of the largest level M was allocated for
+    int dop_cap = 0;                           // rows of the largest level the operator may start at
+    float* dop_work = nullptr;                 // per level l: R, E, E2, RES blocks of n_l x dop_cap floats
+    std::vector<size_t> dop_off;               // offset of level l's four blocks in dop_work (SIZE_MAX: none)
+    float* dop_result = nullptr;               // the frame's M (n_F x n_F, row-major), inside dop_work
     std::vector<int> maxv;   // largest body's rows on each level
     std::vector<int2> range_host;
     int max_smem_optin = 0;
@@ -326,8 +328,7 @@ void apply_tuning(mgsb_solver* h) {
         while (h->split < L - 1 && h->maxv[h->split] > kClusterLevelRows) ++h->split;
     }
     h->dense_op = h->tune_dense && !h->fuse_l0 && h->bodies.size() == 1 && h->split >= 1 &&
-                  h->maxv[h->split] <= h->dop_cap && h->dop_M != nullptr &&
-                  coarse_smem_bytes(h, 1, h->split) <= (size_t)h->max_smem_optin;
+                  h->maxv[h->split] <= h->dop_cap && h->dop_work != nullptr;
     if (h->tune_cluster > 0) {
         h->cluster = h->tune_cluster;
     } else if (h->fuse_l0) {
@@ -604,17 +605,25 @@ mgsb_status rebuild(mgsb_solver* h) {
             for (int l = 0; l < L; ++l) h->maxv[l] = std::max(h->maxv[l], P.range[bi * L + l].y);
         // the dense coarse operator's matrix, for the largest coarse level it may start at (one body)
         h->dop_cap = 0;
-        h->dop_M = nullptr;
+        h->dop_work = nullptr;
+        h->dop_result = nullptr;
+        h->dop_off.assign(L, SIZE_MAX);
         if (h->bodies.size() == 1)
             for (int l = 1; l < L; ++l)
                 if (h->maxv[l] <= kDenseOpMaxRows) h->dop_cap = std::max(h->dop_cap, h->maxv[l]);
-        if (h->dop_cap > 0) TRY(dalloc(h, pool, &h->dop_M, (size_t)h->dop_cap * h->dop_cap));
+        if (h->dop_cap > 0) {   // the levels the operator can span: from the first eligible one down
+            size_t tot = 0;
+            for (int l = 1; l < L; ++l)
+                if (h->maxv[l] <= h->dop_cap) {   // levels shrink with l: every level from the first eligible one
+                    h->dop_off[l] = tot;
+                    tot += 4 * (size_t)h->maxv[l] * h->dop_cap;
+                }
+            TRY(dalloc(h, pool, &h->dop_work, tot));
+        }
         for (int l = 1; l < L; ++l)
             if (h->lev[l].S != 32 / kLanesC)
                 return set_err(h, MGSB_NOT_SUPPORTED, "coarse level %d has slice height %d", l, h->lev[l].S);
         apply_tuning(h);
-        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_operator, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         h->max_smem_optin));
         CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         TRY(dalloc(h, pool, &h->c_prev, (size_t)h->lev[L - 1].n));
         TRY(dalloc(h, pool, &h->fac_valid, h->bodies.size()));
@@ -859,7 +868,7 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
         LAUNCH(h, k_lvl_restrict, grid_rows(C.n, 32 / kLanesC), kBlock, 0, C.n, C.rptr, C.rcol, C.rw,
                args.lv[F - 1].res, nullptr, C.r, C.e2, gate);
         LAUNCH(h, k_coarse_apply, (C.n + kDenseApplyRows - 1) / kDenseApplyRows, kDenseApplyThreads,
-               (size_t)C.n * sizeof(float4), C.n, (const float4*)C.r, (const float*)h->dop_M, C.e, gate);
+               (size_t)C.n * sizeof(float4), C.n, (const float4*)C.r, (const float*)h->dop_result, C.e, gate);
     } else {
         TRY(launch_coarse_cluster(h, args));
     }
@@ -1154,15 +1163,60 @@ void enqueue_broad_phase(mgsb_solver* h, const float4* spos, bool narrow) {
 }
 
 // The frame's dense coarse operator M (levels split..L-1 of the one body), once
-// the coarse diagonals and the coarsest inverse are refreshed: one CTA per
-// column, each the one-CTA V-cycle on a unit right-hand side.
-void enqueue_coarse_operator(mgsb_solver* h, const CoarseArgs& ca_in) {
+// the coarse diagonals and the coarsest inverse are refreshed: the V-cycle of
+// those levels applied to the n_F x n_F identity, all columns at once (scalar
+// blocks, one launch per phase: first sweep from zero, further pre-sweeps,
+// residual, restriction going down; the dense coarsest product; prolongation
+// and post-sweeps coming back up).  h->dop_result points at the block that
+// holds M.
+void enqueue_coarse_operator(mgsb_solver* h, const CoarseArgs& ca) {
     if (!h->dense_op) return;
-    CoarseArgs ca = ca_in;
-    ca.first = h->split;
-    ca.fuse_prolong = h->fuse_prolong ? 1 : 0;
-    ca.gate = nullptr;
-    LAUNCH(h, k_coarse_operator, h->maxv[h->split], 256, coarse_smem_bytes(h, 1, h->split), ca, h->dop_M);
+    const mgsb_params& p = h->p;
+    const int L = p.levels, F = h->split;
+    const int m = ca.lv[F].n;
+    auto blk = [&](int l, int v) { return h->dop_work + h->dop_off[l] + (size_t)v * ca.lv[l].n * h->dop_cap; };
+    auto grid = [&](int n) { return (n * 32 + kOpThreads - 1) / kOpThreads; };
+    constexpr int R = 0, E = 1, E2 = 2, RES = 3;
+    float* cur[kMaxLevels] = {};
+    LAUNCH(h, k_op_init, grid(m), kOpThreads, 0, m, m, (p.pre_sweeps > 0 && F < L - 1) ? ca.lv[F].dinv : nullptr,
+           blk(F, R), blk(F, E));
+    cur[F] = blk(F, E);
+    for (int l = F; l < L - 1; ++l) {
+        const LevelView& C = ca.lv[l];
+        for (int k = 1; k < p.pre_sweeps; ++k) {
+            float* dst = cur[l] == blk(l, E) ? blk(l, E2) : blk(l, E);
+            LAUNCH(h, k_op_sweep, grid(C.n), kOpThreads, 0, C.n, m, C.slice_ptr, C.col, C.val, C.dfull, C.dinv,
+                   (const float*)blk(l, R), (const float*)cur[l], dst, 0);
+            cur[l] = dst;
+        }
+        LAUNCH(h, k_op_sweep, grid(C.n), kOpThreads, 0, C.n, m, C.slice_ptr, C.col, C.val, C.dfull, C.dinv,
+               (const float*)blk(l, R), (const float*)cur[l], blk(l, RES), 1);
+        const LevelView& Cc = ca.lv[l + 1];
+        LAUNCH(h, k_op_restrict, grid(Cc.n), kOpThreads, 0, Cc.n, m, Cc.rptr, Cc.rcol, Cc.rw,
+               (const float*)blk(l, RES), (p.pre_sweeps > 0 && l + 1 < L - 1) ? Cc.dinv : nullptr, blk(l + 1, R),
+               blk(l + 1, E));
+        cur[l + 1] = blk(l + 1, E);
+    }
+    if (F < L - 1) {
+        const LevelView& Cl = ca.lv[L - 1];
+        LAUNCH(h, k_op_coarsest, grid(Cl.n), kOpThreads, 0, Cl.n, m, ca.Ainv, ca.Ainv64, (const float*)blk(L - 1, R),
+               blk(L - 1, E));
+    } else {   // the operator is the coarsest solve itself: M = Ainv applied to the identity
+        LAUNCH(h, k_op_coarsest, grid(m), kOpThreads, 0, m, m, ca.Ainv, ca.Ainv64, (const float*)blk(F, R), blk(F, E2));
+        cur[F] = blk(F, E2);
+    }
+    for (int l = L - 2; l >= F; --l) {
+        const LevelView& C = ca.lv[l];
+        const LevelView& Cc = ca.lv[l + 1];
+        LAUNCH(h, k_op_prolong, grid(C.n), kOpThreads, 0, C.n, m, Cc.pid, Cc.pw, (const float*)cur[l + 1], cur[l]);
+        for (int k = 0; k < p.post_sweeps; ++k) {
+            float* dst = cur[l] == blk(l, E) ? blk(l, E2) : blk(l, E);
+            LAUNCH(h, k_op_sweep, grid(C.n), kOpThreads, 0, C.n, m, C.slice_ptr, C.col, C.val, C.dfull, C.dinv,
+                   (const float*)blk(l, R), (const float*)cur[l], dst, 0);
+            cur[l] = dst;
+        }
+    }
+    h->dop_result = cur[F];
 }
 
 void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
@@ -2230,8 +2284,7 @@ mgsb_status mgsb_set_coarse_dense(mgsb_solver* h, int32_t on) {
     if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
     if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the coarse operator applies to the multigrid kind");
     TRY(ensure_ready(h));
-    if (on && (h->bodies.size() != 1 || h->fuse_l0 || h->maxv[h->split] > h->dop_cap ||
-               coarse_smem_bytes(h, 1, h->split) > (size_t)h->max_smem_optin))
+    if (on && (h->bodies.size() != 1 || h->fuse_l0 || h->maxv[h->split] > h->dop_cap))
         return set_err(h, MGSB_NOT_SUPPORTED,
                        "the dense coarse operator needs one body and at most %d rows on the coarse split's level "
                        "(split %d has %d)",
@@ -2308,7 +2361,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     // the dense coarse operator at every split it can start at (one body)
     if (nb == 1)
         for (int sp = 1; sp < L; ++sp)
-            if (h->maxv[sp] <= h->dop_cap && coarse_smem_bytes(h, 1, sp) <= (size_t)h->max_smem_optin)
+            if (h->maxv[sp] <= h->dop_cap)
                 cands.push_back({1, 256, 0, sp, 1});
     float best = 1e30f;
     Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0, h->split, h->dense_op ? 1 : 0};
