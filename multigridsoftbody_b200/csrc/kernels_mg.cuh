@@ -1200,6 +1200,17 @@ constexpr int kDenseApplyThreads = 256;
 // vectors held as n_l x m row-major blocks (m = n_F columns).  One warp per
 // row, lanes over the columns; one launch per phase of the V-cycle.
 constexpr int kOpThreads = 256;
+constexpr int kOpCols = kDenseOpMaxRows / 32;   // columns per lane (column c = lane + 32 j)
+
+// acc[j] += a * X[row * m + lane + 32 j] for this lane's columns: the loads of one
+// entry are independent, so they are in flight together.
+__device__ __forceinline__ void op_axpy_row(float (&acc)[kOpCols], float a, const float* __restrict__ X, size_t row,
+                                            int m, int lane) {
+    const float* x = X + row * m + lane;
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j)
+        if (lane + 32 * j < m) acc[j] = fmaf(a, x[32 * j], acc[j]);
+}
 
 // R = I (row i: 1 in column i), E = dinv R (the first Jacobi sweep from zero; 0 without dinv).
 __global__ void __launch_bounds__(kOpThreads) k_op_init(int n, int m, const float* __restrict__ dinv,
@@ -1231,12 +1242,17 @@ __global__ void __launch_bounds__(kOpThreads) k_op_sweep(int n, int m, const int
     if (i >= n) return;
     const int slice = i / S;
     const int e0 = __ldg(sp + slice) + (i - slice * S), e1 = __ldg(sp + slice + 1);
+    float acc[kOpCols];
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
+    for (int e = e0; e < e1; e += S) op_axpy_row(acc, __ldg(val + e), Xin, (size_t)__ldg(col + e), m, lane);
     const float D = __ldg(dfull + i), w = residual ? 0.f : __ldg(dinv + i);
-    for (int c = lane; c < m; c += 32) {
-        float acc = 0.f;
-        for (int e = e0; e < e1; e += S) acc = fmaf(__ldg(val + e), Xin[(size_t)__ldg(col + e) * m + c], acc);
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j) {
+        const int c = lane + 32 * j;
+        if (c >= m) continue;
         const float x = Xin[(size_t)i * m + c];
-        const float r = R[(size_t)i * m + c] - fmaf(D, x, acc);
+        const float r = R[(size_t)i * m + c] - fmaf(D, x, acc[j]);
         Xout[(size_t)i * m + c] = residual ? r : fmaf(w, r, x);
     }
 }
@@ -1252,17 +1268,22 @@ __global__ void __launch_bounds__(kOpThreads) k_op_restrict(int n, int m, const 
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n) return;
-    const int k0 = __ldg(rptr + i), k1 = __ldg(rptr + i + 1);
+    float acc[kOpCols];
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
+    const int k1 = __ldg(rptr + i + 1);
+    for (int k = __ldg(rptr + i); k < k1; ++k) op_axpy_row(acc, __ldg(rw + k), Resf, (size_t)__ldg(rcol + k), m, lane);
     const float di = dinv ? __ldg(dinv + i) : 0.f;
-    for (int c = lane; c < m; c += 32) {
-        float acc = 0.f;
-        for (int k = k0; k < k1; ++k) acc = fmaf(__ldg(rw + k), Resf[(size_t)__ldg(rcol + k) * m + c], acc);
-        Rc[(size_t)i * m + c] = acc;
-        Ec[(size_t)i * m + c] = di * acc;
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j) {
+        const int c = lane + 32 * j;
+        if (c >= m) continue;
+        Rc[(size_t)i * m + c] = acc[j];
+        Ec[(size_t)i * m + c] = di * acc[j];
     }
 }
 
-// Coarsest level: E = Ainv R (dense inverse of the one body, FP64 when Ainv64 is set).
+// Coarsest level: E = Ainv R (dense inverse of the one body; FP64 products when Ainv64 is set).
 __global__ void __launch_bounds__(kOpThreads) k_op_coarsest(int n, int m, const float* __restrict__ Ainv,
                                                            const double* __restrict__ Ainv64,
                                                            const float* __restrict__ R, float* __restrict__ E) {
@@ -1270,16 +1291,28 @@ __global__ void __launch_bounds__(kOpThreads) k_op_coarsest(int n, int m, const 
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n) return;
-    for (int c = lane; c < m; c += 32) {
-        if (Ainv64) {
-            double acc = 0.0;
-            for (int k = 0; k < n; ++k) acc = fma(__ldg(Ainv64 + (size_t)i * n + k), (double)R[(size_t)k * m + c], acc);
-            E[(size_t)i * m + c] = (float)acc;
-        } else {
-            float acc = 0.f;
-            for (int k = 0; k < n; ++k) acc = fmaf(__ldg(Ainv + (size_t)i * n + k), R[(size_t)k * m + c], acc);
-            E[(size_t)i * m + c] = acc;
+    if (Ainv64) {
+        double acc[kOpCols];
+#pragma unroll
+        for (int j = 0; j < kOpCols; ++j) acc[j] = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double a = __ldg(Ainv64 + (size_t)i * n + k);
+            const float* x = R + (size_t)k * m + lane;
+#pragma unroll
+            for (int j = 0; j < kOpCols; ++j)
+                if (lane + 32 * j < m) acc[j] = fma(a, (double)x[32 * j], acc[j]);
         }
+#pragma unroll
+        for (int j = 0; j < kOpCols; ++j)
+            if (lane + 32 * j < m) E[(size_t)i * m + lane + 32 * j] = (float)acc[j];
+    } else {
+        float acc[kOpCols];
+#pragma unroll
+        for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
+        for (int k = 0; k < n; ++k) op_axpy_row(acc, __ldg(Ainv + (size_t)i * n + k), R, (size_t)k, m, lane);
+#pragma unroll
+        for (int j = 0; j < kOpCols; ++j)
+            if (lane + 32 * j < m) E[(size_t)i * m + lane + 32 * j] = acc[j];
     }
 }
 
@@ -1293,11 +1326,19 @@ __global__ void __launch_bounds__(kOpThreads) k_op_prolong(int n, int m, const i
     if (i >= n) return;
     const int4 id = __ldg(pid + i);
     const float4 w = __ldg(pw + i);
-    for (int c = lane; c < m; c += 32)
-        Ef[(size_t)i * m + c] += w.x * Ec[(size_t)id.x * m + c] + w.y * Ec[(size_t)id.y * m + c] +
-                                 w.z * Ec[(size_t)id.z * m + c] + w.w * Ec[(size_t)id.w * m + c];
+    float acc[kOpCols];
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
+    op_axpy_row(acc, w.x, Ec, (size_t)id.x, m, lane);
+    op_axpy_row(acc, w.y, Ec, (size_t)id.y, m, lane);
+    op_axpy_row(acc, w.z, Ec, (size_t)id.z, m, lane);
+    op_axpy_row(acc, w.w, Ec, (size_t)id.w, m, lane);
+#pragma unroll
+    for (int j = 0; j < kOpCols; ++j) {
+        const int c = lane + 32 * j;
+        if (c < m) Ef[(size_t)i * m + c] += acc[j];
+    }
 }
-
 
 __global__ void __launch_bounds__(kDenseApplyThreads) k_coarse_apply(int nf, const float4* __restrict__ r,
                                                                     const float* __restrict__ M, float4* __restrict__ e,
