@@ -60,8 +60,9 @@ def make_workload(name, mg):
         p = mg.default_params(mg.SOLVER_MULTIGRID, levels=levels, iterations=10, gravity=(0.0, 0.0, 0.0),
                               precision=mg.PRECISION_MIXED if mixed else mg.PRECISION_FP32,
                               refinement_passes=(1 if name == "beam" else 2) if mixed else 1)
-        # Start the tool 0.3 above the top face so every timed frame has contacts.
-        path = capsule_path(4096, start=(0.0, 0.0, 1.5))
+        # The tool starts 0.3 above the top face so every timed frame has contacts: frames 75-300 of the
+        # configured 300-frame path (z from 1.5 down to -3), repeated, so the timed states stay within it.
+        path = capsule_path(225, start=(0.0, 0.0, 1.5))
 
         def tool(f):
             a, b = path[f % len(path)]
@@ -73,7 +74,7 @@ def make_workload(name, mg):
             mats = [(np.exp(rng.uniform(np.log(5e4), np.log(2e5), m.num_tets)).astype(np.float32), 0.3)]
         desc = (f"beam {dims[0]}x{dims[1]}x{dims[2]} hexes ({m.num_verts} verts, {m.num_tets} tets), "
                 f"{levels} MG levels, 10 PD iterations/frame, capsule r=0.3 len 8 "
-                f"moving -z 0.02/frame + N(0,0.005^2) jitter (seed 1), in contact"
+                f"moving -z 0.02/frame + N(0,0.005^2) jitter (seed 1), in contact (frames 75-300 of the configured path, repeated)"
                 + (", learned smoother (1 learned sweep before and after the coarse correction, residual guard "
                    "with plain fallback)" if name == "beam" else ", 2+2 Jacobi sweeps")
                 + ((", mixed precision (FP64 residual, %d refinement pass%s)" % (p.refinement_passes,
@@ -84,7 +85,7 @@ def make_workload(name, mg):
     if name == "blob":
         from multigridsoftbody_b200.learned import blob_scene, blob_tool_path
         m, fixed, p = blob_scene(precision=mg.PRECISION_MIXED, refinement_passes=1)
-        path = blob_tool_path(4096, seed=1)
+        path = blob_tool_path(300, seed=1)   # 300 frames as config 1's tool path, repeated
 
         def tool(f):
             a, b = path[f % len(path)]
@@ -110,8 +111,8 @@ def make_workload(name, mg):
         start = np.array([0.0, 0.0, 1.15]) + rng.uniform(-0.5, 0.5, (256, 3))
         vel = np.random.default_rng(12)
 
-        traj = [start]
-        for _ in range(4096):
+        traj = [start]   # the configured 200 frames, repeated
+        for _ in range(199):
             traj.append(traj[-1] + vel.normal(0.0, 0.01, (256, 3)))
 
         def tool(f):
