@@ -1185,45 +1185,31 @@ __global__ void __launch_bounds__(1024) k_coarse_vcycle_cta(const CoarseArgs A) 
 // the cluster kernel's chain of barrier-separated phases.
 //   k_op_*:         the V-cycle applied to the identity, all columns at once
 //                   (below), leaves M in a scratch block.
-//   k_coarse_apply: after k_lvl_restrict has formed the level-F right-hand
-//                   side r_F, every CTA stages r_F in shared memory and its
-//                   warps form 8 rows of e_F = M r_F (warp per row, lanes over
-//                   the columns).
+//   k_coarse_apply: every CTA restricts the level-(F-1) residual to the level-F
+//                   right-hand side r_F in shared memory and its warps form 16
+//                   rows of e_F = M r_F (warp per row, lanes over the columns).
+// When F is the coarsest level, M is its inverse itself and nothing is built.
 // ---------------------------------------------------------------------------
 constexpr int kDenseOpMaxRows = 1024;   // M at most 4 MiB
-constexpr int kDenseApplyRows = 8;      // rows of M per CTA of k_coarse_apply
-constexpr int kDenseApplyThreads = 256;
+constexpr int kDenseApplyThreads = 512;
+constexpr int kDenseApplyRows = kDenseApplyThreads / 32;   // rows of M per CTA of k_coarse_apply (one per warp)
 
 // ---- the operator built for all columns at once ------------------------------
 // M acts on the three components alike, so it is built as a scalar operator:
 // the V-cycle of levels F..L-1 applied to the n_F x n_F identity, every level's
-// vectors held as n_l x m row-major blocks (m = n_F columns).  One warp per
-// row, lanes over the columns; one launch per phase of the V-cycle.
-constexpr int kOpThreads = 256;
-constexpr int kOpCols = kDenseOpMaxRows / 32;   // columns per lane (column c = lane + 32 j)
-
-// acc[j] += a * X[row * m + lane + 32 j] for this lane's columns: the loads of one
-// entry are independent, so they are in flight together.
-__device__ __forceinline__ void op_axpy_row(float (&acc)[kOpCols], float a, const float* __restrict__ X, size_t row,
-                                            int m, int lane) {
-    const float* x = X + row * m + lane;
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j)
-        if (lane + 32 * j < m) acc[j] = fmaf(a, x[32 * j], acc[j]);
-}
+// vectors held as n_l x m row-major blocks (m = n_F columns).  One CTA per
+// (row, 128 columns), one thread per column; one launch per phase of the V-cycle.
+constexpr int kOpThreads = 128;   // columns per CTA: grid (rows, ceil(m / kOpThreads)), thread per column
 
 // R = I (row i: 1 in column i), E = dinv R (the first Jacobi sweep from zero; 0 without dinv).
 __global__ void __launch_bounds__(kOpThreads) k_op_init(int n, int m, const float* __restrict__ dinv,
                                                        float* __restrict__ R, float* __restrict__ E) {
     pdl_enter();
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
+    const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= n || c >= m) return;
     const float di = dinv ? __ldg(dinv + i) : 0.f;
-    for (int c = lane; c < m; c += 32) {
-        R[(size_t)i * m + c] = c == i ? 1.f : 0.f;
-        E[(size_t)i * m + c] = c == i ? di : 0.f;
-    }
+    R[(size_t)i * m + c] = c == i ? 1.f : 0.f;
+    E[(size_t)i * m + c] = c == i ? di : 0.f;
 }
 
 // residual == 0: Xout = Xin + dinv (R - D Xin - Off Xin); residual != 0: Xout = R - D Xin - Off Xin.
@@ -1237,24 +1223,16 @@ __global__ void __launch_bounds__(kOpThreads) k_op_sweep(int n, int m, const int
                                                         int residual) {
     pdl_enter();
     constexpr int S = 32 / kLanesC;
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
+    const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= n || c >= m) return;
     const int slice = i / S;
     const int e0 = __ldg(sp + slice) + (i - slice * S), e1 = __ldg(sp + slice + 1);
-    float acc[kOpCols];
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
-    for (int e = e0; e < e1; e += S) op_axpy_row(acc, __ldg(val + e), Xin, (size_t)__ldg(col + e), m, lane);
-    const float D = __ldg(dfull + i), w = residual ? 0.f : __ldg(dinv + i);
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j) {
-        const int c = lane + 32 * j;
-        if (c >= m) continue;
-        const float x = Xin[(size_t)i * m + c];
-        const float r = R[(size_t)i * m + c] - fmaf(D, x, acc[j]);
-        Xout[(size_t)i * m + c] = residual ? r : fmaf(w, r, x);
-    }
+    float acc = 0.f;
+#pragma unroll 8
+    for (int e = e0; e < e1; e += S) acc = fmaf(__ldg(val + e), Xin[(size_t)__ldg(col + e) * m + c], acc);
+    const float x = Xin[(size_t)i * m + c];
+    const float r = R[(size_t)i * m + c] - fmaf(__ldg(dfull + i), x, acc);
+    Xout[(size_t)i * m + c] = residual ? r : fmaf(__ldg(dinv + i), r, x);
 }
 
 // Rc = restriction of Resf (children of each coarse row, CSR); Ec = dinv Rc (0 without dinv).
@@ -1265,22 +1243,14 @@ __global__ void __launch_bounds__(kOpThreads) k_op_restrict(int n, int m, const 
                                                            const float* __restrict__ dinv, float* __restrict__ Rc,
                                                            float* __restrict__ Ec) {
     pdl_enter();
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
-    float acc[kOpCols];
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
+    const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= n || c >= m) return;
+    float acc = 0.f;
     const int k1 = __ldg(rptr + i + 1);
-    for (int k = __ldg(rptr + i); k < k1; ++k) op_axpy_row(acc, __ldg(rw + k), Resf, (size_t)__ldg(rcol + k), m, lane);
-    const float di = dinv ? __ldg(dinv + i) : 0.f;
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j) {
-        const int c = lane + 32 * j;
-        if (c >= m) continue;
-        Rc[(size_t)i * m + c] = acc[j];
-        Ec[(size_t)i * m + c] = di * acc[j];
-    }
+#pragma unroll 8
+    for (int k = __ldg(rptr + i); k < k1; ++k) acc = fmaf(__ldg(rw + k), Resf[(size_t)__ldg(rcol + k) * m + c], acc);
+    Rc[(size_t)i * m + c] = acc;
+    Ec[(size_t)i * m + c] = (dinv ? __ldg(dinv + i) : 0.f) * acc;
 }
 
 // Coarsest level: E = Ainv R (dense inverse of the one body; FP64 products when Ainv64 is set).
@@ -1288,31 +1258,18 @@ __global__ void __launch_bounds__(kOpThreads) k_op_coarsest(int n, int m, const 
                                                            const double* __restrict__ Ainv64,
                                                            const float* __restrict__ R, float* __restrict__ E) {
     pdl_enter();
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
+    const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= n || c >= m) return;
     if (Ainv64) {
-        double acc[kOpCols];
-#pragma unroll
-        for (int j = 0; j < kOpCols; ++j) acc[j] = 0.0;
-        for (int k = 0; k < n; ++k) {
-            const double a = __ldg(Ainv64 + (size_t)i * n + k);
-            const float* x = R + (size_t)k * m + lane;
-#pragma unroll
-            for (int j = 0; j < kOpCols; ++j)
-                if (lane + 32 * j < m) acc[j] = fma(a, (double)x[32 * j], acc[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < kOpCols; ++j)
-            if (lane + 32 * j < m) E[(size_t)i * m + lane + 32 * j] = (float)acc[j];
+        double acc = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < n; ++k) acc = fma(__ldg(Ainv64 + (size_t)i * n + k), (double)R[(size_t)k * m + c], acc);
+        E[(size_t)i * m + c] = (float)acc;
     } else {
-        float acc[kOpCols];
-#pragma unroll
-        for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
-        for (int k = 0; k < n; ++k) op_axpy_row(acc, __ldg(Ainv + (size_t)i * n + k), R, (size_t)k, m, lane);
-#pragma unroll
-        for (int j = 0; j < kOpCols; ++j)
-            if (lane + 32 * j < m) E[(size_t)i * m + lane + 32 * j] = acc[j];
+        float acc = 0.f;
+#pragma unroll 8
+        for (int k = 0; k < n; ++k) acc = fmaf(__ldg(Ainv + (size_t)i * n + k), R[(size_t)k * m + c], acc);
+        E[(size_t)i * m + c] = acc;
     }
 }
 
@@ -1321,54 +1278,135 @@ __global__ void __launch_bounds__(kOpThreads) k_op_prolong(int n, int m, const i
                                                           const float4* __restrict__ pw, const float* __restrict__ Ec,
                                                           float* __restrict__ Ef) {
     pdl_enter();
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
+    const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= n || c >= m) return;
     const int4 id = __ldg(pid + i);
     const float4 w = __ldg(pw + i);
-    float acc[kOpCols];
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j) acc[j] = 0.f;
-    op_axpy_row(acc, w.x, Ec, (size_t)id.x, m, lane);
-    op_axpy_row(acc, w.y, Ec, (size_t)id.y, m, lane);
-    op_axpy_row(acc, w.z, Ec, (size_t)id.z, m, lane);
-    op_axpy_row(acc, w.w, Ec, (size_t)id.w, m, lane);
-#pragma unroll
-    for (int j = 0; j < kOpCols; ++j) {
-        const int c = lane + 32 * j;
-        if (c < m) Ef[(size_t)i * m + c] += acc[j];
-    }
+    Ef[(size_t)i * m + c] += w.x * Ec[(size_t)id.x * m + c] + w.y * Ec[(size_t)id.y * m + c] +
+                             w.z * Ec[(size_t)id.z * m + c] + w.w * Ec[(size_t)id.w * m + c];
 }
 
-__global__ void __launch_bounds__(kDenseApplyThreads) k_coarse_apply(int nf, const float4* __restrict__ r,
+// FP64 inverse of the coarsest level rounded to FP32: the operator when the
+// dense part is the coarsest solve alone.
+__global__ void __launch_bounds__(256) k_op_round(int count, const double* __restrict__ src, float* __restrict__ dst) {
+    pdl_enter();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) dst[i] = (float)src[i];
+}
+
+// e_F = M r_F, r_F the restriction of the level-(F-1) residual (children of
+// each level-F row, CSR).  One row of M per warp.  Before the dependency wait
+// (while the previous kernel runs) every thread loads the static restriction
+// structure of its rows: kApplyG lanes per restricted row, kApplyK children
+// per lane, kApplyPasses rows per thread; longer rows and later rows take a
+// tail loop.  After the wait the CTA stages the whole level-(F-1) residual in
+// shared memory (coalesced) while each warp fetches its row of M, forms all of
+// r_F from shared memory, then its row of e_F.
+constexpr int kApplyG = 4;         // lanes per restricted row
+constexpr int kApplyK = 4;         // children per lane held in registers
+constexpr int kApplyPasses = 2;    // restricted rows per thread held in registers
+constexpr int kApplyMRegs = 16;    // entries of the warp's row of M per lane held in registers
+
+__host__ __device__ constexpr size_t coarse_apply_smem_bytes(int nf, int nfine) {
+    return (size_t)(nf + nfine) * sizeof(float4);
+}
+
+__global__ void __launch_bounds__(kDenseApplyThreads, 1) k_coarse_apply(int nf, int nfine, const int32_t* __restrict__ rptr,
+                                                                    const int32_t* __restrict__ rcol,
+                                                                    const float* __restrict__ rw,
+                                                                    const float4* __restrict__ res_fine,
                                                                     const float* __restrict__ M, float4* __restrict__ e,
                                                                     const int32_t* __restrict__ gate) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;
-    extern __shared__ float4 rs[];   // the level-F right-hand side, nf rows
-    for (int i = threadIdx.x; i < nf; i += blockDim.x) rs[i] = r[i];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int row0 = blockIdx.x * kDenseApplyRows;
-    for (int i = row0 + warp; i < min(nf, row0 + kDenseApplyRows); i += nwarp) {
-        const float* Mi = M + (size_t)i * nf;
-        float ax = 0.f, ay = 0.f, az = 0.f;
-#pragma unroll 4
-        for (int k = lane; k < nf; k += 32) {
-            const float a = __ldg(Mi + k);
-            const float4 t = rs[k];
-            ax = fmaf(a, t.x, ax);
-            ay = fmaf(a, t.y, ay);
-            az = fmaf(a, t.z, az);
-        }
+    pdl_trigger();
+    extern __shared__ float4 apply_smem[];
+    float4* rs = apply_smem;          // r_F, nf rows
+    float4* resf = apply_smem + nf;   // the level-(F-1) residual, nfine rows
+    constexpr int RPP = kDenseApplyThreads / kApplyG;   // restricted rows per pass
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int sub = tid % kApplyG, rloc = tid / kApplyG;
+    // static structure (written once at set-up): safe before the wait
+    int beg[kApplyPasses], end[kApplyPasses], cc[kApplyPasses][kApplyK];
+    float cw[kApplyPasses][kApplyK];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            ax += __shfl_xor_sync(0xffffffffu, ax, o);
-            ay += __shfl_xor_sync(0xffffffffu, ay, o);
-            az += __shfl_xor_sync(0xffffffffu, az, o);
+    for (int p = 0; p < kApplyPasses; ++p) {
+        const int row = p * RPP + rloc;
+        beg[p] = row < nf ? __ldg(rptr + row) : 0;
+        end[p] = row < nf ? __ldg(rptr + row + 1) : 0;
+#pragma unroll
+        for (int k = 0; k < kApplyK; ++k) {
+            const int q = beg[p] + sub + k * kApplyG;
+            cc[p][k] = q < end[p] ? __ldg(rcol + q) : 0;
+            cw[p][k] = q < end[p] ? __ldg(rw + q) : 0.f;
         }
-        if (lane == 0) e[i] = make_float4(ax, ay, az, 0.f);
     }
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    const int i = blockIdx.x * kDenseApplyRows + warp;   // this warp's row of M
+    float mr[kApplyMRegs];
+#pragma unroll
+    for (int j = 0; j < kApplyMRegs; ++j) {
+        const int k = lane + 32 * j;
+        mr[j] = (i < nf && k < nf) ? __ldg(M + (size_t)i * nf + k) : 0.f;
+    }
+    for (int r = tid; r < nfine; r += kDenseApplyThreads) resf[r] = res_fine[r];
+    __syncthreads();
+    auto group_sum = [&](float4 a) {
+#pragma unroll
+        for (int o = 1; o < kApplyG; o <<= 1) {
+            a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+            a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
+            a.z += __shfl_xor_sync(0xffffffffu, a.z, o);
+        }
+        return a;
+    };
+#pragma unroll
+    for (int p = 0; p < kApplyPasses; ++p) {
+        const int row = p * RPP + rloc;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < kApplyK; ++k) acc = f4fma(cw[p][k], resf[cc[p][k]], acc);
+        for (int q = beg[p] + sub + kApplyK * kApplyG; q < end[p]; q += kApplyG)
+            acc = f4fma(__ldg(rw + q), resf[__ldg(rcol + q)], acc);
+        acc = group_sum(acc);
+        if (sub == 0 && row < nf) rs[row] = acc;
+    }
+    for (int base = kApplyPasses * RPP; base < nf; base += RPP) {   // rows past the register passes
+        const int row = base + rloc;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (row < nf) {
+            const int q1 = __ldg(rptr + row + 1);
+            for (int q = __ldg(rptr + row) + sub; q < q1; q += kApplyG)
+                acc = f4fma(__ldg(rw + q), resf[__ldg(rcol + q)], acc);
+        }
+        acc = group_sum(acc);
+        if (sub == 0 && row < nf) rs[row] = acc;
+    }
+    __syncthreads();
+    if (i >= nf) return;   // warp-uniform
+    float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+    for (int j = 0; j < kApplyMRegs; ++j) {
+        const int k = lane + 32 * j;
+        if (k < nf) {
+            const float4 t = rs[k];
+            ax = fmaf(mr[j], t.x, ax);
+            ay = fmaf(mr[j], t.y, ay);
+            az = fmaf(mr[j], t.z, az);
+        }
+    }
+    for (int k = lane + 32 * kApplyMRegs; k < nf; k += 32) {
+        const float a = __ldg(M + (size_t)i * nf + k);
+        const float4 t = rs[k];
+        ax = fmaf(a, t.x, ax);
+        ay = fmaf(a, t.y, ay);
+        az = fmaf(a, t.z, az);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (lane == 0) e[i] = make_float4(ax, ay, az, 0.f);
 }
 
 // ---------------------------------------------------------------------------

@@ -189,7 +189,7 @@ struct mgsb_solver {
     int dop_cap = 0;                           // rows of the largest level the operator may start at
     float* dop_work = nullptr;                 // per level l: R, E, E2, RES blocks of n_l x dop_cap floats
     std::vector<size_t> dop_off;               // offset of level l's four blocks in dop_work (SIZE_MAX: none)
-    float* dop_result = nullptr;               // the frame's M (n_F x n_F, row-major), inside dop_work
+    const float* dop_result = nullptr;         // the frame's M (n_F x n_F, row-major): in dop_work, or the coarsest inverse
     std::vector<int> maxv;   // largest body's rows on each level
     std::vector<int2> range_host;
     int max_smem_optin = 0;
@@ -312,6 +312,14 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split);
 // kernel by default; larger levels run as grid-wide kernels over all SMs.
 constexpr int kClusterLevelRows = 1024;
 
+// The dense coarse operator can start at level `split`: one body, at most
+// dop_cap rows there, and the apply kernel's shared memory (the rows of levels
+// split and split - 1) within the device's limit.
+bool dense_eligible(const mgsb_solver* h, int split) {
+    return h->bodies.size() == 1 && split >= 1 && h->dop_work != nullptr && h->maxv[split] <= h->dop_cap &&
+           coarse_apply_smem_bytes(h->maxv[split], h->maxv[split - 1]) <= (size_t)h->max_smem_optin;
+}
+
 void apply_tuning(mgsb_solver* h) {
     // Default: the distributed-shared-memory kernel for the levels up to
     // kClusterLevelRows rows; larger coarse levels run grid-wide.
@@ -327,8 +335,7 @@ void apply_tuning(mgsb_solver* h) {
         h->split = 1;
         while (h->split < L - 1 && h->maxv[h->split] > kClusterLevelRows) ++h->split;
     }
-    h->dense_op = h->tune_dense && !h->fuse_l0 && h->bodies.size() == 1 && h->split >= 1 &&
-                  h->maxv[h->split] <= h->dop_cap && h->dop_work != nullptr;
+    h->dense_op = h->tune_dense && !h->fuse_l0 && dense_eligible(h, h->split);
     if (h->tune_cluster > 0) {
         h->cluster = h->tune_cluster;
     } else if (h->fuse_l0) {
@@ -597,6 +604,8 @@ mgsb_status rebuild(mgsb_solver* h) {
                                          h->max_smem_optin));
         CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_vcycle_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          h->max_smem_optin));
+        CUDA_TRY(h, cudaFuncSetAttribute(k_coarse_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         h->max_smem_optin));
         TRY(dupload(h, pool, &h->dense_off_d, P.dense_off));
         // cluster size of the coarse V-cycle kernel: sized by the rows one body
         // brings to it (level 0 when fused, else level 1)
@@ -738,10 +747,10 @@ void prof_end(mgsb_solver* h, const char* name) {
 // completed (every kernel launched here calls it first).  Arguments are
 // converted to the kernel's parameter types, so every parameter is passed.
 template <typename... KArgs, typename... Args>
-void launch_kernel(mgsb_solver* h, void (*kernel)(KArgs...), int grid, int block, size_t smem, Args&&... args) {
+void launch_kernel(mgsb_solver* h, void (*kernel)(KArgs...), dim3 grid, int block, size_t smem, Args&&... args) {
     static_assert(sizeof...(KArgs) == sizeof...(Args), "pass every kernel parameter");
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid);
+    cfg.gridDim = grid;
     cfg.blockDim = dim3((unsigned)block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = h->stream;
@@ -865,10 +874,10 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
     }
     if (h->dense_op) {   // levels F..L-1: the restriction to level F (grid-wide), then the dense operator
         const LevelView& C = args.lv[F];
-        LAUNCH(h, k_lvl_restrict, grid_rows(C.n, 32 / kLanesC), kBlock, 0, C.n, C.rptr, C.rcol, C.rw,
-               args.lv[F - 1].res, nullptr, C.r, C.e2, gate);
+        const int nfine = args.lv[F - 1].n;
         LAUNCH(h, k_coarse_apply, (C.n + kDenseApplyRows - 1) / kDenseApplyRows, kDenseApplyThreads,
-               (size_t)C.n * sizeof(float4), C.n, (const float4*)C.r, (const float*)h->dop_result, C.e, gate);
+               coarse_apply_smem_bytes(C.n, nfine), C.n, nfine, C.rptr, C.rcol, C.rw,
+               (const float4*)args.lv[F - 1].res, (const float*)h->dop_result, C.e, gate);
     } else {
         TRY(launch_coarse_cluster(h, args));
     }
@@ -1165,7 +1174,7 @@ void enqueue_broad_phase(mgsb_solver* h, const float4* spos, bool narrow) {
 // The frame's dense coarse operator M (levels split..L-1 of the one body), once
 // the coarse diagonals and the coarsest inverse are refreshed: the V-cycle of
 // those levels applied to the n_F x n_F identity, all columns at once (scalar
-// blocks, one launch per phase: first sweep from zero, further pre-sweeps,
+// blocks, a thread per column, one launch per phase: first sweep from zero, further pre-sweeps,
 // residual, restriction going down; the dense coarsest product; prolongation
 // and post-sweeps coming back up).  h->dop_result points at the block that
 // holds M.
@@ -1175,7 +1184,16 @@ void enqueue_coarse_operator(mgsb_solver* h, const CoarseArgs& ca) {
     const int L = p.levels, F = h->split;
     const int m = ca.lv[F].n;
     auto blk = [&](int l, int v) { return h->dop_work + h->dop_off[l] + (size_t)v * ca.lv[l].n * h->dop_cap; };
-    auto grid = [&](int n) { return (n * 32 + kOpThreads - 1) / kOpThreads; };
+    if (F == L - 1) {   // the operator is the coarsest inverse itself
+        if (ca.Ainv64) {
+            LAUNCH(h, k_op_round, grid_for(m * m), kBlock, 0, m * m, ca.Ainv64, blk(F, 0));
+            h->dop_result = blk(F, 0);
+        } else {
+            h->dop_result = ca.Ainv;
+        }
+        return;
+    }
+    auto grid = [&](int n) { return dim3((unsigned)n, (unsigned)((m + kOpThreads - 1) / kOpThreads)); };
     constexpr int R = 0, E = 1, E2 = 2, RES = 3;
     float* cur[kMaxLevels] = {};
     LAUNCH(h, k_op_init, grid(m), kOpThreads, 0, m, m, (p.pre_sweeps > 0 && F < L - 1) ? ca.lv[F].dinv : nullptr,
@@ -1197,14 +1215,9 @@ void enqueue_coarse_operator(mgsb_solver* h, const CoarseArgs& ca) {
                blk(l + 1, E));
         cur[l + 1] = blk(l + 1, E);
     }
-    if (F < L - 1) {
-        const LevelView& Cl = ca.lv[L - 1];
-        LAUNCH(h, k_op_coarsest, grid(Cl.n), kOpThreads, 0, Cl.n, m, ca.Ainv, ca.Ainv64, (const float*)blk(L - 1, R),
-               blk(L - 1, E));
-    } else {   // the operator is the coarsest solve itself: M = Ainv applied to the identity
-        LAUNCH(h, k_op_coarsest, grid(m), kOpThreads, 0, m, m, ca.Ainv, ca.Ainv64, (const float*)blk(F, R), blk(F, E2));
-        cur[F] = blk(F, E2);
-    }
+    const LevelView& Cl = ca.lv[L - 1];
+    LAUNCH(h, k_op_coarsest, grid(Cl.n), kOpThreads, 0, Cl.n, m, ca.Ainv, ca.Ainv64, (const float*)blk(L - 1, R),
+           blk(L - 1, E));
     for (int l = L - 2; l >= F; --l) {
         const LevelView& C = ca.lv[l];
         const LevelView& Cc = ca.lv[l + 1];
@@ -2284,10 +2297,10 @@ mgsb_status mgsb_set_coarse_dense(mgsb_solver* h, int32_t on) {
     if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
     if (!is_mg(h)) return set_err(h, MGSB_NOT_SUPPORTED, "the coarse operator applies to the multigrid kind");
     TRY(ensure_ready(h));
-    if (on && (h->bodies.size() != 1 || h->fuse_l0 || h->maxv[h->split] > h->dop_cap))
+    if (on && (h->fuse_l0 || !dense_eligible(h, h->split)))
         return set_err(h, MGSB_NOT_SUPPORTED,
-                       "the dense coarse operator needs one body and at most %d rows on the coarse split's level "
-                       "(split %d has %d)",
+                       "the dense coarse operator needs one body, at most %d rows on the coarse split's level "
+                       "(split %d has %d) and the rows of that level and the one above in shared memory",
                        kDenseOpMaxRows, h->split, h->maxv[h->split]);
     h->tune_dense = on;
     apply_tuning(h);
@@ -2361,8 +2374,7 @@ mgsb_status mgsb_autotune(mgsb_solver* h, int32_t frames, int32_t* chosen) {
     // the dense coarse operator at every split it can start at (one body)
     if (nb == 1)
         for (int sp = 1; sp < L; ++sp)
-            if (h->maxv[sp] <= h->dop_cap)
-                cands.push_back({1, 256, 0, sp, 1});
+            if (dense_eligible(h, sp)) cands.push_back({1, 256, 0, sp, 1});
     float best = 1e30f;
     Cand bestc = {h->cluster, h->coarse_block, h->fuse_l0, h->split, h->dense_op ? 1 : 0};
     cudaEvent_t a, b;

@@ -59,17 +59,19 @@ def test_dense_operator_matches_kernel_and_oracle(lib, oracle_built, precision, 
     assert np.array_equal(fd[-1], np.nonzero(o.contact_flags())[0]) and len(fd[-1]) > 0
 
 
-def test_dense_operator_config1_learned(lib):
-    """The headline's beam (levels 2-3 as a 496 x 496 operator) with the learned smoother and mixed
-    precision: the same frames as the cluster kernel up to rounding, no more failed checks."""
+@pytest.mark.parametrize("split", [2, 3])
+def test_dense_operator_config1_learned(lib, split):
+    """The headline's beam (levels 2-3 as a 496 x 496 operator, or the 144 x 144 coarsest inverse
+    alone) with the learned smoother and mixed precision: the same frames as the cluster kernel up
+    to rounding, the same contact sets."""
     from multigridsoftbody_b200.learned import MLP
     m, fixed = beam(12, 120, 12)
     p = mg_params(levels=4, gravity=(0.0, 0.0, 0.0), precision=mg.PRECISION_MIXED, refinement_passes=2,
                   pre_sweeps=1, post_sweeps=1)
     net = MLP(device=0, seed=0)
     net.params = np.load(os.path.join(ROOT, "tests", "golden", "beam_smoother.npy"))
-    xk, fk = _run(m, fixed, p, 2, False, 20, net)
-    xd, fd = _run(m, fixed, p, 2, True, 20, net)
+    xk, fk = _run(m, fixed, p, split, False, 20, net)
+    xd, fd = _run(m, fixed, p, split, True, 20, net)
     assert max_vertex_error(xd, xk) / m.bbox_diagonal() < 1e-6
     assert all(np.array_equal(u, v) for u, v in zip(fd, fk))
 
