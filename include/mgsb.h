@@ -442,6 +442,12 @@ mgsb_status mgsb_mlp_train(mgsb_mlp* h, const float* x, const float* t, int64_t 
 mgsb_status mgsb_set_learned_smoother(mgsb_solver* h, const mgsb_mlp* net, float guard_ratio);
 /* Learned V-cycles checked, and checks failed, since the network was attached. */
 mgsb_status mgsb_learned_stats(mgsb_solver* h, uint64_t out[2]);
+/* The last frame's learned V-cycles (PD iteration-major, refinement pass
+ * minor): before[c] = |r| where cycle c started, after[c] = |r| after it (the
+ * quantities the guard compares: a cycle passes when after <= guard_ratio x
+ * before).  *n receives the frame's cycle count; at most cap values are
+ * written to each array.  Diagnostic: synchronises the solver's stream. */
+mgsb_status mgsb_learned_cycle_norms(mgsb_solver* h, double* before, double* after, int32_t cap, int32_t* n);
 /* Training pairs from the plain FP32 multigrid solver's current state: the
  * learned sweep is trained to reproduce `sweeps` weighted-Jacobi sweeps from
  * zero in one step.  Three residuals are used: r = b - A d of the last global

@@ -115,6 +115,8 @@ SIGNATURES = [
     ("mgsb_get_normals_noalloc", C.c_int, [_P, C.c_int32, _FP]),
     ("mgsb_set_learned_smoother", C.c_int, [_P, _P, C.c_float]),
     ("mgsb_learned_stats", C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    ("mgsb_learned_cycle_norms", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32,
+                                           C.POINTER(C.c_int32)]),
     ("mgsb_smoother_pairs", C.c_int, [_P, C.c_int32, _FP, _FP, C.c_int64, C.POINTER(C.c_int64)]),
     ("mgsb_vcycle_residuals", C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     ("mgsb_mg2_create", C.c_int, [C.POINTER(Mesh), C.POINTER(Mesh), C.POINTER(Params), C.POINTER(_P)]),

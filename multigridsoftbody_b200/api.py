@@ -315,6 +315,17 @@ class Solver:
         _check(self._lib.mgsb_learned_stats(self.h, out), self.h)
         return int(out[0]), int(out[1])
 
+    def learned_cycle_norms(self) -> tuple[np.ndarray, np.ndarray]:
+        """|r| before and after each learned V-cycle of the last frame (mgsb_learned_cycle_norms)."""
+        n = C.c_int32()
+        _check(self._lib.mgsb_learned_cycle_norms(self.h, None, None, 0, C.byref(n)), self.h)
+        before, after = np.zeros(n.value), np.zeros(n.value)
+        if n.value:
+            dp = C.POINTER(C.c_double)
+            _check(self._lib.mgsb_learned_cycle_norms(self.h, before.ctypes.data_as(dp), after.ctypes.data_as(dp),
+                                                      n.value, C.byref(n)), self.h)
+        return before, after
+
     def smoother_pairs(self, sweeps: int = 4) -> tuple[np.ndarray, np.ndarray]:
         """Training pairs (features [n,9], targets [n,3]) from the current state (mgsb_smoother_pairs)."""
         n = C.c_int64()

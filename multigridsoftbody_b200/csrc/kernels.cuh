@@ -546,12 +546,19 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
                                                   const float4* __restrict__ gB, const float2* __restrict__ gC,
                                                   const float4* __restrict__ s, const float4* __restrict__ d,
                                                   const int4* __restrict__ slot_of, float4* __restrict__ slots) {
-    pdl_enter();
+    pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
+    if (t >= T) {
+        pdl_wait();
+        return;
+    }
+    // the tet's set-up data (vertices, shape gradients, weight, slots) is written by no kernel:
+    // loaded before the dependency wait, while the previous kernel runs
     const int4 id = __ldg(tets + t);
     const float4 a = __ldg(gA + t), b = __ldg(gB + t);
     const float2 c = __ldg(gC + t);
+    const int4 so = __ldg(slot_of + t);
+    pdl_wait();
     // g1 = (a.x a.y a.z), g2 = (a.w b.x b.y), g3 = (b.z b.w c.x), w = c.y
     const float g1[3] = {a.x, a.y, a.z}, g2[3] = {a.w, b.x, b.y}, g3[3] = {b.z, b.w, c.x};
     const float w = c.y;
@@ -582,7 +589,6 @@ __global__ void __launch_bounds__(256) k_mg_local(int T, const int4* __restrict_
         o2[r] = w * (R[r * 3 + 0] * g2[0] + R[r * 3 + 1] * g2[1] + R[r * 3 + 2] * g2[2]);
         o3[r] = w * (R[r * 3 + 0] * g3[0] + R[r * 3 + 1] * g3[1] + R[r * 3 + 2] * g3[2]);
     }
-    const int4 so = __ldg(slot_of + t);
     slots[so.x] = make_float4(-(o1[0] + o2[0] + o3[0]), -(o1[1] + o2[1] + o3[1]), -(o1[2] + o2[2] + o3[2]), 0.f);
     slots[so.y] = make_float4(o1[0], o1[1], o1[2], 0.f);
     slots[so.z] = make_float4(o2[0], o2[1], o2[2], 0.f);

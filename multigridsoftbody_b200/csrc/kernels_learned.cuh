@@ -233,25 +233,19 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
     // weight copy (the weight image is not written by any kernel of a frame);
     // the copy also overlaps the first tile's feature gather.
     const uint32_t tmem = mlp_cta_setup(Sm, img, ws, ph_load, err, false);
-    pdl_wait();
-    bool weights_pending = true;
-    __shared__ float part[3][kMlpTile];   // second half's 1-ring sums
     const int rt = threadIdx.x & (kMlpTile - 1), half = threadIdx.x >> 7;   // 2 threads per row
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        __syncthreads();
-        if (Sm.stop) break;
-        const int2 wv = __ldg(win + tile);
-        const bool use_win = wv.y > wv.x;
-        if (use_win && threadIdx.x == 0) {   // the residual rows this tile reads, in one bulk copy
-            mbar_expect_tx(&Sm.bar_win, (uint32_t)(wv.y - wv.x) * 16u);
-            bulk_g2s(rwin, r + wv.x, (uint32_t)(wv.y - wv.x) * 16u, &Sm.bar_win);
-        }
+    // The tile's set-up structure (its residual window, this thread's ELL entries of the row -- the
+    // two threads of a row take alternate entries -- and the row's fix flag) is written by no kernel:
+    // the first tile's is loaded before the dependency wait, while the previous kernel runs.
+    int2 wv = make_int2(0, 0);
+    int e0 = 0, end = 0;
+    int jc[kLsPerThread];
+    float av[kLsPerThread];
+    float fxr = 0.f;
+    auto load_structure = [&](int tile) {
+        wv = __ldg(win + tile);
         const int row = tile * kMlpTile + rt;
-        // this thread's entries of the row (the two threads of a row take alternate entries), loaded
-        // while the window is in flight
-        int e0 = 0, end = 0;
-        int jc[kLsPerThread];
-        float av[kLsPerThread];
+        e0 = end = 0;
         if (row < n) {
             const int slice = row / S;
             end = __ldg(sp + slice + 1);
@@ -264,14 +258,29 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
             jc[k] = ok ? __ldg(col + e) : -1;
             av[k] = ok ? fabsf(__ldg(val + e)) : 0.f;
         }
-        // the row's own data (its feature constants, fix flag, diagonal, displacement) does not depend on
-        // the window: loaded now, so that its latency overlaps the window copy
+        fxr = (!half && row < n) ? __ldg(fixf + row) : 0.f;
+    };
+    if ((int)blockIdx.x < ntiles) load_structure(blockIdx.x);
+    pdl_wait();
+    bool weights_pending = true;
+    __shared__ float part[3][kMlpTile];   // second half's 1-ring sums
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if (tile != (int)blockIdx.x) load_structure(tile);
+        __syncthreads();
+        if (Sm.stop) break;
+        const bool use_win = wv.y > wv.x;
+        if (use_win && threadIdx.x == 0) {   // the residual rows this tile reads, in one bulk copy
+            mbar_expect_tx(&Sm.bar_win, (uint32_t)(wv.y - wv.x) * 16u);
+            bulk_g2s(rwin, r + wv.x, (uint32_t)(wv.y - wv.x) * 16u, &Sm.bar_win);
+        }
+        const int row = tile * kMlpTile + rt;
+        // the row's own data (its feature constants, diagonal, displacement) does not depend on the
+        // window: loaded now, so that its latency overlaps the window copy
         float4 rcv = make_float4(0.f, 0.f, 0.f, 0.f), dq = make_float4(0.f, 0.f, 0.f, 0.f);
-        float fxr = 0.f, Dr = 1.f;
+        float Dr = 1.f;
         double4 dv = make_double4(0.0, 0.0, 0.0, 0.0);
         if (!half && row < n) {
             rcv = __ldg(rc + row);
-            fxr = __ldg(fixf + row);
             Dr = __ldg(dfull + row);
             dq = d[row];
             if (dd64) dv = dd64[row];

@@ -138,6 +138,99 @@ __device__ __forceinline__ float4 rg_csr_sum(bool valid, int lane, int beg, int 
     return make_float4(ax, ay, az, 0.f);
 }
 
+// ---------------------------------------------------------------------------
+// Row structure held in registers.  The sliced-ELL and CSR arrays of every
+// level (columns, values, children, weights, parents) are uploaded once at
+// set-up and never written by a kernel, so a kernel may load this lane's
+// share of its row's entries before the dependency wait (while the previous
+// kernel still runs): after the wait, only the loads of the vector that the
+// previous kernel wrote remain on the critical path.  The first K entries of
+// the lane are held; a longer row reads the rest after the wait.  The sums run
+// over the entries in the same order as rg_offdiag / rg_csr_sum: the same bits.
+// ---------------------------------------------------------------------------
+template <int K>
+struct HeldEntries {
+    int32_t c[K];   // column (or child); -1: none
+    float v[K];
+    int next, end, stride;   // first entry not held, the row's end, entry stride
+};
+
+// This lane's entries of `row` of a sliced-ELL matrix (slice height 32 / G).
+template <int G, int K>
+__device__ __forceinline__ void hold_ell_row(HeldEntries<K>& h, int row, bool valid, int lane,
+                                             const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                             const float* __restrict__ val) {
+    constexpr int S = 32 / G;
+    int e = 0, end = 0;
+    if (valid) {
+        const int slice = row / S;
+        end = __ldg(sp + slice + 1);
+        e = __ldg(sp + slice) + (lane / S) * S + (row - slice * S);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const bool ok = e + 32 * k < end;
+        h.c[k] = ok ? __ldg(col + e + 32 * k) : -1;
+        h.v[k] = ok ? __ldg(val + e + 32 * k) : 0.f;
+    }
+    h.next = e + 32 * K;
+    h.end = end;
+    h.stride = 32;
+}
+
+// This lane's entries [beg, end) of a CSR row split across G lanes.
+template <int G, int K>
+__device__ __forceinline__ void hold_csr_row(HeldEntries<K>& h, bool valid, int lane, int beg, int end,
+                                             const int32_t* __restrict__ idx, const float* __restrict__ w) {
+    constexpr int S = 32 / G;
+    const int q = beg + lane / S;
+    if (!valid) end = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const bool ok = q + G * k < end;
+        h.c[k] = ok ? __ldg(idx + q + G * k) : -1;
+        h.v[k] = ok ? __ldg(w + q + G * k) : 0.f;
+    }
+    h.next = q + G * K;
+    h.end = end;
+    h.stride = G;
+}
+
+// Sum of v * x[c] over the held entries and the row's tail, reduced over the
+// G lanes of the row.  Every lane of the warp must call it.
+template <int G, int K, bool kReadOnly = true>
+__device__ __forceinline__ float4 held_sum(const HeldEntries<K>& h, int lane, const int32_t* __restrict__ idx,
+                                           const float* __restrict__ w, const float4* x) {
+    constexpr int S = 32 / G;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (h.c[k] >= 0) {
+            const float4 xv = vload<kReadOnly>(x + h.c[k]);
+            ax = fmaf(h.v[k], xv.x, ax);
+            ay = fmaf(h.v[k], xv.y, ay);
+            az = fmaf(h.v[k], xv.z, az);
+        }
+    }
+    for (int e = h.next; e < h.end; e += h.stride) {
+        const float a = __ldg(w + e);
+        const float4 xv = vload<kReadOnly>(x + __ldg(idx + e));
+        ax = fmaf(a, xv.x, ax);
+        ay = fmaf(a, xv.y, ay);
+        az = fmaf(a, xv.z, az);
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return make_float4(ax, ay, az, 0.f);
+}
+
+constexpr int kHeldL0 = 4;   // level-0 entries held per lane (4 lanes per row: 16 per row)
+constexpr int kHeldC = 6;    // coarse-level entries held per lane (8 lanes per row: 48 per row)
+
 // Sum of the contiguous float4 slots [beg, end) split across the G lanes.
 template <int G>
 __device__ __forceinline__ float4 rg_slot_sum(bool valid, int lane, int beg, int end, const float4* __restrict__ slots) {
@@ -173,24 +266,27 @@ __global__ void __launch_bounds__(256) k_l0_sweep_rg(int n, const int32_t* __res
                                                      const float4* __restrict__ b0, const int32_t* __restrict__ slot_ptr,
                                                      const float4* __restrict__ slots, int gather,
                                                      const int32_t* __restrict__ gate = nullptr) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;   // gated launches run only when the learned V-cycle was rejected
+    pdl_trigger();
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
+    HeldEntries<kHeldL0> he;
+    hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    const int sbeg = (gather && valid) ? __ldg(slot_ptr + row) : 0, send = (gather && valid) ? __ldg(slot_ptr + row + 1) : 0;
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;   // gated launches run only when the learned V-cycle was rejected
     float4 bi;
     if (gather) {
-        const int beg = valid ? __ldg(slot_ptr + row) : 0, end = valid ? __ldg(slot_ptr + row + 1) : 0;
-        const float4 sl = rg_slot_sum<G>(valid, lane, beg, end, slots);
+        const float4 sl = rg_slot_sum<G>(valid, lane, sbeg, send, slots);
         const float4 bb = valid ? __ldg(b0 + row) : f4z();
         bi = make_float4(bb.x + sl.x, bb.y + sl.y, bb.z + sl.z, 0.f);
         if (valid && lane < S) b[row] = bi;
     } else {
         bi = valid ? b[row] : f4z();
     }
-    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, din);
+    const float4 off = held_sum<G>(he, lane, col, val, din);
     if (!valid || lane >= S) return;
     const float4 di4 = __ldg(din + row);
     const float D = __ldg(dfull + row), w = __ldg(dinv + row);
@@ -203,14 +299,17 @@ __global__ void __launch_bounds__(256) k_l0_residual_rg(int n, const int32_t* __
                                                         const float* __restrict__ val, const float* __restrict__ dfull,
                                                         const float4* __restrict__ dvec, const float4* __restrict__ b,
                                                         float4* __restrict__ res, const int32_t* __restrict__ gate = nullptr) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;
+    pdl_trigger();
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
-    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, dvec);
+    HeldEntries<kHeldL0> he;
+    hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    const float4 off = held_sum<G>(he, lane, col, val, dvec);
     if (!valid || lane >= S) return;
     const float4 x = __ldg(dvec + row), bi = __ldg(b + row);
     const float D = __ldg(dfull + row);
@@ -247,15 +346,18 @@ __global__ void __launch_bounds__(256) k_lvl_restrict(int n, const int32_t* __re
                                                       const float* __restrict__ rw, const float4* __restrict__ res_fine,
                                                       const float* __restrict__ dinv, float4* __restrict__ r,
                                                       float4* __restrict__ e, const int32_t* __restrict__ gate) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;
+    pdl_trigger();
     constexpr int G = kLanesC, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
     const int beg = valid ? __ldg(rptr + row) : 0, end = valid ? __ldg(rptr + row + 1) : 0;
-    const float4 s = rg_csr_sum<G>(valid, lane, beg, end, rcol, rw, res_fine);
+    HeldEntries<kHeldC> he;
+    hold_csr_row<G>(he, valid, lane, beg, end, rcol, rw);
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    const float4 s = held_sum<G>(he, lane, rcol, rw, res_fine);
     if (!valid || lane >= S) return;
     r[row] = s;
     const float di = dinv ? __ldg(dinv + row) : 0.f;
@@ -268,14 +370,17 @@ __global__ void __launch_bounds__(256) k_lvl_sweep(int n, const int32_t* __restr
                                                    const float* __restrict__ dinv, const float4* __restrict__ r,
                                                    const float4* __restrict__ ein, float4* __restrict__ eout,
                                                    const int32_t* __restrict__ gate) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;
+    pdl_trigger();
     constexpr int G = kLanesC, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
-    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, ein);
+    HeldEntries<kHeldC> he;
+    hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    const float4 off = held_sum<G>(he, lane, col, val, ein);
     if (!valid || lane >= S) return;
     const float4 x = __ldg(ein + row), ri = __ldg(r + row);
     const float D = __ldg(dfull + row), w = __ldg(dinv + row);
@@ -288,14 +393,17 @@ __global__ void __launch_bounds__(256) k_lvl_residual(int n, const int32_t* __re
                                                       const float* __restrict__ val, const float* __restrict__ dfull,
                                                       const float4* __restrict__ r, const float4* __restrict__ e,
                                                       float4* __restrict__ res, const int32_t* __restrict__ gate) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;
+    pdl_trigger();
     constexpr int G = kLanesC, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
-    const float4 off = rg_offdiag<G>(row, valid, lane, sp, col, val, e);
+    HeldEntries<kHeldC> he;
+    hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    const float4 off = held_sum<G>(he, lane, col, val, e);
     if (!valid || lane >= S) return;
     const float4 x = __ldg(e + row), ri = __ldg(r + row);
     const float D = __ldg(dfull + row);
@@ -340,17 +448,21 @@ __global__ void __launch_bounds__(256) k_prolong_sweep(int n, const int4* __rest
                                                        const float4* __restrict__ res, const float4* din, float4* dout,
                                                        const float* __restrict__ fixf, float4* __restrict__ ls_r,
                                                        const int32_t* __restrict__ gate) {
-    pdl_enter();
-    if (gate && __ldg(gate) == 0) return;
+    pdl_trigger();
     constexpr int S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
-    const float4 q = rg_offdiag<G>(row, valid, lane, sp, col, val, ec);
-    if (!valid || lane >= S) return;
-    const int4 id = __ldg(pid + row);
-    const float4 w = __ldg(pw + row);
+    HeldEntries<G == kLanesL0 ? kHeldL0 : kHeldC> he;
+    hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    const bool own = valid && lane < S;
+    const int4 id = own ? __ldg(pid + row) : make_int4(0, 0, 0, 0);
+    const float4 w = own ? __ldg(pw + row) : f4z();
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    const float4 q = held_sum<G>(he, lane, col, val, ec);
+    if (!own) return;
     const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
     const float4 pe = make_float4(w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x,
                                   w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y,
@@ -1212,6 +1324,12 @@ __global__ void __launch_bounds__(kOpThreads) k_op_init(int n, int m, const floa
     E[(size_t)i * m + c] = c == i ? di : 0.f;
 }
 
+// The sweep, restriction and prolongation kernels stage the row's static
+// structure (ELL or CSR entries, parents and weights, uploaded once at set-up)
+// before the dependency wait, so that after it every load of the previous
+// phase's block is independent of the others.
+constexpr int kOpMaxEntries = 64;   // entries of one row staged in shared memory; longer rows take a tail loop
+
 // residual == 0: Xout = Xin + dinv (R - D Xin - Off Xin); residual != 0: Xout = R - D Xin - Off Xin.
 // Level of slice height 32 / kLanesC (coarse levels), off-diagonal sliced ELL.
 __global__ void __launch_bounds__(kOpThreads) k_op_sweep(int n, int m, const int32_t* __restrict__ sp,
@@ -1221,15 +1339,26 @@ __global__ void __launch_bounds__(kOpThreads) k_op_sweep(int n, int m, const int
                                                         const float* __restrict__ dinv, const float* __restrict__ R,
                                                         const float* __restrict__ Xin, float* __restrict__ Xout,
                                                         int residual) {
-    pdl_enter();
+    pdl_trigger();
     constexpr int S = 32 / kLanesC;
+    __shared__ int32_t scol[kOpMaxEntries];
+    __shared__ float sval[kOpMaxEntries];
     const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= n || c >= m) return;
+    if (i >= n) return;   // CTA-uniform
     const int slice = i / S;
     const int e0 = __ldg(sp + slice) + (i - slice * S), e1 = __ldg(sp + slice + 1);
+    const int cnt = (e1 - e0 + S - 1) / S, staged = min(cnt, kOpMaxEntries);
+    for (int t = threadIdx.x; t < staged; t += blockDim.x) {
+        scol[t] = __ldg(col + e0 + t * S);
+        sval[t] = __ldg(val + e0 + t * S);
+    }
+    __syncthreads();
+    pdl_wait();
+    if (c >= m) return;
     float acc = 0.f;
-#pragma unroll 8
-    for (int e = e0; e < e1; e += S) acc = fmaf(__ldg(val + e), Xin[(size_t)__ldg(col + e) * m + c], acc);
+#pragma unroll 16
+    for (int t = 0; t < staged; ++t) acc = fmaf(sval[t], Xin[(size_t)scol[t] * m + c], acc);
+    for (int e = e0 + kOpMaxEntries * S; e < e1; e += S) acc = fmaf(__ldg(val + e), Xin[(size_t)__ldg(col + e) * m + c], acc);
     const float x = Xin[(size_t)i * m + c];
     const float r = R[(size_t)i * m + c] - fmaf(__ldg(dfull + i), x, acc);
     Xout[(size_t)i * m + c] = residual ? r : fmaf(__ldg(dinv + i), r, x);
@@ -1242,34 +1371,71 @@ __global__ void __launch_bounds__(kOpThreads) k_op_restrict(int n, int m, const 
                                                            const float* __restrict__ Resf,
                                                            const float* __restrict__ dinv, float* __restrict__ Rc,
                                                            float* __restrict__ Ec) {
-    pdl_enter();
+    pdl_trigger();
+    __shared__ int32_t scol[kOpMaxEntries];
+    __shared__ float sw[kOpMaxEntries];
     const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= n || c >= m) return;
+    if (i >= n) return;   // CTA-uniform
+    const int k0 = __ldg(rptr + i), k1 = __ldg(rptr + i + 1);
+    const int staged = min(k1 - k0, kOpMaxEntries);
+    for (int t = threadIdx.x; t < staged; t += blockDim.x) {
+        scol[t] = __ldg(rcol + k0 + t);
+        sw[t] = __ldg(rw + k0 + t);
+    }
+    __syncthreads();
+    pdl_wait();
+    if (c >= m) return;
     float acc = 0.f;
-    const int k1 = __ldg(rptr + i + 1);
-#pragma unroll 8
-    for (int k = __ldg(rptr + i); k < k1; ++k) acc = fmaf(__ldg(rw + k), Resf[(size_t)__ldg(rcol + k) * m + c], acc);
+#pragma unroll 16
+    for (int t = 0; t < staged; ++t) acc = fmaf(sw[t], Resf[(size_t)scol[t] * m + c], acc);
+    for (int k = k0 + kOpMaxEntries; k < k1; ++k) acc = fmaf(__ldg(rw + k), Resf[(size_t)__ldg(rcol + k) * m + c], acc);
     Rc[(size_t)i * m + c] = acc;
     Ec[(size_t)i * m + c] = (dinv ? __ldg(dinv + i) : 0.f) * acc;
 }
 
-// Coarsest level: E = Ainv R (dense inverse of the one body; FP64 products when Ainv64 is set).
-__global__ void __launch_bounds__(kOpThreads) k_op_coarsest(int n, int m, const float* __restrict__ Ainv,
-                                                           const double* __restrict__ Ainv64,
-                                                           const float* __restrict__ R, float* __restrict__ E) {
+// Coarsest level: E = Ainv R (n x n dense inverse of the one body times the
+// n x m block; T = double for the FP64 inverse of the mixed kind).  A CTA forms
+// a 4-row x 64-column tile of E: its 4 rows of Ainv staged in shared memory,
+// the k range split over 4 thread groups (a column per thread, coalesced rows
+// of R), the 4 partial sums added in shared memory.
+constexpr int kOpcRows = 4, kOpcCols = 64, kOpcSplit = 4, kOpcThreads = kOpcCols * kOpcSplit;
+template <typename T>
+__global__ void __launch_bounds__(kOpcThreads) k_op_coarsest(int n, int m, const T* __restrict__ Ainv,
+                                                            const float* __restrict__ R, float* __restrict__ E) {
     pdl_enter();
-    const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= n || c >= m) return;
-    if (Ainv64) {
-        double acc = 0.0;
-#pragma unroll 8
-        for (int k = 0; k < n; ++k) acc = fma(__ldg(Ainv64 + (size_t)i * n + k), (double)R[(size_t)k * m + c], acc);
-        E[(size_t)i * m + c] = (float)acc;
-    } else {
-        float acc = 0.f;
-#pragma unroll 8
-        for (int k = 0; k < n; ++k) acc = fmaf(__ldg(Ainv + (size_t)i * n + k), R[(size_t)k * m + c], acc);
-        E[(size_t)i * m + c] = acc;
+    __shared__ T As[kOpcRows][kDenseOpMaxRows];
+    __shared__ T part[kOpcSplit - 1][kOpcRows][kOpcCols];
+    const int i0 = blockIdx.x * kOpcRows, c0 = blockIdx.y * kOpcCols;
+    const int tc = threadIdx.x % kOpcCols, kq = threadIdx.x / kOpcCols;
+    for (int t = threadIdx.x; t < kOpcRows * n; t += kOpcThreads) {
+        const int r = t / n, k = t - r * n;
+        As[r][k] = i0 + r < n ? Ainv[(size_t)(i0 + r) * n + k] : T(0);
+    }
+    __syncthreads();
+    const int c = c0 + tc;
+    const int kb = kq * n / kOpcSplit, ke = (kq + 1) * n / kOpcSplit;
+    T acc[kOpcRows];
+#pragma unroll
+    for (int j = 0; j < kOpcRows; ++j) acc[j] = T(0);
+    if (c < m) {
+#pragma unroll 12
+        for (int k = kb; k < ke; ++k) {
+            const T r = (T)R[(size_t)k * m + c];
+#pragma unroll
+            for (int j = 0; j < kOpcRows; ++j) acc[j] = fma(As[j][k], r, acc[j]);
+        }
+    }
+    if (kq > 0)
+#pragma unroll
+        for (int j = 0; j < kOpcRows; ++j) part[kq - 1][j][tc] = acc[j];
+    __syncthreads();
+    if (kq != 0 || c >= m) return;
+#pragma unroll
+    for (int j = 0; j < kOpcRows; ++j) {
+        T v = acc[j];
+#pragma unroll
+        for (int q = 0; q < kOpcSplit - 1; ++q) v += part[q][j][tc];
+        if (i0 + j < n) E[(size_t)(i0 + j) * m + c] = (float)v;
     }
 }
 
@@ -1277,11 +1443,13 @@ __global__ void __launch_bounds__(kOpThreads) k_op_coarsest(int n, int m, const 
 __global__ void __launch_bounds__(kOpThreads) k_op_prolong(int n, int m, const int4* __restrict__ pid,
                                                           const float4* __restrict__ pw, const float* __restrict__ Ec,
                                                           float* __restrict__ Ef) {
-    pdl_enter();
+    pdl_trigger();
     const int i = blockIdx.x, c = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= n || c >= m) return;
+    if (i >= n) return;
     const int4 id = __ldg(pid + i);
     const float4 w = __ldg(pw + i);
+    pdl_wait();
+    if (c >= m) return;
     Ef[(size_t)i * m + c] += w.x * Ec[(size_t)id.x * m + c] + w.y * Ec[(size_t)id.y * m + c] +
                              w.z * Ec[(size_t)id.z * m + c] + w.w * Ec[(size_t)id.w * m + c];
 }
@@ -1303,7 +1471,7 @@ __global__ void __launch_bounds__(256) k_op_round(int count, const double* __res
 // r_F from shared memory, then its row of e_F.
 constexpr int kApplyG = 4;         // lanes per restricted row
 constexpr int kApplyK = 4;         // children per lane held in registers
-constexpr int kApplyPasses = 2;    // restricted rows per thread held in registers
+constexpr int kApplyPasses = 4;    // restricted rows per thread held in registers (512 rows)
 constexpr int kApplyMRegs = 16;    // entries of the warp's row of M per lane held in registers
 
 __host__ __device__ constexpr size_t coarse_apply_smem_bytes(int nf, int nfine) {

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kMxThreads, 3) k_mx_residual(int n, const int3
                                                      const float4* __restrict__ slots, const float* __restrict__ fixf,
                                                      float4* __restrict__ ls_r, float* __restrict__ part,
                                                      float* __restrict__ part_end) {
-    pdl_enter();
+    pdl_trigger();
     __shared__ float red[kMxThreads / 32];
     constexpr int G = kLanesMx, RW = 32 / G;   // lanes per row, rows per warp
     constexpr int SH = 32 / kLanesL0;           // slice height of the level-0 sliced ELL
@@ -143,7 +143,9 @@ __global__ void __launch_bounds__(kMxThreads, 3) k_mx_residual(int n, const int3
     // Every load whose address is known is issued before the first sum: the row's slots (up to
     // kMxSlotsAhead per lane) and its ELL entries (up to kMxEllAhead per lane), then the neighbour
     // displacements; the sums then run in the order of the plain loops (same bits).  Rows with more
-    // entries finish in the tail loops.
+    // entries finish in the tail loops.  The set-up structure (slot and ELL offsets, columns, FP64
+    // values, the contact-free diagonal, the fix mask) is written by no kernel: it is loaded before
+    // the dependency wait, while the previous kernel runs.
     constexpr int kMxSlotsAhead = 6, kMxEllAhead = 4;
     int s_beg = 0, s_end = 0, q0 = 0, end = 0;
     if (valid) {
@@ -155,14 +157,6 @@ __global__ void __launch_bounds__(kMxThreads, 3) k_mx_residual(int n, const int3
         q0 = __ldg(sp + slice) + j * SH + (row - slice * SH);
         end = __ldg(sp + slice + 1);
     }
-    float4 sl[kMxSlotsAhead];
-    if (b0) {
-#pragma unroll
-        for (int k = 0; k < kMxSlotsAhead; ++k) {
-            const int q = s_beg + k * G;
-            sl[k] = q < s_end ? __ldg(slots + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    }
     int cj[kMxEllAhead];
     double av[kMxEllAhead];
 #pragma unroll
@@ -172,11 +166,21 @@ __global__ void __launch_bounds__(kMxThreads, 3) k_mx_residual(int n, const int3
         cj[k] = ok ? __ldg(col + q) : -1;
         av[k] = ok ? __ldg(val + q) : 0.0;
     }
-    // the row's own data, on the row's first lane
     const bool own = valid && lane < RW;
-    const double4 xown = own ? d[row] : d4z();
-    const double Down = own ? __ldg(diag64 + row) + (double)__ldg(c + row) : 0.0;
+    const double D0 = own ? __ldg(diag64 + row) : 0.0;
     const float fxown = own ? __ldg(fixf + row) : 0.f;
+    pdl_wait();
+    float4 sl[kMxSlotsAhead];
+    if (b0) {
+#pragma unroll
+        for (int k = 0; k < kMxSlotsAhead; ++k) {
+            const int q = s_beg + k * G;
+            sl[k] = q < s_end ? __ldg(slots + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+    // the row's own data, on the row's first lane
+    const double4 xown = own ? d[row] : d4z();
+    const double Down = own ? D0 + (double)__ldg(c + row) : 0.0;
     const float wown = (own && first_sweep) ? __ldg(dinv + row) : 0.f;
     double4 bi = d4z(), bprev = d4z();
     if (b0) {   // uniform over the block: the row's slots split over its G lanes, FP64 sums

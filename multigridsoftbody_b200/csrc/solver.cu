@@ -1216,8 +1216,13 @@ void enqueue_coarse_operator(mgsb_solver* h, const CoarseArgs& ca) {
         cur[l + 1] = blk(l + 1, E);
     }
     const LevelView& Cl = ca.lv[L - 1];
-    LAUNCH(h, k_op_coarsest, grid(Cl.n), kOpThreads, 0, Cl.n, m, ca.Ainv, ca.Ainv64, (const float*)blk(L - 1, R),
-           blk(L - 1, E));
+    const dim3 gc((unsigned)((Cl.n + kOpcRows - 1) / kOpcRows), (unsigned)((m + kOpcCols - 1) / kOpcCols));
+    if (ca.Ainv64)
+        LAUNCH(h, k_op_coarsest<double>, gc, kOpcThreads, 0, Cl.n, m, ca.Ainv64, (const float*)blk(L - 1, R),
+               blk(L - 1, E));
+    else
+        LAUNCH(h, k_op_coarsest<float>, gc, kOpcThreads, 0, Cl.n, m, ca.Ainv, (const float*)blk(L - 1, R),
+               blk(L - 1, E));
     for (int l = L - 2; l >= F; --l) {
         const LevelView& C = ca.lv[l];
         const LevelView& Cc = ca.lv[l + 1];
@@ -2673,6 +2678,30 @@ extern "C" mgsb_status mgsb_learned_stats(mgsb_solver* h, uint64_t out[2]) {
     CUDA_TRY(h, cudaMemcpy(tmp, h->ls_stats, sizeof tmp, cudaMemcpyDeviceToHost));
     out[0] = tmp[0];
     out[1] = tmp[1];
+    return MGSB_OK;
+}
+
+extern "C" mgsb_status mgsb_learned_cycle_norms(mgsb_solver* h, double* before, double* after, int32_t cap,
+                                                int32_t* n) {
+    if (!h || !n || cap < 0 || (cap > 0 && (!before || !after))) return MGSB_INVALID_ARG;
+    *n = 0;
+    if (!is_mg(h) || h->dirty || !h->ls_part0) return MGSB_OK;
+    TRY(sync_check(h));
+    const size_t count = (size_t)h->ls_cycles * h->ls_nblk;
+    std::vector<float> p0(count), p1(count);
+    CUDA_TRY(h, cudaMemcpy(p0.data(), h->ls_part0, count * sizeof(float), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(p1.data(), h->ls_part1, count * sizeof(float), cudaMemcpyDeviceToHost));
+    const int cycles = h->ls_cycles;
+    for (int c = 0; c < cycles && c < cap; ++c) {
+        double a = 0.0, q = 0.0;
+        for (int i = 0; i < h->ls_nblk; ++i) {
+            a += p0[(size_t)c * h->ls_nblk + i];
+            q += p1[(size_t)c * h->ls_nblk + i];
+        }
+        before[c] = std::sqrt(a);
+        after[c] = std::sqrt(q);
+    }
+    *n = cycles;
     return MGSB_OK;
 }
 
