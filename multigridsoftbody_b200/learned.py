@@ -129,3 +129,29 @@ def train_smoother(x, t, steps: int = 20000, batch: int = 4096, lr: float = 2e-3
     net = MLP(device=device, seed=seed)
     losses = net.train(x, t, steps=steps, batch=batch, lr=lr, seed=seed + 1)
     return net, losses
+
+
+def held_out_contraction(net, mesh, fixed, params, tool_path, guard_ratio: float = 0.5):
+    """How well `net` smooths inside the learned V-cycle on a held-out run: steps a solver with
+    `params` (a learned form: mixed precision, its sweeps and passes) along `tool_path` ((a, b)
+    capsule ends per frame, radius 0.3) and collects, per learned V-cycle, |r_after| / |r_before|
+    (mgsb_learned_cycle_norms).  Returns {"failed_checks", "cycles", "ratio_p50", "ratio_p99",
+    "ratio_max"}; fewer failed checks, then a lower 99th percentile, is better."""
+    from .api import Solver
+    s = Solver(mesh, params)
+    try:
+        s.set_fixed(fixed)
+        s.set_learned_smoother(net, guard_ratio)
+        ratios = []
+        for a, b in tool_path:
+            s.set_capsule(a, b, 0.3)
+            s.step()
+            before, after = s.learned_cycle_norms()
+            ok = before > 0
+            ratios.extend((after[ok] / before[ok]).tolist())
+        checks, failed = s.learned_stats()
+    finally:
+        s.close()
+    r = np.asarray(ratios) if ratios else np.zeros(1)
+    return {"failed_checks": int(failed), "cycles": int(checks), "ratio_p50": float(np.percentile(r, 50)),
+            "ratio_p99": float(np.percentile(r, 99)), "ratio_max": float(r.max())}
