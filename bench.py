@@ -556,6 +556,9 @@ def accuracy(mg, meshes, fixeds, params, paths, net, variants, frames=100):
 # Sweep counts picked by accuracy (multigridsoftbody_b200.sweeps), the same search for both families
 # ---------------------------------------------------------------------------
 ERROR_BAR = 1e-5   # max vertex error / bbox diagonal after 100 frames
+# The selection chooses among forms within half the bar on its held-out paths: a form just under the
+# bar there (the learned 1-pass form: 8e-6) can be well over it on the check paths (2e-4 seen).
+SELECTION_MARGIN = 0.5
 
 
 def accuracy_paths(name, seed):
@@ -776,7 +779,7 @@ def run_ours(args):
         held = accuracy_paths(args.workload, 301)
         selection = swp.select_sweeps(meshes[0], fixeds[0], params[0], net, [t for _, t in held],
                                       time_fn=lambda p, netx: time_config(p, netx, held[-1][1]),
-                                      bar=ERROR_BAR, time_all=True)
+                                      bar=ERROR_BAR, time_all=True, margin=SELECTION_MARGIN)
         selection["held_out_paths"] = [label + ", tool seed 301" for label, _ in held]
         choice = selection["learned_mixed"]["chosen"]
         if dist is not None:   # every rank runs rank 0's choice

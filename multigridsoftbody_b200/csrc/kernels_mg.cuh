@@ -1473,6 +1473,7 @@ constexpr int kApplyG = 4;         // lanes per restricted row
 constexpr int kApplyK = 4;         // children per lane held in registers
 constexpr int kApplyPasses = 4;    // restricted rows per thread held in registers (512 rows)
 constexpr int kApplyMRegs = 16;    // entries of the warp's row of M per lane held in registers
+constexpr int kApplyStage = 8;     // residual rows per thread loaded at once when staging (4,096 per pass)
 
 __host__ __device__ constexpr size_t coarse_apply_smem_bytes(int nf, int nfine) {
     return (size_t)(nf + nfine) * sizeof(float4);
@@ -1515,7 +1516,20 @@ __global__ void __launch_bounds__(kDenseApplyThreads, 1) k_coarse_apply(int nf, 
         const int k = lane + 32 * j;
         mr[j] = (i < nf && k < nf) ? __ldg(M + (size_t)i * nf + k) : 0.f;
     }
-    for (int r = tid; r < nfine; r += kDenseApplyThreads) resf[r] = res_fine[r];
+    // the level-(F-1) residual: every load of a thread in flight at once, then the stores
+    for (int base = 0; base < nfine; base += kDenseApplyThreads * kApplyStage) {
+        float4 v[kApplyStage];
+#pragma unroll
+        for (int u = 0; u < kApplyStage; ++u) {
+            const int r = base + u * kDenseApplyThreads + tid;
+            v[u] = r < nfine ? res_fine[r] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < kApplyStage; ++u) {
+            const int r = base + u * kDenseApplyThreads + tid;
+            if (r < nfine) resf[r] = v[u];
+        }
+    }
     __syncthreads();
     auto group_sum = [&](float4 a) {
 #pragma unroll

@@ -51,12 +51,15 @@ __device__ __forceinline__ float tanh_hw(float x) {
     return y;
 }
 constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+// u = x (C + C A x^2), g = h + h t with h = x/2: six instructions (the
+// epilogues apply it to every hidden activation).
 __device__ __forceinline__ float gelu(float x) {
-    const float t = tanh_hw(kGeluC * fmaf(kGeluA * x, x * x, x));
-    return 0.5f * x * (1.f + t);
+    const float t = tanh_hw(x * fmaf(kGeluC * kGeluA, x * x, kGeluC));
+    const float h = 0.5f * x;
+    return fmaf(h, t, h);
 }
 __device__ __forceinline__ float gelu_grad(float x) {
-    const float t = tanh_hw(kGeluC * fmaf(kGeluA * x, x * x, x));
+    const float t = tanh_hw(x * fmaf(kGeluC * kGeluA, x * x, kGeluC));
     return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * kGeluC * fmaf(3.f * kGeluA, x * x, 1.f);
 }
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
@@ -276,16 +279,20 @@ __device__ __forceinline__ void mlp_cta_teardown(MlpSmem& S, uint32_t tmem, Wait
 // interleaved, K = 64).
 __device__ __forceinline__ void mlp_hidden_epilogue(MlpSmem& S, uint32_t taddr, const float* bias, int row_in_tile,
                                                     int c0) {
+    // both 16-column loads in flight before the one wait
+    static_assert(kMlpHid / 2 == 32, "a warp's half of the hidden columns is two 16-column loads");
+    float v[2][16];
+    tmem_ld16(taddr + c0, v[0]);
+    tmem_ld16(taddr + c0 + 16, v[1]);
+    tmem_wait_ld();
 #pragma unroll
-    for (int c = c0; c < c0 + kMlpHid / 2; c += 16) {
-        float v[16];
-        tmem_ld16(taddr + c, v);
-        tmem_wait_ld();
+    for (int h = 0; h < 2; ++h) {
+        const int c = c0 + 16 * h;
         uint32_t packed[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const __nv_bfloat162 two = __floats2bfloat162_rn(gelu(v[2 * i] + bias[c + 2 * i]),
-                                                             gelu(v[2 * i + 1] + bias[c + 2 * i + 1]));
+            const __nv_bfloat162 two = __floats2bfloat162_rn(gelu(v[h][2 * i] + bias[c + 2 * i]),
+                                                             gelu(v[h][2 * i + 1] + bias[c + 2 * i + 1]));
             packed[i] = *reinterpret_cast<const uint32_t*>(&two);
         }
         uint8_t* base = S.h + interleaved_offset(row_in_tile, c, kMlpHid);

@@ -97,20 +97,21 @@ def time_frames(mesh, fixed, p, net, tool, frames=60, warm=10, tune=True, solver
 
 def select_sweeps(mesh, fixed, base, net, tool, time_fn=None, bar=ERROR_BAR, frames=100,
                   learned_candidates=LEARNED_CANDIDATES, plain_candidates=PLAIN_CANDIDATES, solver_cls=Solver,
-                  time_all=False):
+                  time_all=False, margin=1.0):
     """For each family, every candidate's max vertex error / bbox diagonal after `frames` frames from
     rest against the converged solver -- the largest over the tool paths when `tool` is a list of tool
     callbacks --, the frame time (time_fn(params, net) in ms; default `time_frames` on the first path)
     of those within `bar` (of every candidate with `time_all`, so that the margins can be read), and the
-    fastest candidate within the bar as the family's choice (None when none is within it).  `net` is
-    the learned smoother (None skips that family)."""
+    fastest candidate within margin x bar as the family's choice (None when none is within it): a
+    margin below 1 keeps forms whose error sits just under the bar on these paths, and may exceed it
+    on others, out of the choice.  `net` is the learned smoother (None skips that family)."""
     tools = list(tool) if isinstance(tool, (list, tuple)) else [tool]
     if time_fn is None:
         def time_fn(p, netx):
             return time_frames(mesh, fixed, p, netx, tools[0], solver_cls=solver_cls)
     refs = [converged_positions(mesh, fixed, base, t, frames, solver_cls) for t in tools]
     diag = mesh.bbox_diagonal()
-    out = {"frames": frames, "bar": bar, "paths": len(tools),
+    out = {"frames": frames, "bar": bar, "paths": len(tools), "margin": margin,
            "error": "max over vertices of the Euclidean distance / bbox diagonal, worst over the paths"}
     families = [("plain_fp32", plain_candidates, False)]
     if net is not None:
@@ -129,6 +130,6 @@ def select_sweeps(mesh, fixed, base, net, tool, time_fn=None, bar=ERROR_BAR, fra
             if row["within_bar"] or time_all:
                 row["ms_per_frame"] = float(time_fn(p, net if learned else None))
             rows.append(row)
-        ok = [r for r in rows if r["within_bar"]]
+        ok = [r for r in rows if r["err_over_diag"] <= margin * bar]
         out[fam] = {"candidates": rows, "chosen": min(ok, key=lambda r: r["ms_per_frame"]) if ok else None}
     return out

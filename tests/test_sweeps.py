@@ -144,3 +144,17 @@ def test_worst_path_decides():
     for r in out["plain_fp32"]["candidates"]:
         assert r["err_per_path"] == pytest.approx([0.6e-5, 1.2e-5]) and not r["within_bar"]
     assert out["plain_fp32"]["chosen"] is None and out["paths"] == 2
+
+
+def test_margin_keeps_forms_near_the_bar_out():
+    """With margin 0.5 a form at 0.8 x bar is timed (within the bar) but not chosen; the slower form at
+    0.4 x bar is."""
+    def err(p, learned):   # error / diag = value / 10
+        return 0.8e-4 if p.refinement_passes == 1 else 0.4e-4
+
+    out = sweeps.select_sweeps(FakeMesh(), None, FakeParams(2, 2, 1, 1), None, tool,
+                               lambda p, net: float(p.refinement_passes), frames=2, solver_cls=fake_solver(err),
+                               margin=0.5)
+    rows = {r["key"]: r for r in out["plain_fp32"]["candidates"]}
+    assert rows["plain_fp32_1pass_2+2"]["within_bar"] and "ms_per_frame" in rows["plain_fp32_1pass_2+2"]
+    assert out["plain_fp32"]["chosen"]["passes"] == 2 and out["margin"] == 0.5
