@@ -283,6 +283,14 @@ mgsb_status mgsb_set_launch_overlap(mgsb_solver* h, int32_t on);
  * and the post-smoothing residual).  0 = separate launches.  The same
  * V-cycle; results agree to rounding.  No reference counterpart. */
 mgsb_status mgsb_set_fused_prolongation(mgsb_solver* h, int32_t on);
+/* Level-1 restriction straight from level 0 (default 0): with RO = R * Off(level 0)
+ * precomputed, R (b - A d) = R (b - D d) - RO d, so when level 1 runs grid-wide
+ * (coarse split >= 2) and the prolongation is fused, the level-0 residual is
+ * not formed as a launch of its own (the fused prolongation forms the rows it
+ * needs).  0 = the separate residual launch.  The same V-cycle; results agree
+ * to rounding.  On config 1 the fused launch costs what the two it replaces
+ * cost (4.9 vs 2.2 + 2.9 µs), hence off by default.  No reference counterpart. */
+mgsb_status mgsb_set_fused_restriction(mgsb_solver* h, int32_t on);
 /* Tool-contact broad phase of the multigrid kinds (default 0 = every
  * surface vertex against its body's capsule).  1: a uniform grid per body
  * over the rest bounding box of its surface, rebuilt every frame from the

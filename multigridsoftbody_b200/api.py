@@ -476,6 +476,10 @@ class Solver:
         """Prolongation + first post-smoothing sweep as one kernel (default on)."""
         _check(self._lib.mgsb_set_fused_prolongation(self.h, 1 if on else 0), self.h)
 
+    def set_fused_restriction(self, on: bool = True) -> None:
+        """Level-1 restriction straight from level 0, no level-0 residual launch (default off)."""
+        _check(self._lib.mgsb_set_fused_restriction(self.h, 1 if on else 0), self.h)
+
     def set_launch_overlap(self, on: bool = True) -> None:
         """Programmatic dependent launch between the frame's kernels (default on)."""
         _check(self._lib.mgsb_set_launch_overlap(self.h, 1 if on else 0), self.h)

@@ -214,6 +214,9 @@ inline size_t ls_sweep_smem_bytes() {
 // is taken by the next outer residual), the finished correction is also applied
 // to the FP64 displacement, dd64_i += d_i, with its FP32 mirror d32_i: each row
 // belongs to one thread, so this is the work of k_mx_update for that row.
+// With din set the sweep reads the iterate from din and writes every row of d
+// (d = din + update): the post-smoothing kernel before it then leaves din intact
+// while it reads its neighbours.
 __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, const int32_t* __restrict__ sp,
                                                              const int32_t* __restrict__ col, const float* __restrict__ val,
                                                              const float* __restrict__ dfull,
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
                                                              const float* __restrict__ fixf, const float4* __restrict__ r,
                                                              const uint8_t* __restrict__ img, float4* __restrict__ d,
                                                              int32_t* __restrict__ err, double4* __restrict__ dd64,
-                                                             float4* __restrict__ d32) {
+                                                             float4* __restrict__ d32, const float4* __restrict__ din) {
     pdl_trigger();
     constexpr int S = 32 / kLanesL0;   // level-0 slice height
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -282,7 +285,7 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
         if (!half && row < n) {
             rcv = __ldg(rc + row);
             Dr = __ldg(dfull + row);
-            dq = d[row];
+            dq = din ? din[row] : d[row];
             if (dd64) dv = dd64[row];
         }
         bool win_ok = true;
@@ -360,14 +363,14 @@ __global__ void __launch_bounds__(kMlpThreads) k_ls_sweep_tc(int n, int ntiles, 
             if (err) atomicExch(err, 1);
         }
         // threads 0..127 hold row rt's outputs (warps 0-3 serve TMEM lanes 0..127)
-        if (ok && !half && row < n && (sc != 0.f || dd64)) {
+        if (ok && !half && row < n && (sc != 0.f || dd64 || din)) {
             float4 q = dq;
             if (sc != 0.f) {
                 q.x += sc * out[0];
                 q.y += sc * out[1];
                 q.z += sc * out[2];
-                d[row] = q;
             }
+            if (sc != 0.f || din) d[row] = q;
             if (dd64) {
                 double4 v = dv;
                 v.x += q.x;

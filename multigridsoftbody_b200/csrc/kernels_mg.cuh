@@ -54,6 +54,12 @@ struct CoarseArgs {
     const float4* b;         // level-0 right-hand side
     float4* d;               // level-0 unknown (displacement)
     const int32_t* gate;     // if set, the kernel runs only when *gate != 0 (learned-smoother fallback)
+    // level-1 right-hand side straight from level 0 (host launches only): with res0_b set, level 1's
+    // restriction forms R (res0_b - D0 d) - RO d, RO = R Off(level 0), and lv[0].res is not read
+    const float4* res0_b;
+    const int32_t* ro_ptr;
+    const int32_t* ro_col;
+    const float* ro_val;
     LevelView lv[kMaxLevels];
 };
 
@@ -364,6 +370,64 @@ __global__ void __launch_bounds__(256) k_lvl_restrict(int n, const int32_t* __re
     e[row] = make_float4(di * s.x, di * s.y, di * s.z, 0.f);
 }
 
+// Level 1's restriction without the level-0 residual: with res0 = b0 - D0 d0 -
+// Off0 d0 and RO = R Off0 (precomputed, CSR over level-1 rows),
+//     r = R res0 = R (b0 - D0 d0) - RO d0,
+// so the level-0 residual launch is not needed (its rows are formed by the
+// post-smoothing kernel, k_prolong_sweep, where it needs them).  e = dinv r as
+// k_lvl_restrict.  8 lanes per row; children and RO entries held before the wait.
+constexpr int kHeldRO = 16;   // RO entries held per lane (128 per row; config 1: ~125)
+__global__ void __launch_bounds__(256) k_lvl_restrict_res0(int n, const int32_t* __restrict__ rptr,
+                                                           const int32_t* __restrict__ rcol,
+                                                           const float* __restrict__ rw,
+                                                           const int32_t* __restrict__ roptr,
+                                                           const int32_t* __restrict__ rocol,
+                                                           const float* __restrict__ roval,
+                                                           const float4* __restrict__ b0, const float* __restrict__ dfull0,
+                                                           const float4* __restrict__ d0, const float* __restrict__ dinv,
+                                                           float4* __restrict__ r, float4* __restrict__ e,
+                                                           const int32_t* __restrict__ gate) {
+    pdl_trigger();
+    constexpr int G = kLanesC, S = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = warp * S + (lane % S);
+    const bool valid = row < n;
+    const int beg = valid ? __ldg(rptr + row) : 0, end = valid ? __ldg(rptr + row + 1) : 0;
+    const int obeg = valid ? __ldg(roptr + row) : 0, oend = valid ? __ldg(roptr + row + 1) : 0;
+    HeldEntries<kHeldC> hc;
+    hold_csr_row<G>(hc, valid, lane, beg, end, rcol, rw);
+    HeldEntries<kHeldRO> ho;
+    hold_csr_row<G>(ho, valid, lane, obeg, oend, rocol, roval);
+    pdl_wait();
+    if (gate && __ldg(gate) == 0) return;
+    // R (b0 - D0 d0): this lane's children, in the order of hold_csr_row
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    auto child = [&](int i, float w) {
+        const float4 bb = __ldg(b0 + i), dd = __ldg(d0 + i);
+        const float D = __ldg(dfull0 + i);
+        ax = fmaf(w, bb.x - D * dd.x, ax);
+        ay = fmaf(w, bb.y - D * dd.y, ay);
+        az = fmaf(w, bb.z - D * dd.z, az);
+    };
+#pragma unroll
+    for (int k = 0; k < kHeldC; ++k)
+        if (hc.c[k] >= 0) child(hc.c[k], hc.v[k]);
+    for (int q = hc.next; q < hc.end; q += hc.stride) child(__ldg(rcol + q), __ldg(rw + q));
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    const float4 q = held_sum<G>(ho, lane, rocol, roval, d0);
+    if (!valid || lane >= S) return;
+    const float4 s = make_float4(ax - q.x, ay - q.y, az - q.z, 0.f);
+    r[row] = s;
+    const float di = dinv ? __ldg(dinv + row) : 0.f;
+    e[row] = make_float4(di * s.x, di * s.y, di * s.z, 0.f);
+}
+
 // eout = ein + dinv (r - A ein)
 __global__ void __launch_bounds__(256) k_lvl_sweep(int n, const int32_t* __restrict__ sp, const int32_t* __restrict__ col,
                                                    const float* __restrict__ val, const float* __restrict__ dfull,
@@ -438,7 +502,10 @@ __global__ void k_lvl_prolong(int n, const int4* __restrict__ pid, const float4*
 // needs no neighbour of the prolonged vector: one launch instead of two.
 // G lanes per row over OP's sliced-ELL row; dout may be din.  With ls_r set
 // (the learned cycle) the output is instead the post-smoothing residual
-// ls_r = fix (res - D pe - OP e_c), and d += pe in place.
+// ls_r = fix (res - D pe - OP e_c), and dout = din + pe.  With res null the
+// kernel forms its rows of res = b - A din itself (the level's own sliced ELL
+// sp0 / col0 / val0, same arithmetic as k_l0_residual_rg): din must then not
+// be dout.
 // ---------------------------------------------------------------------------
 template <int G>
 __global__ void __launch_bounds__(256) k_prolong_sweep(int n, const int4* __restrict__ pid, const float4* __restrict__ pw,
@@ -447,28 +514,39 @@ __global__ void __launch_bounds__(256) k_prolong_sweep(int n, const int4* __rest
                                                        const float* __restrict__ dfull, const float* __restrict__ dinv,
                                                        const float4* __restrict__ res, const float4* din, float4* dout,
                                                        const float* __restrict__ fixf, float4* __restrict__ ls_r,
-                                                       const int32_t* __restrict__ gate) {
+                                                       const int32_t* __restrict__ gate, const float4* __restrict__ b,
+                                                       const int32_t* __restrict__ sp0, const int32_t* __restrict__ col0,
+                                                       const float* __restrict__ val0) {
     pdl_trigger();
     constexpr int S = 32 / G;
+    const bool form_res = res == nullptr;   // uniform over the launch
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
-    HeldEntries<G == kLanesL0 ? kHeldL0 : kHeldC> he;
+    HeldEntries<G == kLanesL0 ? kHeldL0 : kHeldC> he, ha;
     hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    if (form_res) hold_ell_row<G>(ha, row, valid, lane, sp0, col0, val0);
     const bool own = valid && lane < S;
     const int4 id = own ? __ldg(pid + row) : make_int4(0, 0, 0, 0);
     const float4 w = own ? __ldg(pw + row) : f4z();
     pdl_wait();
     if (gate && __ldg(gate) == 0) return;
     const float4 q = held_sum<G>(he, lane, col, val, ec);
+    const float4 offd = form_res ? held_sum<G>(ha, lane, col0, val0, din) : f4z();
     if (!own) return;
     const float4 e0 = __ldg(ec + id.x), e1 = __ldg(ec + id.y), e2 = __ldg(ec + id.z), e3 = __ldg(ec + id.w);
     const float4 pe = make_float4(w.x * e0.x + w.y * e1.x + w.z * e2.x + w.w * e3.x,
                                   w.x * e0.y + w.y * e1.y + w.z * e2.y + w.w * e3.y,
                                   w.x * e0.z + w.y * e1.z + w.z * e2.z + w.w * e3.z, 0.f);
-    const float4 r0 = __ldg(res + row);
     const float D = __ldg(dfull + row);
+    float4 r0;
+    if (form_res) {
+        const float4 xd = __ldg(din + row), bi = __ldg(b + row);
+        r0 = make_float4(bi.x - fmaf(D, xd.x, offd.x), bi.y - fmaf(D, xd.y, offd.y), bi.z - fmaf(D, xd.z, offd.z), 0.f);
+    } else {
+        r0 = __ldg(res + row);
+    }
     const float rx = r0.x - fmaf(D, pe.x, q.x), ry = r0.y - fmaf(D, pe.y, q.y), rz = r0.z - fmaf(D, pe.z, q.z);
     float4 x = din[row];
     x.x += pe.x;

@@ -295,6 +295,37 @@ bool build_plan(std::vector<PlanBody>& bodies, const mgsb_params& p, Plan& P, st
                     }
             }
         }
+        if (l == 1) {
+            // RO = R * Off(level 0): row I = sum over its children i (weight w_Ii) of w_Ii * (row i of
+            // the level-0 off-diagonal), accumulated in FP64, columns ascending
+            ld.ro_ptr.assign(n + 1, 0);
+            std::vector<double> acc(nfin, 0.0);
+            std::vector<uint8_t> mark(nfin, 0);
+            std::vector<int32_t> touched;
+            for (int I = 0; I < n; ++I) {
+                touched.clear();
+                for (int q = ld.rptr[I]; q < ld.rptr[I + 1]; ++q) {
+                    const int i = ld.rcol[q];
+                    const double w = (double)ld.rw[q];
+                    for (int e = prev_ptr[i]; e < prev_ptr[i + 1]; ++e) {
+                        const int k = prev_col[e];
+                        if (!mark[k]) {
+                            mark[k] = 1;
+                            touched.push_back(k);
+                        }
+                        acc[k] += w * prev_val[e];
+                    }
+                }
+                std::sort(touched.begin(), touched.end());
+                for (int k : touched) {
+                    ld.ro_col.push_back(k);
+                    ld.ro_val.push_back((float)acc[k]);
+                    acc[k] = 0.0;
+                    mark[k] = 0;
+                }
+                ld.ro_ptr[I + 1] = (int32_t)ld.ro_col.size();
+            }
+        }
         ld.S = kSliceCoarse;
         build_ell(ptr, col, val, n, ld.S, ld.slice_ptr, ld.ell_col, ld.ell_val);
         ld.nnz = (int)col.size();

@@ -49,6 +49,12 @@ struct PlanLevel {
     std::vector<int32_t> op_slice_ptr, op_col;
     std::vector<float> op_val;
     int op_nnz = 0;
+    // level 1 only: RO = R * Off(level 0) as CSR over this level's rows
+    // (columns: level-0 vertices, ascending).  With it the restriction of the
+    // level-0 residual is R (b - D d) - RO d: the level-1 right-hand side comes
+    // from b, D and d without the level-0 residual being formed first.
+    std::vector<int32_t> ro_ptr, ro_col;
+    std::vector<float> ro_val;
 };
 
 struct Plan {

@@ -71,6 +71,10 @@ struct LevelDev {
     int32_t* rptr = nullptr;
     int32_t* rcol = nullptr;
     float* rw = nullptr;
+    // level 1: RO = R * Off(level 0), CSR (columns: level-0 vertices)
+    int32_t* ro_ptr = nullptr;
+    int32_t* ro_col = nullptr;
+    float* ro_val = nullptr;
 };
 
 }  // namespace
@@ -180,6 +184,7 @@ struct mgsb_solver {
     int split = 1;   // first level of the cluster kernel; levels 1..split-1 run grid-wide
     bool pdl = true;  // programmatic dependent launch between consecutive kernels
     bool fuse_prolong = true;   // prolongation + first post-sweep as one kernel (k_prolong_sweep)
+    bool fuse_res0 = false;     // level-1 restriction straight from level 0 (k_lvl_restrict_res0)
     // autotuner overrides (0 / -1 = pick by size)
     int tune_cluster = 0, tune_fuse = -1, tune_split = 0;
     // dense coarse operator (one body): levels split..L-1 as M = their V-cycle's matrix,
@@ -205,7 +210,7 @@ struct mgsb_solver {
     int ls_ntiles = 0, ls_nblk = 0, sm_count = 148;
     uint8_t* ls_tiles = nullptr;
     float* ls_scale = nullptr;
-    float4 *ls_r = nullptr, *ls_save = nullptr;
+    float4 *ls_r = nullptr, *ls_save = nullptr, *ls_dpost = nullptr;
     float4* ls_rc = nullptr;    // per-frame row constants of the sweep's features (k_ls_row_consts)
     int2* ls_win = nullptr;     // per 128-row tile: the residual rows the sweep stages in shared memory
     float *ls_part0 = nullptr, *ls_part1 = nullptr;
@@ -544,6 +549,11 @@ mgsb_status rebuild(mgsb_solver* h) {
                 TRY(dupload(h, pool, &ld.op_col, pl.op_col));
                 TRY(dupload(h, pool, &ld.op_val, pl.op_val));
             }
+            if (!pl.ro_ptr.empty() && !pl.ro_col.empty()) {
+                TRY(dupload(h, pool, &ld.ro_ptr, pl.ro_ptr));
+                TRY(dupload(h, pool, &ld.ro_col, pl.ro_col));
+                TRY(dupload(h, pool, &ld.ro_val, pl.ro_val));
+            }
             TRY(dalloc(h, pool, &ld.dfull, pl.n));
             TRY(dalloc(h, pool, &ld.dinv, pl.n));
             TRY(dalloc(h, pool, &ld.res, pl.n));
@@ -675,6 +685,7 @@ mgsb_status rebuild(mgsb_solver* h) {
         TRY(dalloc(h, pool, &h->ls_tiles, (size_t)h->ls_ntiles * kTileBytes));
         TRY(dalloc(h, pool, &h->ls_scale, (size_t)N0));
         TRY(dalloc(h, pool, &h->ls_r, (size_t)N0));
+        TRY(dalloc(h, pool, &h->ls_dpost, (size_t)N0));
         TRY(dalloc(h, pool, &h->ls_rc, (size_t)N0));
         {   // residual window per tile: the tile's rows and every column its rows' ELL entries name
             const PlanLevel& pl = P.levels[0];
@@ -862,8 +873,13 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
     for (int l = 1; l < F; ++l) {
         const LevelView& C = args.lv[l];
         const int g = grid_rows(C.n, 32 / kLanesC);
-        LAUNCH(h, k_lvl_restrict, g, kBlock, 0, C.n, C.rptr, C.rcol, C.rw, args.lv[l - 1].res,
-               args.pre > 0 ? C.dinv : nullptr, C.r, C.e, gate);
+        if (l == 1 && args.res0_b)
+            LAUNCH(h, k_lvl_restrict_res0, g, kBlock, 0, C.n, C.rptr, C.rcol, C.rw, args.ro_ptr, args.ro_col,
+                   args.ro_val, args.res0_b, args.lv[0].dfull, (const float4*)args.d, args.pre > 0 ? C.dinv : nullptr,
+                   C.r, C.e, gate);
+        else
+            LAUNCH(h, k_lvl_restrict, g, kBlock, 0, C.n, C.rptr, C.rcol, C.rw, args.lv[l - 1].res,
+                   args.pre > 0 ? C.dinv : nullptr, C.r, C.e, gate);
         float4 *a = C.e, *b = C.e2;
         for (int k = 1; k < args.pre; ++k) {
             LAUNCH(h, k_lvl_sweep, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.dinv, C.r, a, b, gate);
@@ -890,7 +906,8 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
             float4* a = ((args.post - 1) % 2 == 0) ? C.e : C.e2;
             float4* b = (a == C.e) ? C.e2 : C.e;
             LAUNCH(h, k_prolong_sweep<kLanesC>, g, kBlock, 0, C.n, Cc.pid, Cc.pw, Cc.e, C.op_slice_ptr, C.op_col,
-                   C.op_val, C.dfull, C.dinv, C.res, cur[l], a, nullptr, nullptr, gate);
+                   C.op_val, C.dfull, C.dinv, C.res, cur[l], a, nullptr, nullptr, gate, nullptr, nullptr, nullptr,
+                   nullptr);
             for (int k = 1; k < args.post; ++k) {
                 LAUNCH(h, k_lvl_sweep, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.dinv, C.r, a, b, gate);
                 std::swap(a, b);
@@ -952,11 +969,21 @@ mgsb_status launch_coarse_cluster(mgsb_solver* h, const CoarseArgs& args) {
     return MGSB_OK;
 }
 
+// Level 1's restriction forms R (b - D d) - RO d from level 0 directly
+// (k_lvl_restrict_res0) when level 1 runs grid-wide (split >= 2), the fused
+// prolongation forms the level-0 residual rows it needs, and RO exists; the
+// level-0 residual launch is then left out of the V-cycle.
+bool res0_fused(const mgsb_solver* h) {
+    return h->fuse_res0 && h->fuse_prolong && !h->fuse_l0 && h->split >= 2 && h->lev.size() > 1 &&
+           h->lev[1].ro_ptr != nullptr;
+}
+
 // Level-0 prolongation d += P e1 and the post-smoothing sweeps (ping-pong
 // xa -> xb; on return xa holds the result): the first sweep fused with the
 // prolongation (k_prolong_sweep, from the level-0 residual lv[0].res of the
 // descent) unless disabled.  b: the right-hand side of the sweeps.
-void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const int32_t* gate, int post = -1) {
+void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const int32_t* gate, int post = -1,
+                     bool form_res = false) {
     const mgsb_params& p = h->p;
     if (post < 0) post = p.post_sweeps;
     const int n0 = h->N0;
@@ -966,7 +993,8 @@ void enqueue_l0_post(mgsb_solver* h, float4*& xa, float4*& xb, float4* b, const 
     int k0 = 0;
     if (h->fuse_prolong && post > 0) {
         LAUNCH(h, k_prolong_sweep<kLanesL0>, g0, kBlock, 0, n0, l1.pid, l1.pw, l1.e, l0.op_slice_ptr, l0.op_col,
-               l0.op_val, l0.dfull, l0.dinv, l0.res, xa, xb, nullptr, nullptr, gate);
+               l0.op_val, l0.dfull, l0.dinv, form_res ? nullptr : l0.res, xa, xb, nullptr, nullptr, gate,
+               form_res ? b : nullptr, l0.slice_ptr, l0.ell_col, l0.ell_val);
         std::swap(xa, xb);
         k0 = 1;
     } else {
@@ -1005,16 +1033,23 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
                gather_b ? h->slots : nullptr, gather_b ? bw : nullptr);
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
            l0.dfull, (const float4*)h->ls_rc, (const int2*)h->ls_win, h->fixf, h->ls_r, img, d, h->ls_werr, nullptr,
-           nullptr);
-    // coarse correction
-    LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, d, b, l0.res, nullptr);
+           nullptr, nullptr);
+    // coarse correction (with res0_fused the level-0 residual is not formed: level 1's restriction
+    // takes b and d, the post-smoothing kernel forms its rows into ls_dpost's sweep)
+    const bool fr = res0_fused(h);
+    if (!fr)
+        LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, d, b, l0.res,
+               nullptr);
     ca.d = d;
     ca.gate = nullptr;
+    ca.res0_b = fr ? b : nullptr;
     launch_coarse(h, ca);
     // post-smoothing: d += P e1 and the residual the learned sweep starts from
+    float4* dpost = fr ? h->ls_dpost : d;
     if (h->fuse_prolong) {
         LAUNCH(h, k_prolong_sweep<kLanesL0>, g0, kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, l0.op_slice_ptr,
-               l0.op_col, l0.op_val, l0.dfull, l0.dinv, l0.res, d, d, h->fixf, h->ls_r, nullptr);
+               l0.op_col, l0.op_val, l0.dfull, l0.dinv, fr ? nullptr : l0.res, d, dpost, h->fixf, h->ls_r, nullptr,
+               fr ? b : nullptr, l0.slice_ptr, l0.ell_col, l0.ell_val);
     } else {
         LAUNCH(h, k_l0_prolong, grid_for(n0), kBlock, 0, n0, lv[1].pid, lv[1].pw, lv[1].e, d, nullptr);
         LAUNCH(h, k_ls_residual, g0, kLsThreads, 0, n0, l0.slice_ptr, l0.ell_col, l0.ell_val, l0.dfull, h->fixf, d, b,
@@ -1022,7 +1057,8 @@ void enqueue_learned_vcycle(mgsb_solver* h, float4* d, const float4* b, bool fro
     }
     // with dd64 (mixed kind, check taken by the next outer residual) the sweep also applies d to dd64
     LAUNCH(h, k_ls_sweep_tc, mgrid, kMlpThreads, msmem, n0, h->ls_ntiles, l0.slice_ptr, l0.ell_col, l0.ell_val,
-           l0.dfull, (const float4*)h->ls_rc, (const int2*)h->ls_win, h->fixf, h->ls_r, img, d, h->ls_werr, dd64, d32);
+           l0.dfull, (const float4*)h->ls_rc, (const int2*)h->ls_win, h->fixf, h->ls_r, img, d, h->ls_werr, dd64, d32,
+           dpost != d ? (const float4*)dpost : nullptr);
 }
 
 // The learned sweep's per-frame row constants, once the frame's level-0
@@ -1250,6 +1286,12 @@ void fill_coarse_args(mgsb_solver* h, CoarseArgs& ca) {
     ca.dense_off = h->dense_off_d;
     ca.Ainv = h->Lfac;
     ca.Ainv64 = nullptr;
+    ca.res0_b = nullptr;
+    if (L > 1) {
+        ca.ro_ptr = h->lev[1].ro_ptr;
+        ca.ro_col = h->lev[1].ro_col;
+        ca.ro_val = h->lev[1].ro_val;
+    }
     ca.b = h->b;
     for (int l = 0; l < L; ++l) {
         LevelView& v = ca.lv[l];
@@ -1322,13 +1364,15 @@ float4* enqueue_mg_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
                 std::swap(xa, xb);
             }
             if (!gathered) LAUNCH(h, k_gather_rhs, grid_for(n0), kBlock, 0, n0, h->b, h->b0, h->slot_ptr, h->slots);
-            if (!h->fuse_l0)
+            const bool fr = res0_fused(h);
+            if (!h->fuse_l0 && !fr)
                 LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
                        lv[0].dfull, xa, h->b, lv[0].res, nullptr);
             ca.d = xa;
+            ca.res0_b = fr ? h->b : nullptr;
             launch_coarse(h, ca);
             if (!h->fuse_l0) {   // the shared-memory kernel leaves the level-1 correction in lv[1].e
-                enqueue_l0_post(h, xa, xb, h->b, nullptr, l0_post);
+                enqueue_l0_post(h, xa, xb, h->b, nullptr, l0_post, fr);
             } else {
                 for (int k = 0; k < l0_post; ++k) {
                     LAUNCH(h, k_l0_sweep_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
@@ -1432,10 +1476,14 @@ void enqueue_mixed_solve(mgsb_solver* h, bool learned, const LearnedFallback& fb
                        lv[0].dinv, ea, eb, h->r32, h->b0, h->slot_ptr, h->slots, 0, nullptr);
                 std::swap(ea, eb);
             }
-            LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val, lv[0].dfull,
-                   ea, h->r32, lv[0].res, nullptr);
+            const bool fr = res0_fused(h);
+            if (!fr)
+                LAUNCH(h, k_l0_residual_rg, g0, kBlock, 0, n0, lv[0].slice_ptr, lv[0].ell_col, lv[0].ell_val,
+                       lv[0].dfull, ea, h->r32, lv[0].res, nullptr);
+            ca.d = ea;
+            ca.res0_b = fr ? h->r32 : nullptr;
             launch_coarse(h, ca);
-            enqueue_l0_post(h, ea, eb, h->r32, nullptr, l0_post);
+            enqueue_l0_post(h, ea, eb, h->r32, nullptr, l0_post, fr);
             LAUNCH(h, k_mx_update, grid_for(n0), kBlock, 0, n0, ea, h->dd64, h->d32);
         }
     }
@@ -2287,6 +2335,13 @@ mgsb_status mgsb_set_broad_phase(mgsb_solver* h, int32_t on) {
 mgsb_status mgsb_set_fused_prolongation(mgsb_solver* h, int32_t on) {
     if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
     h->fuse_prolong = on != 0;
+    invalidate_graph(h);
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_set_fused_restriction(mgsb_solver* h, int32_t on) {
+    if (!h || (on != 0 && on != 1)) return MGSB_INVALID_ARG;
+    h->fuse_res0 = on != 0;
     invalidate_graph(h);
     return MGSB_OK;
 }

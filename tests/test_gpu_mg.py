@@ -425,6 +425,51 @@ def test_fused_prolongation_same_vcycle(lib, oracle_built, precision, split):
     assert np.abs(runs[True][0] - o.positions()).max() < 1e-5 * diag
 
 
+@pytest.mark.parametrize("precision,split,learned", [(mg.PRECISION_FP32, 2, False), (mg.PRECISION_MIXED, 3, False),
+                                                      (mg.PRECISION_MIXED, 2, True), (mg.PRECISION_FP32, 3, True)])
+def test_fused_restriction_same_vcycle(lib, oracle_built, precision, split, learned):
+    """Level 1's restriction straight from level 0 (R (b - D d) - RO d, RO = R Off0) and the
+    level-0 residual rows formed by the fused prolongation are the same V-cycle: frames agree with
+    the separate residual launch to rounding, contact sets are equal, one launch per V-cycle less,
+    and the frames match the oracle (plain cycles)."""
+    import os
+    from multigridsoftbody_b200.learned import MLP
+    m, fixed = beam(8, 80, 8)
+    p = mg_params(levels=4, gravity=(0, 0, 0), precision=precision, refinement_passes=2)
+    path = capsule_path(20, start=(0.0, 0.0, 1.3))
+    net = None
+    if learned:
+        net = MLP(device=0, seed=0)
+        net.params = np.load(os.path.join(os.path.dirname(__file__), "golden", "beam_smoother.npy"))
+    runs, launches = {}, {}
+    for fused in (True, False):
+        s = mg.Solver(m, p)
+        s.set_fixed(fixed)
+        if net is not None:
+            s.set_learned_smoother(net, 0.5)
+        s.set_coarse_split(split)
+        s.set_fused_restriction(fused)
+        for a, b in path:
+            s.set_capsule(a, b, 0.3)
+            s.step()
+        runs[fused] = (s.positions_f64() if precision == mg.PRECISION_MIXED else s.positions().astype(np.float64),
+                       np.nonzero(s.contact_flags())[0])
+        launches[fused] = s.launches_per_frame()
+        s.close()
+    diag = m.bbox_diagonal()
+    assert np.abs(runs[True][0] - runs[False][0]).max() < 1e-6 * diag
+    assert np.array_equal(runs[True][1], runs[False][1])
+    # one launch per V-cycle (the count covers the frame's main solve)
+    assert launches[False] - launches[True] == p.iterations * p.refinement_passes, launches
+    if not learned:
+        o = Oracle(m, p)
+        o.set_fixed(fixed)
+        for a, b in path:
+            o.set_capsule(a, b, 0.3)
+            o.step()
+        assert np.abs(runs[True][0] - o.positions()).max() < 1e-5 * diag
+
+
 @pytest.mark.parametrize("precision", [mg.PRECISION_FP32, mg.PRECISION_MIXED])
 def test_time_kernel_replays_without_changing_the_run(lib, precision):
     """Replay timing of every kernel of the frame: a positive time per launch,
