@@ -180,6 +180,11 @@ mgsb_status mgsb_get_contact_flags(mgsb_solver* h, int32_t body, int32_t* out /*
 /* Contact flags of every body, concatenated in body order (one copy).  No
  * reference counterpart (the reference simulates one body). */
 mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out /* [sum V] */);
+/* The frame's result in one readback: positions (as mgsb_get_all_positions)
+ * and contact flags (as mgsb_get_all_contact_flags) of every body, copied
+ * with one stream synchronisation instead of two.  MGSB_DIVERGED as the
+ * single readbacks.  No reference counterpart. */
+mgsb_status mgsb_get_frame(mgsb_solver* h, float* positions /* [3 sum V] */, int32_t* contact_flags /* [sum V] */);
 /* Contact vertex indices, ascending.  *n receives the count; if cap < count
  * only cap entries are written and MGSB_INVALID_ARG is returned. */
 mgsb_status mgsb_get_contacts(mgsb_solver* h, int32_t body, int32_t* idx, size_t cap, size_t* n);

@@ -305,6 +305,23 @@ class Solver:
         _check(self._lib.mgsb_get_all_contact_flags(self.h, _iptr(out)), self.h)
         return out
 
+    def frame(self, positions: np.ndarray = None, contact_flags: np.ndarray = None):
+        """Positions [sum V, 3] and contact flags [sum V] of every body in one readback (mgsb_get_frame);
+        pass preallocated arrays to reuse them across frames."""
+        n = getattr(self, "_nv_total", None)
+        if n is None:
+            n = self._nv_total = sum(self.num_verts(b) for b in range(self.num_bodies))
+        if positions is None:
+            positions = np.empty((n, 3), np.float32)
+        if contact_flags is None:
+            contact_flags = np.empty(n, np.int32)
+        if positions.shape != (n, 3) or positions.dtype != np.float32 or not positions.flags.c_contiguous:
+            raise ValueError("positions must be a C-contiguous float32 array of shape (%d, 3)" % n)
+        if contact_flags.shape != (n,) or contact_flags.dtype != np.int32 or not contact_flags.flags.c_contiguous:
+            raise ValueError("contact_flags must be a C-contiguous int32 array of shape (%d,)" % n)
+        _check(self._lib.mgsb_get_frame(self.h, _fptr(positions), _iptr(contact_flags)), self.h)
+        return positions, contact_flags
+
     def set_learned_smoother(self, net, guard_ratio: float = 0.5) -> None:
         """Attach a trained learned.MLP (None detaches); see mgsb_set_learned_smoother."""
         self._net = net   # keep the network alive while attached

@@ -1540,53 +1540,60 @@ __global__ void __launch_bounds__(256) k_op_round(int count, const double* __res
 }
 
 // e_F = M r_F, r_F the restriction of the level-(F-1) residual (children of
-// each level-F row, CSR).  One row of M per warp.  Before the dependency wait
-// (while the previous kernel runs) every thread loads the static restriction
-// structure of its rows: kApplyG lanes per restricted row, kApplyK children
-// per lane, kApplyPasses rows per thread; longer rows and later rows take a
-// tail loop.  After the wait the CTA stages the whole level-(F-1) residual in
-// shared memory (coalesced) while each warp fetches its row of M, forms all of
-// r_F from shared memory, then its row of e_F.
+// each level-F row, CSR).  One row of M per warp; CTAs in clusters of
+// kApplyCluster.  The CTAs of a cluster split r_F: rank k forms rows
+// [k c, (k+1) c), c = ceil(n_F / kApplyCluster), kApplyG lanes per row, its
+// children and weights held in registers before the dependency wait and the
+// children's residual rows read straight from global memory after it; after a
+// cluster barrier every CTA gathers all of r_F from the cluster's shared
+// memory (distributed shared memory), and a second barrier keeps every share
+// alive until all reads are done.  Each warp fetches its row of M while the
+// restriction runs.
 constexpr int kApplyG = 4;         // lanes per restricted row
-constexpr int kApplyK = 4;         // children per lane held in registers
-constexpr int kApplyPasses = 4;    // restricted rows per thread held in registers (512 rows)
+constexpr int kApplyK = 4;         // children per lane held in registers (16 per row; longer rows: tail loop)
 constexpr int kApplyMRegs = 16;    // entries of the warp's row of M per lane held in registers
-constexpr int kApplyStage = 8;     // residual rows per thread loaded at once when staging (4,096 per pass)
+constexpr int kApplyCluster = 8;   // CTAs per cluster (portable size)
+static_assert(kDenseOpMaxRows <= kApplyCluster * (kDenseApplyThreads / kApplyG),
+              "a CTA restricts at most one row per lane group");
 
-__host__ __device__ constexpr size_t coarse_apply_smem_bytes(int nf, int nfine) {
-    return (size_t)(nf + nfine) * sizeof(float4);
+__host__ __device__ constexpr int coarse_apply_chunk(int nf) { return (nf + kApplyCluster - 1) / kApplyCluster; }
+__host__ __device__ constexpr size_t coarse_apply_smem_bytes(int nf) {
+    return (size_t)(nf + coarse_apply_chunk(nf)) * sizeof(float4);
+}
+// CTAs of one launch: one per kDenseApplyRows rows of M, rounded up to whole clusters
+__host__ __device__ constexpr int coarse_apply_ctas(int nf) {
+    return ((nf + kDenseApplyRows - 1) / kDenseApplyRows + kApplyCluster - 1) / kApplyCluster * kApplyCluster;
 }
 
-__global__ void __launch_bounds__(kDenseApplyThreads, 1) k_coarse_apply(int nf, int nfine, const int32_t* __restrict__ rptr,
-                                                                    const int32_t* __restrict__ rcol,
-                                                                    const float* __restrict__ rw,
-                                                                    const float4* __restrict__ res_fine,
-                                                                    const float* __restrict__ M, float4* __restrict__ e,
-                                                                    const int32_t* __restrict__ gate) {
+__global__ void __launch_bounds__(kDenseApplyThreads, 1) k_coarse_apply(int nf, const int32_t* __restrict__ rptr,
+                                                                       const int32_t* __restrict__ rcol,
+                                                                       const float* __restrict__ rw,
+                                                                       const float4* __restrict__ res_fine,
+                                                                       const float* __restrict__ M,
+                                                                       float4* __restrict__ e,
+                                                                       const int32_t* __restrict__ gate) {
     pdl_trigger();
+    cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ float4 apply_smem[];
-    float4* rs = apply_smem;          // r_F, nf rows
-    float4* resf = apply_smem + nf;   // the level-(F-1) residual, nfine rows
-    constexpr int RPP = kDenseApplyThreads / kApplyG;   // restricted rows per pass
+    const int chunk = coarse_apply_chunk(nf);
+    float4* rs = apply_smem;          // r_F, nf rows (gathered)
+    float4* mine = apply_smem + nf;   // this CTA's share of r_F, chunk rows
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int sub = tid % kApplyG, rloc = tid / kApplyG;
+    const int row = (int)cluster.block_rank() * chunk + rloc;
+    const bool valid = rloc < chunk && row < nf;
     // static structure (written once at set-up): safe before the wait
-    int beg[kApplyPasses], end[kApplyPasses], cc[kApplyPasses][kApplyK];
-    float cw[kApplyPasses][kApplyK];
+    const int beg = valid ? __ldg(rptr + row) : 0, end = valid ? __ldg(rptr + row + 1) : 0;
+    int cc[kApplyK];
+    float cw[kApplyK];
 #pragma unroll
-    for (int p = 0; p < kApplyPasses; ++p) {
-        const int row = p * RPP + rloc;
-        beg[p] = row < nf ? __ldg(rptr + row) : 0;
-        end[p] = row < nf ? __ldg(rptr + row + 1) : 0;
-#pragma unroll
-        for (int k = 0; k < kApplyK; ++k) {
-            const int q = beg[p] + sub + k * kApplyG;
-            cc[p][k] = q < end[p] ? __ldg(rcol + q) : 0;
-            cw[p][k] = q < end[p] ? __ldg(rw + q) : 0.f;
-        }
+    for (int k = 0; k < kApplyK; ++k) {
+        const int q = beg + sub + k * kApplyG;
+        cc[k] = q < end ? __ldg(rcol + q) : -1;
+        cw[k] = q < end ? __ldg(rw + q) : 0.f;
     }
     pdl_wait();
-    if (gate && __ldg(gate) == 0) return;
+    if (gate && __ldg(gate) == 0) return;   // uniform over the launch: every CTA of the cluster leaves
     const int i = blockIdx.x * kDenseApplyRows + warp;   // this warp's row of M
     float mr[kApplyMRegs];
 #pragma unroll
@@ -1594,53 +1601,25 @@ __global__ void __launch_bounds__(kDenseApplyThreads, 1) k_coarse_apply(int nf, 
         const int k = lane + 32 * j;
         mr[j] = (i < nf && k < nf) ? __ldg(M + (size_t)i * nf + k) : 0.f;
     }
-    // the level-(F-1) residual: every load of a thread in flight at once, then the stores
-    for (int base = 0; base < nfine; base += kDenseApplyThreads * kApplyStage) {
-        float4 v[kApplyStage];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int u = 0; u < kApplyStage; ++u) {
-            const int r = base + u * kDenseApplyThreads + tid;
-            v[u] = r < nfine ? res_fine[r] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+    for (int k = 0; k < kApplyK; ++k)
+        if (cc[k] >= 0) acc = f4fma(cw[k], __ldg(res_fine + cc[k]), acc);
+    for (int q = beg + sub + kApplyK * kApplyG; q < end; q += kApplyG)
+        acc = f4fma(__ldg(rw + q), __ldg(res_fine + __ldg(rcol + q)), acc);
 #pragma unroll
-        for (int u = 0; u < kApplyStage; ++u) {
-            const int r = base + u * kDenseApplyThreads + tid;
-            if (r < nfine) resf[r] = v[u];
-        }
+    for (int o = 1; o < kApplyG; o <<= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
     }
-    __syncthreads();
-    auto group_sum = [&](float4 a) {
-#pragma unroll
-        for (int o = 1; o < kApplyG; o <<= 1) {
-            a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
-            a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
-            a.z += __shfl_xor_sync(0xffffffffu, a.z, o);
-        }
-        return a;
-    };
-#pragma unroll
-    for (int p = 0; p < kApplyPasses; ++p) {
-        const int row = p * RPP + rloc;
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int k = 0; k < kApplyK; ++k) acc = f4fma(cw[p][k], resf[cc[p][k]], acc);
-        for (int q = beg[p] + sub + kApplyK * kApplyG; q < end[p]; q += kApplyG)
-            acc = f4fma(__ldg(rw + q), resf[__ldg(rcol + q)], acc);
-        acc = group_sum(acc);
-        if (sub == 0 && row < nf) rs[row] = acc;
+    if (sub == 0 && valid) mine[rloc] = acc;
+    cluster.sync();   // every share written and visible to the cluster
+    for (int r = tid; r < nf; r += kDenseApplyThreads) {
+        const int owner = r / chunk;
+        rs[r] = *cluster.map_shared_rank(mine + (r - owner * chunk), owner);
     }
-    for (int base = kApplyPasses * RPP; base < nf; base += RPP) {   // rows past the register passes
-        const int row = base + rloc;
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row < nf) {
-            const int q1 = __ldg(rptr + row + 1);
-            for (int q = __ldg(rptr + row) + sub; q < q1; q += kApplyG)
-                acc = f4fma(__ldg(rw + q), resf[__ldg(rcol + q)], acc);
-        }
-        acc = group_sum(acc);
-        if (sub == 0 && row < nf) rs[row] = acc;
-    }
-    __syncthreads();
+    cluster.sync();   // r_F complete here; no share is read after this point
     if (i >= nf) return;   // warp-uniform
     float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll

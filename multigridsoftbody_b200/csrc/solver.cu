@@ -318,11 +318,11 @@ size_t coarse_smem_bytes(const mgsb_solver* h, int cs, int split);
 constexpr int kClusterLevelRows = 1024;
 
 // The dense coarse operator can start at level `split`: one body, at most
-// dop_cap rows there, and the apply kernel's shared memory (the rows of levels
-// split and split - 1) within the device's limit.
+// dop_cap rows there, and the apply kernel's shared memory (the split level's
+// rows and this CTA's share of them) within the device's limit.
 bool dense_eligible(const mgsb_solver* h, int split) {
     return h->bodies.size() == 1 && split >= 1 && h->dop_work != nullptr && h->maxv[split] <= h->dop_cap &&
-           coarse_apply_smem_bytes(h->maxv[split], h->maxv[split - 1]) <= (size_t)h->max_smem_optin;
+           coarse_apply_smem_bytes(h->maxv[split]) <= (size_t)h->max_smem_optin;
 }
 
 void apply_tuning(mgsb_solver* h) {
@@ -888,12 +888,33 @@ mgsb_status launch_coarse(mgsb_solver* h, const CoarseArgs& args_in) {
         LAUNCH(h, k_lvl_residual, g, kBlock, 0, C.n, C.slice_ptr, C.col, C.val, C.dfull, C.r, a, C.res, gate);
         cur[l] = a;
     }
-    if (h->dense_op) {   // levels F..L-1: the restriction to level F (grid-wide), then the dense operator
+    if (h->dense_op) {   // levels F..L-1: the restriction to level F and the dense operator, one launch
         const LevelView& C = args.lv[F];
-        const int nfine = args.lv[F - 1].n;
-        LAUNCH(h, k_coarse_apply, (C.n + kDenseApplyRows - 1) / kDenseApplyRows, kDenseApplyThreads,
-               coarse_apply_smem_bytes(C.n, nfine), C.n, nfine, C.rptr, C.rcol, C.rw,
-               (const float4*)args.lv[F - 1].res, (const float*)h->dop_result, C.e, gate);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)coarse_apply_ctas(C.n));
+        cfg.blockDim = dim3((unsigned)kDenseApplyThreads);
+        cfg.dynamicSmemBytes = coarse_apply_smem_bytes(C.n);
+        cfg.stream = h->stream;
+        cudaLaunchAttribute attr[2];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)kApplyCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = h->pdl ? 2 : 1;
+        const int reps = prof_begin(h, "k_coarse_apply");
+        cudaError_t e = cudaSuccess;
+        for (int r = 0; r < reps && e == cudaSuccess; ++r)
+            e = cudaLaunchKernelEx(&cfg, k_coarse_apply, C.n, (const int32_t*)C.rptr, (const int32_t*)C.rcol,
+                                   (const float*)C.rw, (const float4*)args.lv[F - 1].res,
+                                   (const float*)h->dop_result, C.e, gate);
+        prof_end(h, "k_coarse_apply");
+        ++h->launches;
+        if (e != cudaSuccess)
+            return h->enqueue_status = set_err(h, MGSB_CUDA_ERROR, "dense coarse apply launch failed: %s",
+                                               cudaGetErrorString(e));
     } else {
         TRY(launch_coarse_cluster(h, args));
     }
@@ -1680,7 +1701,9 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     auto& pool = h->state_mem;
     const int N0 = h->N0;
     // N0 float4 + the non-finite flag that every readback fetches with its data
-    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback, (size_t)std::max(N0, 1) * sizeof(float4) + 16));
+    // pinned readback: N0 float4 rows, the non-finite flag (16 B), N0 contact flags (mgsb_get_frame)
+    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback,
+                                (size_t)std::max(N0, 1) * (sizeof(float4) + sizeof(int32_t)) + 16));
     TRY(dalloc(hp, pool, &h->x, N0));
     TRY(dalloc(hp, pool, &h->xb, N0));
     TRY(dalloc(hp, pool, &h->v, N0));
@@ -2025,6 +2048,23 @@ mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out) {
     return MGSB_OK;
 }
 
+mgsb_status mgsb_get_frame(mgsb_solver* h, float* positions, int32_t* contact_flags) {
+    if (!h || !positions || !contact_flags) return MGSB_INVALID_ARG;
+    const size_t n = (size_t)h->N0;
+    int32_t* flags = reinterpret_cast<int32_t*>(h->readback + std::max(n, (size_t)1) * sizeof(float4) + 16);
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    if (n) CUDA_TRY(h, cudaMemcpyAsync(flags, h->cflag, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    TRY(readback_checked(h, h->x, n * sizeof(float4)));   // the same stream: one synchronisation for all
+    const float4* tmp = reinterpret_cast<const float4*>(h->readback);
+    for (size_t i = 0; i < n; ++i) {
+        positions[3 * i] = tmp[i].x;
+        positions[3 * i + 1] = tmp[i].y;
+        positions[3 * i + 2] = tmp[i].z;
+    }
+    std::memcpy(contact_flags, flags, n * sizeof(int32_t));
+    return MGSB_OK;
+}
+
 mgsb_status mgsb_get_contacts(mgsb_solver* h, int32_t body, int32_t* idx, size_t cap, size_t* n) {
     if (!n) return MGSB_INVALID_ARG;
     TRY(check_body(h, body));
@@ -2360,7 +2400,7 @@ mgsb_status mgsb_set_coarse_dense(mgsb_solver* h, int32_t on) {
     if (on && (h->fuse_l0 || !dense_eligible(h, h->split)))
         return set_err(h, MGSB_NOT_SUPPORTED,
                        "the dense coarse operator needs one body, at most %d rows on the coarse split's level "
-                       "(split %d has %d) and the rows of that level and the one above in shared memory",
+                       "(split %d has %d) and that level's rows in shared memory",
                        kDenseOpMaxRows, h->split, h->maxv[h->split]);
     h->tune_dense = on;
     apply_tuning(h);

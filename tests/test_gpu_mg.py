@@ -512,3 +512,29 @@ def test_time_kernel_replays_without_changing_the_run(lib, precision):
         s.close()
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
+
+
+def test_frame_readback_equals_the_single_readbacks(lib):
+    """mgsb_get_frame (positions + contact flags, one synchronisation) returns what the two single
+    readbacks return, for a batch of bodies, into caller-owned arrays."""
+    meshes, fixeds = [], []
+    for n in (2, 3):
+        m, fx = beam(n, 10 * n, n, half_len=2.5 * n)
+        meshes.append(m)
+        fixeds.append(fx)
+    p = mg_params(levels=3, gravity=(0, 0, 0))
+    s = mg.Solver(meshes, [p, p])
+    for b, fx in enumerate(fixeds):
+        s.set_fixed(fx, body=b)
+    for a, b in capsule_path(12, start=(0.0, 0.0, 1.2)):
+        s.set_capsules(np.stack([a, a]), np.stack([b, b]), np.array([0.3, 0.3], np.float32))
+        s.step()
+    nv = sum(m.num_verts for m in meshes)
+    pos, flags = np.zeros((nv, 3), np.float32), np.zeros(nv, np.int32)
+    out = s.frame(pos, flags)
+    assert out[0] is pos and out[1] is flags
+    assert np.array_equal(pos, s.all_positions())
+    assert np.array_equal(flags, s.all_contact_flags()) and flags.sum() > 0
+    with pytest.raises(ValueError):
+        s.frame(np.zeros((nv, 3), np.float64), flags)
+    s.close()
