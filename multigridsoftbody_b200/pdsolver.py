@@ -119,8 +119,9 @@ class PDSolver:
 
     # runCpyTetVertForRender (PDSolver.cu:261-268)
     def RenderOnce(self) -> None:
-        self.m_tetVertPos = self._solver.positions().reshape(-1)
-        self.m_tetVertIsCollide = self._solver.contact_flags()
+        pos, flags = self._solver.frame()   # positions and contact flags in one readback
+        self.m_tetVertPos = pos.reshape(-1)
+        self.m_tetVertIsCollide = flags
         self.m_tetVertCollisionDepth = self._solver.collision_depth()
 
     @property
