@@ -185,6 +185,13 @@ mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out /* [sum V] *
  * with one stream synchronisation instead of two.  MGSB_DIVERGED as the
  * single readbacks.  No reference counterpart. */
 mgsb_status mgsb_get_frame(mgsb_solver* h, float* positions /* [3 sum V] */, int32_t* contact_flags /* [sum V] */);
+/* The same without a host copy: the positions are packed to xyz on the device
+ * and copied with the contact flags into the solver's pinned readback buffer
+ * (one synchronisation); *positions [3 sum V] and *contact_flags [sum V] point
+ * into that buffer and stay valid until the next readback call on this solver
+ * (any mgsb_get_* that returns host data) or mgsb_destroy.  No reference
+ * counterpart. */
+mgsb_status mgsb_get_frame_view(mgsb_solver* h, const float** positions, const int32_t** contact_flags);
 /* Contact vertex indices, ascending.  *n receives the count; if cap < count
  * only cap entries are written and MGSB_INVALID_ARG is returned. */
 mgsb_status mgsb_get_contacts(mgsb_solver* h, int32_t body, int32_t* idx, size_t cap, size_t* n);

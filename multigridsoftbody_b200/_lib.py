@@ -154,6 +154,7 @@ SIGNATURES = [
     ("mgsb_set_fused_prolongation", C.c_int, [_P, C.c_int32]),
     ("mgsb_set_fused_restriction", C.c_int, [_P, C.c_int32]),
     ("mgsb_get_frame", C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
+    ("mgsb_get_frame_view", C.c_int, [_P, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.POINTER(C.c_int32))]),
     ("mgsb_set_surface_contact", C.c_int, [_P, C.c_int32]),
     ("mgsb_set_coarse_dense", C.c_int, [_P, C.c_int32]),
     ("mgsb_get_coarse_dense", C.c_int, [_P, _IP]),

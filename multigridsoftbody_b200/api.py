@@ -322,6 +322,19 @@ class Solver:
         _check(self._lib.mgsb_get_frame(self.h, _fptr(positions), _iptr(contact_flags)), self.h)
         return positions, contact_flags
 
+    def frame_view(self):
+        """Positions [sum V, 3] and contact flags [sum V] as numpy views of the solver's pinned readback
+        buffer (mgsb_get_frame_view): no host copy.  The views stay valid until the next readback call
+        on this solver; copy them to keep a frame."""
+        n = getattr(self, "_nv_total", None)
+        if n is None:
+            n = self._nv_total = sum(self.num_verts(b) for b in range(self.num_bodies))
+        pp, fp = C.POINTER(C.c_float)(), C.POINTER(C.c_int32)()
+        _check(self._lib.mgsb_get_frame_view(self.h, C.byref(pp), C.byref(fp)), self.h)
+        if n == 0:
+            return np.zeros((0, 3), np.float32), np.zeros(0, np.int32)
+        return np.ctypeslib.as_array(pp, shape=(n, 3)), np.ctypeslib.as_array(fp, shape=(n,))
+
     def set_learned_smoother(self, net, guard_ratio: float = 0.5) -> None:
         """Attach a trained learned.MLP (None detaches); see mgsb_set_learned_smoother."""
         self._net = net   # keep the network alive while attached

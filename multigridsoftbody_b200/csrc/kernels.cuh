@@ -503,6 +503,17 @@ __global__ void k_l0_frame(int n, const float4* __restrict__ s, const float* __r
     d[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// Positions as packed xyz (3 floats per vertex) for the zero-copy frame
+// readback; launched on its own after a frame, outside the frame's graph.
+__global__ void k_pack_xyz(int n, const float4* __restrict__ x, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = x[i];
+    out[3 * i] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+}
+
 // End of frame: x = s + d, v = v_predicted + d/dt (= (x - x_prev)/dt), and a
 // finiteness check of the new positions.
 __global__ void k_mg_finish(int n, const float4* __restrict__ s, const float4* __restrict__ d, float4* __restrict__ x,

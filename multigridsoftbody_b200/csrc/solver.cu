@@ -116,6 +116,7 @@ struct mgsb_solver {
     int stage_idx = 0;
     // pinned host buffer for readbacks (N0 x 16 bytes: positions, velocities, flags)
     char* readback = nullptr;
+    float* xpack = nullptr;   // positions as packed xyz (mgsb_get_frame_view)
     // ---- state (kept across rebuilds)
     float4 *x = nullptr, *xb = nullptr, *v = nullptr, *s = nullptr, *last = nullptr, *prev = nullptr;
     int32_t* cflag = nullptr;
@@ -1700,11 +1701,13 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     }
     auto& pool = h->state_mem;
     const int N0 = h->N0;
-    // N0 float4 + the non-finite flag that every readback fetches with its data
-    // pinned readback: N0 float4 rows, the non-finite flag (16 B), N0 contact flags (mgsb_get_frame)
+    // pinned readback: N0 float4 rows (or, for mgsb_get_frame_view, N0 packed xyz + N0 contact
+    // flags), the non-finite flag that every readback fetches with its data (at N0 x 16 B), then
+    // N0 contact flags (mgsb_get_frame)
     CUDA_TRY(hp, cudaMallocHost((void**)&h->readback,
                                 (size_t)std::max(N0, 1) * (sizeof(float4) + sizeof(int32_t)) + 16));
     TRY(dalloc(hp, pool, &h->x, N0));
+    TRY(dalloc(hp, pool, &h->xpack, (size_t)3 * std::max(N0, 1)));
     TRY(dalloc(hp, pool, &h->xb, N0));
     TRY(dalloc(hp, pool, &h->v, N0));
     TRY(dalloc(hp, pool, &h->s, N0));
@@ -2062,6 +2065,24 @@ mgsb_status mgsb_get_frame(mgsb_solver* h, float* positions, int32_t* contact_fl
         positions[3 * i + 2] = tmp[i].z;
     }
     std::memcpy(contact_flags, flags, n * sizeof(int32_t));
+    return MGSB_OK;
+}
+
+mgsb_status mgsb_get_frame_view(mgsb_solver* h, const float** positions, const int32_t** contact_flags) {
+    if (!h || !positions || !contact_flags) return MGSB_INVALID_ARG;
+    const size_t n = (size_t)h->N0;
+    float* pos = reinterpret_cast<float*>(h->readback);                           // [0, 12 N)
+    int32_t* flags = reinterpret_cast<int32_t*>(h->readback + n * 3 * sizeof(float));   // [12 N, 16 N)
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    if (n) {
+        k_pack_xyz<<<grid_for((int)n), kBlock, 0, h->stream>>>((int)n, h->x, h->xpack);
+        CUDA_TRY(h, cudaGetLastError());
+        CUDA_TRY(h, cudaMemcpyAsync(pos, h->xpack, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(flags, h->cflag, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    }
+    TRY(readback_checked(h, nullptr, 0));   // the non-finite flag (at 16 N) and one synchronisation
+    *positions = pos;
+    *contact_flags = flags;
     return MGSB_OK;
 }
 

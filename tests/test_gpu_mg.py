@@ -537,4 +537,8 @@ def test_frame_readback_equals_the_single_readbacks(lib):
     assert np.array_equal(flags, s.all_contact_flags()) and flags.sum() > 0
     with pytest.raises(ValueError):
         s.frame(np.zeros((nv, 3), np.float64), flags)
+    # zero-copy: views of the pinned readback buffer, the same values
+    pv, fv = s.frame_view()
+    assert pv.shape == (nv, 3) and fv.shape == (nv,)
+    assert np.array_equal(pv, pos) and np.array_equal(fv, flags)
     s.close()
