@@ -1702,10 +1702,8 @@ mgsb_status create_impl(int32_t nbodies, const mgsb_mesh* meshes, const mgsb_par
     auto& pool = h->state_mem;
     const int N0 = h->N0;
     // pinned readback: N0 float4 rows (or, for mgsb_get_frame_view, N0 packed xyz + N0 contact
-    // flags), the non-finite flag that every readback fetches with its data (at N0 x 16 B), then
-    // N0 contact flags (mgsb_get_frame)
-    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback,
-                                (size_t)std::max(N0, 1) * (sizeof(float4) + sizeof(int32_t)) + 16));
+    // flags), then the non-finite flag that every readback fetches with its data (at N0 x 16 B)
+    CUDA_TRY(hp, cudaMallocHost((void**)&h->readback, (size_t)std::max(N0, 1) * sizeof(float4) + 16));
     TRY(dalloc(hp, pool, &h->x, N0));
     TRY(dalloc(hp, pool, &h->xpack, (size_t)3 * std::max(N0, 1)));
     TRY(dalloc(hp, pool, &h->xb, N0));
@@ -2053,17 +2051,11 @@ mgsb_status mgsb_get_all_contact_flags(mgsb_solver* h, int32_t* out) {
 
 mgsb_status mgsb_get_frame(mgsb_solver* h, float* positions, int32_t* contact_flags) {
     if (!h || !positions || !contact_flags) return MGSB_INVALID_ARG;
+    const float* pos = nullptr;
+    const int32_t* flags = nullptr;
+    TRY(mgsb_get_frame_view(h, &pos, &flags));
     const size_t n = (size_t)h->N0;
-    int32_t* flags = reinterpret_cast<int32_t*>(h->readback + std::max(n, (size_t)1) * sizeof(float4) + 16);
-    CUDA_TRY(h, cudaSetDevice(h->device));
-    if (n) CUDA_TRY(h, cudaMemcpyAsync(flags, h->cflag, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-    TRY(readback_checked(h, h->x, n * sizeof(float4)));   // the same stream: one synchronisation for all
-    const float4* tmp = reinterpret_cast<const float4*>(h->readback);
-    for (size_t i = 0; i < n; ++i) {
-        positions[3 * i] = tmp[i].x;
-        positions[3 * i + 1] = tmp[i].y;
-        positions[3 * i + 2] = tmp[i].z;
-    }
+    std::memcpy(positions, pos, n * 3 * sizeof(float));
     std::memcpy(contact_flags, flags, n * sizeof(int32_t));
     return MGSB_OK;
 }
