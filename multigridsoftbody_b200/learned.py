@@ -131,14 +131,15 @@ def train_smoother(x, t, steps: int = 20000, batch: int = 4096, lr: float = 2e-3
     return net, losses
 
 
-def held_out_contraction(net, mesh, fixed, params, tool_path, guard_ratio: float = 0.5):
+def held_out_contraction(net, mesh, fixed, params, tool_path, guard_ratio: float = 0.5, solver_cls=None):
     """How well `net` smooths inside the learned V-cycle on a held-out run: steps a solver with
     `params` (a learned form: mixed precision, its sweeps and passes) along `tool_path` ((a, b)
     capsule ends per frame, radius 0.3) and collects, per learned V-cycle, |r_after| / |r_before|
     (mgsb_learned_cycle_norms).  Returns {"failed_checks", "cycles", "ratio_p50", "ratio_p99",
     "ratio_max"}; fewer failed checks, then a lower 99th percentile, is better."""
-    from .api import Solver
-    s = Solver(mesh, params)
+    if solver_cls is None:
+        from .api import Solver as solver_cls
+    s = solver_cls(mesh, params)
     try:
         s.set_fixed(fixed)
         s.set_learned_smoother(net, guard_ratio)

@@ -158,3 +158,40 @@ def test_margin_keeps_forms_near_the_bar_out():
     rows = {r["key"]: r for r in out["plain_fp32"]["candidates"]}
     assert rows["plain_fp32_1pass_2+2"]["within_bar"] and "ms_per_frame" in rows["plain_fp32_1pass_2+2"]
     assert out["plain_fp32"]["chosen"]["passes"] == 2 and out["margin"] == 0.5
+
+
+def test_held_out_contraction_counts_and_ratios():
+    """learned.held_out_contraction steps the solver along the path and summarises |r_after|/|r_before|
+    over every learned V-cycle of every frame, with the solver's failed-check count."""
+    from multigridsoftbody_b200.learned import held_out_contraction
+
+    class FakeSolver:
+        def __init__(self, mesh, params):
+            self.frames = 0
+            self.closed = False
+
+        def set_fixed(self, mask):
+            pass
+
+        def set_learned_smoother(self, net, ratio):
+            self.ratio = ratio
+
+        def set_capsule(self, a, b, r):
+            pass
+
+        def step(self):
+            self.frames += 1
+
+        def learned_cycle_norms(self):   # two cycles per frame: ratios 0.1 and 0.6 (the second fails)
+            return np.array([10.0, 1.0, 0.0]), np.array([1.0, 0.6, 0.0])
+
+        def learned_stats(self):
+            return 3 * self.frames, self.frames
+
+        def close(self):
+            self.closed = True
+
+    path = [(np.zeros(3, np.float32), np.ones(3, np.float32))] * 5
+    out = held_out_contraction(object(), None, None, None, path, solver_cls=FakeSolver)
+    assert out["failed_checks"] == 5 and out["cycles"] == 15
+    assert abs(out["ratio_max"] - 0.6) < 1e-12 and abs(out["ratio_p50"] - 0.35) < 1e-12
