@@ -87,3 +87,23 @@ def test_dense_operator_refused_for_a_batch(lib):
     with pytest.raises(mg.MgsbError):
         s.set_coarse_dense(True)
     s.close()
+
+
+def test_dense_operator_refused_above_its_row_limit(lib):
+    """Config 1's level 1 has 2,989 rows, above the operator's 1,024: the dense operator is refused at
+    split 1 and the solver keeps stepping with the kernel path; at split 2 (496 rows) it is accepted."""
+    m, fixed = beam(12, 120, 12)
+    s = mg.Solver(m, mg_params(levels=4, gravity=(0.0, 0.0, 0.0)))
+    s.set_fixed(fixed)
+    assert s.body_level_size(0, 1) > 1024 >= s.body_level_size(0, 2)
+    s.set_coarse_split(1)
+    with pytest.raises(mg.MgsbError):
+        s.set_coarse_dense(True)
+    assert not s.coarse_dense()
+    s.step()
+    s.set_coarse_split(2)
+    s.set_coarse_dense(True)
+    assert s.coarse_dense()
+    s.step()
+    assert np.isfinite(s.positions()).all()
+    s.close()
