@@ -782,14 +782,19 @@ def run_ours(args):
                                       bar=ERROR_BAR, time_all=True, margin=SELECTION_MARGIN)
         selection["held_out_paths"] = [label + ", tool seed 301" for label, _ in held]
         choice = selection["learned_mixed"]["chosen"]
+        source = "selected by accuracy on held-out tool paths"
+        if choice is None and selection["learned_mixed"]["candidates"]:
+            # no learned form within the selection's margin: the most accurate one, not the default
+            choice = min(selection["learned_mixed"]["candidates"], key=lambda r: r["err_over_diag"])
+            source = "no learned form within the selection margin on the held-out paths: the most accurate one"
         if dist is not None:   # every rank runs rank 0's choice
-            box = [choice]
+            box = [choice, source]
             dist.broadcast_object_list(box, src=0)
-            choice = box[0]
+            choice, source = box
         if choice is not None:
             params[0].pre_sweeps, params[0].post_sweeps = choice["sweeps"]
             params[0].refinement_passes = choice["passes"]
-            sweeps_source = "selected by accuracy on held-out tool paths"
+            sweeps_source = source
     solver = mg.Solver(meshes, params)
     for b, fx in enumerate(fixeds):
         solver.set_fixed(fx, body=b)
