@@ -533,18 +533,32 @@ __global__ void k_mg_finish(int n, const float4* __restrict__ s, const float4* _
 }
 
 // Per frame, level l >= 1: lumped contact weight c_l = P^T c_{l-1}, D and dinv.
+// The children, their weights and the contact-free diagonal are set-up data:
+// the first kCoarseFrameHeld children are loaded before the dependency wait.
+constexpr int kCoarseFrameHeld = 8;
 __global__ void k_coarse_frame(int n, const int32_t* __restrict__ rptr, const int32_t* __restrict__ rcol,
                                const float* __restrict__ rw, const float* __restrict__ cfine,
                                const float* __restrict__ diag0, float omega, float* __restrict__ c,
                                float* __restrict__ dfull, float* __restrict__ dinv) {
-    pdl_enter();
+    pdl_trigger();
     const int J = blockIdx.x * blockDim.x + threadIdx.x;
     if (J >= n) return;
-    float acc = 0.f;
-    const int e1 = __ldg(rptr + J + 1);
-    for (int e = __ldg(rptr + J); e < e1; ++e) acc = fmaf(__ldg(rw + e), __ldg(cfine + __ldg(rcol + e)), acc);
-    c[J] = acc;
+    const int e0 = __ldg(rptr + J), e1 = __ldg(rptr + J + 1);
+    int ch[kCoarseFrameHeld];
+    float w[kCoarseFrameHeld];
+#pragma unroll
+    for (int k = 0; k < kCoarseFrameHeld; ++k) {
+        ch[k] = e0 + k < e1 ? __ldg(rcol + e0 + k) : -1;
+        w[k] = e0 + k < e1 ? __ldg(rw + e0 + k) : 0.f;
+    }
     const float d0 = __ldg(diag0 + J);
+    pdl_wait();
+    float acc = 0.f;   // the children in CSR order, as one loop over them
+#pragma unroll
+    for (int k = 0; k < kCoarseFrameHeld; ++k)
+        if (ch[k] >= 0) acc = fmaf(w[k], __ldg(cfine + ch[k]), acc);
+    for (int e = e0 + kCoarseFrameHeld; e < e1; ++e) acc = fmaf(__ldg(rw + e), __ldg(cfine + __ldg(rcol + e)), acc);
+    c[J] = acc;
     const float D = d0 + acc;
     dfull[J] = D;
     dinv[J] = d0 > 0.f ? omega / D : 0.f;

@@ -165,21 +165,30 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_row_consts(int n, const int32
                                                               const float* __restrict__ val,
                                                               const float* __restrict__ dfull,
                                                               const float* __restrict__ diag0, float4* __restrict__ rc) {
-    pdl_enter();
+    pdl_trigger();
     constexpr int G = kLanesL0, S = 32 / G;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int row = warp * S + (lane % S);
     const bool valid = row < n;
-    float sa = 0.f, sd = 0.f;
-    if (valid) {
-        const int slice = row / S;
-        const int beg = __ldg(sp + slice), end = __ldg(sp + slice + 1);
-        for (int e = beg + (lane / S) * S + (row - slice * S); e < end; e += 32) {
-            const float a = fabsf(__ldg(val + e));
+    // the row's entries and its contact-free diagonal are set-up data: loaded before the wait
+    HeldEntries<kHeldL0> he;
+    hold_ell_row<G>(he, row, valid, lane, sp, col, val);
+    const float L = (valid && lane < S) ? __ldg(diag0 + row) : 0.f;
+    pdl_wait();
+    float sa = 0.f, sd = 0.f;   // the entries in the order of the row's ELL loop
+#pragma unroll
+    for (int k = 0; k < kHeldL0; ++k) {
+        if (he.c[k] >= 0) {
+            const float a = fabsf(he.v[k]);
             sa += a;
-            sd = fmaf(a, __ldg(dfull + __ldg(col + e)), sd);
+            sd = fmaf(a, __ldg(dfull + he.c[k]), sd);
         }
+    }
+    for (int e = he.next; e < he.end; e += he.stride) {
+        const float a = fabsf(__ldg(val + e));
+        sa += a;
+        sd = fmaf(a, __ldg(dfull + __ldg(col + e)), sd);
     }
 #pragma unroll
     for (int o = S; o < 32; o <<= 1) {
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_row_consts(int n, const int32
         sd += __shfl_xor_sync(0xffffffffu, sd, o);
     }
     if (!valid || lane >= S) return;
-    const float D = __ldg(dfull + row), L = __ldg(diag0 + row);
+    const float D = __ldg(dfull + row);
     const float inv_a = sa > 0.f ? 1.f / sa : 0.f;
     rc[row] = make_float4(D * inv_a, (D - L) / D, sd > 0.f ? D * sa / sd : 1.f, inv_a);
 }
